@@ -1,0 +1,1202 @@
+// ddc_api.cu -- host side of the B200 ddCOSMO library: the C ABI of
+// include/ddcosmo_gpu.h, the module state (context), the ddinit pipeline and
+// the Jacobi/DIIS driver.  All device work runs on the context's stream.
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "ddc_internal.h"
+#include "lebedev_orbits.inc"
+
+using namespace ddc;
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// device buffer
+// ---------------------------------------------------------------------------
+struct DBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  ~DBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  cudaError_t ensure(size_t b) {
+    if (b <= bytes && p) return cudaSuccess;
+    release();
+    if (b == 0) b = 16;
+    cudaError_t e = cudaMalloc(&p, b);
+    if (e == cudaSuccess) bytes = b;
+    return e;
+  }
+  template <class T>
+  T* as() const {
+    return reinterpret_cast<T*>(p);
+  }
+};
+
+double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch())
+      .count();
+}
+
+// ---------------------------------------------------------------------------
+// Lebedev grid (llgrid, llgnew.f:5-91).  Each orbit record {code, a, b, v}
+// expands to its Oh-symmetric points (gen_oh, llgnew.f:93-681): for every
+// coordinate pattern ("shape") of the orbit, the signs of the non-zero
+// coordinates are enumerated with the first non-zero coordinate varying
+// fastest.  This reproduces the reference's point order, which fixes the
+// order of the cavity points.
+// ---------------------------------------------------------------------------
+int snap_ngrid(int ngrid) {
+  int best = 0, inear = 100000;
+  for (int i = 0; i < LEB_NSIZES; i++) {
+    int d = std::abs(leb_sizes[i] - ngrid);
+    if (d < inear) {
+      inear = d;
+      best = i;
+    }
+  }
+  return leb_sizes[best];
+}
+
+void expand_orbit(int code, double a, double b, double v, std::vector<double>& out) {
+  // shapes: indices into {0, a, b, c}; 0 = zero coordinate
+  static const int shapes1[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+  static const int shapes2[3][3] = {{0, 1, 1}, {1, 0, 1}, {1, 1, 0}};
+  static const int shapes3[1][3] = {{1, 1, 1}};
+  static const int shapes4[3][3] = {{1, 1, 2}, {1, 2, 1}, {2, 1, 1}};
+  static const int shapes5[6][3] = {{1, 2, 0}, {2, 1, 0}, {1, 0, 2},
+                                    {2, 0, 1}, {0, 1, 2}, {0, 2, 1}};
+  static const int shapes6[6][3] = {{1, 2, 3}, {1, 3, 2}, {2, 1, 3},
+                                    {2, 3, 1}, {3, 1, 2}, {3, 2, 1}};
+  const int(*shp)[3] = nullptr;
+  int nshape = 0;
+  double c = 0.0;
+  switch (code) {
+    case 1: a = 1.0; shp = shapes1; nshape = 3; break;
+    case 2: a = std::sqrt(0.5); shp = shapes2; nshape = 3; break;
+    case 3: a = std::sqrt(1.0 / 3.0); shp = shapes3; nshape = 1; break;
+    case 4: b = std::sqrt(1.0 - 2.0 * a * a); shp = shapes4; nshape = 3; break;
+    case 5: b = std::sqrt(1.0 - a * a); shp = shapes5; nshape = 6; break;
+    case 6: c = std::sqrt(1.0 - a * a - b * b); shp = shapes6; nshape = 6; break;
+    default: return;
+  }
+  const double val[4] = {0.0, a, b, c};
+  for (int s = 0; s < nshape; s++) {
+    int nz[3], nnz = 0;
+    for (int k = 0; k < 3; k++)
+      if (shp[s][k]) nz[nnz++] = k;
+    for (int sg = 0; sg < (1 << nnz); sg++) {
+      double p[3];
+      for (int k = 0; k < 3; k++) p[k] = val[shp[s][k]];
+      for (int q = 0; q < nnz; q++)
+        if (sg & (1 << q)) p[nz[q]] = -p[nz[q]];
+      out.push_back(p[0]);
+      out.push_back(p[1]);
+      out.push_back(p[2]);
+      out.push_back(v);
+    }
+  }
+}
+
+bool lebedev(int ngrid, std::vector<double>& g4) {
+  int gi = -1;
+  for (int i = 0; i < LEB_NSIZES; i++)
+    if (leb_sizes[i] == ngrid) gi = i;
+  if (gi < 0) return false;
+  g4.clear();
+  for (int o = 0; o < leb_orbit_cnt[gi]; o++) {
+    const leb_orbit_rec& r = leb_orbits[leb_orbit_off[gi] + o];
+    expand_orbit(r.code, r.a, r.b, r.v, g4);
+  }
+  const double pi = 4.0 * std::atan(1.0);
+  for (size_t i = 3; i < g4.size(); i += 4) g4[i] = g4[i] * 4.0 * pi;
+  return (int)(g4.size() / 4) == ngrid;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// context (the module state of ddcosmo.f90:87-127)
+// ---------------------------------------------------------------------------
+struct ddc_ctx {
+  ddc_params prm{};
+  YlmTables tb{};
+  cudaStream_t st = nullptr;
+  bool own_stream = true;
+  long long launches = 0;
+  // stage timers: event pairs recorded around stages, resolved at sync points
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_pending;
+  double st_ms[ST_N] = {0};
+  long long st_calls[ST_N] = {0};
+  std::string err;
+  bool ready = false;
+  int nsph = 0, ncav = 0, nylm = 0, ngrid = 0, npair = 0;
+  long long ntri = 0;
+  std::vector<double> h_grid;  // x,y,z,w per point
+  // geometry
+  DBuf sph, grid, basis, bw, fi, ui, zi, inl, nl, rev, pn_ptr, pn, ls_ptr, ls, ntri_pt;
+  DBuf cavoff, cavidx, cavpt, ccav, cnt, scan_tmp;
+  DBuf csph, cx, cy, cz;  // csph(3,n) and SoA centres
+  // work
+  DBuf pot, xig, gbuf, rhs, x, y, xn, partials, red, hist_x, hist_e;
+  DBuf phi, psi, sigma, s, q, fx, zeta, ef1, ef2, ef_scratch, uchi;
+  DBuf in1, in2, in3, in4, out1;  // staging for host-pointer calls
+
+  Launch L() { return Launch{st, &launches}; }
+  DevGeo geo() const {
+    DevGeo g;
+    g.nsph = nsph;
+    g.ngrid = ngrid;
+    g.nylm = nylm;
+    g.ncav = ncav;
+    g.npair = npair;
+    g.ntri = ntri;
+    g.sph = sph.as<double4>();
+    g.grid = grid.as<double4>();
+    g.basis = basis.as<double>();
+    g.bw = bw.as<double>();
+    g.fi = fi.as<double>();
+    g.ui = ui.as<double>();
+    g.zi = zi.as<double>();
+    g.inl = inl.as<int>();
+    g.nl = nl.as<int>();
+    g.rev = rev.as<int>();
+    g.pn_ptr = pn_ptr.as<int>();
+    g.pn = pn.as<uint16_t>();
+    g.ls_ptr = ls_ptr.as<int>();
+    g.ls = ls.as<int2>();
+    g.ntri_pt = ntri_pt.as<uint8_t>();
+    g.cavoff = cavoff.as<int>();
+    g.cavidx = cavidx.as<int>();
+    g.cavpt = cavpt.as<int>();
+    g.ccav = ccav.as<double>();
+    return g;
+  }
+};
+
+namespace {
+
+int fail(ddc_ctx* c, int code, const std::string& msg) {
+  if (c) c->err = msg;
+  return code;
+}
+
+#define CK(expr)                                                                          \
+  do {                                                                                    \
+    cudaError_t _e = (expr);                                                              \
+    if (_e != cudaSuccess)                                                                \
+      return fail(ctx, _e == cudaErrorMemoryAllocation ? DDC_ERR_NOMEM : DDC_ERR_CUDA,    \
+                  std::string(#expr) + ": " + cudaGetErrorString(_e));                    \
+  } while (0)
+
+#define CKI(expr)                  \
+  do {                             \
+    int _r = (expr);               \
+    if (_r != DDC_OK) return _r;   \
+  } while (0)
+
+// input array: device pointer as is, host array copied into staging
+int stage_in(ddc_ctx* ctx, const double* p, size_t count, DBuf& buf, const double** out) {
+  if (count == 0) {
+    *out = p;
+    return DDC_OK;
+  }
+  if (!p) return fail(ctx, DDC_ERR_PARAM, "null input array");
+  if (ctx->prm.device_pointers) {
+    *out = p;
+    return DDC_OK;
+  }
+  CK(buf.ensure(count * sizeof(double)));
+  CK(cudaMemcpyAsync(buf.p, p, count * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
+  *out = buf.as<double>();
+  return DDC_OK;
+}
+// output: device pointer written directly; host array via a device buffer
+int out_ptr(ddc_ctx* ctx, double* p, size_t count, DBuf& buf, double** dev) {
+  if (ctx->prm.device_pointers && p) {
+    *dev = p;
+    return DDC_OK;
+  }
+  CK(buf.ensure((count ? count : 1) * sizeof(double)));
+  *dev = buf.as<double>();
+  return DDC_OK;
+}
+int finish_out(ddc_ctx* ctx, double* p, const double* dev, size_t count) {
+  if (p && dev != p && count)
+    CK(cudaMemcpyAsync(p, dev, count * sizeof(double),
+                       ctx->prm.device_pointers ? cudaMemcpyDeviceToDevice
+                                                : cudaMemcpyDeviceToHost,
+                       ctx->st));
+  return DDC_OK;
+}
+int sync(ddc_ctx* ctx) {
+  CK(cudaStreamSynchronize(ctx->st));
+  for (auto& pe : ctx->ev_pending) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, pe.second.first, pe.second.second) == cudaSuccess) {
+      ctx->st_ms[pe.first] += ms;
+      ctx->st_calls[pe.first] += 1;
+    }
+    ctx->ev_pool.push_back(pe.second.first);
+    ctx->ev_pool.push_back(pe.second.second);
+  }
+  ctx->ev_pending.clear();
+  return DDC_OK;
+}
+
+// Times the enclosed launches on the context stream (when timing is on).
+struct StageScope {
+  ddc_ctx* c;
+  int stage;
+  cudaEvent_t a = nullptr, b = nullptr;
+  cudaEvent_t take() {
+    cudaEvent_t e = nullptr;
+    if (!c->ev_pool.empty()) {
+      e = c->ev_pool.back();
+      c->ev_pool.pop_back();
+    } else if (cudaEventCreate(&e) != cudaSuccess) {
+      e = nullptr;
+    }
+    return e;
+  }
+  StageScope(ddc_ctx* ctx, int s) : c(ctx), stage(s) {
+    if (!c->prm.timing) return;
+    a = take();
+    b = take();
+    if (a && b) cudaEventRecord(a, c->st);
+  }
+  ~StageScope() {
+    if (!a || !b) return;
+    cudaEventRecord(b, c->st);
+    c->ev_pending.push_back({stage, {a, b}});
+  }
+};
+
+void build_tables(ddc_ctx* c) {
+  YlmTables& tb = c->tb;
+  memset(&tb, 0, sizeof(tb));
+  const int lmax = c->prm.lmax;
+  const double pi = 4.0 * std::atan(1.0), sq2 = std::sqrt(2.0);
+  std::vector<double> fact(std::max(2 * lmax + 1, 2));
+  fact[0] = 1.0;
+  fact[1] = 1.0;
+  for (int i = 3; i <= 2 * lmax + 1; i++) fact[i - 1] = (double)(i - 1) * fact[i - 2];
+  for (int l = 0; l <= lmax; l++) {
+    double fl = (2.0 * (double)l + 1.0) / (4.0 * pi);
+    double ffl = std::sqrt(fl);
+    tb.facl[l] = fl;
+    tb.facs[l * (l + 1) / 2] = ffl;
+    for (int m = 1; m <= l; m++) {
+      double fnorm = sq2 * ffl * std::sqrt(fact[l - m] / fact[l + m]);
+      if (m % 2 == 1) fnorm = -fnorm;
+      tb.facs[l * (l + 1) / 2 + m] = fnorm;
+    }
+    for (int m = 0; m <= l; m++) {
+      int e = l * (l + 1) / 2 + m;
+      tb.K[e] = tb.facs[e] / fl;
+      if (l >= m + 2) {
+        tb.A[e] = (2.0 * l - 1.0) / (double)(l - m);
+        tb.B[e] = ((double)(l + m) - 1.0) / (double)(l - m);
+      }
+    }
+  }
+  tb.eta = c->prm.eta;
+  tb.lmax = lmax;
+  tb.nylm = (lmax + 1) * (lmax + 1);
+  tb.ngrid = c->ngrid;
+}
+
+// deterministic reduction of `nvals` partial columns into red[0..nvals-1], copied to host
+int reduce_to_host(ddc_ctx* ctx, int nvals, double* host) {
+  {
+    StageScope sc(ctx, ST_REDUCE);
+    CK(launch_reduce_partials(ctx->L(), ctx->partials.as<double>(), reduce_blocks(), nvals,
+                            ctx->red.as<double>()));
+  }
+  CK(cudaMemcpyAsync(host, ctx->red.p, sizeof(double) * nvals, cudaMemcpyDeviceToHost, ctx->st));
+  return sync(ctx);
+}
+
+// ---------------------------------------------------------------------------
+// ddinit (ddcosmo.f90:159-483) on device buffers
+// ---------------------------------------------------------------------------
+int do_init(ddc_ctx* ctx, int n, const std::vector<double4>* hsph, const double4* dsph) {
+  ctx->ready = false;
+  ctx->nsph = n;
+  ctx->nylm = (ctx->prm.lmax + 1) * (ctx->prm.lmax + 1);
+  ctx->ngrid = snap_ngrid(ctx->prm.ngrid);
+  build_tables(ctx);
+  if (!lebedev(ctx->ngrid, ctx->h_grid)) return fail(ctx, DDC_ERR_PARAM, "bad Lebedev size");
+  const int N = n, G = ctx->ngrid, NY = ctx->nylm;
+  const long long NP = (long long)N * G;
+  auto L = ctx->L();
+  CK(ctx->sph.ensure(sizeof(double4) * std::max(N, 1)));
+  if (hsph)
+    CK(cudaMemcpyAsync(ctx->sph.p, hsph->data(), sizeof(double4) * N, cudaMemcpyHostToDevice,
+                       ctx->st));
+  else if (dsph != ctx->sph.as<double4>())
+    CK(cudaMemcpyAsync(ctx->sph.p, dsph, sizeof(double4) * N, cudaMemcpyDeviceToDevice, ctx->st));
+  CK(ctx->grid.ensure(sizeof(double4) * G));
+  CK(cudaMemcpyAsync(ctx->grid.p, ctx->h_grid.data(), sizeof(double4) * G, cudaMemcpyHostToDevice,
+                     ctx->st));
+  CK(ctx->basis.ensure(sizeof(double) * G * NY));
+  CK(ctx->bw.ensure(sizeof(double) * G * NY));
+  CK(launch_basis(L, ctx->tb, ctx->grid.as<double4>(), ctx->basis.as<double>(),
+                  ctx->bw.as<double>()));
+  // neighbour list
+  size_t scan_n = (size_t)std::max<long long>(N, 1);
+  CK(ctx->cnt.ensure(sizeof(int) * (scan_n + 1)));
+  CK(ctx->inl.ensure(sizeof(int) * (N + 1)));
+  CK(cudaMemsetAsync(ctx->cnt.p, 0, sizeof(int) * (N + 1), ctx->st));
+  if (N > 0) CK(launch_csr_count(L, N, ctx->sph.as<double4>(), ctx->cnt.as<int>()));
+  size_t tb_bytes = scan_temp_bytes(N);
+  CK(ctx->scan_tmp.ensure(tb_bytes));
+  CK(scan_exclusive(L, ctx->cnt.as<int>(), ctx->inl.as<int>(), N, ctx->scan_tmp.p, tb_bytes));
+  int npair = 0;
+  CK(cudaMemcpyAsync(&npair, ctx->inl.as<int>() + N, sizeof(int), cudaMemcpyDeviceToHost,
+                     ctx->st));
+  CKI(sync(ctx));
+  ctx->npair = npair;
+  CK(ctx->nl.ensure(sizeof(int) * std::max(npair, 1)));
+  CK(ctx->rev.ensure(sizeof(int) * std::max(npair, 1)));
+  if (N > 0) {
+    CK(launch_csr_fill(L, N, ctx->sph.as<double4>(), ctx->inl.as<int>(), ctx->nl.as<int>()));
+    CK(launch_csr_rev(L, N, ctx->inl.as<int>(), ctx->nl.as<int>(), ctx->rev.as<int>()));
+  }
+  // fi, ui, zi
+  CK(ctx->fi.ensure(sizeof(double) * std::max(NP, 1LL)));
+  CK(ctx->ui.ensure(sizeof(double) * std::max(NP, 1LL)));
+  CK(ctx->ntri_pt.ensure(std::max(NP, 1LL)));
+  if (ctx->prm.igrad) CK(ctx->zi.ensure(sizeof(double) * 3 * std::max(NP, 1LL)));
+  else ctx->zi.release();
+  CK(launch_fiui(L, ctx->tb, N, ctx->sph.as<double4>(), ctx->grid.as<double4>(),
+                 ctx->inl.as<int>(), ctx->nl.as<int>(), ctx->fi.as<double>(), ctx->ui.as<double>(),
+                 ctx->prm.igrad ? ctx->zi.as<double>() : nullptr, ctx->ntri_pt.as<uint8_t>()));
+  // cavity
+  CK(ctx->cavoff.ensure(sizeof(int) * (N + 1)));
+  CK(cudaMemsetAsync(ctx->cnt.p, 0, sizeof(int) * (N + 1), ctx->st));
+  CK(launch_cav_count(L, N, G, ctx->ui.as<double>(), ctx->cnt.as<int>()));
+  CK(scan_exclusive(L, ctx->cnt.as<int>(), ctx->cavoff.as<int>(), N, ctx->scan_tmp.p, tb_bytes));
+  int ncav = 0;
+  CK(cudaMemcpyAsync(&ncav, ctx->cavoff.as<int>() + N, sizeof(int), cudaMemcpyDeviceToHost,
+                     ctx->st));
+  CKI(sync(ctx));
+  ctx->ncav = ncav;
+  CK(ctx->cavidx.ensure(sizeof(int) * std::max(NP, 1LL)));
+  CK(ctx->cavpt.ensure(sizeof(int) * std::max(ncav, 1)));
+  CK(ctx->ccav.ensure(sizeof(double) * 3 * std::max(ncav, 1)));
+  CK(launch_cav_fill(L, N, G, ctx->ui.as<double>(), ctx->sph.as<double4>(),
+                     ctx->grid.as<double4>(), ctx->cavoff.as<int>(), ctx->cavidx.as<int>(),
+                     ctx->cavpt.as<int>(), ctx->ccav.as<double>()));
+  // pair-major triple lists
+  size_t pscan = (size_t)std::max(npair, 1);
+  CK(ctx->cnt.ensure(sizeof(int) * (std::max(scan_n, pscan) + 1)));
+  CK(ctx->pn_ptr.ensure(sizeof(int) * (npair + 1)));
+  CK(cudaMemsetAsync(ctx->cnt.p, 0, sizeof(int) * (npair + 1), ctx->st));
+  CK(launch_pair_count(L, N, G, ctx->sph.as<double4>(), ctx->grid.as<double4>(),
+                       ctx->inl.as<int>(), ctx->nl.as<int>(), ctx->cnt.as<int>()));
+  size_t tb2 = scan_temp_bytes(npair);
+  CK(ctx->scan_tmp.ensure(std::max(tb_bytes, tb2)));
+  CK(scan_exclusive(L, ctx->cnt.as<int>(), ctx->pn_ptr.as<int>(), npair, ctx->scan_tmp.p,
+                    ctx->scan_tmp.bytes));
+  int ntri = 0;
+  CK(cudaMemcpyAsync(&ntri, ctx->pn_ptr.as<int>() + npair, sizeof(int), cudaMemcpyDeviceToHost,
+                     ctx->st));
+  CKI(sync(ctx));
+  ctx->ntri = ntri;
+  CK(ctx->pn.ensure(sizeof(uint16_t) * std::max(ntri, 1)));
+  CK(launch_pair_fill(L, N, G, ctx->sph.as<double4>(), ctx->grid.as<double4>(), ctx->inl.as<int>(),
+                      ctx->nl.as<int>(), ctx->pn_ptr.as<int>(), ctx->pn.as<uint16_t>()));
+  CK(ctx->ls_ptr.ensure(sizeof(int) * (N + 1)));
+  CK(cudaMemsetAsync(ctx->cnt.p, 0, sizeof(int) * (N + 1), ctx->st));
+  CK(launch_ls_count(L, N, ctx->inl.as<int>(), ctx->rev.as<int>(), ctx->pn_ptr.as<int>(),
+                     ctx->cnt.as<int>()));
+  CK(scan_exclusive(L, ctx->cnt.as<int>(), ctx->ls_ptr.as<int>(), N, ctx->scan_tmp.p,
+                    ctx->scan_tmp.bytes));
+  CK(ctx->ls.ensure(sizeof(int2) * std::max(ntri, 1)));
+  CK(launch_ls_fill(L, N, ctx->inl.as<int>(), ctx->nl.as<int>(), ctx->rev.as<int>(),
+                    ctx->pn_ptr.as<int>(), ctx->pn.as<uint16_t>(), ctx->ls_ptr.as<int>(),
+                    ctx->ls.as<int2>()));
+  // centres for the electrostatics
+  CK(ctx->csph.ensure(sizeof(double) * 3 * std::max(N, 1)));
+  CK(ctx->cx.ensure(sizeof(double) * std::max(N, 1)));
+  CK(ctx->cy.ensure(sizeof(double) * std::max(N, 1)));
+  CK(ctx->cz.ensure(sizeof(double) * std::max(N, 1)));
+  CK(launch_csph_pack(L, N, ctx->sph.as<double4>(), ctx->csph.as<double>(), ctx->cx.as<double>(),
+                      ctx->cy.as<double>(), ctx->cz.as<double>()));
+  // solver work buffers
+  const size_t nv = (size_t)N * NY;
+  const int nd = std::max(ctx->prm.ndiis, 1);
+  CK(ctx->pot.ensure(sizeof(double) * std::max(NP, 1LL)));
+  CK(ctx->xig.ensure(sizeof(double) * std::max(NP, 1LL)));
+  CK(ctx->uchi.ensure(sizeof(double) * std::max(NP, 1LL)));
+  for (DBuf* b : {&ctx->rhs, &ctx->x, &ctx->y, &ctx->xn, &ctx->psi, &ctx->sigma, &ctx->s})
+    CK(b->ensure(sizeof(double) * std::max(nv, (size_t)1)));
+  CK(ctx->hist_x.ensure(sizeof(double) * std::max(nv, (size_t)1) * nd));
+  CK(ctx->hist_e.ensure(sizeof(double) * std::max(nv, (size_t)1) * nd));
+  CK(ctx->partials.ensure(sizeof(double) * reduce_blocks() * (kMaxHist + 1)));
+  CK(ctx->red.ensure(sizeof(double) * (kMaxHist + 1)));
+  CKI(sync(ctx));
+  ctx->ready = true;
+  return DDC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// operators on device vectors
+// ---------------------------------------------------------------------------
+int op_lx(ddc_ctx* ctx, const double* x, double* y) {
+  DevGeo g = ctx->geo();
+  {
+    StageScope sc(ctx, ST_LX_POT);
+    CK(launch_lx_pot(ctx->L(), ctx->tb, g, x, ctx->pot.as<double>(), false));
+  }
+  StageScope sc(ctx, ST_PROJ);
+  // y = -Bw pot   (intrhs then negate, matvec.f90:131-135)
+  CK(launch_dgemm(ctx->L(), false, ctx->nylm, ctx->nsph, ctx->ngrid, -1.0, ctx->bw.as<double>(),
+                  ctx->nylm, ctx->pot.as<double>(), ctx->ngrid, 0.0, y, ctx->nylm));
+  return DDC_OK;
+}
+int op_xi(ddc_ctx* ctx, const double* x, double* xig) {
+  // xi(n,i) = sum_lm basis(lm,n) x(lm,i)   (matvec.f90:189-204)
+  StageScope sc(ctx, ST_XI);
+  CK(launch_dgemm(ctx->L(), true, ctx->ngrid, ctx->nsph, ctx->nylm, 1.0, ctx->basis.as<double>(),
+                  ctx->nylm, x, ctx->nylm, 0.0, xig, ctx->ngrid));
+  return DDC_OK;
+}
+int op_lstarx(ddc_ctx* ctx, const double* x, double* y) {
+  CKI(op_xi(ctx, x, ctx->xig.as<double>()));
+  StageScope sc(ctx, ST_LSTARX);
+  CK(launch_lstarx_acc(ctx->L(), ctx->tb, ctx->geo(), ctx->xig.as<double>(), y));
+  return DDC_OK;
+}
+
+// gjinv (jacobi_diis.f90:272-360): Gauss-Jordan, full pivoting, one rhs.
+bool gjinv(int n, std::vector<double>& a, std::vector<double>& b) {
+  std::vector<int> indxc(n + 1), indxr(n + 1), piv(n + 1, 0);
+  auto A = [&](int j, int k) -> double& { return a[(size_t)(k - 1) * n + (j - 1)]; };
+  int irow = 0, icol = 0;
+  for (int i = 1; i <= n; i++) {
+    double big = 0.0;
+    for (int j = 1; j <= n; j++)
+      if (piv[j] != 1)
+        for (int k = 1; k <= n; k++)
+          if (piv[k] == 0 && std::fabs(A(j, k)) > big) {
+            big = std::fabs(A(j, k));
+            irow = j;
+            icol = k;
+          }
+    if (icol == 0) return false;
+    piv[icol] += 1;
+    if (piv[icol] > 1) return false;
+    if (irow != icol) {
+      for (int k = 1; k <= n; k++) std::swap(A(irow, k), A(icol, k));
+      std::swap(b[irow - 1], b[icol - 1]);
+    }
+    indxr[i] = irow;
+    indxc[i] = icol;
+    if (A(icol, icol) == 0.0) return false;
+    double pinv = 1.0 / A(icol, icol);
+    A(icol, icol) = 1.0;
+    for (int k = 1; k <= n; k++) A(icol, k) *= pinv;
+    b[icol - 1] *= pinv;
+    for (int j = 1; j <= n; j++)
+      if (j != icol) {
+        double dum = A(j, icol);
+        A(j, icol) = 0.0;
+        for (int k = 1; k <= n; k++) A(j, k) -= A(icol, k) * dum;
+        b[j - 1] -= b[icol - 1] * dum;
+      }
+  }
+  for (int j = n; j >= 1; j--)
+    if (indxr[j] != indxc[j])
+      for (int k = 1; k <= n; k++) std::swap(A(k, indxr[j]), A(k, indxc[j]));
+  return true;
+}
+
+// jacobi_diis (jacobi_diis.f90:1-176), norm mode 4 (hnorm).  x holds the
+// initial guess on entry and the solution on exit (device).
+int solve(ddc_ctx* ctx, bool adjoint, const double* rhs, double* x, ddc_solve_info* info) {
+  const double t0 = now_s();
+  const long long n = (long long)ctx->nsph * ctx->nylm;
+  const double tol = std::pow(10.0, -(double)ctx->prm.iconv);
+  const int ndiis = ctx->prm.ndiis, max_iter = ctx->prm.max_iter;
+  const bool dodiis = ndiis != 0;
+  const int nblk = reduce_blocks();
+  double* y = ctx->y.as<double>();
+  double* hx = ctx->hist_x.as<double>();
+  double* he = ctx->hist_e.as<double>();
+  double* xjac = ctx->xn.as<double>();
+  const int lenb = ndiis + 1;
+  std::vector<double> B((size_t)lenb * lenb, 0.0);
+  auto Bm = [&](int j, int k) -> double& { return B[(size_t)(k - 1) * lenb + (j - 1)]; };
+  std::vector<int> map(std::max(ndiis, 1));
+  for (int k = 0; k < (int)map.size(); k++) map[k] = k;
+  int nmat = 1, it = 0, restarts = 0;
+  bool ok = false;
+  double rms = 0.0;
+  ddc_solve_info loc{};
+  ddc_solve_info* inf = info ? info : &loc;
+  memset(inf, 0, sizeof(*inf));
+  std::vector<double> row(kMaxHist + 2);
+  for (it = 1; it <= max_iter; it++) {
+    if (adjoint) CKI(op_lstarx(ctx, x, y));
+    else CKI(op_lx(ctx, x, y));
+    HistPtrs hist{};
+    HistPtrs comb{};
+    const double* xj = xjac;
+    if (dodiis) {
+      const int phys_new = map[nmat - 1];
+      int nm = nmat;
+      std::vector<int> pmap = map;
+      const bool shift = nmat >= ndiis;
+      if (shift) {  // drop the 10 oldest (jacobi_diis.f90:196-205)
+        std::vector<int> r(map.begin() + 10, map.end());
+        r.insert(r.end(), map.begin(), map.begin() + 10);
+        pmap = r;
+        nm = nmat - 10;
+      }
+      hist.n = nm - 1;
+      for (int k = 0; k < nm - 1; k++) hist.p[k] = he + (size_t)pmap[k] * n;
+      double* xnew = hx + (size_t)phys_new * n;
+      double* enew = he + (size_t)phys_new * n;
+      {
+        StageScope sc(ctx, ST_JACOBI);
+        CK(launch_jacobi_step(ctx->L(), ctx->tb, n, rhs, y, x, xnew, enew, hist,
+                            ctx->partials.as<double>(), nblk));
+      }
+      CKI(reduce_to_host(ctx, nm, row.data()));
+      if (shift) {
+        for (int j = 2; j <= nmat - 10; j++)
+          for (int k = 2; k <= nmat - 10; k++) Bm(j, k) = Bm(j + 10, k + 10);
+        map = pmap;
+      }
+      nmat = nm;
+      // makeb (jacobi_diis.f90:232-270)
+      if (nmat == 1) {
+        Bm(1, 1) = 0.0;
+        Bm(1, 2) = 1.0;
+        Bm(2, 1) = 1.0;
+        Bm(2, 2) = row[0];
+      } else {
+        Bm(nmat + 1, 1) = 1.0;
+        Bm(1, nmat + 1) = 1.0;
+        for (int i = 1; i <= nmat - 1; i++) {
+          Bm(nmat + 1, i + 1) = row[i - 1];
+          Bm(i + 1, nmat + 1) = row[i - 1];
+        }
+        Bm(nmat + 1, nmat + 1) = row[nmat - 1];
+      }
+      const int nmat1 = nmat + 1;
+      std::vector<double> bloc((size_t)nmat1 * nmat1), cex(nmat1, 0.0);
+      for (int k = 1; k <= nmat1; k++)
+        for (int j = 1; j <= nmat1; j++) bloc[(size_t)(k - 1) * nmat1 + (j - 1)] = Bm(j, k);
+      cex[0] = 1.0;
+      if (gjinv(nmat1, bloc, cex)) {
+        comb.n = nmat;
+        for (int k = 0; k < nmat; k++) {
+          comb.p[k] = hx + (size_t)map[k] * n;
+          comb.c[k] = cex[k + 1];
+        }
+        nmat = nmat + 1;
+      } else {  // singular: restart the history (jacobi_diis.f90:214-217)
+        nmat = 1;
+        restarts++;
+        comb.n = 0;
+      }
+      xj = xnew;
+    } else {
+      hist.n = 0;
+      StageScope sc(ctx, ST_JACOBI);
+      CK(launch_jacobi_step(ctx->L(), ctx->tb, n, rhs, y, x, hx, he, hist,
+                            ctx->partials.as<double>(), nblk));
+      comb.n = 0;
+      xj = hx;
+    }
+    {
+      StageScope sc(ctx, ST_COMBINE);
+      CK(launch_diis_combine(ctx->L(), ctx->tb, n, comb, xj, x, ctx->partials.as<double>(),
+                             nblk));
+    }
+    double ss = 0.0;
+    CKI(reduce_to_host(ctx, 1, &ss));
+    rms = std::sqrt(ss / (double)std::max(ctx->nsph, 1));
+    if (it <= 256) inf->norms[it - 1] = rms;
+    if (ctx->prm.iprint > 0) printf("  iter=%4d residual norm: %14.4E\n", it, rms);
+    if (!std::isfinite(rms)) {
+      inf->iterations = it;
+      return fail(ctx, DDC_ERR_NUMERIC, "non-finite increment norm");
+    }
+    ok = rms < tol;
+    if (ok) break;
+  }
+  inf->iterations = ok ? it : max_iter;
+  inf->converged = ok ? 1 : 0;
+  inf->diis_restarts = restarts;
+  inf->final_norm = rms;
+  inf->seconds = now_s() - t0;
+  if (!ok) return fail(ctx, DDC_ERR_NOCONV, adjoint ? "adjoint ddCOSMO did not converge"
+                                                    : "ddCOSMO did not converge");
+  return DDC_OK;
+}
+
+int need_ready(ddc_ctx* ctx) {
+  if (!ctx) return DDC_ERR_PARAM;
+  if (!ctx->ready) return fail(ctx, DDC_ERR_STATE, "context not initialised (call ddc_init)");
+  return DDC_OK;
+}
+
+// dot product on device, deterministic
+int dot_dev(ddc_ctx* ctx, long long n, const double* a, const double* b, double* out) {
+  CK(launch_dot_partial(ctx->L(), n, a, b, ctx->partials.as<double>(), reduce_blocks()));
+  return reduce_to_host(ctx, 1, out);
+}
+
+// cosmo on device vectors: phi (ncav) or glm -> sigma
+int cosmo_dev(ddc_ctx* ctx, int star, int cart, const double* phi, const double* glm,
+              const double* psi, double* sigma, double* esolv, ddc_solve_info* info) {
+  const long long n = (long long)ctx->nsph * ctx->nylm;
+  const int gmode = ctx->prm.guess == DDC_GUESS_ZERO ? 1 : 0;
+  if (!star) {
+    double* rhs = ctx->rhs.as<double>();
+    if (cart) {
+      CK(ctx->gbuf.ensure(sizeof(double) * std::max<long long>((long long)ctx->nsph * ctx->ngrid, 1)));
+      StageScope sc(ctx, ST_RHS);
+      CK(launch_wghpot(ctx->L(), ctx->geo(), phi, ctx->gbuf.as<double>()));
+      CK(launch_dgemm(ctx->L(), false, ctx->nylm, ctx->nsph, ctx->ngrid, 1.0, ctx->bw.as<double>(),
+                      ctx->nylm, ctx->gbuf.as<double>(), ctx->ngrid, 0.0, rhs, ctx->nylm));
+    } else {
+      CK(cudaMemcpyAsync(rhs, glm, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx->st));
+    }
+    if (ctx->prm.guess != DDC_GUESS_USER) CK(launch_guess(ctx->L(), ctx->tb, n, rhs, sigma, gmode));
+    CKI(solve(ctx, false, rhs, sigma, info));
+    if (esolv) {
+      double d = 0.0;
+      CKI(dot_dev(ctx, n, sigma, psi, &d));
+      *esolv = 0.5 * ((ctx->prm.eps - 1.0) / ctx->prm.eps) * d;
+    }
+  } else {
+    if (ctx->prm.guess != DDC_GUESS_USER) CK(launch_guess(ctx->L(), ctx->tb, n, psi, sigma, gmode));
+    CKI(solve(ctx, true, psi, sigma, info));
+  }
+  return DDC_OK;
+}
+
+// forces_dd on device vectors (forces_dd.f90:91-164)
+int forces_dev(ddc_ctx* ctx, const double* phi, const double* sigma, const double* s, double* fx) {
+  if (!ctx->prm.igrad || !ctx->zi.p)
+    return fail(ctx, DDC_ERR_STATE, "forces need igrad=1 at init (zi)");
+  CKI(op_xi(ctx, s, ctx->xig.as<double>()));
+  {
+    StageScope sc(ctx, ST_UCHI);
+    CK(launch_lx_pot(ctx->L(), ctx->tb, ctx->geo(), sigma, ctx->uchi.as<double>(), true));
+  }
+  const double fep = 0.5 * (ctx->prm.eps - 1.0) / ctx->prm.eps;
+  StageScope sc(ctx, ST_FORCES);
+  CK(launch_forces(ctx->L(), ctx->tb, ctx->geo(), sigma, ctx->xig.as<double>(),
+                   ctx->uchi.as<double>(), phi, fep, fx));
+  return DDC_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+int ddc_default_params(ddc_params* p) {
+  if (!p) return DDC_ERR_PARAM;
+  memset(p, 0, sizeof(*p));
+  p->lmax = 6;
+  p->ngrid = 110;
+  p->iconv = 7;
+  p->igrad = 1;
+  p->eps = 78.3553;
+  p->eta = 0.2;
+  p->iprint = 0;
+  p->max_iter = 200;
+  p->ndiis = 25;
+  p->precision = DDC_PREC_FP64;
+  p->guess = DDC_GUESS_REFERENCE;
+  p->device = 0;
+  p->device_pointers = 0;
+  return DDC_OK;
+}
+
+const char* ddc_status_string(int s) {
+  switch (s) {
+    case DDC_OK: return "ok";
+    case DDC_ERR_PARAM: return "invalid parameter";
+    case DDC_ERR_STATE: return "invalid call order";
+    case DDC_ERR_CUDA: return "CUDA error";
+    case DDC_ERR_NOMEM: return "device allocation failed";
+    case DDC_ERR_NOCONV: return "solver did not converge";
+    case DDC_ERR_UNSUPPORTED: return "unsupported parameter";
+    case DDC_ERR_NUMERIC: return "non-finite result";
+    default: return "unknown status";
+  }
+}
+
+int ddc_create(const ddc_params* p, ddc_ctx** out) {
+  if (!p || !out) return DDC_ERR_PARAM;
+  *out = nullptr;
+  if (p->lmax < 0 || p->lmax > DDC_MAX_LMAX) return DDC_ERR_UNSUPPORTED;
+  if (p->ngrid <= 0 || p->iconv < 0 || p->eps <= 0.0 || !(p->eta > 0.0 && p->eta <= 1.0) ||
+      p->max_iter <= 0 || p->ndiis < 0 || p->ndiis > kMaxHist || (p->ndiis > 0 && p->ndiis <= 10))
+    return DDC_ERR_PARAM;
+  if (p->precision != DDC_PREC_FP64 && p->precision != DDC_PREC_MIXED) return DDC_ERR_PARAM;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return DDC_ERR_CUDA;
+  if (p->device < 0 || p->device >= ndev) return DDC_ERR_PARAM;
+  if (cudaSetDevice(p->device) != cudaSuccess) return DDC_ERR_CUDA;
+  ddc_ctx* c = new ddc_ctx();
+  c->prm = *p;
+  if (p->stream) {
+    c->st = (cudaStream_t)p->stream;
+    c->own_stream = false;
+  } else if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) {
+    delete c;
+    return DDC_ERR_CUDA;
+  }
+  *out = c;
+  return DDC_OK;
+}
+
+int ddc_destroy(ddc_ctx* c) {
+  if (!c) return DDC_OK;
+  cudaSetDevice(c->prm.device);
+  if (c->st) cudaStreamSynchronize(c->st);
+  cudaStream_t st = c->own_stream ? c->st : nullptr;
+  for (auto& pe : c->ev_pending) {
+    cudaEventDestroy(pe.second.first);
+    cudaEventDestroy(pe.second.second);
+  }
+  for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
+  delete c;
+  if (st) cudaStreamDestroy(st);
+  return DDC_OK;
+}
+
+const char* ddc_last_error(ddc_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+long long ddc_launch_count(ddc_ctx* c) { return c ? c->launches : 0; }
+
+int ddc_stage_count(void) { return ST_N; }
+const char* ddc_stage_name(int k) {
+  static const char* names[ST_N] = {"init",    "coulomb_pot", "rhs",       "lx_pot",
+                                    "proj_gemm", "xi_gemm",   "lstarx",    "jacobi_step",
+                                    "diis_combine", "reduce", "uchi_pot",  "forces",
+                                    "zeta",    "efield",      "contract"};
+  return (k >= 0 && k < ST_N) ? names[k] : "";
+}
+int ddc_stage_times(ddc_ctx* c, double* ms, long long* calls) {
+  if (!c) return DDC_ERR_PARAM;
+  for (int k = 0; k < ST_N; k++) {
+    if (ms) ms[k] = c->st_ms[k];
+    if (calls) calls[k] = c->st_calls[k];
+  }
+  return DDC_OK;
+}
+int ddc_reset_stage_times(ddc_ctx* c) {
+  if (!c) return DDC_ERR_PARAM;
+  for (int k = 0; k < ST_N; k++) {
+    c->st_ms[k] = 0.0;
+    c->st_calls[k] = 0;
+  }
+  return DDC_OK;
+}
+
+int ddc_fp64_peak(int device, double* gflops) {
+  if (!gflops) return DDC_ERR_PARAM;
+  if (cudaSetDevice(device) != cudaSuccess) return DDC_ERR_CUDA;
+  cudaDeviceProp pr;
+  if (cudaGetDeviceProperties(&pr, device) != cudaSuccess) return DDC_ERR_CUDA;
+  long long launches = 0;
+  cudaStream_t st;
+  if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return DDC_ERR_CUDA;
+  Launch L{st, &launches};
+  double* out = nullptr;
+  cudaEvent_t a, b;
+  cudaMalloc(&out, sizeof(double));
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  const int blocks = pr.multiProcessorCount * 8, iters = 4096;
+  launch_fp64_probe(L, blocks, 64, out);  // warm up
+  cudaEventRecord(a, st);
+  launch_fp64_probe(L, blocks, iters, out);
+  cudaEventRecord(b, st);
+  cudaError_t e = cudaStreamSynchronize(st);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, a, b);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaFree(out);
+  cudaStreamDestroy(st);
+  if (e != cudaSuccess || ms <= 0.f) return DDC_ERR_CUDA;
+  double flops = 2.0 * 8.0 * (double)iters * blocks * 256.0;
+  *gflops = flops / (ms * 1e-3) / 1e9;
+  return DDC_OK;
+}
+
+int ddc_init(ddc_ctx* ctx, int n, const double* x, const double* y, const double* z,
+             const double* r) {
+  if (!ctx) return DDC_ERR_PARAM;
+  if (n < 0 || (n > 0 && (!x || !y || !z || !r))) return fail(ctx, DDC_ERR_PARAM, "bad input");
+  cudaSetDevice(ctx->prm.device);
+  std::vector<double4> hs(n);
+  if (ctx->prm.device_pointers) {
+    std::vector<double> hx(n), hy(n), hz(n), hr(n);
+    if (n) {
+      CK(cudaMemcpy(hx.data(), x, sizeof(double) * n, cudaMemcpyDeviceToHost));
+      CK(cudaMemcpy(hy.data(), y, sizeof(double) * n, cudaMemcpyDeviceToHost));
+      CK(cudaMemcpy(hz.data(), z, sizeof(double) * n, cudaMemcpyDeviceToHost));
+      CK(cudaMemcpy(hr.data(), r, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    }
+    for (int i = 0; i < n; i++) hs[i] = make_double4(hx[i], hy[i], hz[i], hr[i]);
+  } else {
+    for (int i = 0; i < n; i++) hs[i] = make_double4(x[i], y[i], z[i], r[i]);
+  }
+  for (int i = 0; i < n; i++)
+    if (!(hs[i].w > 0.0)) return fail(ctx, DDC_ERR_PARAM, "radii must be positive");
+  int rc;
+  {
+    StageScope sc(ctx, ST_INIT);
+    rc = do_init(ctx, n, &hs, nullptr);
+  }
+  if (rc == DDC_OK) CKI(sync(ctx));
+  return rc;
+}
+
+int ddc_sizes(ddc_ctx* ctx, int* nsph, int* ncav, int* nylm, int* ngrid) {
+  CKI(need_ready(ctx));
+  if (nsph) *nsph = ctx->nsph;
+  if (ncav) *ncav = ctx->ncav;
+  if (nylm) *nylm = ctx->nylm;
+  if (ngrid) *ngrid = ctx->ngrid;
+  return DDC_OK;
+}
+
+static int get_dev_array(ddc_ctx* ctx, double* out, const void* src, size_t count) {
+  CKI(need_ready(ctx));
+  if (!out) return fail(ctx, DDC_ERR_PARAM, "null output");
+  if (count == 0) return DDC_OK;
+  CK(cudaMemcpyAsync(out, src, sizeof(double) * count,
+                     ctx->prm.device_pointers ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                     ctx->st));
+  return sync(ctx);
+}
+
+int ddc_get_ccav(ddc_ctx* ctx, double* ccav) {
+  CKI(need_ready(ctx));
+  return get_dev_array(ctx, ccav, ctx->ccav.p, 3 * (size_t)ctx->ncav);
+}
+int ddc_get_ui(ddc_ctx* ctx, double* ui) {
+  CKI(need_ready(ctx));
+  return get_dev_array(ctx, ui, ctx->ui.p, (size_t)ctx->nsph * ctx->ngrid);
+}
+int ddc_get_csph(ddc_ctx* ctx, double* csph) {
+  CKI(need_ready(ctx));
+  return get_dev_array(ctx, csph, ctx->csph.p, 3 * (size_t)ctx->nsph);
+}
+int ddc_get_grid(ddc_ctx* ctx, double* grid, double* w) {
+  CKI(need_ready(ctx));
+  for (int i = 0; i < ctx->ngrid; i++) {
+    if (grid)
+      for (int k = 0; k < 3; k++) grid[3 * i + k] = ctx->h_grid[4 * i + k];
+    if (w) w[i] = ctx->h_grid[4 * i + 3];
+  }
+  return DDC_OK;
+}
+
+int ddc_mkrhs(ddc_ctx* ctx, int n, const double* charge, const double* x, const double* y,
+              const double* z, int ncav, const double* ccav, double* phi, int nylm, double* psi) {
+  if (!ctx) return DDC_ERR_PARAM;
+  cudaSetDevice(ctx->prm.device);
+  if (n < 0 || ncav < 0 || nylm <= 0) return fail(ctx, DDC_ERR_PARAM, "bad sizes");
+  if (!ccav) {
+    CKI(need_ready(ctx));
+    if (ncav != ctx->ncav) return fail(ctx, DDC_ERR_PARAM, "ncav does not match the context");
+  }
+  const double *dq, *dx, *dy, *dz, *dc;
+  CKI(stage_in(ctx, charge, n, ctx->in1, &dq));
+  CKI(stage_in(ctx, x, n, ctx->in2, &dx));
+  CKI(stage_in(ctx, y, n, ctx->in3, &dy));
+  CKI(stage_in(ctx, z, n, ctx->in4, &dz));
+  if (ccav) CKI(stage_in(ctx, ccav, 3 * (size_t)ncav, ctx->ef2, &dc));
+  else dc = ctx->ccav.as<double>();
+  double *dphi, *dpsi;
+  CKI(out_ptr(ctx, phi, ncav, ctx->phi, &dphi));
+  CKI(out_ptr(ctx, psi, (size_t)n * nylm, ctx->out1, &dpsi));
+  CK(launch_coulomb_pot(ctx->L(), n, dq, dx, dy, dz, ncav, dc, dphi));
+  CK(launch_psi(ctx->L(), n, nylm, dq, dpsi));
+  CKI(finish_out(ctx, phi, dphi, ncav));
+  CKI(finish_out(ctx, psi, dpsi, (size_t)n * nylm));
+  return sync(ctx);
+}
+
+int ddc_rhs(ddc_ctx* ctx, const double* phi, double* g) {
+  CKI(need_ready(ctx));
+  cudaSetDevice(ctx->prm.device);
+  const double* dphi;
+  CKI(stage_in(ctx, phi, ctx->ncav, ctx->in1, &dphi));
+  double* dg;
+  CKI(out_ptr(ctx, g, (size_t)ctx->nsph * ctx->nylm, ctx->out1, &dg));
+  CK(ctx->gbuf.ensure(sizeof(double) * std::max<long long>((long long)ctx->nsph * ctx->ngrid, 1)));
+  CK(launch_wghpot(ctx->L(), ctx->geo(), dphi, ctx->gbuf.as<double>()));
+  CK(launch_dgemm(ctx->L(), false, ctx->nylm, ctx->nsph, ctx->ngrid, 1.0, ctx->bw.as<double>(),
+                  ctx->nylm, ctx->gbuf.as<double>(), ctx->ngrid, 0.0, dg, ctx->nylm));
+  CKI(finish_out(ctx, g, dg, (size_t)ctx->nsph * ctx->nylm));
+  return sync(ctx);
+}
+
+int ddc_cosmo(ddc_ctx* ctx, int star, int cart, const double* phi, const double* glm,
+              const double* psi, double* sigma, double* esolv, ddc_solve_info* info) {
+  CKI(need_ready(ctx));
+  cudaSetDevice(ctx->prm.device);
+  if (!sigma) return fail(ctx, DDC_ERR_PARAM, "null sigma");
+  const size_t nv = (size_t)ctx->nsph * ctx->nylm;
+  const double *dphi = nullptr, *dglm = nullptr, *dpsi = nullptr;
+  if (!star) {
+    if (cart) CKI(stage_in(ctx, phi, ctx->ncav, ctx->in1, &dphi));
+    else CKI(stage_in(ctx, glm, nv, ctx->in1, &dglm));
+    if (esolv) CKI(stage_in(ctx, psi, nv, ctx->in2, &dpsi));
+  } else {
+    CKI(stage_in(ctx, psi, nv, ctx->in2, &dpsi));
+  }
+  double* dsig;
+  if (ctx->prm.device_pointers) {
+    dsig = sigma;
+  } else {
+    dsig = ctx->sigma.as<double>();
+    if (ctx->prm.guess == DDC_GUESS_USER)
+      CK(cudaMemcpyAsync(dsig, sigma, sizeof(double) * nv, cudaMemcpyHostToDevice, ctx->st));
+  }
+  int rc = cosmo_dev(ctx, star, cart, dphi, dglm, dpsi, dsig, star ? nullptr : esolv, info);
+  if (rc != DDC_OK && rc != DDC_ERR_NOCONV) return rc;
+  if (!ctx->prm.device_pointers)
+    CK(cudaMemcpyAsync(sigma, dsig, sizeof(double) * nv, cudaMemcpyDeviceToHost, ctx->st));
+  CKI(sync(ctx));
+  return rc;
+}
+
+int ddc_forces_dd(ddc_ctx* ctx, const double* phi, const double* sigma, const double* s,
+                  double* fx) {
+  CKI(need_ready(ctx));
+  cudaSetDevice(ctx->prm.device);
+  const size_t nv = (size_t)ctx->nsph * ctx->nylm;
+  const double *dphi, *dsig, *ds;
+  CKI(stage_in(ctx, phi, ctx->ncav, ctx->in1, &dphi));
+  CKI(stage_in(ctx, sigma, nv, ctx->in2, &dsig));
+  CKI(stage_in(ctx, s, nv, ctx->in3, &ds));
+  double* dfx;
+  CKI(out_ptr(ctx, fx, 3 * (size_t)ctx->nsph, ctx->fx, &dfx));
+  CKI(forces_dev(ctx, dphi, dsig, ds, dfx));
+  CKI(finish_out(ctx, fx, dfx, 3 * (size_t)ctx->nsph));
+  return sync(ctx);
+}
+
+static int mkxi_common(ddc_ctx* ctx, const double* s, double* out, double scale) {
+  CKI(need_ready(ctx));
+  cudaSetDevice(ctx->prm.device);
+  const double* ds;
+  CKI(stage_in(ctx, s, (size_t)ctx->nsph * ctx->nylm, ctx->in1, &ds));
+  double* dout;
+  CKI(out_ptr(ctx, out, ctx->ncav, ctx->zeta, &dout));
+  CKI(op_xi(ctx, ds, ctx->xig.as<double>()));
+  CK(launch_mkxi(ctx->L(), ctx->tb, ctx->geo(), ctx->xig.as<double>(), scale, dout));
+  CKI(finish_out(ctx, out, dout, ctx->ncav));
+  return sync(ctx);
+}
+int ddc_mkzeta(ddc_ctx* ctx, const double* s, double* zeta) {
+  if (!ctx) return DDC_ERR_PARAM;
+  return mkxi_common(ctx, s, zeta, 0.5 * ((ctx->prm.eps - 1.0) / ctx->prm.eps));
+}
+int ddc_mkxi(ddc_ctx* ctx, const double* s, double* xi) { return mkxi_common(ctx, s, xi, 1.0); }
+
+int ddc_efld(ddc_ctx* ctx, int nsrc, const double* src, const double* csrc, int ntrg,
+             const double* ctrg, double* ef) {
+  if (!ctx) return DDC_ERR_PARAM;
+  cudaSetDevice(ctx->prm.device);
+  if (nsrc < 0 || ntrg < 0) return fail(ctx, DDC_ERR_PARAM, "bad sizes");
+  auto ctx_coords = [&](int cnt, const double** out) -> int {
+    CKI(need_ready(ctx));
+    if (cnt == ctx->ncav) *out = ctx->ccav.as<double>();
+    else if (cnt == ctx->nsph) *out = ctx->csph.as<double>();
+    else return fail(ctx, DDC_ERR_PARAM, "NULL coordinates need ncav or nsph points");
+    return DDC_OK;
+  };
+  const double *dsrc, *dcs, *dct;
+  CKI(stage_in(ctx, src, nsrc, ctx->in1, &dsrc));
+  if (csrc) CKI(stage_in(ctx, csrc, 3 * (size_t)nsrc, ctx->in2, &dcs));
+  else CKI(ctx_coords(nsrc, &dcs));
+  if (ctrg) CKI(stage_in(ctx, ctrg, 3 * (size_t)ntrg, ctx->in3, &dct));
+  else CKI(ctx_coords(ntrg, &dct));
+  double* def;
+  CKI(out_ptr(ctx, ef, 3 * (size_t)ntrg, ctx->out1, &def));
+  int nchunk = efield_chunks(nsrc, ntrg);
+  CK(ctx->ef_scratch.ensure(sizeof(double) * 3 * (size_t)std::max(ntrg, 1) * nchunk));
+  CK(launch_efield(ctx->L(), nsrc, dsrc, dcs, ntrg, dct, def, ctx->ef_scratch.as<double>(),
+                   nchunk));
+  CKI(finish_out(ctx, ef, def, 3 * (size_t)ntrg));
+  return sync(ctx);
+}
+
+int ddc_lx(ddc_ctx* ctx, const double* x, double* y) {
+  CKI(need_ready(ctx));
+  cudaSetDevice(ctx->prm.device);
+  const size_t nv = (size_t)ctx->nsph * ctx->nylm;
+  const double* dx;
+  CKI(stage_in(ctx, x, nv, ctx->in1, &dx));
+  double* dy;
+  CKI(out_ptr(ctx, y, nv, ctx->out1, &dy));
+  CKI(op_lx(ctx, dx, dy));
+  CKI(finish_out(ctx, y, dy, nv));
+  return sync(ctx);
+}
+int ddc_lstarx(ddc_ctx* ctx, const double* x, double* y) {
+  CKI(need_ready(ctx));
+  cudaSetDevice(ctx->prm.device);
+  const size_t nv = (size_t)ctx->nsph * ctx->nylm;
+  const double* dx;
+  CKI(stage_in(ctx, x, nv, ctx->in1, &dx));
+  double* dy;
+  CKI(out_ptr(ctx, y, nv, ctx->out1, &dy));
+  CKI(op_lstarx(ctx, dx, dy));
+  CKI(finish_out(ctx, y, dy, nv));
+  return sync(ctx);
+}
+int ddc_ldm1x(ddc_ctx* ctx, const double* x, double* y) {
+  CKI(need_ready(ctx));
+  cudaSetDevice(ctx->prm.device);
+  const size_t nv = (size_t)ctx->nsph * ctx->nylm;
+  const double* dx;
+  CKI(stage_in(ctx, x, nv, ctx->in1, &dx));
+  double* dy;
+  CKI(out_ptr(ctx, y, nv, ctx->out1, &dy));
+  CK(launch_ldm1x(ctx->L(), ctx->tb, (long long)nv, dx, dy));
+  CKI(finish_out(ctx, y, dy, nv));
+  return sync(ctx);
+}
+int ddc_hnorm(ddc_ctx* ctx, const double* x, double* norm) {
+  CKI(need_ready(ctx));
+  cudaSetDevice(ctx->prm.device);
+  if (!norm) return fail(ctx, DDC_ERR_PARAM, "null norm");
+  const size_t nv = (size_t)ctx->nsph * ctx->nylm;
+  const double* dx;
+  CKI(stage_in(ctx, x, nv, ctx->in1, &dx));
+  CK(launch_hnorm_partial(ctx->L(), ctx->tb, (long long)nv, dx, ctx->partials.as<double>(),
+                          reduce_blocks()));
+  double ss = 0.0;
+  CKI(reduce_to_host(ctx, 1, &ss));
+  *norm = std::sqrt(ss / (double)std::max(ctx->nsph, 1));
+  return DDC_OK;
+}
+
+int ddc_energy_forces(ddc_ctx* ctx, int n, const double* charge, const double* x,
+                      const double* y, const double* z, const double* rvdw, double* esolv,
+                      double* sigma, double* s, double* fx, ddc_run_info* info) {
+  if (!ctx || !esolv) return DDC_ERR_PARAM;
+  cudaSetDevice(ctx->prm.device);
+  ddc_run_info loc{};
+  ddc_run_info* inf = info ? info : &loc;
+  memset(inf, 0, sizeof(*inf));
+  double t0 = now_s();
+  CKI(ddc_init(ctx, n, x, y, z, rvdw));
+  double t1 = now_s();
+  inf->t_init = t1 - t0;
+  const int N = ctx->nsph, NC = ctx->ncav;
+  const size_t nv = (size_t)N * ctx->nylm;
+  const double* dq;
+  CKI(stage_in(ctx, charge, N, ctx->q, &dq));
+  CK(ctx->phi.ensure(sizeof(double) * std::max(NC, 1)));
+  double* dphi = ctx->phi.as<double>();
+  double* dpsi = ctx->psi.as<double>();
+  // mkrhs (mkrhs.f90:102-120) with the context's own centres and cavity
+  {
+  StageScope sc(ctx, ST_COULOMB);
+  CK(launch_coulomb_pot(ctx->L(), N, dq, ctx->cx.as<double>(), ctx->cy.as<double>(),
+                        ctx->cz.as<double>(), NC, ctx->ccav.as<double>(), dphi));
+  CK(launch_psi(ctx->L(), N, ctx->nylm, dq, dpsi));
+  }
+  CKI(sync(ctx));
+  double t2 = now_s();
+  inf->t_mkrhs = t2 - t1;
+  double* dsig = ctx->sigma.as<double>();
+  double* ds = ctx->s.as<double>();
+  CKI(cosmo_dev(ctx, 0, 1, dphi, nullptr, dpsi, dsig, esolv, &inf->direct));
+  double t3 = now_s();
+  inf->t_direct = t3 - t2;
+  double* dfx = nullptr;
+  if (ctx->prm.igrad) {
+    CKI(cosmo_dev(ctx, 1, 0, nullptr, nullptr, dpsi, ds, nullptr, &inf->adjoint));
+    double t4 = now_s();
+    inf->t_adjoint = t4 - t3;
+    CK(ctx->fx.ensure(sizeof(double) * 3 * std::max(N, 1)));
+    dfx = ctx->fx.as<double>();
+    CKI(forces_dev(ctx, dphi, dsig, ds, dfx));
+    CK(ctx->zeta.ensure(sizeof(double) * std::max(NC, 1)));
+    double fep = 0.5 * ((ctx->prm.eps - 1.0) / ctx->prm.eps);
+    {
+      StageScope sc(ctx, ST_ZETA);
+      CK(launch_mkxi(ctx->L(), ctx->tb, ctx->geo(), ctx->xig.as<double>(), fep,
+                     ctx->zeta.as<double>()));
+    }
+    CKI(sync(ctx));
+    double t5 = now_s();
+    inf->t_forces = t5 - t4;
+    // solute field at the cavity times zeta (main.f90:241-253)
+    CK(ctx->ef1.ensure(sizeof(double) * 3 * std::max(NC, 1)));
+    CK(ctx->ef2.ensure(sizeof(double) * 3 * std::max(N, 1)));
+    int ch1 = efield_chunks(N, NC), ch2 = efield_chunks(NC, N);
+    CK(ctx->ef_scratch.ensure(sizeof(double) * 3 *
+                              std::max((size_t)ch1 * NC, (size_t)ch2 * N + 1)));
+    {
+      StageScope sc(ctx, ST_EFIELD);
+      CK(launch_efield(ctx->L(), N, dq, ctx->csph.as<double>(), NC, ctx->ccav.as<double>(),
+                       ctx->ef1.as<double>(), ctx->ef_scratch.as<double>(), ch1));
+    }
+    {
+      StageScope sc(ctx, ST_CONTRACT);
+      CK(launch_zeta_efld_contract(ctx->L(), ctx->geo(), ctx->zeta.as<double>(),
+                                   ctx->ef1.as<double>(), dfx));
+    }
+    // field of zeta at the nuclei times the charges (main.f90:259-265)
+    {
+      StageScope sc(ctx, ST_EFIELD);
+      CK(launch_efield(ctx->L(), NC, ctx->zeta.as<double>(), ctx->ccav.as<double>(), N,
+                       ctx->csph.as<double>(), ctx->ef2.as<double>(),
+                       ctx->ef_scratch.as<double>(), ch2));
+    }
+    {
+      StageScope sc(ctx, ST_CONTRACT);
+      CK(launch_charge_efld_contract(ctx->L(), N, dq, ctx->ef2.as<double>(), dfx));
+    }
+    CKI(sync(ctx));
+    inf->t_efld = now_s() - t5;
+  }
+  CKI(finish_out(ctx, sigma, dsig, nv));
+  if (ctx->prm.igrad) {
+    CKI(finish_out(ctx, s, ds, nv));
+    CKI(finish_out(ctx, fx, dfx, 3 * (size_t)N));
+  }
+  CKI(sync(ctx));
+  inf->nsph = N;
+  inf->ncav = NC;
+  inf->nylm = ctx->nylm;
+  inf->ngrid = ctx->ngrid;
+  inf->ntriples = ctx->ntri;
+  inf->npairs = ctx->npair;
+  return DDC_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,179 @@
+// ddc_internal.h -- shared declarations of the B200 ddCOSMO library.
+//
+// Layout in HBM (one molecule per context, sizes for N spheres, G grid
+// points, Y = (lmax+1)^2 harmonics, P neighbour pairs, T triples):
+//   sph[N]         double4 {x, y, z, r} (bohr)
+//   grid[G]        double4 {sx, sy, sz, w} (unit vectors, 4pi-scaled weights)
+//   basis[G][Y]    Y_lm(s_n); bw[G][Y] = basis * w  (the intrhs operator)
+//   inl[N+1], nl[P]      CSR neighbour list, 0-based, ascending j (ddinit)
+//   rev[P]               index of (j,i) for the entry (i,j)
+//   fi, ui[N][G]         overlap count f_i(n) and cavity weight U_i(n)
+//   zi[N][G][3]          grad f (forces only)
+//   pn_ptr[P+1], pn[T]   per pair (i,j): grid points n of sphere i with
+//                        t_n^ij < 1 (point inside sphere j), ascending n
+//   ls_ptr[N+1], ls[T]   per sphere i: (j, n) for j in N_i (CSR order) and the
+//                        points n of sphere j inside sphere i (adjoint gather)
+//   ntri[N][G]           number of neighbours containing point (i,n)
+//   cavoff[N+1], cavidx[N][G], cavpt[ncav], ccav[ncav][3]
+// Vectors X(nylm,nsph) live as X[i*nylm + lm], like the reference.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/ddcosmo_gpu.h"
+
+#define DDC_NLM_CAP ((DDC_MAX_LMAX + 1) * (DDC_MAX_LMAX + 2) / 2)
+
+namespace ddc {
+
+// Constants of the spherical-harmonic recurrences, indexed by (l, m >= 0)
+// packed as l*(l+1)/2 + m.  Passed by value to the kernels (parameter space
+// is a broadcast constant bank, so per-(l,m) reads are free).
+struct YlmTables {
+  double facl[DDC_MAX_LMAX + 1];  // (2l+1)/(4pi): D^-1 block (ddcosmo.f90:233)
+  double facs[DDC_NLM_CAP];       // Y_lm normalisation incl. odd-m sign (:236-242)
+  double K[DDC_NLM_CAP];          // facs / facl
+  double A[DDC_NLM_CAP];          // (2l-1)/(l-m): Legendre recurrence
+  double B[DDC_NLM_CAP];          // (l+m-1)/(l-m)
+  double eta;
+  int lmax, nylm, ngrid;
+};
+
+// Device geometry handed to every kernel.
+struct DevGeo {
+  int nsph, ngrid, nylm, ncav, npair;
+  long long ntri;
+  const double4* sph;
+  const double4* grid;
+  const double* basis;
+  const double* bw;
+  const double* fi;
+  const double* ui;
+  const double* zi;
+  const int* inl;
+  const int* nl;
+  const int* rev;
+  const int* pn_ptr;
+  const uint16_t* pn;
+  const int* ls_ptr;
+  const int2* ls;
+  const uint8_t* ntri_pt;
+  const int* cavoff;
+  const int* cavidx;
+  const int* cavpt;
+  const double* ccav;
+};
+
+// Stages timed with CUDA events when ddc_params.timing = 1.
+enum Stage {
+  ST_INIT = 0, ST_COULOMB, ST_RHS, ST_LX_POT, ST_PROJ, ST_XI, ST_LSTARX, ST_JACOBI,
+  ST_COMBINE, ST_REDUCE, ST_UCHI, ST_FORCES, ST_ZETA, ST_EFIELD, ST_CONTRACT, ST_N
+};
+
+// History of DIIS vectors for the fused Jacobi step / extrapolation.
+constexpr int kMaxHist = 32;
+struct HistPtrs {
+  const double* p[kMaxHist];
+  double c[kMaxHist];
+  int n;
+};
+
+// ---------------------------------------------------------------------------
+// Kernel launchers (ddc_kernels.cu).  All run on `st` and return the CUDA
+// error of the launch.  `launches` is incremented per kernel launched.
+// ---------------------------------------------------------------------------
+struct Launch {
+  cudaStream_t st;
+  long long* launches;
+};
+
+// init
+cudaError_t launch_basis(Launch L, const YlmTables& tb, const double4* grid, double* basis,
+                         double* bw);
+cudaError_t launch_csr_count(Launch L, int nsph, const double4* sph, int* cnt);
+cudaError_t launch_csr_fill(Launch L, int nsph, const double4* sph, const int* inl, int* nl);
+cudaError_t launch_csr_rev(Launch L, int nsph, const int* inl, const int* nl, int* rev);
+cudaError_t launch_fiui(Launch L, const YlmTables& tb, int nsph, const double4* sph,
+                        const double4* grid, const int* inl, const int* nl, double* fi, double* ui,
+                        double* zi, uint8_t* ntri);
+cudaError_t launch_cav_count(Launch L, int nsph, int ngrid, const double* ui, int* cnt);
+cudaError_t launch_cav_fill(Launch L, int nsph, int ngrid, const double* ui, const double4* sph,
+                            const double4* grid, const int* cavoff, int* cavidx, int* cavpt,
+                            double* ccav);
+cudaError_t launch_pair_count(Launch L, int nsph, int ngrid, const double4* sph,
+                              const double4* grid, const int* inl, const int* nl, int* cnt);
+cudaError_t launch_pair_fill(Launch L, int nsph, int ngrid, const double4* sph,
+                             const double4* grid, const int* inl, const int* nl,
+                             const int* pn_ptr, uint16_t* pn);
+cudaError_t launch_ls_count(Launch L, int nsph, const int* inl, const int* rev, const int* pn_ptr,
+                            int* cnt);
+cudaError_t launch_ls_fill(Launch L, int nsph, const int* inl, const int* nl, const int* rev,
+                           const int* pn_ptr, const uint16_t* pn, const int* ls_ptr, int2* ls);
+// exclusive scan of n ints (out[n] = total); temp is device scratch of temp_bytes
+cudaError_t scan_exclusive(Launch L, const int* in, int* out, int n, void* temp,
+                           size_t temp_bytes);
+size_t scan_temp_bytes(int n);
+
+// operators
+cudaError_t launch_lx_pot(Launch L, const YlmTables& tb, const DevGeo& g, const double* X,
+                          double* pot, bool chi_only);
+cudaError_t launch_lstarx_acc(Launch L, const YlmTables& tb, const DevGeo& g, const double* xi,
+                              double* y);
+// C[M x N] = alpha * op(A) * B (+ beta*C), column-major FP64
+cudaError_t launch_dgemm(Launch L, bool transA, int M, int N, int K, double alpha,
+                         const double* A, int lda, const double* B, int ldb, double beta,
+                         double* C, int ldc);
+cudaError_t launch_wghpot(Launch L, const DevGeo& g, const double* phi, double* gbuf);
+cudaError_t launch_ldm1x(Launch L, const YlmTables& tb, long long n, const double* x, double* y);
+cudaError_t launch_scale(Launch L, long long n, double a, const double* x, double* y);
+cudaError_t launch_guess(Launch L, const YlmTables& tb, long long n, const double* rhs,
+                         double* x, int mode);
+
+// solver
+// xnew = facl*(rhs - y); e = xnew - x; partial dots e.h_k (k < hist.n) and e.e
+cudaError_t launch_jacobi_step(Launch L, const YlmTables& tb, long long n, const double* rhs,
+                               const double* y, const double* x, double* xnew, double* e,
+                               const HistPtrs& hist, double* partials, int nblk);
+// xout = sum c_k p_k (or xjac if hist.n == 0); partial of sum_l 1/(l+1) (xout-x)^2; x = xout
+cudaError_t launch_diis_combine(Launch L, const YlmTables& tb, long long n, const HistPtrs& hist,
+                                const double* xjac, double* x, double* partials, int nblk);
+cudaError_t launch_hnorm_partial(Launch L, const YlmTables& tb, long long n, const double* x,
+                                 double* partials, int nblk);
+cudaError_t launch_dot_partial(Launch L, long long n, const double* a, const double* b,
+                               double* partials, int nblk);
+// out[k] = sum_b partials[b*nvals + k], fixed order
+cudaError_t launch_reduce_partials(Launch L, const double* partials, int nblk, int nvals,
+                                   double* out);
+int reduce_blocks();
+
+// electrostatics
+cudaError_t launch_coulomb_pot(Launch L, int nsrc, const double* q, const double* sx,
+                               const double* sy, const double* sz, int ntrg, const double* ctrg,
+                               double* phi);
+cudaError_t launch_psi(Launch L, int n, int nylm, const double* q, double* psi);
+// field of sources (q at csrc(3,nsrc)) at targets ctrg(3,ntrg); partial sums
+// over `nchunk` source chunks go to scratch[nchunk][ntrg][3]
+cudaError_t launch_efield(Launch L, int nsrc, const double* q, const double* csrc, int ntrg,
+                          const double* ctrg, double* ef, double* scratch, int nchunk);
+int efield_chunks(int nsrc, int ntrg);
+
+// forces
+cudaError_t launch_forces(Launch L, const YlmTables& tb, const DevGeo& g, const double* sigma,
+                          const double* s_xi, const double* u_chi, const double* phi,
+                          double fep, double* fx);
+cudaError_t launch_mkxi(Launch L, const YlmTables& tb, const DevGeo& g, const double* xi_grid,
+                        double scale, double* out);
+cudaError_t launch_zeta_efld_contract(Launch L, const DevGeo& g, const double* zeta,
+                                      const double* ef, double* fx);
+cudaError_t launch_charge_efld_contract(Launch L, int n, const double* q, const double* ef,
+                                        double* fx);
+// FP64 FMA throughput probe: each thread runs `iters` x 8 independent FMA chains
+cudaError_t launch_fp64_probe(Launch L, int blocks, int iters, double* out);
+
+cudaError_t launch_csph_pack(Launch L, int n, const double4* sph, double* csph, double* sx,
+                             double* sy, double* sz);
+
+}  // namespace ddc

@@ -1,0 +1,187 @@
+/*
+ * ddcosmo_gpu.h -- C ABI of the B200 ddCOSMO solver.
+ *
+ * Every entry point is a drop-in for one routine of the Fortran reference
+ * (filippolipparini/ddPCM).  The reference keeps its state in module globals
+ * (ddcosmo.f90:87-127); here that state lives in an opaque context, so several
+ * molecules can be set up side by side.  Arrays cross the boundary as FP64 in
+ * exactly the reference's column-major shapes (X(nylm,nsph) is
+ * X[isph*nylm + lm], ccav(3,ncav) is ccav[3*ic + k], ...), by plain pointer.
+ * By default the pointers are host memory and each call is synchronous, like
+ * the reference; with ddc_params.device_pointers = 1 they are device memory of
+ * the context's GPU and no host<->device copy happens.
+ *
+ * Every function returns a status (DDC_OK = 0).  Where the reference prints
+ * and calls `stop`, the library returns an error code instead.
+ */
+#ifndef DDCOSMO_GPU_H
+#define DDCOSMO_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define DDC_OK 0
+#define DDC_ERR_PARAM 1        /* invalid argument or parameter */
+#define DDC_ERR_STATE 2        /* call order (e.g. cosmo before init) */
+#define DDC_ERR_CUDA 3         /* CUDA runtime error */
+#define DDC_ERR_NOMEM 4        /* device allocation failed */
+#define DDC_ERR_NOCONV 5       /* Jacobi/DIIS hit max_iter (cosmo.f90:188-200) */
+#define DDC_ERR_UNSUPPORTED 6  /* lmax outside the compiled range */
+#define DDC_ERR_NUMERIC 7      /* NaN/Inf in a stage output */
+
+/* precision modes */
+#define DDC_PREC_FP64 0   /* every stage in FP64 */
+#define DDC_PREC_MIXED 1  /* FP32 operator inside FP64 iterative refinement */
+
+/* initial guess for the solves */
+#define DDC_GUESS_REFERENCE 0 /* facl * rhs, as cosmo.f90:136-138 / 174-176 */
+#define DDC_GUESS_ZERO 1      /* zero vector */
+#define DDC_GUESS_USER 2      /* the caller's sigma on entry */
+
+#define DDC_MAX_LMAX 12
+
+typedef struct ddc_ctx ddc_ctx;
+
+/* Control parameters: the reference's Input.txt scalars (main.f90:129-136,
+ * ddcosmo.f90:106-107) plus solver knobs that the reference hard-codes
+ * (ndiis=25 ddcosmo.f90:87, n_iter=200 cosmo.f90:81). */
+typedef struct {
+  int lmax;            /* max angular momentum, 0..DDC_MAX_LMAX */
+  int ngrid;           /* requested Lebedev size; snapped like ddinit */
+  int iconv;           /* tolerance 10^-iconv on the increment H-norm */
+  int igrad;           /* 1: prepare the force intermediates (zi) */
+  double eps;          /* solvent dielectric constant */
+  double eta;          /* switch-function regularisation */
+  int iprint;          /* >0: print the iteration log like jacobi_diis */
+  int max_iter;        /* 200 in the reference */
+  int ndiis;           /* 25 in the reference; 0 disables DIIS */
+  int precision;       /* DDC_PREC_* */
+  int guess;           /* DDC_GUESS_* */
+  int device;          /* CUDA device ordinal */
+  int device_pointers; /* 0: host arrays, 1: device arrays */
+  void* stream;        /* cudaStream_t to run on; NULL: the context's own */
+  int timing;          /* 1: time each stage with CUDA events (ddc_stage_times) */
+} ddc_params;
+
+/* Solver report of one cosmo call (replaces the iprint log and the
+ * non-convergence stop of cosmo.f90:188-221). */
+typedef struct {
+  int iterations;      /* Jacobi iterations taken (n_iter on return) */
+  int converged;       /* 1 if the increment norm fell below 10^-iconv */
+  int diis_restarts;   /* singular DIIS systems that reset the history */
+  int refinements;     /* outer FP64 refinement steps (mixed precision) */
+  double final_norm;   /* last increment norm */
+  double seconds;      /* wall time of the solve */
+  double norms[256];   /* increment norm of each iteration (first 256) */
+} ddc_solve_info;
+
+/* Report of the fused energy+forces flow. */
+typedef struct {
+  ddc_solve_info direct, adjoint;
+  double t_init, t_mkrhs, t_direct, t_adjoint, t_forces, t_efld; /* seconds */
+  int nsph, ncav, nylm, ngrid;
+  long long ntriples;  /* (sphere, point, neighbour) triples with t < 1 */
+  int npairs;          /* neighbour pairs in the CSR list */
+} ddc_run_info;
+
+/* Defaults: lmax 6, ngrid 110, iconv 7, igrad 1, eps 78.3553, eta 0.2,
+ * max_iter 200, ndiis 25, FP64, reference guess, device 0, host pointers. */
+int ddc_default_params(ddc_params* p);
+
+/* Create / destroy a context (module state; memfree ddcosmo.f90:491). */
+int ddc_create(const ddc_params* p, ddc_ctx** ctx);
+int ddc_destroy(ddc_ctx* ctx);
+
+/* Last error message of this context (static storage, never NULL). */
+const char* ddc_last_error(ddc_ctx* ctx);
+const char* ddc_status_string(int status);
+
+/* ddinit(n, x, y, z, rvdw)  ddcosmo.f90:159-483.  Coordinates and radii in
+ * bohr.  Builds the grid, basis, neighbour list, fi/ui/zi and the cavity. */
+int ddc_init(ddc_ctx* ctx, int n, const double* x, const double* y, const double* z,
+             const double* rvdw);
+
+/* Module sizes after init: nsph, ncav, nylm and the snapped ngrid. */
+int ddc_sizes(ddc_ctx* ctx, int* nsph, int* ncav, int* nylm, int* ngrid);
+
+/* Module arrays read by the host code (main.f90:184-265):
+ * ccav(3,ncav), ui(ngrid,nsph), csph(3,nsph), grid(3,ngrid), w(ngrid). */
+int ddc_get_ccav(ddc_ctx* ctx, double* ccav);
+int ddc_get_ui(ddc_ctx* ctx, double* ui);
+int ddc_get_csph(ddc_ctx* ctx, double* csph);
+int ddc_get_grid(ddc_ctx* ctx, double* grid, double* w);
+
+/* mkrhs(n, charge, x, y, z, ncav, ccav, phi, nylm, psi)  mkrhs.f90:1-123.
+ * phi(ncav) = sum_j q_j / |ccav - x_j|; psi(nylm,n) with psi(1,i)=sqrt(4pi)q_i.
+ * ccav may be NULL: the context's own cavity points are used (no copy). */
+int ddc_mkrhs(ddc_ctx* ctx, int n, const double* charge, const double* x, const double* y,
+              const double* z, int ncav, const double* ccav, double* phi, int nylm, double* psi);
+
+/* cosmo(star, cart, phi, glm, psi, sigma, esolv)  cosmo.f90:1-226.
+ * star=0: solve L X = g (g from phi if cart, else glm); returns sigma = X and
+ * esolv = 1/2 (eps-1)/eps <X, psi>.  star=1: solve L* S = psi; sigma = S.
+ * info may be NULL.  Returns DDC_ERR_NOCONV (with sigma holding the last
+ * iterate) where the reference stops. */
+int ddc_cosmo(ddc_ctx* ctx, int star, int cart, const double* phi, const double* glm,
+              const double* psi, double* sigma, double* esolv, ddc_solve_info* info);
+
+/* forces_dd(n, phi, sigma, s, fx)  forces_dd.f90:1-164: fep * (fdoka + fdokb
+ * + fdoga) into fx(3,n) (overwritten). */
+int ddc_forces_dd(ddc_ctx* ctx, const double* phi, const double* sigma, const double* s,
+                  double* fx);
+
+/* ddmkzeta(s, zeta) ddcosmo.f90:1787-1806 and ddmkxi(s, xi) 1758-1781. */
+int ddc_mkzeta(ddc_ctx* ctx, const double* s, double* zeta);
+int ddc_mkxi(ddc_ctx* ctx, const double* s, double* xi);
+
+/* efld(nsrc, src, csrc, ntrg, ctrg, ef)  efld.f90:1-116: field of point
+ * sources at the targets.  csrc/ctrg may be NULL to mean the context's
+ * cavity points (ccav) when the count equals ncav, or its sphere centres
+ * (csph) when the count equals nsph. */
+int ddc_efld(ddc_ctx* ctx, int nsrc, const double* src, const double* csrc, int ntrg,
+             const double* ctrg, double* ef);
+
+/* The main.f90 energy+forces flow in one call (main.f90:164-265): ddinit,
+ * mkrhs, direct solve, energy, adjoint solve, forces_dd, ddmkzeta and the two
+ * efld contractions.  Inputs: charges and bohr coordinates/radii; outputs
+ * esolv (Hartree), sigma = X and s = S (nylm,n), fx(3,n) total forces
+ * (Hartree/bohr; any of sigma, s, fx may be NULL).  info may be NULL. */
+int ddc_energy_forces(ddc_ctx* ctx, int n, const double* charge, const double* x,
+                      const double* y, const double* z, const double* rvdw, double* esolv,
+                      double* sigma, double* s, double* fx, ddc_run_info* info);
+
+/* The operators the solver iterates (matvec.f90): y = off-diagonal L x
+ * (lx, :94), y = off-diagonal L* x (lstarx, :161), y = D^-1 x (ldm1x, :246)
+ * and the increment norm hnorm (:281).  x, y are (nylm,nsph). */
+int ddc_lx(ddc_ctx* ctx, const double* x, double* y);
+int ddc_lstarx(ddc_ctx* ctx, const double* x, double* y);
+int ddc_ldm1x(ddc_ctx* ctx, const double* x, double* y);
+int ddc_hnorm(ddc_ctx* ctx, const double* x, double* norm);
+
+/* RHS of the direct equation from phi (wghpot + intrhs, cosmo.f90:104-117). */
+int ddc_rhs(ddc_ctx* ctx, const double* phi, double* g);
+
+/* Number of kernel launches issued by this context since creation. */
+long long ddc_launch_count(ddc_ctx* ctx);
+
+/* Per-stage device time, measured with CUDA events on the context's stream
+ * when ddc_params.timing = 1.  No reference counterpart (the reference only
+ * times whole solves, cosmo.f90:84-85, 202).  ms/calls have
+ * ddc_stage_count() entries; ddc_stage_name(k) names stage k. */
+int ddc_stage_count(void);
+const char* ddc_stage_name(int k);
+int ddc_stage_times(ddc_ctx* ctx, double* ms, long long* calls);
+int ddc_reset_stage_times(ddc_ctx* ctx);
+
+/* Measured FP64 FMA throughput of the device (GFLOP/s, 2 flops per FMA),
+ * from a register-resident FMA kernel timed with CUDA events.  No
+ * reference counterpart: it is the roofline denominator of the FP64-bound
+ * kernels. */
+int ddc_fp64_peak(int device, double* gflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DDCOSMO_GPU_H */

@@ -16,7 +16,22 @@ import subprocess
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "_build", "libddc_ref.so")
+
+
+def _host_tag():
+    """Build folder per host CPU: the oracle is compiled with -march=native."""
+    import hashlib
+    try:
+        info = open("/proc/cpuinfo").read()
+        model = next((ln for ln in info.splitlines() if ln.startswith("model name")), "")
+        flags = next((ln for ln in info.splitlines() if ln.startswith("flags")), "")
+        return hashlib.sha1((model + flags).encode()).hexdigest()[:10]
+    except OSError:
+        return "generic"
+
+
+BUILD_DIR = os.path.join(HERE, "_build", _host_tag())
+LIB_PATH = os.path.join(BUILD_DIR, "libddc_ref.so")
 
 _lib = None
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -24,7 +39,7 @@ _ip = ctypes.POINTER(ctypes.c_int)
 
 
 def build():
-    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    subprocess.run(["make", "-s", "-C", HERE, "OUT=" + BUILD_DIR], check=True)
 
 
 def lib():

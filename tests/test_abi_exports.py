@@ -1,0 +1,37 @@
+"""The C ABI library loads without a GPU and exports every declared entry point."""
+import ctypes
+import os
+import re
+
+from conftest import ROOT
+
+
+def test_library_exports_every_header_symbol():
+    from ddpcm_b200.build import build
+    lib = build()
+    hdr = open(os.path.join(ROOT, "include", "ddcosmo_gpu.h")).read()
+    names = sorted(set(re.findall(r"^\s*(?:const\s+)?\w+\**\s+\**(ddc_\w+)\s*\(", hdr, re.M)))
+    assert len(names) >= 25
+    L = ctypes.CDLL(lib)
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, missing
+
+
+def test_status_strings_and_defaults_without_gpu():
+    from ddpcm_b200.ddcosmo import Params, load_library
+    L = load_library()
+    p = Params()
+    assert L.ddc_default_params(ctypes.byref(p)) == 0
+    assert (p.lmax, p.ngrid, p.iconv, p.max_iter, p.ndiis) == (6, 110, 7, 200, 25)
+    assert L.ddc_status_string(5) == b"solver did not converge"
+    assert L.ddc_stage_count() >= 10
+
+
+def test_product_does_not_import_oracle():
+    pkg = os.path.join(ROOT, "ddpcm_b200")
+    for dirpath, _, files in os.walk(pkg):
+        for f in files:
+            if f.endswith((".py", ".cu", ".h", ".cpp", ".inc")):
+                src = open(os.path.join(dirpath, f)).read()
+                assert "import oracle" not in src and "from oracle" not in src, f
+                assert "ddc_ref" not in src, f
