@@ -1,0 +1,447 @@
+#!/usr/bin/env python3
+"""Benchmark of the ddCOSMO energy+force path on B200.
+
+Workload (one "step"): the reference's main.f90 flow -- ddinit, mkrhs, direct
+solve, energy, adjoint solve, forces_dd, ddmkzeta and the two efld
+contractions -- on the 20,000-sphere globule (lmax 10, 590 Lebedev points,
+eta 0.1, eps 78.3553, tol 1e-10), synthetic seeded input.  Metric: energy+force
+solves per second.
+
+* ``value``: whole-job solves/s with the inputs (charges, centres, radii)
+  already resident in HBM (C ABI in device-pointer mode), timed with CUDA
+  events on the library's stream, max over ranks.
+* ``e2e``: the same through the C ABI with host arrays: the host->device copy
+  of the inputs and the device->host copy of Esolv and the forces are inside
+  the timed region.
+* ``roofline``: the dominant kernel of the step, timed live with the
+  library's CUDA-event stage timers.
+* ``cpu_baseline``: the CPU oracle (restatement of the reference, OpenMP over
+  all host cores) on a bounded sample of the same workload, scaled to one
+  solve.
+
+Multi-GPU: the path does not shard (one molecule per GPU); ``--gpus N`` runs N
+independent replicas, one per rank, and reports the aggregate ("weak").
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+WORKLOAD = 2  # 20,000 spheres, lmax 10, ngrid 590
+METRIC = "energy+force solves/s"
+UNIT = "solves/s"
+
+
+def _workload_config():
+    from ddpcm_b200 import molecules as M
+    c = dict(M.CONFIGS[WORKLOAD])
+    mol = M.to_bohr(M.config_molecule(WORKLOAD))
+    return c, mol
+
+
+def _config_json(c, nranks, extra=None):
+    d = {"workload": f"globule N={c['n']} lmax={c['lmax']} ngrid={c['ngrid']} eta={c['eta']} "
+                     f"tol=1e-{c['iconv']} energy+forces",
+         "nsph": c["n"], "lmax": c["lmax"], "ngrid": c["ngrid"], "eta": c["eta"],
+         "eps": c["eps"], "iconv": c["iconv"], "seed": c["seed"],
+         "parallelism": f"replicas x{nranks}" if nranks > 1 else "single GPU",
+         "l2": "working set > L2 (DIIS history ~1 GB, grid fields ~0.5 GB); no flush needed",
+         "guess": "reference (facl*rhs)", "precision": "fp64"}
+    if extra:
+        d.update(extra)
+    return d
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing (one process per GPU; replicas, no data collective)
+# ---------------------------------------------------------------------------
+def _dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        backend = os.environ.get("DDC_BENCH_BACKEND", "nccl")
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    return world, rank, local, pg
+
+
+def _max_over_ranks(value, pg, device=None):
+    if pg is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _barrier(pg, device=None):
+    if pg is None:
+        return
+    import torch
+    t = torch.zeros(1, device=device)
+    pg.all_reduce(t)
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if f[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# roofline bookkeeping
+# ---------------------------------------------------------------------------
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return p.get("hbm_gbs", 6650.0), "measured"
+    except OSError:
+        return 6650.0, "fallback"
+
+
+def _stage_work(stage, info, c):
+    """Algorithmic FLOPs of one launch of a stage (FP64 pipe)."""
+    N, NC, NY, G, T = info["nsph"], info["ncav"], info["nylm"], info["ngrid"], info["ntriples"]
+    if stage == "coulomb_pot":
+        return 10.0 * N * NC                    # mkrhs: 10 flops per pair
+    if stage == "efield":
+        return 20.0 * N * NC                    # efld: 20 flops per pair (per launch)
+    if stage in ("lx_pot", "uchi_pot", "lstarx"):
+        return 6.0 * NY * T                     # 4*nylm (Y t^l) + 2*nylm (contraction)
+    if stage in ("proj_gemm", "xi_gemm"):
+        return 2.0 * NY * G * N
+    return None
+
+
+def _traffic_from_profiles(kernel):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "dram_traffic.txt")
+    try:
+        for ln in open(path):
+            f = ln.split()
+            if len(f) >= 2 and f[0] == kernel:
+                return float(f[1])
+    except OSError:
+        pass
+    return None
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def run_ours(args):
+    import torch
+
+    world, rank, local, pg = _dist_setup()
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    from ddpcm_b200.ddcosmo import DDCosmo, fp64_peak_gflops
+
+    c, mol = _workload_config()
+    stream = torch.cuda.current_stream(dev)
+    keys = "qxyzr"
+    d_in = {k: torch.tensor(mol[k], dtype=torch.float64, device=dev) for k in keys}
+    N = len(mol["q"])
+    nylm = (c["lmax"] + 1) ** 2
+    d_sig = torch.zeros((N, nylm), dtype=torch.float64, device=dev)
+    d_s = torch.zeros_like(d_sig)
+    d_fx = torch.zeros((N, 3), dtype=torch.float64, device=dev)
+    common = dict(lmax=c["lmax"], ngrid=c["ngrid"], iconv=c["iconv"], eps=c["eps"], eta=c["eta"],
+                  device=local)
+    dd = DDCosmo(device_pointers=1, stream=stream.cuda_stream, timing=1, **common)
+
+    def step_dev():
+        return dd.energy_forces_ptr(*(d_in[k].data_ptr() for k in keys), N,
+                                    d_sig.data_ptr(), d_s.data_ptr(), d_fx.data_ptr())
+
+    for _ in range(args.warmup):
+        info = step_dev()
+    torch.cuda.synchronize(dev)
+    dd.reset_stage_times()
+    l0 = dd.launches
+    _barrier(pg, dev)
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            info = step_dev()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+    _barrier(pg, dev)
+    ms = e0.elapsed_time(e1)
+    launches = (dd.launches - l0) // max(args.steps, 1)
+    stages = dd.stage_times()
+    ms_max = _max_over_ranks(ms, pg, dev)
+    ms_step = ms_max / args.steps
+    value = world * args.steps / (ms_max * 1e-3)
+
+    # end to end: host arrays in pinned memory, copies inside the timed region
+    de = DDCosmo(stream=stream.cuda_stream, **common)
+    h_in = {k: torch.tensor(mol[k], dtype=torch.float64).pin_memory() for k in keys}
+    h_fx = torch.zeros((N, 3), dtype=torch.float64).pin_memory()
+
+    def step_host():
+        return de.energy_forces_ptr(*(h_in[k].data_ptr() for k in keys), N, 0, 0,
+                                    h_fx.data_ptr())
+
+    for _ in range(max(1, args.warmup // 2)):
+        step_host()
+    torch.cuda.synchronize(dev)
+    _barrier(pg, dev)
+    t0 = time.perf_counter()
+    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    for _ in range(args.steps):
+        info_h = step_host()
+    e3.record(stream)
+    torch.cuda.synchronize(dev)
+    wall = time.perf_counter() - t0
+    ms_e2e = max(e2.elapsed_time(e3), wall * 1e3)
+    ms_e2e = _max_over_ranks(ms_e2e, pg, dev)
+    e2e_value = world * args.steps / (ms_e2e * 1e-3)
+    h2d = 5 * N * 8
+    d2h = 3 * N * 8 + 8
+
+    # dominant kernel and its roofline
+    per = {k: v for k, v in stages.items() if v[1] > 0 and k != "init"}
+    dom = max(per, key=lambda k: per[k][0])
+    dom_ms, dom_calls = per[dom]
+    work = _stage_work(dom, info, c)
+    fp64 = fp64_peak_gflops(local) if rank == 0 else None
+    hbm, hbm_src = _peaks()
+    avg_ms = dom_ms / dom_calls
+    roof = {"kernel": dom, "bound": "fp64", "unit": "TFLOP/s",
+            "achieved": (work / (avg_ms * 1e-3) / 1e12) if work else None,
+            "peak": fp64 / 1e3 if fp64 else None,
+            "peak_source": "measured FP64 FMA probe (ddc_fp64_peak), this run",
+            "launch_ms": avg_ms, "launches_per_step": dom_calls / args.steps,
+            "traffic": _traffic_from_profiles(dom)}
+    if roof["achieved"] and roof["peak"]:
+        roof["frac"] = roof["achieved"] / roof["peak"]
+    stage_ms = {k: round(v[0] / args.steps, 3) for k, v in stages.items() if v[1] > 0}
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded globule, PCG64)",
+            "config": _config_json(c, world),
+            "iterations": {"direct": info["direct"]["iterations"],
+                           "adjoint": info["adjoint"]["iterations"]},
+            "esolv_hartree": info["esolv"],
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e / args.steps},
+            "gpu_launches": launches, "stage_ms_per_step": stage_ms,
+            "roofline": roof, "clocks": clk.summary(),
+            "peaks": {"fp64_gflops_measured": fp64, "hbm_gbs": hbm, "hbm_source": hbm_src}}
+    if rank == 0 and world == 1 and not args.no_cpu:
+        line["cpu_baseline"] = cpu_baseline(info, budget_s=args.cpu_budget)
+    dd.close()
+    de.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the oracle on a bounded sample of the workload
+# ---------------------------------------------------------------------------
+ORACLE_ITERS = None  # filled from a measured run when available
+
+
+def cpu_sample(c, mol, iters, frac=64):
+    """Time the oracle (OpenMP, all host threads) on a bounded sample of one
+    energy+force solve and scale it to one solve.  Sample: the full ddinit;
+    one lx and one lstarx application, scaled by the solve's iteration
+    counts; mkrhs on every frac-th cavity point; forces_dd on 1/frac of the
+    spheres; both efld calls on 1/frac of their targets."""
+    from oracle import oracle as O
+    t = {}
+    nthreads = O.num_threads()
+    d = O.RefDD(c["lmax"], c["ngrid"], c["iconv"], 1, c["eps"], c["eta"])
+    t0 = time.perf_counter()
+    d.init(mol["x"], mol["y"], mol["z"], mol["r"])
+    t["init"] = time.perf_counter() - t0
+    ccav = d.get("ccav")
+    NC, N, NY = d.ncav, d.nsph, d.nylm
+    sub = ccav[::frac]
+    t0 = time.perf_counter()
+    phi_s, psi = O.mkrhs(mol["q"], mol["x"], mol["y"], mol["z"], sub, NY)
+    t["mkrhs"] = (time.perf_counter() - t0) * NC / max(len(sub), 1)
+    rng = np.random.default_rng(0)
+    x = rng.standard_normal((N, NY)) * 1e-3
+    t0 = time.perf_counter()
+    d.lx(x)
+    t["lx"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    d.lstarx(x)
+    t["lstarx"] = time.perf_counter() - t0
+    phi = rng.standard_normal(NC) * 1e-2
+    n1 = max(1, N // frac)
+    t0 = time.perf_counter()
+    d.forces_dd_range(phi, x, x, 0, n1)
+    t["forces"] = (time.perf_counter() - t0) * N / n1
+    csph = d.get("csph")
+    t0 = time.perf_counter()
+    O.efld(mol["q"], csph, sub)
+    t["efld1"] = (time.perf_counter() - t0) * NC / max(len(sub), 1)
+    zeta = rng.standard_normal(NC) * 1e-4
+    t0 = time.perf_counter()
+    O.efld(zeta, ccav, csph[:n1])
+    t["efld2"] = (time.perf_counter() - t0) * N / n1
+    total = (t["init"] + t["mkrhs"] + iters[0] * t["lx"] + iters[1] * t["lstarx"] + t["forces"]
+             + t["efld1"] + t["efld2"])
+    return total, t, nthreads
+
+
+def cpu_baseline(info, budget_s=None):
+    c, mol = _workload_config()
+    iters = (info["direct"]["iterations"], info["adjoint"]["iterations"])
+    t0 = time.perf_counter()
+    total, parts, nth = cpu_sample(c, mol, iters)
+    spent = time.perf_counter() - t0
+    return {"value": 1.0 / total, "unit": UNIT, "cores": nth, "kind": "port",
+            "sample": (f"oracle (C restatement of the reference, OpenMP {nth} threads): full "
+                       f"ddinit + one lx + one lstarx scaled by {iters[0]}/{iters[1]} "
+                       f"iterations + 1/64 of mkrhs, forces_dd and both efld, scaled to one "
+                       f"solve; {spent:.1f} s of CPU wall time"),
+            "seconds_per_solve": total, "parts_s": {k: round(v, 4) for k, v in parts.items()}}
+
+
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    c, mol = _workload_config()
+    iters = _reference_iters()
+    vals = []
+    spent = []
+    for k in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        total, parts, nth = cpu_sample(c, mol, iters)
+        if k >= args.warmup:
+            vals.append(total)
+            spent.append(time.perf_counter() - t0)
+    sec = statistics.mean(vals)
+    value = 1.0 / sec
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded globule, PCG64)", "impl": "reference",
+            "config": _config_json(c, 1),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": nth, "kind": "port",
+                             "sample": (f"per step: full ddinit + one lx + one lstarx scaled by "
+                                        f"{iters[0]}/{iters[1]} iterations + 1/64 of mkrhs, "
+                                        f"forces_dd and both efld, scaled to one solve; "
+                                        f"{statistics.mean(spent):.1f} s CPU wall per step")},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def _reference_iters():
+    """Jacobi/DIIS iteration counts of the reference algorithm on this workload
+    (direct, adjoint), from the committed measurement, else a typical count."""
+    path = os.path.join(ROOT, "profiles", "workload_iterations.txt")
+    try:
+        for ln in open(path):
+            f = ln.split()
+            if len(f) >= 3 and f[0] == "fp64_reference_guess":
+                return int(f[1]), int(f[2])
+    except OSError:
+        pass
+    return 45, 45
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline sample")
+    ap.add_argument("--cpu-budget", type=float, default=None)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -342,6 +342,21 @@ class DDCosmo:
         self._check(self.L.ddc_rhs(self.h, _p(_f64(phi)), _p(g)))
         return g
 
+    def energy_forces_ptr(self, q, x, y, z, r, n, sigma, s, fx):
+        """ddc_energy_forces on raw pointers (ints): device pointers when the
+        context was created with device_pointers=1, else host pointers (e.g.
+        pinned buffers).  0 for an output means "not requested".  Returns the
+        run info dict with ``esolv`` added."""
+        es = ctypes.c_double()
+        info = RunInfo()
+        self._check(self.L.ddc_energy_forces(self.h, n, _p(q), _p(x), _p(y), _p(z), _p(r),
+                                             ctypes.byref(es), _p(sigma or None), _p(s or None),
+                                             _p(fx or None), ctypes.byref(info)))
+        d = info.as_dict()
+        d["esolv"] = es.value
+        self.nsph, self.ncav, self.nylm, self.ngrid = d["nsph"], d["ncav"], d["nylm"], d["ngrid"]
+        return d
+
     def energy_forces(self, charge, x, y, z, rvdw):
         """The main.f90 flow (main.f90:164-265) in one library call.
         Returns dict(esolv, sigma, s, fx, info)."""

@@ -1077,9 +1077,16 @@ static void fdoga(const ref_ctx *c, int isph, const double *xi, const double *ph
   }
 }
 
-/* forces_dd (forces_dd.f90:91-164); fx(3,n) is overwritten. */
+/* forces_dd (forces_dd.f90:91-164) restricted to spheres [i0, i1): fx(3,n)
+ * rows i0..i1-1 are overwritten (used to time a bounded sample). */
+int ref_forces_dd_range(const ref_ctx *c, const double *phi, const double *sigma, const double *s,
+                        double *fx, int i0, int i1);
 int ref_forces_dd(const ref_ctx *c, const double *phi, const double *sigma, const double *s,
                   double *fx) {
+  return ref_forces_dd_range(c, phi, sigma, s, fx, 0, c->nsph);
+}
+int ref_forces_dd_range(const ref_ctx *c, const double *phi, const double *sigma, const double *s,
+                        double *fx, int i0, int i1) {
   int nsph = c->nsph, ngrid = c->ngrid, nylm = c->nylm;
   if (!c->zi) return -1;
   double *xi = malloc(sizeof(double) * (size_t)ngrid * nsph);
@@ -1106,7 +1113,7 @@ int ref_forces_dd(const ref_ctx *c, const double *phi, const double *sigma, cons
     /* each sphere writes only its own fx(:,isph): the parallel loop gives the
      * same result as the reference's serial loop (forces_dd.f90:132-136). */
 #pragma omp for schedule(dynamic)
-    for (int isph = 0; isph < nsph; isph++) {
+    for (int isph = i0; isph < i1; isph++) {
       double *f = fx + 3 * isph;
       f[0] = f[1] = f[2] = 0.0;
       fdoka(c, isph, sigma, xi + (size_t)isph * ngrid, &ws, f);
@@ -1116,7 +1123,7 @@ int ref_forces_dd(const ref_ctx *c, const double *phi, const double *sigma, cons
     free(ws.basloc); free(ws.dbsloc); free(ws.vplm); free(ws.vcos); free(ws.vsin);
   }
   double fep = 0.5 * (c->eps - 1.0) / c->eps;
-  for (int k = 0; k < 3 * nsph; k++) fx[k] = fep * fx[k];
+  for (int k = 3 * i0; k < 3 * i1; k++) fx[k] = fep * fx[k];
   free(xi);
   free(phiexp);
   return 0;
@@ -1228,3 +1235,11 @@ int ref_energy_forces(ref_ctx *c, int n, const double *q, const double *x, const
 }
 
 int ref_last_iters(const ref_ctx *c) { return c->last_iters; }
+
+int ref_num_threads(void) {
+#ifdef _OPENMP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
+}

@@ -64,6 +64,9 @@ def lib():
         L.ref_cosmo.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, _dp,
                                 _dp, _ip, _dp]
         L.ref_forces_dd.argtypes = [ctypes.c_void_p, _dp, _dp, _dp, _dp]
+        L.ref_forces_dd_range.argtypes = [ctypes.c_void_p, _dp, _dp, _dp, _dp, ctypes.c_int,
+                                          ctypes.c_int]
+        L.ref_num_threads.restype = ctypes.c_int
         L.ref_mkxi.argtypes = [ctypes.c_void_p, _dp, _dp, ctypes.c_int]
         L.ref_mkrhs.argtypes = [ctypes.c_int, _dp, _dp, _dp, _dp, ctypes.c_int, _dp, _dp,
                                 ctypes.c_int, _dp]
@@ -172,6 +175,11 @@ class RefDD:
         self.L.ref_forces_dd(self.h, _p(_c(phi)), _p(_c(sigma)), _p(_c(s)), _p(fx))
         return fx
 
+    def forces_dd_range(self, phi, sigma, s, i0, i1):
+        fx = np.zeros((self.nsph, 3))
+        self.L.ref_forces_dd_range(self.h, _p(_c(phi)), _p(_c(sigma)), _p(_c(s)), _p(fx), i0, i1)
+        return fx
+
     def mkzeta(self, s):      # ddcosmo.f90:1787
         out = np.zeros(max(self.ncav, 1))
         self.L.ref_mkxi(self.h, _p(_c(s)), _p(out), 1)
@@ -221,6 +229,10 @@ def energy_forces(mol, lmax, ngrid, iconv, eps, eta, igrad=1, nthreads=0):
     lib().ref_sizes(d.h, sz)
     return dict(rc=rc, esolv=es.value, sigma=sigma, s=s, fx=fx, iters=(it[0], it[1]),
                 ncav=sz[1], nylm=sz[2], ngrid=sz[3])
+
+
+def num_threads():
+    return lib().ref_num_threads()
 
 
 def snap_ngrid(n):

@@ -40,14 +40,17 @@ def test_golden_energy_forces(oracle, name):
     assert abs(out["esolv"] - ref["esolv"]) <= ESOLV_RTOL * abs(ref["esolv"])
     assert abs(out["esolv"] - ref["esolv"]) <= 1e-12 * abs(ref["esolv"]) + 1e-15
     assert abs(out["esolv"] * TOKCAL - g["energy_kcal"]) <= 1e-6
+    # the iterates are defined to the solver tolerance 10^-iconv; last-bit
+    # differences of the operator pass through DIIS, so the tight checks are
+    # relative to that tolerance
+    tol = 10.0 ** -p["iconv"]
     np.testing.assert_allclose(out["fx"], ref["fx"], rtol=0, atol=FORCE_ATOL)
-    np.testing.assert_allclose(out["fx"], ref["fx"], rtol=0, atol=1e-11)
+    np.testing.assert_allclose(out["fx"], ref["fx"], rtol=0, atol=max(1e-2 * tol, 1e-12))
     np.testing.assert_allclose(out["fx"], np.array(g["forces"]), rtol=0, atol=6e-9)
     assert (out["info"]["direct"]["iterations"], out["info"]["adjoint"]["iterations"]) == \
         ref["iters"]
-    scale = np.abs(ref["sigma"]).max()
-    np.testing.assert_allclose(out["sigma"], ref["sigma"], rtol=0, atol=1e-11 * scale)
-    np.testing.assert_allclose(out["s"], ref["s"], rtol=0, atol=1e-11 * np.abs(ref["s"]).max())
+    np.testing.assert_allclose(out["sigma"], ref["sigma"], rtol=0, atol=1e-2 * tol)
+    np.testing.assert_allclose(out["s"], ref["s"], rtol=0, atol=1e-2 * tol)
 
 
 @pytest.mark.parametrize("name", ["formaldehyde", "caffeine", "crambin"])
@@ -177,6 +180,16 @@ def test_config2_full_size_properties():
         F = out["fx"]
         assert np.abs(F.sum(axis=0)).max() <= 1e-9 * np.abs(F).sum()
         assert np.isfinite(out["esolv"]) and out["esolv"] < 0
+    # against the oracle's full-size run (tests/golden/make_config2.py)
+    import os
+    from conftest import GOLDEN
+    ref = np.load(os.path.join(GOLDEN, "config2_oracle.npz"))
+    assert out["info"]["ncav"] == int(ref["ncav"])
+    assert abs(out["esolv"] - float(ref["esolv"])) <= ESOLV_RTOL * abs(float(ref["esolv"]))
+    np.testing.assert_allclose(out["fx"], ref["fx"], rtol=0, atol=FORCE_ATOL)
+    it = ref["iters"]
+    assert abs(out["info"]["direct"]["iterations"] - int(it[0])) <= 1
+    assert abs(out["info"]["adjoint"]["iterations"] - int(it[1])) <= 1
 
 
 def test_edge_single_and_separated_spheres(oracle):
