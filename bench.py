@@ -40,7 +40,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
-WORKLOAD = 2  # 20,000 spheres, lmax 10, ngrid 590
+WORKLOAD = 2  # 20,000 spheres, lmax 10, ngrid 590 (override: --workload)
 METRIC = "energy+force solves/s"
 UNIT = "solves/s"
 
@@ -200,6 +200,10 @@ def _traffic_from_profiles(kernel):
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
+def dd_stages(stages):
+    return {k: v for k, v in stages.items() if v[1] > 0}
+
+
 def run_ours(args):
     import torch
 
@@ -248,6 +252,18 @@ def run_ours(args):
     value = world * args.steps / (ms_max * 1e-3)
 
     # end to end: host arrays in pinned memory, copies inside the timed region
+    if args.no_e2e:
+        dd.close()
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+                              "ms_per_step": ms_step, "profile_run": True,
+                              "stage_ms_per_step": {k: round(v[0] / args.steps, 3)
+                                                    for k, v in dd_stages(stages).items()},
+                              "info": {k: info[k] for k in ("nsph", "ncav", "ntriples",
+                                                            "npairs")}}), flush=True)
+        if pg is not None:
+            pg.destroy_process_group()
+        return
     de = DDCosmo(stream=stream.cuda_stream, **common)
     h_in = {k: torch.tensor(mol[k], dtype=torch.float64).pin_memory() for k in keys}
     h_fx = torch.zeros((N, 3), dtype=torch.float64).pin_memory()
@@ -299,6 +315,8 @@ def run_ours(args):
             "config": _config_json(c, world),
             "iterations": {"direct": info["direct"]["iterations"],
                            "adjoint": info["adjoint"]["iterations"]},
+            "sizes": {k: info[k] for k in ("nsph", "ncav", "nylm", "ngrid", "ntriples",
+                                           "npairs")},
             "esolv_hartree": info["esolv"],
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e / args.steps},
@@ -434,7 +452,12 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline sample")
     ap.add_argument("--cpu-budget", type=float, default=None)
+    ap.add_argument("--workload", type=int, default=WORKLOAD, choices=[0, 1, 2, 9],
+                    help="molecule configuration (2: the benchmark workload)")
+    ap.add_argument("--no-e2e", action="store_true",
+                    help="time only the device-resident step (profiling runs)")
     args = ap.parse_args()
+    globals()["WORKLOAD"] = args.workload
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

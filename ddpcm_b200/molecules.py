@@ -96,6 +96,9 @@ CONFIGS = {
     0: dict(n=12, globule=False, lmax=6, ngrid=110, eta=0.1, eps=78.3553, iconv=10, seed=1000),
     1: dict(n=600, globule=True, lmax=8, ngrid=302, eta=0.1, eps=78.3553, iconv=10, seed=1001),
     2: dict(n=20000, globule=True, lmax=10, ngrid=590, eta=0.1, eps=78.3553, iconv=10, seed=1002),
+    # profiling case: same settings as 2 at 5,000 spheres (working set above
+    # L2, small enough for a full counter capture)
+    9: dict(n=5000, globule=True, lmax=10, ngrid=590, eta=0.1, eps=78.3553, iconv=10, seed=1009),
 }
 
 
