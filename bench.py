@@ -204,6 +204,26 @@ def dd_stages(stages):
     return {k: v for k, v in stages.items() if v[1] > 0}
 
 
+VARIANTS = {
+    # name: (precision, guess); the first is the headline
+    "mixed_ref_guess": (1, 0),
+    "fp64_ref_guess": (0, 0),
+    "fp64_zero_guess": (0, 1),
+    "mixed_zero_guess": (1, 1),
+}
+
+
+def _oracle_fixture():
+    """FP64 oracle result of the benchmark workload (tests/golden/make_config2.py)."""
+    if WORKLOAD != 2:
+        return None
+    path = os.path.join(ROOT, "tests", "golden", "config2_oracle.npz")
+    try:
+        return np.load(path)
+    except OSError:
+        return None
+
+
 def run_ours(args):
     import torch
 
@@ -223,35 +243,79 @@ def run_ours(args):
     d_fx = torch.zeros((N, 3), dtype=torch.float64, device=dev)
     common = dict(lmax=c["lmax"], ngrid=c["ngrid"], iconv=c["iconv"], eps=c["eps"], eta=c["eta"],
                   device=local)
-    dd = DDCosmo(device_pointers=1, stream=stream.cuda_stream, timing=1, **common)
+    ref = _oracle_fixture()
 
-    def step_dev():
-        return dd.energy_forces_ptr(*(d_in[k].data_ptr() for k in keys), N,
-                                    d_sig.data_ptr(), d_s.data_ptr(), d_fx.data_ptr())
+    def make(prec, guess, **kw):
+        return DDCosmo(precision=prec, guess=guess, stream=stream.cuda_stream, **common, **kw)
 
-    for _ in range(args.warmup):
-        info = step_dev()
-    torch.cuda.synchronize(dev)
-    dd.reset_stage_times()
-    l0 = dd.launches
-    _barrier(pg, dev)
-    torch.cuda.synchronize(dev)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clk:
+    def timed(dd, step, warmup, steps, clocks=False):
+        for _ in range(warmup):
+            info = step()
+        torch.cuda.synchronize(dev)
+        dd.reset_stage_times()
+        l0 = dd.launches
+        _barrier(pg, dev)
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        clk = ClockSampler(local) if clocks else None
+        if clk:
+            clk.__enter__()
         e0.record(stream)
-        for _ in range(args.steps):
-            info = step_dev()
+        for _ in range(steps):
+            info = step()
         e1.record(stream)
         torch.cuda.synchronize(dev)
-    _barrier(pg, dev)
-    ms = e0.elapsed_time(e1)
-    launches = (dd.launches - l0) // max(args.steps, 1)
-    stages = dd.stage_times()
-    ms_max = _max_over_ranks(ms, pg, dev)
-    ms_step = ms_max / args.steps
-    value = world * args.steps / (ms_max * 1e-3)
+        if clk:
+            clk.__exit__(None, None, None)
+        _barrier(pg, dev)
+        ms = _max_over_ranks(e0.elapsed_time(e1), pg, dev)
+        return ms, info, (dd.launches - l0) // max(steps, 1), clk
 
-    # end to end: host arrays in pinned memory, copies inside the timed region
+    def accuracy(info):
+        if ref is None:
+            return None
+        fx = d_fx.cpu().numpy()
+        return {"esolv_rel": abs(info["esolv"] - float(ref["esolv"])) / abs(float(ref["esolv"])),
+                "forces_max_abs": float(np.abs(fx - ref["fx"]).max()),
+                "against": "FP64 CPU oracle (tests/golden/config2_oracle.npz)"}
+
+    def dev_step(dd):
+        return lambda: dd.energy_forces_ptr(*(d_in[k].data_ptr() for k in keys), N,
+                                            d_sig.data_ptr(), d_s.data_ptr(), d_fx.data_ptr())
+
+    # headline: mixed precision (FP32 operator in FP64 refinement), reference guess
+    names = list(VARIANTS)
+    prec, guess = VARIANTS[names[0]]
+    dd = make(prec, guess, device_pointers=1, timing=1)
+    ms, info, launches, clk = timed(dd, dev_step(dd), args.warmup, args.steps, clocks=True)
+    stages = dd.stage_times()
+    acc_head = accuracy(info)
+    ms_step = ms / args.steps
+    value = world * args.steps / (ms * 1e-3)
+
+    # comparison variants: one warm-up, one timed step each
+    variants = {names[0]: {"ms_per_solve": ms_step,
+                           "iterations": [info["direct"]["iterations"],
+                                          info["adjoint"]["iterations"]],
+                           "refinements": [info["direct"]["refinements"],
+                                           info["adjoint"]["refinements"]],
+                           "error": acc_head}}
+    if not args.no_variants:
+        for name in names[1:]:
+            pv, gv = VARIANTS[name]
+            dv = make(pv, gv, device_pointers=1)
+            msv, infov, _, _ = timed(dv, dev_step(dv), 1, 1)
+            variants[name] = {"ms_per_solve": msv,
+                              "iterations": [infov["direct"]["iterations"],
+                                             infov["adjoint"]["iterations"]],
+                              "refinements": [infov["direct"]["refinements"],
+                                              infov["adjoint"]["refinements"]],
+                              "error": accuracy(infov)}
+            dv.close()
+        base = variants["fp64_zero_guess"]["ms_per_solve"]
+        for v in variants.values():
+            v["speedup_vs_fp64_zero_guess"] = base / v["ms_per_solve"]
+
     if args.no_e2e:
         dd.close()
         if rank == 0:
@@ -259,12 +323,15 @@ def run_ours(args):
                               "ms_per_step": ms_step, "profile_run": True,
                               "stage_ms_per_step": {k: round(v[0] / args.steps, 3)
                                                     for k, v in dd_stages(stages).items()},
+                              "variants": variants,
                               "info": {k: info[k] for k in ("nsph", "ncav", "ntriples",
                                                             "npairs")}}), flush=True)
         if pg is not None:
             pg.destroy_process_group()
         return
-    de = DDCosmo(stream=stream.cuda_stream, **common)
+
+    # end to end: host arrays in pinned memory, copies inside the timed region
+    de = make(prec, guess)
     h_in = {k: torch.tensor(mol[k], dtype=torch.float64).pin_memory() for k in keys}
     h_fx = torch.zeros((N, 3), dtype=torch.float64).pin_memory()
 
@@ -280,7 +347,7 @@ def run_ours(args):
     e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e2.record(stream)
     for _ in range(args.steps):
-        info_h = step_host()
+        step_host()
     e3.record(stream)
     torch.cuda.synchronize(dev)
     wall = time.perf_counter() - t0
@@ -304,6 +371,9 @@ def run_ours(args):
             "peak_source": "measured FP64 FMA probe (ddc_fp64_peak), this run",
             "launch_ms": avg_ms, "launches_per_step": dom_calls / args.steps,
             "traffic": _traffic_from_profiles(dom)}
+    if prec == 1 and dom in ("lx_pot", "lstarx", "proj_gemm", "xi_gemm"):
+        roof["note"] = ("kernel runs in FP32 in the mixed path; fraction given against the "
+                        "measured FP64 peak, the FP32 peak is 2x that")
     if roof["achieved"] and roof["peak"]:
         roof["frac"] = roof["achieved"] / roof["peak"]
     stage_ms = {k: round(v[0] / args.steps, 3) for k, v in stages.items() if v[1] > 0}
@@ -312,19 +382,22 @@ def run_ours(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded globule, PCG64)",
-            "config": _config_json(c, world),
+            "config": _config_json(c, world, {"precision": "mixed (FP32 operator, FP64 "
+                                                            "refinement/DIIS/energy/forces)"}),
             "iterations": {"direct": info["direct"]["iterations"],
                            "adjoint": info["adjoint"]["iterations"]},
             "sizes": {k: info[k] for k in ("nsph", "ncav", "nylm", "ngrid", "ntriples",
                                            "npairs")},
-            "esolv_hartree": info["esolv"],
+            "esolv_hartree": info["esolv"], "error_vs_fp64_oracle": acc_head,
+            "variants": variants,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e / args.steps},
             "gpu_launches": launches, "stage_ms_per_step": stage_ms,
             "roofline": roof, "clocks": clk.summary(),
             "peaks": {"fp64_gflops_measured": fp64, "hbm_gbs": hbm, "hbm_source": hbm_src}}
     if rank == 0 and world == 1 and not args.no_cpu:
-        line["cpu_baseline"] = cpu_baseline(info, budget_s=args.cpu_budget)
+        line["cpu_baseline"] = cpu_baseline(variants.get("fp64_ref_guess", variants[names[0]]),
+                                            budget_s=args.cpu_budget)
     dd.close()
     de.close()
     if rank == 0:
@@ -384,9 +457,9 @@ def cpu_sample(c, mol, iters, frac=64):
     return total, t, nthreads
 
 
-def cpu_baseline(info, budget_s=None):
+def cpu_baseline(variant, budget_s=None):
     c, mol = _workload_config()
-    iters = (info["direct"]["iterations"], info["adjoint"]["iterations"])
+    iters = tuple(variant["iterations"])
     t0 = time.perf_counter()
     total, parts, nth = cpu_sample(c, mol, iters)
     spent = time.perf_counter() - t0
@@ -454,6 +527,8 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=None)
     ap.add_argument("--workload", type=int, default=WORKLOAD, choices=[0, 1, 2, 9],
                     help="molecule configuration (2: the benchmark workload)")
+    ap.add_argument("--no-variants", action="store_true",
+                    help="skip the comparison variants (plain FP64, zero guess)")
     ap.add_argument("--no-e2e", action="store_true",
                     help="time only the device-resident step (profiling runs)")
     args = ap.parse_args()

@@ -151,6 +151,8 @@ struct ddc_ctx {
   DBuf pot, xig, gbuf, rhs, x, y, xn, partials, red, hist_x, hist_e;
   DBuf phi, psi, sigma, s, q, fx, zeta, ef1, ef2, ef_scratch, uchi;
   DBuf in1, in2, in3, in4, out1;  // staging for host-pointer calls
+  // mixed precision: FP32 grid/basis copies, FP32 grid fields, refinement vectors
+  DBuf gridf, basis_f, bw_f, pot_f, xi_f, rres, dres, eres;
 
   Launch L() { return Launch{st, &launches}; }
   DevGeo geo() const {
@@ -163,6 +165,7 @@ struct ddc_ctx {
     g.ntri = ntri;
     g.sph = sph.as<double4>();
     g.grid = grid.as<double4>();
+    g.gridf = gridf.as<float4>();
     g.basis = basis.as<double>();
     g.bw = bw.as<double>();
     g.fi = fi.as<double>();
@@ -310,6 +313,11 @@ void build_tables(ddc_ctx* c) {
       }
     }
   }
+  for (int e = 0; e < DDC_NLM_CAP; e++) {
+    tb.Kf[e] = (float)tb.K[e];
+    tb.Af[e] = (float)tb.A[e];
+    tb.Bf[e] = (float)tb.B[e];
+  }
   tb.eta = c->prm.eta;
   tb.lmax = lmax;
   tb.nylm = (lmax + 1) * (lmax + 1);
@@ -446,6 +454,21 @@ int do_init(ddc_ctx* ctx, int n, const std::vector<double4>* hsph, const double4
   CK(ctx->hist_e.ensure(sizeof(double) * std::max(nv, (size_t)1) * nd));
   CK(ctx->partials.ensure(sizeof(double) * reduce_blocks() * (kMaxHist + 1)));
   CK(ctx->red.ensure(sizeof(double) * (kMaxHist + 1)));
+  if (ctx->prm.precision == DDC_PREC_MIXED) {
+    std::vector<float> gf(4 * (size_t)G);
+    for (size_t k = 0; k < gf.size(); k++) gf[k] = (float)ctx->h_grid[k];
+    CK(ctx->gridf.ensure(sizeof(float) * 4 * G));
+    CK(cudaMemcpyAsync(ctx->gridf.p, gf.data(), sizeof(float) * 4 * G, cudaMemcpyHostToDevice,
+                       ctx->st));
+    CK(ctx->basis_f.ensure(sizeof(float) * G * NY));
+    CK(ctx->bw_f.ensure(sizeof(float) * G * NY));
+    CK(launch_to_float(L, (long long)G * NY, ctx->basis.as<double>(), ctx->basis_f.as<float>()));
+    CK(launch_to_float(L, (long long)G * NY, ctx->bw.as<double>(), ctx->bw_f.as<float>()));
+    CK(ctx->pot_f.ensure(sizeof(float) * std::max(NP, 1LL)));
+    CK(ctx->xi_f.ensure(sizeof(float) * std::max(NP, 1LL)));
+    for (DBuf* b : {&ctx->rres, &ctx->dres, &ctx->eres})
+      CK(b->ensure(sizeof(double) * std::max(nv, (size_t)1)));
+  }
   CKI(sync(ctx));
   ctx->ready = true;
   return DDC_OK;
@@ -477,6 +500,28 @@ int op_lstarx(ddc_ctx* ctx, const double* x, double* y) {
   CKI(op_xi(ctx, x, ctx->xig.as<double>()));
   StageScope sc(ctx, ST_LSTARX);
   CK(launch_lstarx_acc(ctx->L(), ctx->tb, ctx->geo(), ctx->xig.as<double>(), y));
+  return DDC_OK;
+}
+
+// FP32 operators of the mixed-precision path (vectors stay FP64)
+int op_lx_f32(ddc_ctx* ctx, const double* x, double* y) {
+  {
+    StageScope sc(ctx, ST_LX_POT);
+    CK(launch_lx_pot_f32(ctx->L(), ctx->tb, ctx->geo(), x, ctx->pot_f.as<float>()));
+  }
+  StageScope sc(ctx, ST_PROJ);
+  CK(launch_sgemm(ctx->L(), false, ctx->nylm, ctx->nsph, ctx->ngrid, -1.f, ctx->bw_f.as<float>(),
+                  ctx->nylm, ctx->pot_f.as<float>(), ctx->ngrid, y, ctx->nylm));
+  return DDC_OK;
+}
+int op_lstarx_f32(ddc_ctx* ctx, const double* x, double* y) {
+  {
+    StageScope sc(ctx, ST_XI);
+    CK(launch_sgemm_xi(ctx->L(), ctx->ngrid, ctx->nsph, ctx->nylm, ctx->basis_f.as<float>(),
+                       ctx->nylm, x, ctx->nylm, ctx->xi_f.as<float>(), ctx->ngrid));
+  }
+  StageScope sc(ctx, ST_LSTARX);
+  CK(launch_lstarx_acc_f32(ctx->L(), ctx->tb, ctx->geo(), ctx->xi_f.as<float>(), y));
   return DDC_OK;
 }
 
@@ -523,13 +568,16 @@ bool gjinv(int n, std::vector<double>& a, std::vector<double>& b) {
   return true;
 }
 
+typedef int (*OpFn)(ddc_ctx*, const double*, double*);
+
 // jacobi_diis (jacobi_diis.f90:1-176), norm mode 4 (hnorm).  x holds the
-// initial guess on entry and the solution on exit (device).
-int solve(ddc_ctx* ctx, bool adjoint, const double* rhs, double* x, ddc_solve_info* info) {
-  const double t0 = now_s();
+// initial guess on entry and the solution on exit (device).  The log of
+// increment norms continues at inf->norms[*logpos].
+int jacobi_diis(ddc_ctx* ctx, OpFn op, const double* rhs, double* x, double tol, int max_iter,
+                ddc_solve_info* inf, int* logpos, int* iters_done, int* restarts_out,
+                double* last_norm) {
   const long long n = (long long)ctx->nsph * ctx->nylm;
-  const double tol = std::pow(10.0, -(double)ctx->prm.iconv);
-  const int ndiis = ctx->prm.ndiis, max_iter = ctx->prm.max_iter;
+  const int ndiis = ctx->prm.ndiis;
   const bool dodiis = ndiis != 0;
   const int nblk = reduce_blocks();
   double* y = ctx->y.as<double>();
@@ -544,13 +592,9 @@ int solve(ddc_ctx* ctx, bool adjoint, const double* rhs, double* x, ddc_solve_in
   int nmat = 1, it = 0, restarts = 0;
   bool ok = false;
   double rms = 0.0;
-  ddc_solve_info loc{};
-  ddc_solve_info* inf = info ? info : &loc;
-  memset(inf, 0, sizeof(*inf));
   std::vector<double> row(kMaxHist + 2);
   for (it = 1; it <= max_iter; it++) {
-    if (adjoint) CKI(op_lstarx(ctx, x, y));
-    else CKI(op_lx(ctx, x, y));
+    CKI(op(ctx, x, y));
     HistPtrs hist{};
     HistPtrs comb{};
     const double* xj = xjac;
@@ -630,22 +674,94 @@ int solve(ddc_ctx* ctx, bool adjoint, const double* rhs, double* x, ddc_solve_in
     double ss = 0.0;
     CKI(reduce_to_host(ctx, 1, &ss));
     rms = std::sqrt(ss / (double)std::max(ctx->nsph, 1));
-    if (it <= 256) inf->norms[it - 1] = rms;
-    if (ctx->prm.iprint > 0) printf("  iter=%4d residual norm: %14.4E\n", it, rms);
+    if (*logpos < 256) inf->norms[*logpos] = rms;
+    ++*logpos;
+    if (ctx->prm.iprint > 0) printf("  iter=%4d residual norm: %14.4E\n", *logpos, rms);
     if (!std::isfinite(rms)) {
-      inf->iterations = it;
+      *iters_done = it;
       return fail(ctx, DDC_ERR_NUMERIC, "non-finite increment norm");
     }
     ok = rms < tol;
     if (ok) break;
   }
-  inf->iterations = ok ? it : max_iter;
-  inf->converged = ok ? 1 : 0;
+  *iters_done = ok ? it : max_iter;
+  *restarts_out += restarts;
+  *last_norm = rms;
+  return ok ? DDC_OK : DDC_ERR_NOCONV;
+}
+
+// FP64 solve: the reference's Jacobi/DIIS on the FP64 operator.
+// Mixed solve: iterative refinement.  Each outer step forms in FP64 the
+// residual r = rhs - L x and the Jacobi increment d = D^-1 r at x; its
+// H-norm is the reference's convergence test (jacobi_diis.f90:143-150), so
+// the solve stops exactly when the FP64 Jacobi increment is below
+// 10^-iconv.  Otherwise the correction equation L e = r is solved with
+// Jacobi/DIIS on the FP32 operator (from e = d, to 1e-5 relative) and x += e.
+int solve(ddc_ctx* ctx, bool adjoint, const double* rhs, double* x, ddc_solve_info* info) {
+  const double t0 = now_s();
+  const double tol = std::pow(10.0, -(double)ctx->prm.iconv);
+  ddc_solve_info loc{};
+  ddc_solve_info* inf = info ? info : &loc;
+  memset(inf, 0, sizeof(*inf));
+  int logpos = 0, its = 0, restarts = 0;
+  double last = 0.0;
+  int rc;
+  if (ctx->prm.precision != DDC_PREC_MIXED) {
+    rc = jacobi_diis(ctx, adjoint ? op_lstarx : op_lx, rhs, x, tol, ctx->prm.max_iter, inf,
+                     &logpos, &its, &restarts, &last);
+    if (rc != DDC_OK && rc != DDC_ERR_NOCONV) return rc;
+    inf->iterations = its;
+  } else {
+    const long long n = (long long)ctx->nsph * ctx->nylm;
+    const int nblk = reduce_blocks();
+    double* r = ctx->rres.as<double>();
+    double* d = ctx->dres.as<double>();
+    double* e = ctx->eres.as<double>();
+    OpFn op64 = adjoint ? op_lstarx : op_lx;
+    OpFn op32 = adjoint ? op_lstarx_f32 : op_lx_f32;
+    const double rho = 1e-5;
+    int budget = ctx->prm.max_iter, outer = 0;
+    rc = DDC_ERR_NOCONV;
+    while (outer < 64) {
+      ++outer;
+      CKI(op64(ctx, x, ctx->y.as<double>()));
+      {
+        StageScope sc(ctx, ST_JACOBI);
+        CK(launch_residual(ctx->L(), ctx->tb, n, rhs, ctx->y.as<double>(), x, r, d,
+                           ctx->partials.as<double>(), nblk));
+      }
+      double ss = 0.0;
+      CKI(reduce_to_host(ctx, 1, &ss));
+      last = std::sqrt(ss / (double)std::max(ctx->nsph, 1));
+      if (ctx->prm.iprint > 0) printf("  refinement %d: FP64 increment norm %14.4E\n", outer, last);
+      if (!std::isfinite(last)) return fail(ctx, DDC_ERR_NUMERIC, "non-finite increment norm");
+      if (last < tol) {
+        rc = DDC_OK;
+        break;
+      }
+      if (budget <= 0) break;
+      // correction: (D + O32) e = r from e = D^-1 r
+      CK(cudaMemcpyAsync(e, d, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx->st));
+      int done = 0;
+      double inner_last = 0.0;
+      const double itol = std::max(rho * last, 0.3 * tol);
+      int irc = jacobi_diis(ctx, op32, r, e, itol, budget, inf, &logpos, &done, &restarts,
+                            &inner_last);
+      if (irc != DDC_OK && irc != DDC_ERR_NOCONV) return irc;
+      its += done;
+      budget -= done;
+      CK(launch_axpy(ctx->L(), n, 1.0, e, x));
+    }
+    inf->iterations = its;
+    inf->refinements = outer;
+  }
+  inf->converged = rc == DDC_OK ? 1 : 0;
   inf->diis_restarts = restarts;
-  inf->final_norm = rms;
+  inf->final_norm = last;
   inf->seconds = now_s() - t0;
-  if (!ok) return fail(ctx, DDC_ERR_NOCONV, adjoint ? "adjoint ddCOSMO did not converge"
-                                                    : "ddCOSMO did not converge");
+  if (rc == DDC_ERR_NOCONV)
+    return fail(ctx, DDC_ERR_NOCONV, adjoint ? "adjoint ddCOSMO did not converge"
+                                             : "ddCOSMO did not converge");
   return DDC_OK;
 }
 
@@ -1160,10 +1276,11 @@ int ddc_energy_forces(ddc_ctx* ctx, int n, const double* charge, const double* x
     int ch1 = efield_chunks(N, NC), ch2 = efield_chunks(NC, N);
     CK(ctx->ef_scratch.ensure(sizeof(double) * 3 *
                               std::max((size_t)ch1 * NC, (size_t)ch2 * N + 1)));
+    auto efield = launch_efield;
     {
       StageScope sc(ctx, ST_EFIELD);
-      CK(launch_efield(ctx->L(), N, dq, ctx->csph.as<double>(), NC, ctx->ccav.as<double>(),
-                       ctx->ef1.as<double>(), ctx->ef_scratch.as<double>(), ch1));
+      CK(efield(ctx->L(), N, dq, ctx->csph.as<double>(), NC, ctx->ccav.as<double>(),
+                ctx->ef1.as<double>(), ctx->ef_scratch.as<double>(), ch1));
     }
     {
       StageScope sc(ctx, ST_CONTRACT);
@@ -1173,9 +1290,9 @@ int ddc_energy_forces(ddc_ctx* ctx, int n, const double* charge, const double* x
     // field of zeta at the nuclei times the charges (main.f90:259-265)
     {
       StageScope sc(ctx, ST_EFIELD);
-      CK(launch_efield(ctx->L(), NC, ctx->zeta.as<double>(), ctx->ccav.as<double>(), N,
-                       ctx->csph.as<double>(), ctx->ef2.as<double>(),
-                       ctx->ef_scratch.as<double>(), ch2));
+      CK(efield(ctx->L(), NC, ctx->zeta.as<double>(), ctx->ccav.as<double>(), N,
+                ctx->csph.as<double>(), ctx->ef2.as<double>(), ctx->ef_scratch.as<double>(),
+                ch2));
     }
     {
       StageScope sc(ctx, ST_CONTRACT);

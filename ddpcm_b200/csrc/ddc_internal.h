@@ -38,6 +38,7 @@ struct YlmTables {
   double K[DDC_NLM_CAP];          // facs / facl
   double A[DDC_NLM_CAP];          // (2l-1)/(l-m): Legendre recurrence
   double B[DDC_NLM_CAP];          // (l+m-1)/(l-m)
+  float Kf[DDC_NLM_CAP], Af[DDC_NLM_CAP], Bf[DDC_NLM_CAP];  // FP32 copies (mixed path)
   double eta;
   int lmax, nylm, ngrid;
 };
@@ -48,6 +49,7 @@ struct DevGeo {
   long long ntri;
   const double4* sph;
   const double4* grid;
+  const float4* gridf;  // FP32 copy of grid (mixed path)
   const double* basis;
   const double* bw;
   const double* fi;
@@ -122,6 +124,22 @@ cudaError_t launch_lx_pot(Launch L, const YlmTables& tb, const DevGeo& g, const 
                           double* pot, bool chi_only);
 cudaError_t launch_lstarx_acc(Launch L, const YlmTables& tb, const DevGeo& g, const double* xi,
                               double* y);
+// FP32 operator variants (mixed precision): pot/xi in FP32, y in FP64
+cudaError_t launch_lx_pot_f32(Launch L, const YlmTables& tb, const DevGeo& g, const double* X,
+                              float* pot);
+cudaError_t launch_lstarx_acc_f32(Launch L, const YlmTables& tb, const DevGeo& g,
+                                  const float* xi, double* y);
+// C[M x N] = alpha * op(A) * B in FP32 arithmetic, A float, B float or double, C float/double
+cudaError_t launch_sgemm(Launch L, bool transA, int M, int N, int K, float alpha, const float* A,
+                         int lda, const float* B, int ldb, double* C, int ldc);
+cudaError_t launch_sgemm_xi(Launch L, int M, int N, int K, const float* A, int lda,
+                            const double* B, int ldb, float* C, int ldc);
+cudaError_t launch_to_float(Launch L, long long n, const double* x, float* y);
+// r = rhs - y - x/facl ; d = facl*r (Jacobi increment at x), partial H-norm of d
+cudaError_t launch_residual(Launch L, const YlmTables& tb, long long n, const double* rhs,
+                            const double* y, const double* x, double* r, double* d,
+                            double* partials, int nblk);
+cudaError_t launch_axpy(Launch L, long long n, double a, const double* x, double* y);
 // C[M x N] = alpha * op(A) * B (+ beta*C), column-major FP64
 cudaError_t launch_dgemm(Launch L, bool transA, int M, int N, int K, double alpha,
                          const double* A, int lda, const double* B, int ldb, double beta,
@@ -159,6 +177,7 @@ cudaError_t launch_psi(Launch L, int n, int nylm, const double* q, double* psi);
 cudaError_t launch_efield(Launch L, int nsrc, const double* q, const double* csrc, int ntrg,
                           const double* ctrg, double* ef, double* scratch, int nchunk);
 int efield_chunks(int nsrc, int ntrg);
+
 
 // forces
 cudaError_t launch_forces(Launch L, const YlmTables& tb, const DevGeo& g, const double* sigma,

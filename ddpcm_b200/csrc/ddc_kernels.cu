@@ -592,168 +592,220 @@ cudaError_t launch_lx_pot(Launch L, const YlmTables& tb, const DevGeo& g, const 
 // lstarx (adjrhs ddcosmo.f90:1301-1384, matvec.f90:161-235):
 //   y_i,lm = - sum_{j in N_i} sum_{n: t_n^ji<1} w_n xi_j(n) W_ji(n)
 //                4pi/(2l+1) t^l Y_lm(s_n^ji)
-// Block per sphere, threads over its gather list.  The (l,m) outputs are
-// split into passes over m-ranges so that each thread keeps the pass's
-// accumulators in registers; partial sums are reduced over the block in a
-// fixed tree order.
+// Block per sphere i, one warp per "role".  A role owns the Legendre
+// columns m and lmax-m (and the middle column when lmax is even), which
+// balances the recurrence work (lmax+2 steps per role) and caps the
+// register accumulators at 2*lmax+4.  Per chunk of triples (one per thread):
+//   phase A: every thread computes one triple's geometry, weight and the
+//            prefix Pt_m^m (coef folded in), cos(m phi), sin(m phi) for all m
+//            into shared memory;
+//   phase B: each role warp runs its columns over the chunk, lanes over
+//            triples, accumulating in registers.
+// At the end each role reduces its accumulators across its 32 lanes with a
+// fixed shuffle tree.  No atomics: the result is bit-reproducible.
 // ---------------------------------------------------------------------------
-__host__ __device__ constexpr int nvals_m(int L, int m) { return m == 0 ? L + 1 : 2 * (L + 1 - m); }
-__host__ __device__ constexpr int pass_end(int L, int m0, int cap) {
-  int s = 0, m = m0;
-  while (m <= L && s + nvals_m(L, m) <= cap) {
-    s += nvals_m(L, m);
-    ++m;
-  }
-  return m == m0 ? m0 + 1 : m;
-}
-__host__ __device__ constexpr int pass_nvals(int L, int m0, int m1) {
-  int s = 0;
-  for (int m = m0; m < m1; ++m) s += nvals_m(L, m);
-  return s;
-}
-// offset of (l, m, sign) inside a pass: per m the +m values then the -m values
-__host__ __device__ constexpr int pass_off(int L, int m0, int m, int l, int neg) {
-  int s = 0;
-  for (int mm = m0; mm < m; ++mm) s += nvals_m(L, mm);
-  return s + (neg ? (L + 1 - m) : 0) + (l - m);
-}
+template <class Rl> __device__ __forceinline__ Rl cA(const YlmTables& tb, int e);
+template <> __device__ __forceinline__ double cA<double>(const YlmTables& tb, int e) { return tb.A[e]; }
+template <> __device__ __forceinline__ float cA<float>(const YlmTables& tb, int e) { return tb.Af[e]; }
+template <class Rl> __device__ __forceinline__ Rl cB(const YlmTables& tb, int e);
+template <> __device__ __forceinline__ double cB<double>(const YlmTables& tb, int e) { return tb.B[e]; }
+template <> __device__ __forceinline__ float cB<float>(const YlmTables& tb, int e) { return tb.Bf[e]; }
+template <class Rl> __device__ __forceinline__ Rl cK(const YlmTables& tb, int e);
+template <> __device__ __forceinline__ double cK<double>(const YlmTables& tb, int e) { return tb.K[e]; }
+template <> __device__ __forceinline__ float cK<float>(const YlmTables& tb, int e) { return tb.Kf[e]; }
 
-constexpr int kLsCap = 52;
-constexpr int kLsThreads = 128;
+__host__ __device__ constexpr int ls_nroles(int L) { return L / 2 + 1; }
+__host__ __device__ constexpr int ls_col2(int L, int r) { return L - r; }  // second column
+__host__ __device__ constexpr bool ls_has2(int L, int r) { return L - r > r; }
+__host__ __device__ constexpr int ls_nvals_m(int L, int m) { return m == 0 ? L + 1 : 2 * (L + 1 - m); }
+__host__ __device__ constexpr int ls_role_nvals(int L, int r) {
+  return ls_nvals_m(L, r) + (ls_has2(L, r) ? ls_nvals_m(L, L - r) : 0);
+}
+// shared-memory fields per triple: ct, t2, then pmm[m], cos[m], sin[m]
+__host__ __device__ constexpr int ls_nfields(int L) { return 2 + 3 * (L + 1); }
 
-template <int LMAX, int M0, int M1>
-__device__ __forceinline__ void lstarx_pass(const YlmTables& tb, const DevGeo& g,
-                                            const double* __restrict__ xi, double* y, int i,
-                                            double4 ci, double* red) {
-  constexpr int NV = pass_nvals(LMAX, M0, M1);
-  double acc[NV];
+template <int LMAX, int M, int OFF, class Rl>
+__device__ __forceinline__ void ls_column(const YlmTables& tb, Rl ct, Rl t2, Rl p0, Rl cm, Rl sm,
+                                          Rl* acc) {
+  Rl p1 = 0;
 #pragma unroll
-  for (int v = 0; v < NV; ++v) acc[v] = 0.0;
+  for (int l = M; l <= LMAX; ++l) {
+    Rl P;
+    if (l == M) {
+      P = p0;
+    } else if (l == M + 1) {
+      p1 = (Rl)(2 * M + 1) * ct * p0;
+      P = p1;
+    } else {
+      P = (cA<Rl>(tb, lmi(l, M)) * ct) * p1 - (cB<Rl>(tb, lmi(l, M)) * t2) * p0;
+      p0 = p1;
+      p1 = P;
+    }
+    if (M == 0) {
+      acc[OFF + (l - M)] += P;
+    } else {
+      acc[OFF + (l - M)] = fma(P, cm, acc[OFF + (l - M)]);
+      acc[OFF + (LMAX + 1 - M) + (l - M)] = fma(P, sm, acc[OFF + (LMAX + 1 - M) + (l - M)]);
+    }
+  }
+}
+
+template <int LMAX, int M, int OFF, class Rl>
+__device__ __forceinline__ void ls_store(const YlmTables& tb, const Rl* acc, double* yi,
+                                         int lane) {
+#pragma unroll
+  for (int l = M; l <= LMAX; ++l) {
+    const int ind = l * l + l;
+    if (M == 0) {
+      if (lane == 0) yi[ind] = -tb.K[lmi(l, 0)] * (double)acc[OFF + (l - M)];
+    } else if (lane == 0) {
+      yi[ind + M] = -tb.K[lmi(l, M)] * (double)acc[OFF + (l - M)];
+      yi[ind - M] = -tb.K[lmi(l, M)] * (double)acc[OFF + (LMAX + 1 - M) + (l - M)];
+    }
+  }
+}
+
+// fields are stored [field][stride]; lanes take triples q < count
+template <int LMAX, int R, class Rl>
+__device__ __forceinline__ void ls_role(const YlmTables& tb, const Rl* sh, int stride,
+                                        int count, int lane, Rl* acc) {
+  constexpr int M1 = R, M2 = LMAX - R;
+  for (int q = lane; q < count; q += 32) {
+    const Rl ct = sh[q], t2 = sh[stride + q];
+    ls_column<LMAX, M1, 0, Rl>(tb, ct, t2, sh[(2 + 3 * M1) * stride + q],
+                               sh[(3 + 3 * M1) * stride + q], sh[(4 + 3 * M1) * stride + q], acc);
+    if constexpr (ls_has2(LMAX, R))
+      ls_column<LMAX, M2, ls_nvals_m(LMAX, M1), Rl>(tb, ct, t2, sh[(2 + 3 * M2) * stride + q],
+                                                     sh[(3 + 3 * M2) * stride + q],
+                                                     sh[(4 + 3 * M2) * stride + q], acc);
+  }
+}
+
+template <int LMAX, int R, class Rl>
+__device__ __forceinline__ void ls_role_finish(const YlmTables& tb, Rl* acc, double* yi,
+                                               int lane) {
+  constexpr int NV = ls_role_nvals(LMAX, R);
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) acc[v] += __shfl_xor_sync(0xffffffffu, acc[v], o);
+  }
+  ls_store<LMAX, R, 0, Rl>(tb, acc, yi, lane);
+  if constexpr (ls_has2(LMAX, R))
+    ls_store<LMAX, LMAX - R, ls_nvals_m(LMAX, R), Rl>(tb, acc, yi, lane);
+}
+
+// dispatch a runtime role index to the compile-time role code
+template <int LMAX, int R, class Rl>
+__device__ __forceinline__ void ls_run_role(int role, const YlmTables& tb, const Rl* sh,
+                                            int stride, int count, int lane, Rl* acc) {
+  if (role == R) {
+    ls_role<LMAX, R, Rl>(tb, sh, stride, count, lane, acc);
+    return;
+  }
+  if constexpr (R + 1 < ls_nroles(LMAX))
+    ls_run_role<LMAX, R + 1, Rl>(role, tb, sh, stride, count, lane, acc);
+}
+template <int LMAX, int R, class Rl>
+__device__ __forceinline__ void ls_finish_role(int role, const YlmTables& tb, Rl* acc,
+                                               double* yi, int lane) {
+  if (role == R) {
+    ls_role_finish<LMAX, R, Rl>(tb, acc, yi, lane);
+    return;
+  }
+  if constexpr (R + 1 < ls_nroles(LMAX))
+    ls_finish_role<LMAX, R + 1, Rl>(role, tb, acc, yi, lane);
+}
+
+__host__ __device__ constexpr int ls_max_nvals(int L) {
+  int mx = 0;
+  for (int r = 0; r < ls_nroles(L); ++r) mx = ls_role_nvals(L, r) > mx ? ls_role_nvals(L, r) : mx;
+  return mx;
+}
+
+template <int LMAX>
+__global__ void __launch_bounds__(32 * ls_nroles(LMAX)) k_lstarx(const YlmTables tb,
+                                                                  const DevGeo g,
+                                                                  const double* __restrict__ xi,
+                                                                  double* y) {
+  constexpr int NR = ls_nroles(LMAX);
+  constexpr int CH = 32 * NR;  // triples per chunk = threads per block
+  constexpr int NF = ls_nfields(LMAX);
+  constexpr int NVM = ls_max_nvals(LMAX);
+  extern __shared__ double sh[];  // [NF][CH]
+  const int i = blockIdx.x;
+  const int role = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const double4 ci = g.sph[i];
   const int G = g.ngrid;
   const double eta = tb.eta, flow = 1.0 - eta;
   const double fa = 15.0 * eta - 12.0, fb = 10.0 * eta * eta - 15.0 * eta + 6.0;
   const double ie5 = 1.0 / (eta * eta * eta * eta * eta);
   const double iri = 1.0 / ci.w;
+  double acc[NVM];
+#pragma unroll
+  for (int v = 0; v < NVM; ++v) acc[v] = 0.0;
   const int q0 = g.ls_ptr[i], q1 = g.ls_ptr[i + 1];
-  for (int q = q0 + threadIdx.x; q < q1; q += blockDim.x) {
-    const int2 jn = g.ls[q];
-    const int j = jn.x, n = jn.y;
-    const double4 cj = g.sph[j];
-    const double4 gn = g.grid[n];
-    double vx = fma(cj.w, gn.x, cj.x) - ci.x;
-    double vy = fma(cj.w, gn.y, cj.y) - ci.y;
-    double vz = fma(cj.w, gn.z, cj.z) - ci.z;
-    double r2 = vx * vx + vy * vy + vz * vz;
-    double rinv = rsqrt(r2);
-    double t = r2 * rinv * iri;
-    Angles a = angles_of(vx * rinv, vy * rinv, vz * rinv);
-    const size_t pj = (size_t)j * G + n;
-    double chi = fsw_fast(t, eta, flow, fa, fb, ie5);
-    double f = g.fi[pj];
-    double W = f > 1.0 ? chi / f : chi;
-    double coef = gn.w * xi[pj] * W;
-    const double ct = a.c * t, st = a.s * t, t2 = t * t;
-    // advance P_m^m and cos/sin(m phi) to M0
-    double pmm = coef, cm = 1.0, sm = 0.0, cmm1 = 1.0, smm1 = 0.0;
+  for (int c0 = q0; c0 < q1; c0 += CH) {
+    const int chunk = min(CH, q1 - c0);
+    // phase A: one triple per thread
+    const int q = c0 + threadIdx.x;
+    if (threadIdx.x < chunk) {
+      const int2 jn = g.ls[q];
+      const int j = jn.x, n = jn.y;
+      const double4 cj = g.sph[j];
+      const double4 gn = g.grid[n];
+      double vx = fma(cj.w, gn.x, cj.x) - ci.x;
+      double vy = fma(cj.w, gn.y, cj.y) - ci.y;
+      double vz = fma(cj.w, gn.z, cj.z) - ci.z;
+      double r2 = vx * vx + vy * vy + vz * vz;
+      double rinv = rsqrt(r2);
+      double t = r2 * rinv * iri;
+      Angles a = angles_of(vx * rinv, vy * rinv, vz * rinv);
+      const size_t pj = (size_t)j * G + n;
+      double chi = fsw_fast(t, eta, flow, fa, fb, ie5);
+      double f = g.fi[pj];
+      double W = f > 1.0 ? chi / f : chi;
+      const double st = a.s * t;
+      double* col = sh + threadIdx.x;
+      col[0] = a.c * t;
+      col[CH] = t * t;
+      double pmm = gn.w * xi[pj] * W;
+      double cm = 1.0, sm = 0.0, cmm1 = 1.0, smm1 = 0.0;
 #pragma unroll
-    for (int m = 0; m < M0; ++m) {
-      pmm = -pmm * (2.0 * m + 1.0) * st;
-      if (m == 0) {
-        cm = a.cp; sm = a.sp;
-      } else {
-        double cn = 2.0 * a.cp * cm - cmm1, sn = 2.0 * a.cp * sm - smm1;
-        cmm1 = cm; smm1 = sm; cm = cn; sm = sn;
-      }
-    }
-#pragma unroll
-    for (int m = M0; m < M1; ++m) {
-      if (m > M0) {
+      for (int m = 0; m <= LMAX; ++m) {
         if (m == 1) {
           cm = a.cp; sm = a.sp;
-        } else {
+        } else if (m >= 2) {
           double cn = 2.0 * a.cp * cm - cmm1, sn = 2.0 * a.cp * sm - smm1;
           cmm1 = cm; smm1 = sm; cm = cn; sm = sn;
         }
+        col[(2 + 3 * m) * CH] = pmm;
+        col[(3 + 3 * m) * CH] = cm;
+        col[(4 + 3 * m) * CH] = sm;
+        pmm = -pmm * (2.0 * m + 1.0) * st;
       }
-      double p0 = pmm, p1 = 0.0;
-#pragma unroll
-      for (int l = m; l <= LMAX; ++l) {
-        double P;
-        if (l == m) {
-          P = p0;
-        } else if (l == m + 1) {
-          p1 = (2.0 * m + 1.0) * ct * p0;
-          P = p1;
-        } else {
-          P = (tb.A[lmi(l, m)] * ct) * p1 - (tb.B[lmi(l, m)] * t2) * p0;
-          p0 = p1;
-          p1 = P;
-        }
-        if (m == 0) {
-          acc[pass_off(LMAX, M0, m, l, 0)] += P;
-        } else {
-          acc[pass_off(LMAX, M0, m, l, 0)] = fma(P, cm, acc[pass_off(LMAX, M0, m, l, 0)]);
-          acc[pass_off(LMAX, M0, m, l, 1)] = fma(P, sm, acc[pass_off(LMAX, M0, m, l, 1)]);
-        }
-      }
-      pmm = -pmm * (2.0 * m + 1.0) * st;
-    }
-  }
-  // block reduction: red[NV][kLsThreads], tree over threads
-  const int T = kLsThreads;
-#pragma unroll
-  for (int v = 0; v < NV; ++v) red[v * T + threadIdx.x] = acc[v];
-  __syncthreads();
-  for (int h = T / 2; h >= 1; h >>= 1) {
-    for (int e = threadIdx.x; e < NV * h; e += T) {
-      int v = e / h, tt = e - v * h;
-      red[v * T + tt] += red[v * T + tt + h];
     }
     __syncthreads();
+    // phase B: the role's columns over the chunk
+    ls_run_role<LMAX, 0, double>(role, tb, sh, CH, chunk, lane, acc);
+    __syncthreads();
   }
-  for (int v = threadIdx.x; v < NV; v += T) {
-    // decode v -> (l, m, sign)
-    int m = M0, off = v;
-    while (off >= nvals_m(LMAX, m)) {
-      off -= nvals_m(LMAX, m);
-      ++m;
-    }
-    int neg = off >= (LMAX + 1 - m) ? 1 : 0;
-    int l = m + (neg ? off - (LMAX + 1 - m) : off);
-    int ind = l * l + l + (neg ? -m : m);
-    y[(size_t)i * tb.nylm + ind] = -tb.K[lmi(l, m)] * red[v * T];
-  }
-  __syncthreads();
-}
-
-template <int LMAX, int M0>
-__device__ __forceinline__ void lstarx_passes(const YlmTables& tb, const DevGeo& g,
-                                              const double* __restrict__ xi, double* y, int i,
-                                              double4 ci, double* red) {
-  constexpr int M1 = pass_end(LMAX, M0, kLsCap);
-  lstarx_pass<LMAX, M0, M1>(tb, g, xi, y, i, ci, red);
-  if constexpr (M1 <= LMAX) lstarx_passes<LMAX, M1>(tb, g, xi, y, i, ci, red);
-}
-
-template <int LMAX>
-__global__ void __launch_bounds__(kLsThreads) k_lstarx(const YlmTables tb, const DevGeo g,
-                                                       const double* __restrict__ xi, double* y) {
-  extern __shared__ double red[];
-  const int i = blockIdx.x;
-  lstarx_passes<LMAX, 0>(tb, g, xi, y, i, g.sph[i], red);
+  ls_finish_role<LMAX, 0, double>(role, tb, acc, y + (size_t)i * tb.nylm, lane);
 }
 
 cudaError_t launch_lstarx_acc(Launch L, const YlmTables& tb, const DevGeo& g, const double* xi,
                               double* y) {
   if (g.nsph == 0) return cudaSuccess;
-  size_t sm = sizeof(double) * kLsCap * kLsThreads;
   cudaError_t e = cudaSuccess;
 #define CASE(LV)                                                                              \
   case LV: {                                                                                  \
-    if ((e = cudaFuncSetAttribute(k_lstarx<LV>, cudaFuncAttributeMaxDynamicSharedMemorySize,  \
-                                  (int)sm)))                                                  \
-      return e;                                                                               \
-    k_lstarx<LV><<<g.nsph, kLsThreads, sm, L.st>>>(tb, g, xi, y);                             \
+    constexpr int NR = ls_nroles(LV);                                                         \
+    size_t sm = sizeof(double) * ls_nfields(LV) * 32 * NR;                                    \
+    if (sm > 48 * 1024)                                                                       \
+      if ((e = cudaFuncSetAttribute(k_lstarx<LV>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                    (int)sm)))                                                \
+        return e;                                                                             \
+    k_lstarx<LV><<<g.nsph, 32 * NR, sm, L.st>>>(tb, g, xi, y);                                \
     break;                                                                                    \
   }
   switch (tb.lmax) {
@@ -1549,6 +1601,377 @@ cudaError_t launch_csph_pack(Launch L, int n, const double4* sph, double* csph, 
                              double* sy, double* sz) {
   if (n == 0) return cudaSuccess;
   k_csph_pack<<<(n + 255) / 256, 256, 0, L.st>>>(n, sph, csph, sx, sy, sz);
+  ++*L.launches;
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// FP32 operator (mixed precision).  Same work decomposition as the FP64
+// kernels; geometry differences are formed in FP64 and rounded once to FP32,
+// the recurrences, switch function and accumulations run in FP32.  The
+// result is an operator accurate to ~1e-6 relative, used only inside the
+// FP64 iterative refinement of the solver (the outer residual is FP64).
+// ---------------------------------------------------------------------------
+struct AnglesF {
+  float c, s, cp, sp;
+};
+__device__ __forceinline__ AnglesF angles_of_f(float sx, float sy, float sz) {
+  AnglesF a;
+  a.c = sz;
+  a.s = sqrtf(fmaxf(0.f, 1.f - sz * sz));
+  if (a.s != 0.f) {
+    float r = 1.f / a.s;
+    a.cp = sx * r;
+    a.sp = sy * r;
+  } else {
+    a.cp = 1.f;
+    a.sp = 0.f;
+  }
+  return a;
+}
+__device__ __forceinline__ float fsw_f(float x, float eta, float flow, float a, float b,
+                                       float ie5) {
+  if (x >= 1.f) return 0.f;
+  if (x <= flow) return 1.f;
+  float xm = x - 1.f;
+  return (xm * xm * (1.f - x)) * ((6.f * x + a) * x + b) * ie5;
+}
+
+template <int LMAX>
+__device__ __forceinline__ float ylm_dot_f(const YlmTables& tb, const AnglesF& a, float t,
+                                           const float2* __restrict__ xs) {
+  const float ct = a.c * t, st = a.s * t, t2 = t * t;
+  float acc = 0.f, pmm = 1.f;
+  float cm = 1.f, sm = 0.f, cmm1 = 1.f, smm1 = 0.f;
+#pragma unroll
+  for (int m = 0; m <= LMAX; ++m) {
+    if (m == 1) {
+      cm = a.cp;
+      sm = a.sp;
+    } else if (m >= 2) {
+      float cn = 2.f * a.cp * cm - cmm1, sn = 2.f * a.cp * sm - smm1;
+      cmm1 = cm; smm1 = sm; cm = cn; sm = sn;
+    }
+    float p0 = pmm, p1 = 0.f;
+#pragma unroll
+    for (int l = m; l <= LMAX; ++l) {
+      float P;
+      if (l == m) {
+        P = p0;
+      } else if (l == m + 1) {
+        p1 = (float)(2 * m + 1) * ct * p0;
+        P = p1;
+      } else {
+        P = (tb.Af[lmi(l, m)] * ct) * p1 - (tb.Bf[lmi(l, m)] * t2) * p0;
+        p0 = p1;
+        p1 = P;
+      }
+      float2 xv = xs[lmi(l, m)];
+      float q = (m == 0) ? xv.x : fmaf(cm, xv.x, sm * xv.y);
+      acc = fmaf(P, q, acc);
+    }
+    pmm = -pmm * (float)(2 * m + 1) * st;
+  }
+  return acc;
+}
+
+template <int LMAX>
+__global__ void __launch_bounds__(128) k_lx_pot_f(const YlmTables tb, const DevGeo g,
+                                                  const double* __restrict__ X, float* pot) {
+  constexpr int NLM = (LMAX + 1) * (LMAX + 2) / 2;
+  constexpr int NW = 4;
+  extern __shared__ float smf[];
+  const int G = g.ngrid;
+  float* acc = smf;                                          // [NW][G]
+  float2* xs = reinterpret_cast<float2*>(smf + ((NW * G + 1) & ~1));  // [NW][NLM]
+  const int i = blockIdx.x, w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int q = threadIdx.x; q < NW * G; q += blockDim.x) acc[q] = 0.f;
+  __syncthreads();
+  const double4 ci = g.sph[i];
+  const float ri = (float)ci.w;
+  const float eta = (float)tb.eta, flow = 1.f - eta;
+  const float fa = 15.f * eta - 12.f, fb = 10.f * eta * eta - 15.f * eta + 6.f;
+  const float ie5 = (float)(1.0 / (tb.eta * tb.eta * tb.eta * tb.eta * tb.eta));
+  float* myacc = acc + w * G;
+  float2* myxs = xs + w * NLM;
+  const int k0 = g.inl[i], k1 = g.inl[i + 1];
+  for (int k = k0 + w; k < k1; k += NW) {
+    const int j = g.nl[k];
+    const double* Xj = X + (size_t)j * g.nylm;
+    __syncwarp();
+    for (int e = lane; e < NLM; e += 32) {
+      int l = 0;
+      while (lmi(l + 1, 0) <= e) ++l;
+      int m = e - lmi(l, 0);
+      int ind = l * l + l;
+      double kk = tb.K[e];
+      myxs[e] = make_float2((float)(kk * Xj[ind + m]), m ? (float)(kk * Xj[ind - m]) : 0.f);
+    }
+    __syncwarp();
+    const double4 cj = g.sph[j];
+    const float dx = (float)(ci.x - cj.x), dy = (float)(ci.y - cj.y), dz = (float)(ci.z - cj.z);
+    const float irj = (float)(1.0 / cj.w);
+    const int q0 = g.pn_ptr[k], q1 = g.pn_ptr[k + 1];
+    for (int q = q0 + lane; q < q1; q += 32) {
+      const int n = g.pn[q];
+      const float4 gn = g.gridf[n];
+      float vx = fmaf(ri, gn.x, dx), vy = fmaf(ri, gn.y, dy), vz = fmaf(ri, gn.z, dz);
+      float r2 = vx * vx + vy * vy + vz * vz;
+      float rinv = rsqrtf(r2);
+      float t = r2 * rinv * irj;
+      AnglesF a = angles_of_f(vx * rinv, vy * rinv, vz * rinv);
+      float chi = fsw_f(t, eta, flow, fa, fb, ie5);
+      float f = (float)g.fi[(size_t)i * G + n];
+      float W = f > 1.f ? chi / f : chi;
+      myacc[n] += W * ylm_dot_f<LMAX>(tb, a, t, myxs);
+    }
+  }
+  __syncthreads();
+  for (int n = threadIdx.x; n < G; n += blockDim.x) {
+    float s = acc[n];
+#pragma unroll
+    for (int ww = 1; ww < NW; ++ww) s += acc[ww * G + n];
+    pot[(size_t)i * G + n] = s;
+  }
+}
+
+cudaError_t launch_lx_pot_f32(Launch L, const YlmTables& tb, const DevGeo& g, const double* X,
+                              float* pot) {
+  if (g.nsph == 0) return cudaSuccess;
+  const int NW = 4;
+  int nlm = (tb.lmax + 1) * (tb.lmax + 2) / 2;
+  size_t sm = sizeof(float) * (((size_t)NW * g.ngrid + 1) & ~(size_t)1) + sizeof(float2) * NW * nlm;
+  cudaError_t e = cudaSuccess;
+#define CASE(LV)                                                                              \
+  case LV: {                                                                                  \
+    if (sm > 48 * 1024)                                                                       \
+      if ((e = cudaFuncSetAttribute(k_lx_pot_f<LV>,                                           \
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)))   \
+        return e;                                                                             \
+    k_lx_pot_f<LV><<<g.nsph, 128, sm, L.st>>>(tb, g, X, pot);                                 \
+    break;                                                                                    \
+  }
+  switch (tb.lmax) {
+    DDC_LMAX_CASES(CASE)
+    default:
+      return cudaErrorInvalidValue;
+  }
+#undef CASE
+  ++*L.launches;
+  return cudaGetLastError();
+}
+
+template <int LMAX>
+__global__ void __launch_bounds__(32 * ls_nroles(LMAX)) k_lstarx_f(const YlmTables tb,
+                                                                    const DevGeo g,
+                                                                    const float* __restrict__ xi,
+                                                                    double* y) {
+  constexpr int NR = ls_nroles(LMAX);
+  constexpr int CH = 32 * NR;
+  constexpr int NVM = ls_max_nvals(LMAX);
+  extern __shared__ float shf[];  // [NF][CH]
+  const int i = blockIdx.x;
+  const int role = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const double4 ci = g.sph[i];
+  const int G = g.ngrid;
+  const float eta = (float)tb.eta, flow = 1.f - eta;
+  const float fa = 15.f * eta - 12.f, fb = 10.f * eta * eta - 15.f * eta + 6.f;
+  const float ie5 = (float)(1.0 / (tb.eta * tb.eta * tb.eta * tb.eta * tb.eta));
+  const float iri = (float)(1.0 / ci.w);
+  float acc[NVM];
+#pragma unroll
+  for (int v = 0; v < NVM; ++v) acc[v] = 0.f;
+  const int q0 = g.ls_ptr[i], q1 = g.ls_ptr[i + 1];
+  for (int c0 = q0; c0 < q1; c0 += CH) {
+    const int chunk = min(CH, q1 - c0);
+    const int q = c0 + threadIdx.x;
+    if (threadIdx.x < chunk) {
+      const int2 jn = g.ls[q];
+      const int j = jn.x, n = jn.y;
+      const double4 cj = g.sph[j];
+      const float4 gn = g.gridf[n];
+      const float rj = (float)cj.w;
+      float vx = fmaf(rj, gn.x, (float)(cj.x - ci.x));
+      float vy = fmaf(rj, gn.y, (float)(cj.y - ci.y));
+      float vz = fmaf(rj, gn.z, (float)(cj.z - ci.z));
+      float r2 = vx * vx + vy * vy + vz * vz;
+      float rinv = rsqrtf(r2);
+      float t = r2 * rinv * iri;
+      AnglesF a = angles_of_f(vx * rinv, vy * rinv, vz * rinv);
+      const size_t pj = (size_t)j * G + n;
+      float chi = fsw_f(t, eta, flow, fa, fb, ie5);
+      float f = (float)g.fi[pj];
+      float W = f > 1.f ? chi / f : chi;
+      const float st = a.s * t;
+      float* col = shf + threadIdx.x;
+      col[0] = a.c * t;
+      col[CH] = t * t;
+      float pmm = gn.w * xi[pj] * W;
+      float cm = 1.f, sm = 0.f, cmm1 = 1.f, smm1 = 0.f;
+#pragma unroll
+      for (int m = 0; m <= LMAX; ++m) {
+        if (m == 1) {
+          cm = a.cp; sm = a.sp;
+        } else if (m >= 2) {
+          float cn = 2.f * a.cp * cm - cmm1, sn = 2.f * a.cp * sm - smm1;
+          cmm1 = cm; smm1 = sm; cm = cn; sm = sn;
+        }
+        col[(2 + 3 * m) * CH] = pmm;
+        col[(3 + 3 * m) * CH] = cm;
+        col[(4 + 3 * m) * CH] = sm;
+        pmm = -pmm * (float)(2 * m + 1) * st;
+      }
+    }
+    __syncthreads();
+    ls_run_role<LMAX, 0, float>(role, tb, shf, CH, chunk, lane, acc);
+    __syncthreads();
+  }
+  ls_finish_role<LMAX, 0, float>(role, tb, acc, y + (size_t)i * tb.nylm, lane);
+}
+
+cudaError_t launch_lstarx_acc_f32(Launch L, const YlmTables& tb, const DevGeo& g,
+                                  const float* xi, double* y) {
+  if (g.nsph == 0) return cudaSuccess;
+  cudaError_t e = cudaSuccess;
+#define CASE(LV)                                                                              \
+  case LV: {                                                                                  \
+    constexpr int NR = ls_nroles(LV);                                                         \
+    size_t sm = sizeof(float) * ls_nfields(LV) * 32 * NR;                                     \
+    if (sm > 48 * 1024)                                                                       \
+      if ((e = cudaFuncSetAttribute(k_lstarx_f<LV>,                                           \
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)))   \
+        return e;                                                                             \
+    k_lstarx_f<LV><<<g.nsph, 32 * NR, sm, L.st>>>(tb, g, xi, y);                              \
+    break;                                                                                    \
+  }
+  switch (tb.lmax) {
+    DDC_LMAX_CASES(CASE)
+    default:
+      return cudaErrorInvalidValue;
+  }
+#undef CASE
+  ++*L.launches;
+  return cudaGetLastError();
+}
+
+// FP32 GEMM, column-major, 64x64 tiles, 256 threads x 4x4 outputs.
+// TB: float or double input for B (converted when staged), TC: output type.
+template <bool TA, class TB, class TC>
+__global__ void __launch_bounds__(256) k_sgemm(int M, int N, int K, float alpha,
+                                               const float* __restrict__ A, int lda,
+                                               const TB* __restrict__ B, int ldb, TC* C,
+                                               int ldc) {
+  __shared__ float As[GBK][GBM + 4];
+  __shared__ float Bs[GBK][GBN + 4];
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int m0 = blockIdx.x * GBM, n0 = blockIdx.y * GBN;
+  float acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[a][b] = 0.f;
+  for (int k0 = 0; k0 < K; k0 += GBK) {
+    for (int e = threadIdx.x; e < GBM * GBK; e += 256) {
+      int mm, kk;
+      if (TA) { kk = e % GBK; mm = e / GBK; } else { mm = e % GBM; kk = e / GBM; }
+      int m = m0 + mm, k = k0 + kk;
+      float v = 0.f;
+      if (m < M && k < K) v = TA ? A[(size_t)m * lda + k] : A[(size_t)k * lda + m];
+      As[kk][mm] = v;
+    }
+    for (int e = threadIdx.x; e < GBK * GBN; e += 256) {
+      int kk = e % GBK, nn = e / GBK;
+      int n = n0 + nn, k = k0 + kk;
+      Bs[kk][nn] = (n < N && k < K) ? (float)B[(size_t)n * ldb + k] : 0.f;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < GBK; ++kk) {
+      float a[4], b[4];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) a[r] = As[kk][ty + 16 * r];
+#pragma unroll
+      for (int c = 0; c < 4; ++c) b[c] = Bs[kk][tx + 16 * c];
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) acc[r][c] = fmaf(a[r], b[c], acc[r][c]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      int m = m0 + ty + 16 * r, n = n0 + tx + 16 * c;
+      if (m < M && n < N) C[(size_t)n * ldc + m] = (TC)(alpha * acc[r][c]);
+    }
+}
+cudaError_t launch_sgemm(Launch L, bool transA, int M, int N, int K, float alpha, const float* A,
+                         int lda, const float* B, int ldb, double* C, int ldc) {
+  if (M == 0 || N == 0) return cudaSuccess;
+  dim3 grid((M + GBM - 1) / GBM, (N + GBN - 1) / GBN);
+  if (transA)
+    k_sgemm<true, float, double><<<grid, 256, 0, L.st>>>(M, N, K, alpha, A, lda, B, ldb, C, ldc);
+  else
+    k_sgemm<false, float, double><<<grid, 256, 0, L.st>>>(M, N, K, alpha, A, lda, B, ldb, C, ldc);
+  ++*L.launches;
+  return cudaGetLastError();
+}
+cudaError_t launch_sgemm_xi(Launch L, int M, int N, int K, const float* A, int lda,
+                            const double* B, int ldb, float* C, int ldc) {
+  if (M == 0 || N == 0) return cudaSuccess;
+  dim3 grid((M + GBM - 1) / GBM, (N + GBN - 1) / GBN);
+  k_sgemm<true, double, float><<<grid, 256, 0, L.st>>>(M, N, K, 1.f, A, lda, B, ldb, C, ldc);
+  ++*L.launches;
+  return cudaGetLastError();
+}
+__global__ void k_to_float(long long n, const double* __restrict__ x, float* y) {
+  long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e < n) y[e] = (float)x[e];
+}
+cudaError_t launch_to_float(Launch L, long long n, const double* x, float* y) {
+  if (n == 0) return cudaSuccess;
+  k_to_float<<<(unsigned)((n + 255) / 256), 256, 0, L.st>>>(n, x, y);
+  ++*L.launches;
+  return cudaGetLastError();
+}
+// FP64 residual of the full operator L = D + O at x (y = O x):
+//   r = rhs - y - x / facl,  d = facl * r  (the Jacobi increment at x)
+// plus the partial sum of the increment's H-norm (hnorm, matvec.f90:281-323)
+__global__ void __launch_bounds__(256) k_residual(const YlmTables tb, long long n,
+                                                  const double* __restrict__ rhs,
+                                                  const double* __restrict__ y,
+                                                  const double* __restrict__ x, double* r,
+                                                  double* d, double* partials) {
+  double acc = 0.0;
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n;
+       q += (long long)gridDim.x * blockDim.x) {
+    int l = l_of((int)(q % tb.nylm));
+    double fl = tb.facl[l];
+    double rv = rhs[q] - y[q] - x[q] / fl;
+    double dv = fl * rv;
+    r[q] = rv;
+    d[q] = dv;
+    acc = fma(dv * dv, 1.0 / (1.0 + l), acc);
+  }
+  double v[1] = {acc};
+  block_sum_store<1>(v, 1, partials);
+}
+cudaError_t launch_residual(Launch L, const YlmTables& tb, long long n, const double* rhs,
+                            const double* y, const double* x, double* r, double* d,
+                            double* partials, int nblk) {
+  k_residual<<<nblk, 256, 0, L.st>>>(tb, n, rhs, y, x, r, d, partials);
+  ++*L.launches;
+  return cudaGetLastError();
+}
+__global__ void k_axpy(long long n, double a, const double* __restrict__ x, double* y) {
+  long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e < n) y[e] = fma(a, x[e], y[e]);
+}
+cudaError_t launch_axpy(Launch L, long long n, double a, const double* x, double* y) {
+  if (n == 0) return cudaSuccess;
+  k_axpy<<<(unsigned)((n + 255) / 256), 256, 0, L.st>>>(n, a, x, y);
   ++*L.launches;
   return cudaGetLastError();
 }
