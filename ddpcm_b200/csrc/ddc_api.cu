@@ -859,6 +859,8 @@ const char* ddc_status_string(int s) {
     case DDC_ERR_NOCONV: return "solver did not converge";
     case DDC_ERR_UNSUPPORTED: return "unsupported parameter";
     case DDC_ERR_NUMERIC: return "non-finite result";
+    case DDC_ERR_CAPACITY:
+      return "problem exceeds the fixed scratch of the allocation-free entry point";
     default: return "unknown status";
   }
 }

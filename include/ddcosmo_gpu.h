@@ -30,6 +30,7 @@ extern "C" {
 #define DDC_ERR_NOCONV 5       /* Jacobi/DIIS hit max_iter (cosmo.f90:188-200) */
 #define DDC_ERR_UNSUPPORTED 6  /* lmax outside the compiled range */
 #define DDC_ERR_NUMERIC 7      /* NaN/Inf in a stage output */
+#define DDC_ERR_CAPACITY 8     /* problem larger than the fixed scratch of ddc_efld_noalloc */
 
 /* precision modes */
 #define DDC_PREC_FP64 0   /* every stage in FP64 */
@@ -180,6 +181,23 @@ int ddc_reset_stage_times(ddc_ctx* ctx);
  * reference counterpart: it is the roofline denominator of the FP64-bound
  * kernels. */
 int ddc_fp64_peak(int device, double* gflops);
+
+/* efld without any device allocation.  No counterpart in the reference: it
+ * serves host programs that own all of the GPU's memory (a QM/MM or MD code
+ * that reserves the HBM for its own pool at start-up), for which a cudaMalloc
+ * issued by the library mid-step would fail or stall the device.  Same
+ * result as ddc_efld (efld.f90:1-116); every pointer is DEVICE memory of
+ * `device`: src(nsrc), csrc(3,nsrc), ctrg(3,ntrg), ef(3,ntrg).  The kernels
+ * are queued on `stream` (a cudaStream_t, NULL = legacy default stream) and
+ * the call returns without waiting; ef is valid once that stream reaches it.
+ * Scratch is a fixed 8 MiB array compiled into the library (held on every GPU
+ * that loads it until exit): ntrg is limited to 349,525 targets, larger
+ * problems return DDC_ERR_CAPACITY (use ddc_efld).  The first call on a device
+ * also resolves the array's device address (one-time set-up, done with that
+ * device current).  All calls share the array, so calls whose work overlaps
+ * on the GPU race; order them on one stream. */
+int ddc_efld_noalloc(int device, int nsrc, const double* src, const double* csrc, int ntrg,
+                     const double* ctrg, double* ef, void* stream);
 
 #ifdef __cplusplus
 }
