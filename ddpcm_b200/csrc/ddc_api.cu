@@ -144,7 +144,9 @@ struct ddc_ctx {
   long long ntri = 0;
   std::vector<double> h_grid;  // x,y,z,w per point
   // geometry
-  DBuf sph, grid, basis, bw, fi, ui, zi, inl, nl, rev, pn_ptr, pn, ls_ptr, ls, ntri_pt;
+  DBuf sph, grid, basis, bw, fi, ui, zi, inl, nl, rev, pn_ptr, pn, pn_pair, ls_ptr, ls, ntri_pt;
+  DBuf lsstart, fxa, fda, xk;
+  int maxnb = 0;
   DBuf cavoff, cavidx, cavpt, ccav, cnt, scan_tmp;
   DBuf csph, cx, cy, cz;  // csph(3,n) and SoA centres
   // work
@@ -176,8 +178,11 @@ struct ddc_ctx {
     g.rev = rev.as<int>();
     g.pn_ptr = pn_ptr.as<int>();
     g.pn = pn.as<uint16_t>();
+    g.pn_pair = pn_pair.as<uint8_t>();
+    g.maxnb = maxnb;
     g.ls_ptr = ls_ptr.as<int>();
     g.ls = ls.as<int2>();
+    g.lsstart = lsstart.as<int>();
     g.ntri_pt = ntri_pt.as<uint8_t>();
     g.cavoff = cavoff.as<int>();
     g.cavidx = cavidx.as<int>();
@@ -377,6 +382,21 @@ int do_init(ddc_ctx* ctx, int n, const std::vector<double4>* hsph, const double4
   ctx->npair = npair;
   CK(ctx->nl.ensure(sizeof(int) * std::max(npair, 1)));
   CK(ctx->rev.ensure(sizeof(int) * std::max(npair, 1)));
+  {
+    std::vector<int> h_inl(N + 1);
+    CK(cudaMemcpyAsync(h_inl.data(), ctx->inl.p, sizeof(int) * (N + 1), cudaMemcpyDeviceToHost,
+                       ctx->st));
+    CKI(sync(ctx));
+    int mx = 0;
+    for (int i = 0; i < N; i++) mx = std::max(mx, h_inl[i + 1] - h_inl[i]);
+    ctx->maxnb = mx;
+    // the lx kernel indexes a sphere's neighbours with 8 bits (the reference
+    // caps the list at nngmax = 100 per sphere on average, ddcosmo.f90:87)
+    const size_t smem = 32 * (size_t)mx + 4 * (size_t)mx + 32 * (size_t)G;
+    if (mx > 255 || smem > 200 * 1024)
+      return fail(ctx, DDC_ERR_UNSUPPORTED, "a sphere has too many neighbours (" +
+                                                std::to_string(mx) + ")");
+  }
   if (N > 0) {
     CK(launch_csr_fill(L, N, ctx->sph.as<double4>(), ctx->inl.as<int>(), ctx->nl.as<int>()));
     CK(launch_csr_rev(L, N, ctx->inl.as<int>(), ctx->nl.as<int>(), ctx->rev.as<int>()));
@@ -423,8 +443,10 @@ int do_init(ddc_ctx* ctx, int n, const std::vector<double4>* hsph, const double4
   CKI(sync(ctx));
   ctx->ntri = ntri;
   CK(ctx->pn.ensure(sizeof(uint16_t) * std::max(ntri, 1)));
+  CK(ctx->pn_pair.ensure(std::max(ntri, 1)));
   CK(launch_pair_fill(L, N, G, ctx->sph.as<double4>(), ctx->grid.as<double4>(), ctx->inl.as<int>(),
-                      ctx->nl.as<int>(), ctx->pn_ptr.as<int>(), ctx->pn.as<uint16_t>()));
+                      ctx->nl.as<int>(), ctx->pn_ptr.as<int>(), ctx->pn.as<uint16_t>(),
+                      ctx->pn_pair.as<uint8_t>()));
   CK(ctx->ls_ptr.ensure(sizeof(int) * (N + 1)));
   CK(cudaMemsetAsync(ctx->cnt.p, 0, sizeof(int) * (N + 1), ctx->st));
   CK(launch_ls_count(L, N, ctx->inl.as<int>(), ctx->rev.as<int>(), ctx->pn_ptr.as<int>(),
@@ -432,9 +454,10 @@ int do_init(ddc_ctx* ctx, int n, const std::vector<double4>* hsph, const double4
   CK(scan_exclusive(L, ctx->cnt.as<int>(), ctx->ls_ptr.as<int>(), N, ctx->scan_tmp.p,
                     ctx->scan_tmp.bytes));
   CK(ctx->ls.ensure(sizeof(int2) * std::max(ntri, 1)));
+  CK(ctx->lsstart.ensure(sizeof(int) * std::max(npair, 1)));
   CK(launch_ls_fill(L, N, ctx->inl.as<int>(), ctx->nl.as<int>(), ctx->rev.as<int>(),
                     ctx->pn_ptr.as<int>(), ctx->pn.as<uint16_t>(), ctx->ls_ptr.as<int>(),
-                    ctx->ls.as<int2>()));
+                    ctx->ls.as<int2>(), ctx->lsstart.as<int>()));
   // centres for the electrostatics
   CK(ctx->csph.ensure(sizeof(double) * 3 * std::max(N, 1)));
   CK(ctx->cx.ensure(sizeof(double) * std::max(N, 1)));
@@ -446,6 +469,8 @@ int do_init(ddc_ctx* ctx, int n, const std::vector<double4>* hsph, const double4
   const size_t nv = (size_t)N * NY;
   const int nd = std::max(ctx->prm.ndiis, 1);
   CK(ctx->pot.ensure(sizeof(double) * std::max(NP, 1LL)));
+  CK(ctx->xk.ensure(sizeof(double) * 2 * std::max(N, 1) *
+                    ((ctx->prm.lmax + 1) * (ctx->prm.lmax + 2) / 2)));
   CK(ctx->xig.ensure(sizeof(double) * std::max(NP, 1LL)));
   CK(ctx->uchi.ensure(sizeof(double) * std::max(NP, 1LL)));
   for (DBuf* b : {&ctx->rhs, &ctx->x, &ctx->y, &ctx->xn, &ctx->psi, &ctx->sigma, &ctx->s})
@@ -481,7 +506,7 @@ int op_lx(ddc_ctx* ctx, const double* x, double* y) {
   DevGeo g = ctx->geo();
   {
     StageScope sc(ctx, ST_LX_POT);
-    CK(launch_lx_pot(ctx->L(), ctx->tb, g, x, ctx->pot.as<double>(), false));
+    CK(launch_lx_pot(ctx->L(), ctx->tb, g, x, ctx->pot.as<double>(), false, ctx->xk.p));
   }
   StageScope sc(ctx, ST_PROJ);
   // y = -Bw pot   (intrhs then negate, matvec.f90:131-135)
@@ -507,7 +532,7 @@ int op_lstarx(ddc_ctx* ctx, const double* x, double* y) {
 int op_lx_f32(ddc_ctx* ctx, const double* x, double* y) {
   {
     StageScope sc(ctx, ST_LX_POT);
-    CK(launch_lx_pot_f32(ctx->L(), ctx->tb, ctx->geo(), x, ctx->pot_f.as<float>()));
+    CK(launch_lx_pot_f32(ctx->L(), ctx->tb, ctx->geo(), x, ctx->pot_f.as<float>(), ctx->xk.p));
   }
   StageScope sc(ctx, ST_PROJ);
   CK(launch_sgemm(ctx->L(), false, ctx->nylm, ctx->nsph, ctx->ngrid, -1.f, ctx->bw_f.as<float>(),
@@ -814,12 +839,16 @@ int forces_dev(ddc_ctx* ctx, const double* phi, const double* sigma, const doubl
   CKI(op_xi(ctx, s, ctx->xig.as<double>()));
   {
     StageScope sc(ctx, ST_UCHI);
-    CK(launch_lx_pot(ctx->L(), ctx->tb, ctx->geo(), sigma, ctx->uchi.as<double>(), true));
+    CK(launch_lx_pot(ctx->L(), ctx->tb, ctx->geo(), sigma, ctx->uchi.as<double>(), true,
+                     ctx->xk.p));
   }
   const double fep = 0.5 * (ctx->prm.eps - 1.0) / ctx->prm.eps;
+  CK(ctx->fxa.ensure(sizeof(double) * 3 * std::max(ctx->nsph, 1)));
+  CK(ctx->fda.ensure(sizeof(double) * 3 * std::max<long long>(ctx->ntri, 1)));
   StageScope sc(ctx, ST_FORCES);
   CK(launch_forces(ctx->L(), ctx->tb, ctx->geo(), sigma, ctx->xig.as<double>(),
-                   ctx->uchi.as<double>(), phi, fep, fx));
+                   ctx->uchi.as<double>(), phi, fep, fx, ctx->fxa.as<double>(),
+                   ctx->fda.as<double>()));
   return DDC_OK;
 }
 
@@ -1278,7 +1307,8 @@ int ddc_energy_forces(ddc_ctx* ctx, int n, const double* charge, const double* x
     int ch1 = efield_chunks(N, NC), ch2 = efield_chunks(NC, N);
     CK(ctx->ef_scratch.ensure(sizeof(double) * 3 *
                               std::max((size_t)ch1 * NC, (size_t)ch2 * N + 1)));
-    auto efield = launch_efield;
+    // in mixed precision the two force-only field sums use FP32 pair arithmetic
+    auto efield = ctx->prm.precision == DDC_PREC_MIXED ? launch_efield_f32 : launch_efield;
     {
       StageScope sc(ctx, ST_EFIELD);
       CK(efield(ctx->L(), N, dq, ctx->csph.as<double>(), NC, ctx->ccav.as<double>(),

@@ -46,6 +46,7 @@ struct YlmTables {
 // Device geometry handed to every kernel.
 struct DevGeo {
   int nsph, ngrid, nylm, ncav, npair;
+  int maxnb;  // largest neighbour count of a sphere
   long long ntri;
   const double4* sph;
   const double4* grid;
@@ -60,8 +61,10 @@ struct DevGeo {
   const int* rev;
   const int* pn_ptr;
   const uint16_t* pn;
+  const uint8_t* pn_pair;  // local index (within the sphere's CSR range) of each triple's pair
   const int* ls_ptr;
   const int2* ls;
+  const int* lsstart;  // per CSR entry (j,i): start of that pair's block in i's gather list
   const uint8_t* ntri_pt;
   const int* cavoff;
   const int* cavidx;
@@ -109,24 +112,26 @@ cudaError_t launch_pair_count(Launch L, int nsph, int ngrid, const double4* sph,
                               const double4* grid, const int* inl, const int* nl, int* cnt);
 cudaError_t launch_pair_fill(Launch L, int nsph, int ngrid, const double4* sph,
                              const double4* grid, const int* inl, const int* nl,
-                             const int* pn_ptr, uint16_t* pn);
+                             const int* pn_ptr, uint16_t* pn, uint8_t* pn_pair);
 cudaError_t launch_ls_count(Launch L, int nsph, const int* inl, const int* rev, const int* pn_ptr,
                             int* cnt);
 cudaError_t launch_ls_fill(Launch L, int nsph, const int* inl, const int* nl, const int* rev,
-                           const int* pn_ptr, const uint16_t* pn, const int* ls_ptr, int2* ls);
+                           const int* pn_ptr, const uint16_t* pn, const int* ls_ptr, int2* ls,
+                           int* lsstart);
 // exclusive scan of n ints (out[n] = total); temp is device scratch of temp_bytes
 cudaError_t scan_exclusive(Launch L, const int* in, int* out, int n, void* temp,
                            size_t temp_bytes);
 size_t scan_temp_bytes(int n);
 
 // operators
+// xk: scratch of N*(lmax+1)(lmax+2)/2 double2 (K-scaled X in pair layout)
 cudaError_t launch_lx_pot(Launch L, const YlmTables& tb, const DevGeo& g, const double* X,
-                          double* pot, bool chi_only);
+                          double* pot, bool chi_only, void* xk);
 cudaError_t launch_lstarx_acc(Launch L, const YlmTables& tb, const DevGeo& g, const double* xi,
                               double* y);
 // FP32 operator variants (mixed precision): pot/xi in FP32, y in FP64
 cudaError_t launch_lx_pot_f32(Launch L, const YlmTables& tb, const DevGeo& g, const double* X,
-                              float* pot);
+                              float* pot, void* xk);
 cudaError_t launch_lstarx_acc_f32(Launch L, const YlmTables& tb, const DevGeo& g,
                                   const float* xi, double* y);
 // C[M x N] = alpha * op(A) * B in FP32 arithmetic, A float, B float or double, C float/double
@@ -177,12 +182,15 @@ cudaError_t launch_psi(Launch L, int n, int nylm, const double* q, double* psi);
 cudaError_t launch_efield(Launch L, int nsrc, const double* q, const double* csrc, int ntrg,
                           const double* ctrg, double* ef, double* scratch, int nchunk);
 int efield_chunks(int nsrc, int ntrg);
-
+// FP32 pair arithmetic, FP64 accumulation (mixed-precision force terms)
+cudaError_t launch_efield_f32(Launch L, int nsrc, const double* q, const double* csrc, int ntrg,
+                              const double* ctrg, double* ef, double* scratch, int nchunk);
 
 // forces
+// fxa (3,N) and fda (3,T) are scratch of the two force kernels
 cudaError_t launch_forces(Launch L, const YlmTables& tb, const DevGeo& g, const double* sigma,
                           const double* s_xi, const double* u_chi, const double* phi,
-                          double fep, double* fx);
+                          double fep, double* fx, double* fxa, double* fda);
 cudaError_t launch_mkxi(Launch L, const YlmTables& tb, const DevGeo& g, const double* xi_grid,
                         double scale, double* out);
 cudaError_t launch_zeta_efld_contract(Launch L, const DevGeo& g, const double* zeta,

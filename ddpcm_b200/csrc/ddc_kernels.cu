@@ -20,6 +20,18 @@ namespace ddc {
 
 __host__ __device__ constexpr int lmi(int l, int m) { return l * (l + 1) / 2 + m; }
 
+// recurrence constants in the arithmetic type of the kernel
+template <class Rl> __device__ __forceinline__ Rl cA(const YlmTables& tb, int e);
+template <> __device__ __forceinline__ double cA<double>(const YlmTables& tb, int e) { return tb.A[e]; }
+template <> __device__ __forceinline__ float cA<float>(const YlmTables& tb, int e) { return tb.Af[e]; }
+template <class Rl> __device__ __forceinline__ Rl cB(const YlmTables& tb, int e);
+template <> __device__ __forceinline__ double cB<double>(const YlmTables& tb, int e) { return tb.B[e]; }
+template <> __device__ __forceinline__ float cB<float>(const YlmTables& tb, int e) { return tb.Bf[e]; }
+template <class Rl> __device__ __forceinline__ Rl cK(const YlmTables& tb, int e);
+template <> __device__ __forceinline__ double cK<double>(const YlmTables& tb, int e) { return tb.K[e]; }
+template <> __device__ __forceinline__ float cK<float>(const YlmTables& tb, int e) { return tb.Kf[e]; }
+
+
 // ---------------------------------------------------------------------------
 // exact geometry helpers
 // ---------------------------------------------------------------------------
@@ -321,7 +333,8 @@ cudaError_t launch_cav_fill(Launch L, int nsph, int ngrid, const double* ui, con
 template <bool FILL>
 __global__ void k_pairs(int nsph, int ngrid, const double4* __restrict__ sph,
                         const double4* __restrict__ grid, const int* __restrict__ inl,
-                        const int* __restrict__ nl, int* cnt, const int* pn_ptr, uint16_t* pn) {
+                        const int* __restrict__ nl, int* cnt, const int* pn_ptr, uint16_t* pn,
+                        uint8_t* pn_pair) {
   int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   int npair = inl[nsph];
   if (warp >= npair) return;
@@ -340,7 +353,11 @@ __global__ void k_pairs(int nsph, int ngrid, const double4* __restrict__ sph,
     bool in = false;
     if (n < ngrid) in = rel_exact(ci, grid[n], cj).t < 1.0;
     unsigned mask = __ballot_sync(0xffffffffu, in);
-    if (FILL && in) pn[base + __popc(mask & ((1u << lane) - 1u))] = (uint16_t)n;
+    if (FILL && in) {
+      const int pos = base + __popc(mask & ((1u << lane) - 1u));
+      pn[pos] = (uint16_t)n;
+      pn_pair[pos] = (uint8_t)(k - inl[i]);
+    }
     base += __popc(mask);
   }
   if (!FILL && lane == 0) cnt[k] = base;
@@ -353,20 +370,20 @@ cudaError_t launch_pair_count(Launch L, int nsph, int ngrid, const double4* sph,
   if ((e = cudaStreamSynchronize(L.st))) return e;
   if (npair == 0) return cudaSuccess;
   k_pairs<false><<<(npair + 7) / 8, 256, 0, L.st>>>(nsph, ngrid, sph, grid, inl, nl, cnt, nullptr,
-                                                    nullptr);
+                                                    nullptr, nullptr);
   ++*L.launches;
   return cudaGetLastError();
 }
 cudaError_t launch_pair_fill(Launch L, int nsph, int ngrid, const double4* sph,
                              const double4* grid, const int* inl, const int* nl,
-                             const int* pn_ptr, uint16_t* pn) {
+                             const int* pn_ptr, uint16_t* pn, uint8_t* pn_pair) {
   int npair;
   cudaError_t e = cudaMemcpyAsync(&npair, inl + nsph, sizeof(int), cudaMemcpyDeviceToHost, L.st);
   if (e) return e;
   if ((e = cudaStreamSynchronize(L.st))) return e;
   if (npair == 0) return cudaSuccess;
   k_pairs<true><<<(npair + 7) / 8, 256, 0, L.st>>>(nsph, ngrid, sph, grid, inl, nl, nullptr, pn_ptr,
-                                                   pn);
+                                                   pn, pn_pair);
   ++*L.launches;
   return cudaGetLastError();
 }
@@ -394,20 +411,22 @@ cudaError_t launch_ls_count(Launch L, int nsph, const int* inl, const int* rev, 
 __global__ void k_ls_fill(int nsph, const int* __restrict__ inl, const int* __restrict__ nl,
                           const int* __restrict__ rev, const int* __restrict__ pn_ptr,
                           const uint16_t* __restrict__ pn, const int* __restrict__ ls_ptr,
-                          int2* ls) {
+                          int2* ls, int* lsstart) {
   int i = blockIdx.x;
   int off = ls_ptr[i];
   for (int k = inl[i]; k < inl[i + 1]; k++) {
     int kk = rev[k], j = nl[k];
     int a = pn_ptr[kk], b = pn_ptr[kk + 1];
+    if (threadIdx.x == 0) lsstart[kk] = off;  // where pair (j, i) sits in i's gather list
     for (int q = a + threadIdx.x; q < b; q += blockDim.x) ls[off + (q - a)] = make_int2(j, pn[q]);
     off += b - a;
   }
 }
 cudaError_t launch_ls_fill(Launch L, int nsph, const int* inl, const int* nl, const int* rev,
-                           const int* pn_ptr, const uint16_t* pn, const int* ls_ptr, int2* ls) {
+                           const int* pn_ptr, const uint16_t* pn, const int* ls_ptr, int2* ls,
+                           int* lsstart) {
   if (nsph == 0) return cudaSuccess;
-  k_ls_fill<<<nsph, 128, 0, L.st>>>(nsph, inl, nl, rev, pn_ptr, pn, ls_ptr, ls);
+  k_ls_fill<<<nsph, 128, 0, L.st>>>(nsph, inl, nl, rev, pn_ptr, pn, ls_ptr, ls, lsstart);
   ++*L.launches;
   return cudaGetLastError();
 }
@@ -489,93 +508,222 @@ __device__ __forceinline__ double ylm_dot(const YlmTables& tb, const Angles& a, 
   return acc;
 }
 
-// lx, part 1 (calcv ddcosmo.f90:1671-1746): pot(i,n) = sum_j W_ij(n) *
-// sum_lm 4pi/(2l+1) t^l Y_lm(s) X_j,lm over the pair lists.  Block per
-// sphere; each warp takes pairs round robin, stages K*X_j in shared memory
-// (uniform, broadcast reads) and its lanes take the pair's points.  Each warp
-// accumulates into its own row of pot, rows summed in fixed order at the end.
-// chi_only: weight chi instead of W (the sum of chi*intmlp needed by fdokb).
-template <int LMAX, bool CHI>
-__global__ void __launch_bounds__(128) k_lx_pot(const YlmTables tb, const DevGeo g,
-                                                const double* __restrict__ X, double* pot) {
+// ---------------------------------------------------------------------------
+// lx, part 1 (calcv ddcosmo.f90:1671-1746 with intmlp :1140-1178), second
+// form, both precisions.  Block per sphere i:
+//   * K*X_j of every neighbour j (as (X_{l,m}, X_{l,-m}) pairs) and the
+//     centre differences c_i - c_j are staged in shared memory once;
+//   * the sphere's triples (pair-major list) are spread over all threads, a
+//     per-triple local pair index selects the staged neighbour;
+//   * contributions to the same grid point inside one warp instruction are
+//     combined in lane order (match_any) before the warp-private row update,
+//     so the sum order is fixed and the result bit-reproducible;
+//   * one accumulator per m column keeps independent FMA chains in flight.
+// ---------------------------------------------------------------------------
+template <class Rl> struct RT;
+template <> struct RT<double> {
+  typedef double2 V2;
+};
+template <> struct RT<float> {
+  typedef float2 V2;
+};
+template <class Rl> __device__ __forceinline__ typename RT<Rl>::V2 mk2(Rl a, Rl b);
+template <> __device__ __forceinline__ double2 mk2<double>(double a, double b) {
+  return make_double2(a, b);
+}
+template <> __device__ __forceinline__ float2 mk2<float>(float a, float b) {
+  return make_float2(a, b);
+}
+template <class Rl> struct GP {
+  Rl x, y, z, w;
+};
+__device__ __forceinline__ GP<double> grid_pt(const DevGeo& g, int n, double*) {
+  double4 v = g.grid[n];
+  return GP<double>{v.x, v.y, v.z, v.w};
+}
+__device__ __forceinline__ GP<float> grid_pt(const DevGeo& g, int n, float*) {
+  float4 v = g.gridf[n];
+  return GP<float>{v.x, v.y, v.z, v.w};
+}
+__device__ __forceinline__ double rsqrt_t(double x) { return rsqrt(x); }
+__device__ __forceinline__ float rsqrt_t(float x) { return rsqrtf(x); }
+__device__ __forceinline__ double sqrt_t(double x) { return sqrt(x); }
+__device__ __forceinline__ float sqrt_t(float x) { return sqrtf(x); }
+
+template <int LMAX, class Rl>
+__device__ __forceinline__ Rl ylm_dot2(const YlmTables& tb, Rl sx, Rl sy, Rl sz, Rl t,
+                                       const typename RT<Rl>::V2* __restrict__ xs) {
+  const Rl one = 1;
+  Rl cth = sz, sth = sqrt_t(fmax(Rl(0), one - sz * sz));
+  Rl cp = 1, sp = 0;
+  if (sth != Rl(0)) {
+    Rl r = one / sth;
+    cp = sx * r;
+    sp = sy * r;
+  }
+  const Rl ct = cth * t, st = sth * t, t2 = t * t;
+  Rl accm[LMAX + 1];
+  Rl pmm = 1, cm = 1, sm = 0, cmm1 = 1, smm1 = 0;
+#pragma unroll
+  for (int m = 0; m <= LMAX; ++m) {
+    if (m == 1) {
+      cm = cp;
+      sm = sp;
+    } else if (m >= 2) {
+      Rl cn = Rl(2) * cp * cm - cmm1, sn = Rl(2) * cp * sm - smm1;
+      cmm1 = cm; smm1 = sm; cm = cn; sm = sn;
+    }
+    Rl p0 = pmm, p1 = 0, a = 0;
+#pragma unroll
+    for (int l = m; l <= LMAX; ++l) {
+      Rl P;
+      if (l == m) {
+        P = p0;
+      } else if (l == m + 1) {
+        p1 = Rl(2 * m + 1) * ct * p0;
+        P = p1;
+      } else {
+        P = (cA<Rl>(tb, lmi(l, m)) * ct) * p1 - (cB<Rl>(tb, lmi(l, m)) * t2) * p0;
+        p0 = p1;
+        p1 = P;
+      }
+      const typename RT<Rl>::V2 xv = xs[lmi(l, m)];
+      Rl q = (m == 0) ? xv.x : fma(cm, xv.x, sm * xv.y);
+      a = fma(P, q, a);
+    }
+    accm[m] = a;
+    pmm = -pmm * Rl(2 * m + 1) * st;
+  }
+  Rl s = 0;
+#pragma unroll
+  for (int m = 0; m <= LMAX; ++m) s += accm[m];
+  return s;
+}
+
+template <int LMAX, bool CHI, class Rl>
+__global__ void __launch_bounds__(128) k_lx2(const YlmTables tb, const DevGeo g,
+                                             const typename RT<Rl>::V2* __restrict__ XK,
+                                             Rl* pot) {
+  typedef typename RT<Rl>::V2 V2;
   constexpr int NLM = (LMAX + 1) * (LMAX + 2) / 2;
   constexpr int NW = 4;
-  extern __shared__ double smem[];
+  extern __shared__ __align__(16) unsigned char smraw[];
   const int G = g.ngrid;
-  double* acc = smem;                                    // [NW][G]
-  double2* xs = reinterpret_cast<double2*>(smem + NW * G);  // [NW][NLM]
-  const int i = blockIdx.x, w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int q = threadIdx.x; q < NW * G; q += blockDim.x) acc[q] = 0.0;
-  __syncthreads();
+  const int maxnb = g.maxnb;
+  Rl* nbd = reinterpret_cast<Rl*>(smraw);  // [maxnb][4]: c_i - c_j, 1/r_j
+  int* nbj = reinterpret_cast<int*>(nbd + 4 * maxnb);  // [maxnb]: j
+  Rl* acc = reinterpret_cast<Rl*>(nbj + ((maxnb + 3) & ~3));  // [NW][G]
+  const int i = blockIdx.x, tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
+  const int k0 = g.inl[i], nn = g.inl[i + 1] - k0;
   const double4 ci = g.sph[i];
-  const double eta = tb.eta, flow = 1.0 - eta;
-  const double fa = 15.0 * eta - 12.0, fb = 10.0 * eta * eta - 15.0 * eta + 6.0;
-  const double ie5 = 1.0 / (eta * eta * eta * eta * eta);
-  double* myacc = acc + w * G;
-  double2* myxs = xs + w * NLM;
-  const int k0 = g.inl[i], k1 = g.inl[i + 1];
-  for (int k = k0 + w; k < k1; k += NW) {
-    const int j = g.nl[k];
-    const double* Xj = X + (size_t)j * g.nylm;
-    __syncwarp();
-    for (int e = lane; e < NLM; e += 32) {
-      int l = 0;
-      while (lmi(l + 1, 0) <= e) ++l;
-      int m = e - lmi(l, 0);
-      int ind = l * l + l;
-      double kk = tb.K[e];
-      myxs[e] = make_double2(kk * Xj[ind + m], m ? kk * Xj[ind - m] : 0.0);
-    }
-    __syncwarp();
+  for (int b = tid; b < nn; b += 128) {
+    const int j = g.nl[k0 + b];
     const double4 cj = g.sph[j];
-    const double irj = 1.0 / cj.w;
-    const int q0 = g.pn_ptr[k], q1 = g.pn_ptr[k + 1];
-    for (int q = q0 + lane; q < q1; q += 32) {
-      const int n = g.pn[q];
-      const double4 gn = g.grid[n];
-      double vx = fma(ci.w, gn.x, ci.x) - cj.x;
-      double vy = fma(ci.w, gn.y, ci.y) - cj.y;
-      double vz = fma(ci.w, gn.z, ci.z) - cj.z;
-      double r2 = vx * vx + vy * vy + vz * vz;
-      double rinv = rsqrt(r2);
-      double t = r2 * rinv * irj;
-      Angles a = angles_of(vx * rinv, vy * rinv, vz * rinv);
-      double chi = fsw_fast(t, eta, flow, fa, fb, ie5);
-      double W = chi;
-      if (!CHI) {
-        double f = g.fi[(size_t)i * G + n];
-        if (f > 1.0) W = chi / f;
+    nbd[4 * b + 0] = (Rl)(ci.x - cj.x);
+    nbd[4 * b + 1] = (Rl)(ci.y - cj.y);
+    nbd[4 * b + 2] = (Rl)(ci.z - cj.z);
+    nbd[4 * b + 3] = (Rl)(1.0 / cj.w);
+    nbj[b] = j;
+  }
+  for (int q = tid; q < NW * G; q += 128) acc[q] = 0;
+  __syncthreads();
+  const Rl ri = (Rl)ci.w;
+  const Rl eta = (Rl)tb.eta, flow = Rl(1) - eta;
+  const Rl fa = Rl(15) * eta - Rl(12), fb = Rl(10) * eta * eta - Rl(15) * eta + Rl(6);
+  const Rl ie5 = (Rl)(1.0 / (tb.eta * tb.eta * tb.eta * tb.eta * tb.eta));
+  Rl* myacc = acc + w * G;
+  const int q0 = g.pn_ptr[k0], q1 = g.pn_ptr[k0 + nn];
+  for (int base = q0; base < q1; base += 128) {
+    const int q = base + tid;
+    const bool valid = q < q1;
+    Rl val = 0;
+    int n = 0;
+    if (valid) {
+      n = g.pn[q];
+      const int b = g.pn_pair[q];
+      const GP<Rl> gn = grid_pt(g, n, (Rl*)nullptr);
+      const Rl* d = nbd + 4 * b;
+      Rl vx = fma(ri, gn.x, d[0]), vy = fma(ri, gn.y, d[1]), vz = fma(ri, gn.z, d[2]);
+      Rl r2 = vx * vx + vy * vy + vz * vz;
+      Rl rinv = rsqrt_t(r2);
+      Rl t = r2 * rinv * d[3];
+      Rl chi;
+      if (t >= Rl(1)) chi = 0;
+      else if (t <= flow) chi = 1;
+      else {
+        Rl xm = t - Rl(1);
+        chi = (xm * xm * (Rl(1) - t)) * ((Rl(6) * t + fa) * t + fb) * ie5;
       }
-      myacc[n] += W * ylm_dot<LMAX>(tb, a, t, myxs);
+      Rl W = chi;
+      if (!CHI) {
+        Rl f = (Rl)g.fi[(size_t)i * G + n];
+        if (f > Rl(1)) W = chi / f;
+      }
+      val = W * ylm_dot2<LMAX, Rl>(tb, vx * rinv, vy * rinv, vz * rinv, t,
+                                   XK + (size_t)nbj[b] * NLM);
     }
+    // same point twice in one warp instruction: sum in lane order first
+    const int key = valid ? n : G + lane;
+    const unsigned grp = __match_any_sync(0xffffffffu, key);
+    Rl s = val;
+    if (__any_sync(0xffffffffu, __popc(grp) > 1)) {
+      s = 0;
+      for (int src = 0; src < 32; ++src) {
+        Rl v = __shfl_sync(0xffffffffu, val, src);
+        if (grp & (1u << src)) s += v;
+      }
+    }
+    if (valid && lane == __ffs(grp) - 1) myacc[n] += s;
   }
   __syncthreads();
-  for (int n = threadIdx.x; n < G; n += blockDim.x) {
-    double s = acc[n];
+  for (int n = tid; n < G; n += 128) {
+    Rl sum = acc[n];
 #pragma unroll
-    for (int ww = 1; ww < NW; ++ww) s += acc[ww * G + n];
-    pot[(size_t)i * G + n] = s;
+    for (int ww = 1; ww < NW; ++ww) sum += acc[ww * G + n];
+    pot[(size_t)i * G + n] = sum;
   }
+}
+
+// K-scaled copy of X in (X_{l,m}, X_{l,-m}) pair layout, [N][NLM]
+template <class Rl>
+__global__ void k_xk(const YlmTables tb, int nsph, const double* __restrict__ X,
+                     typename RT<Rl>::V2* XK) {
+  const int nlm = (tb.lmax + 1) * (tb.lmax + 2) / 2;
+  long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (long long)nsph * nlm) return;
+  const int i = (int)(e / nlm), le = (int)(e - (long long)i * nlm);
+  int l = 0;
+  while (lmi(l + 1, 0) <= le) ++l;
+  const int m = le - lmi(l, 0), ind = l * l + l;
+  const double* Xi = X + (size_t)i * tb.nylm;
+  const double kk = tb.K[le];
+  XK[e] = mk2<Rl>((Rl)(kk * Xi[ind + m]), m ? (Rl)(kk * Xi[ind - m]) : Rl(0));
+}
+
+template <class Rl>
+size_t lx2_smem(int ngrid, int nbmax) {
+  return sizeof(Rl) * 4 * nbmax + sizeof(int) * ((nbmax + 3) & ~3) + sizeof(Rl) * 4 * ngrid;
 }
 
 #define DDC_LMAX_CASES(X) \
   X(0) X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12)
 
 cudaError_t launch_lx_pot(Launch L, const YlmTables& tb, const DevGeo& g, const double* X,
-                          double* pot, bool chi_only) {
+                          double* pot, bool chi_only, void* xk) {
   if (g.nsph == 0) return cudaSuccess;
-  const int NW = 4;
-  int nlm = (tb.lmax + 1) * (tb.lmax + 2) / 2;
-  size_t sm = sizeof(double) * NW * g.ngrid + sizeof(double2) * NW * nlm;
-  cudaError_t e = cudaSuccess;
+  size_t sm = lx2_smem<double>(g.ngrid, g.maxnb);
+  const long long nk = (long long)g.nsph * ((tb.lmax + 1) * (tb.lmax + 2) / 2);
+  double2* XK = static_cast<double2*>(xk);
+  k_xk<double><<<(unsigned)((nk + 255) / 256), 256, 0, L.st>>>(tb, g.nsph, X, XK);
+  ++*L.launches;
+  cudaError_t e = cudaGetLastError();
+  if (e) return e;
 #define CASE(LV)                                                                              \
   case LV: {                                                                                  \
-    auto kfn = chi_only ? k_lx_pot<LV, true> : k_lx_pot<LV, false>;                           \
-    if (sm > 48 * 1024)                                                                       \
-      if ((e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize,        \
-                                    (int)sm)))                                                \
-        return e;                                                                             \
-    kfn<<<g.nsph, 128, sm, L.st>>>(tb, g, X, pot);                                            \
+    auto kfn = chi_only ? k_lx2<LV, true, double> : k_lx2<LV, false, double>;                 \
+    if ((e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm))) \
+      return e;                                                                               \
+    kfn<<<g.nsph, 128, sm, L.st>>>(tb, g, XK, pot);                                           \
     break;                                                                                    \
   }
   switch (tb.lmax) {
@@ -604,16 +752,6 @@ cudaError_t launch_lx_pot(Launch L, const YlmTables& tb, const DevGeo& g, const 
 // At the end each role reduces its accumulators across its 32 lanes with a
 // fixed shuffle tree.  No atomics: the result is bit-reproducible.
 // ---------------------------------------------------------------------------
-template <class Rl> __device__ __forceinline__ Rl cA(const YlmTables& tb, int e);
-template <> __device__ __forceinline__ double cA<double>(const YlmTables& tb, int e) { return tb.A[e]; }
-template <> __device__ __forceinline__ float cA<float>(const YlmTables& tb, int e) { return tb.Af[e]; }
-template <class Rl> __device__ __forceinline__ Rl cB(const YlmTables& tb, int e);
-template <> __device__ __forceinline__ double cB<double>(const YlmTables& tb, int e) { return tb.B[e]; }
-template <> __device__ __forceinline__ float cB<float>(const YlmTables& tb, int e) { return tb.Bf[e]; }
-template <class Rl> __device__ __forceinline__ Rl cK(const YlmTables& tb, int e);
-template <> __device__ __forceinline__ double cK<double>(const YlmTables& tb, int e) { return tb.K[e]; }
-template <> __device__ __forceinline__ float cK<float>(const YlmTables& tb, int e) { return tb.Kf[e]; }
-
 __host__ __device__ constexpr int ls_nroles(int L) { return L / 2 + 1; }
 __host__ __device__ constexpr int ls_col2(int L, int r) { return L - r; }  // second column
 __host__ __device__ constexpr bool ls_has2(int L, int r) { return L - r > r; }
@@ -729,7 +867,8 @@ __global__ void __launch_bounds__(32 * ls_nroles(LMAX)) k_lstarx(const YlmTables
                                                                   const double* __restrict__ xi,
                                                                   double* y) {
   constexpr int NR = ls_nroles(LMAX);
-  constexpr int CH = 32 * NR;  // triples per chunk = threads per block
+  constexpr int NT = 32 * NR;  // threads per block
+  constexpr int CH = NT;       // triples per chunk (one per thread in phase A)
   constexpr int NF = ls_nfields(LMAX);
   constexpr int NVM = ls_max_nvals(LMAX);
   extern __shared__ double sh[];  // [NF][CH]
@@ -748,8 +887,8 @@ __global__ void __launch_bounds__(32 * ls_nroles(LMAX)) k_lstarx(const YlmTables
   for (int c0 = q0; c0 < q1; c0 += CH) {
     const int chunk = min(CH, q1 - c0);
     // phase A: one triple per thread
-    const int q = c0 + threadIdx.x;
-    if (threadIdx.x < chunk) {
+    for (int tt = threadIdx.x; tt < chunk; tt += NT) {
+      const int q = c0 + tt;
       const int2 jn = g.ls[q];
       const int j = jn.x, n = jn.y;
       const double4 cj = g.sph[j];
@@ -766,7 +905,7 @@ __global__ void __launch_bounds__(32 * ls_nroles(LMAX)) k_lstarx(const YlmTables
       double f = g.fi[pj];
       double W = f > 1.0 ? chi / f : chi;
       const double st = a.s * t;
-      double* col = sh + threadIdx.x;
+      double* col = sh + tt;
       col[0] = a.c * t;
       col[CH] = t * t;
       double pmm = gn.w * xi[pj] * W;
@@ -1232,6 +1371,83 @@ __global__ void k_efield_reduce(int ntrg, int nchunk, const double* __restrict__
   for (int c = 0; c < nchunk; ++c) s += scratch[(size_t)c * 3 * ntrg + e];
   ef[e] = s;
 }
+// FP32-pair variant (mixed precision, force terms only): coordinates are
+// taken relative to the block's first target in FP64 and rounded once to
+// FP32; each 256-source tile is summed in FP32 and added to FP64
+// accumulators.  Same chunked partial-sum layout as k_efield.
+__global__ void __launch_bounds__(kNbTile) k_efield_f(int nsrc, const double* __restrict__ q,
+                                                      const double* __restrict__ csrc, int ntrg,
+                                                      const double* __restrict__ ctrg, int chunk,
+                                                      double* out) {
+  __shared__ float4 src[kNbTile];
+  __shared__ double org[3];
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = blockIdx.y;
+  if (threadIdx.x == 0) {
+    int t0 = blockIdx.x * blockDim.x;
+    org[0] = ctrg[3 * (size_t)t0];
+    org[1] = ctrg[3 * (size_t)t0 + 1];
+    org[2] = ctrg[3 * (size_t)t0 + 2];
+  }
+  __syncthreads();
+  const double ox = org[0], oy = org[1], oz = org[2];
+  float px = 0.f, py = 0.f, pz = 0.f;
+  if (t < ntrg) {
+    px = (float)(ctrg[3 * (size_t)t] - ox);
+    py = (float)(ctrg[3 * (size_t)t + 1] - oy);
+    pz = (float)(ctrg[3 * (size_t)t + 2] - oz);
+  }
+  double ex = 0.0, ey = 0.0, ez = 0.0;
+  const int s0 = c * chunk, s1 = min(nsrc, s0 + chunk);
+  for (int j0 = s0; j0 < s1; j0 += kNbTile) {
+    int j = j0 + threadIdx.x;
+    __syncthreads();
+    src[threadIdx.x] = j < s1 ? make_float4((float)(csrc[3 * (size_t)j] - ox),
+                                            (float)(csrc[3 * (size_t)j + 1] - oy),
+                                            (float)(csrc[3 * (size_t)j + 2] - oz), (float)q[j])
+                              : make_float4(0.f, 0.f, 0.f, 0.f);
+    __syncthreads();
+    int cnt = min(kNbTile, s1 - j0);
+    float fx = 0.f, fy = 0.f, fz = 0.f;
+#pragma unroll 8
+    for (int k = 0; k < cnt; ++k) {
+      float4 s = src[k];
+      float dx = px - s.x, dy = py - s.y, dz = pz - s.z;
+      float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+      float ri = rsqrtf(r2);
+      float f = s.w * (ri * ri * ri);
+      fx = fmaf(f, dx, fx);
+      fy = fmaf(f, dy, fy);
+      fz = fmaf(f, dz, fz);
+    }
+    ex += fx;
+    ey += fy;
+    ez += fz;
+  }
+  if (t < ntrg) {
+    double* o = out + ((size_t)c * ntrg + t) * 3;
+    o[0] = ex;
+    o[1] = ey;
+    o[2] = ez;
+  }
+}
+cudaError_t launch_efield_f32(Launch L, int nsrc, const double* q, const double* csrc, int ntrg,
+                              const double* ctrg, double* ef, double* scratch, int nchunk) {
+  if (ntrg == 0) return cudaSuccess;
+  int chunk = (nsrc + nchunk - 1) / max(nchunk, 1);
+  chunk = ((chunk + kNbTile - 1) / kNbTile) * kNbTile;
+  if (chunk == 0) chunk = kNbTile;
+  dim3 grid((ntrg + kNbTile - 1) / kNbTile, nchunk);
+  double* out = nchunk == 1 ? ef : scratch;
+  k_efield_f<<<grid, kNbTile, 0, L.st>>>(nsrc, q, csrc, ntrg, ctrg, chunk, out);
+  ++*L.launches;
+  cudaError_t e = cudaGetLastError();
+  if (e || nchunk == 1) return e;
+  k_efield_reduce<<<(unsigned)((3LL * ntrg + 255) / 256), 256, 0, L.st>>>(ntrg, nchunk, scratch, ef);
+  ++*L.launches;
+  return cudaGetLastError();
+}
+
 cudaError_t launch_efield(Launch L, int nsrc, const double* q, const double* csrc, int ntrg,
                           const double* ctrg, double* ef, double* scratch, int nchunk) {
   if (ntrg == 0) return cudaSuccess;
@@ -1368,60 +1584,27 @@ __device__ void dbasis_contract(const YlmTables& tb, double sx, double sy, doubl
   }
 }
 
+// Forces, kernel A: block per sphere i over its gather list, i.e. the
+// triples (j, n, i) with point n of neighbour j inside i.  fdoka(j)
+// (ddcosmo.f90:1436-1504) and fdokb(i) (:1511-1607) both contract
+// dbasis(s_n^ji) with sigma_i at such a triple, so alp and beta are computed
+// once per triple: the fdokb and fdoga-neighbour terms accumulate into
+// fxa(:,i), the fdoka term of sphere j goes to the per-triple slot fda(:,q).
+// fdokb's inner loop over k in N_j (:1575-1590) is u_chi(j,n) - chi_ji*beta
+// with u_chi = sum_k chi_jk intmlp_k (an extra k_lx pass on sigma).
 template <int LMAX>
-__global__ void __launch_bounds__(128) k_forces(const YlmTables tb, const DevGeo g,
-                                                const double* __restrict__ sigma,
-                                                const double* __restrict__ xs,
-                                                const double* __restrict__ uchi,
-                                                const double* __restrict__ phi, double fep,
-                                                double* fx) {
+__global__ void __launch_bounds__(128) k_forces_a(const YlmTables tb, const DevGeo g,
+                                                  const double* __restrict__ sigma,
+                                                  const double* __restrict__ xs,
+                                                  const double* __restrict__ uchi,
+                                                  const double* __restrict__ phi, double* fxa,
+                                                  double* fda) {
   const int i = blockIdx.x;
   const int G = g.ngrid, NY = g.nylm;
   const double4 ci = g.sph[i];
   const double eta = tb.eta, tlow = 1.0 - eta;
   double f0 = 0.0, f1 = 0.0, f2 = 0.0;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  // fdoka: triples (i, n, j) of the pair lists of sphere i
-  for (int k = g.inl[i] + w; k < g.inl[i + 1]; k += nw) {
-    const int j = g.nl[k];
-    const double4 cj = g.sph[j];
-    const double* sj = sigma + (size_t)j * NY;
-    for (int q = g.pn_ptr[k] + lane; q < g.pn_ptr[k + 1]; q += 32) {
-      const int n = g.pn[q];
-      const double4 gn = g.grid[n];
-      const size_t p = (size_t)i * G + n;
-      Rel r = rel_exact(ci, gn, cj);
-      double sx = r.vx / r.vv, sy = r.vy / r.vv, sz = r.vz / r.vv;
-      double alp[3], beta;
-      dbasis_contract<LMAX>(tb, sx, sy, sz, r.t, sj, alp, beta);
-      double xij = fsw_exact(r.t, eta), fi = g.fi[p], oij, fb;
-      if (fi > 1.0) {
-        oij = xij / fi;
-        fb = -oij / fi;
-      } else {
-        oij = xij;
-        fb = 0.0;
-      }
-      double fa = oij / cj.w;
-      double va0 = fa * alp[0] + beta * fb * g.zi[3 * p];
-      double va1 = fa * alp[1] + beta * fb * g.zi[3 * p + 1];
-      double va2 = fa * alp[2] + beta * fb * g.zi[3 * p + 2];
-      if (r.t > tlow) {
-        double f3 = beta * dfsw_exact(r.t, eta) / cj.w;
-        if (fi > 1.0) f3 = f3 / fi;
-        va0 += f3 * sx;
-        va1 += f3 * sy;
-        va2 += f3 * sz;
-      }
-      double c = gn.w * xs[p];
-      f0 -= c * va0;
-      f1 -= c * va1;
-      f2 -= c * va2;
-    }
-  }
-  // fdokb and the neighbour part of fdoga: triples (j, n, i), point n of j
-  // inside i.  The inner k-loop of fdokb (ddcosmo.f90:1575-1590) is
-  // sum_{k != i} chi_jk intmlp_k = uchi(j,n) - chi_ji * beta.
   const double* si = sigma + (size_t)i * NY;
   for (int q = g.ls_ptr[i] + threadIdx.x; q < g.ls_ptr[i + 1]; q += blockDim.x) {
     const int2 jn = g.ls[q];
@@ -1434,14 +1617,41 @@ __global__ void __launch_bounds__(128) k_forces(const YlmTables tb, const DevGeo
     double alp[3], beta;
     dbasis_contract<LMAX>(tb, sx, sy, sz, r.t, si, alp, beta);
     double xji = fsw_exact(r.t, eta), fj = g.fi[pj];
-    double oji = fj > 1.0 ? xji / fj : xji;
     double xij = xs[pj];
+    double dsw = (r.t > tlow) ? dfsw_exact(r.t, eta) : 0.0;
+    // fdoka term of sphere j at its point n (neighbour i): -w xi_j(n) va
+    {
+      double oij, fb;
+      if (fj > 1.0) {
+        oij = xji / fj;
+        fb = -oij / fj;
+      } else {
+        oij = xji;
+        fb = 0.0;
+      }
+      double fa = oij / ci.w;
+      double va0 = fa * alp[0] + beta * fb * g.zi[3 * pj];
+      double va1 = fa * alp[1] + beta * fb * g.zi[3 * pj + 1];
+      double va2 = fa * alp[2] + beta * fb * g.zi[3 * pj + 2];
+      if (r.t > tlow) {
+        double f3 = beta * dsw / ci.w;
+        if (fj > 1.0) f3 = f3 / fj;
+        va0 += f3 * sx;
+        va1 += f3 * sy;
+        va2 += f3 * sz;
+      }
+      double c = -gn.w * xij;
+      fda[3 * (size_t)q + 0] = c * va0;
+      fda[3 * (size_t)q + 1] = c * va1;
+      fda[3 * (size_t)q + 2] = c * va2;
+    }
+    // fdokb and the neighbour part of fdoga for sphere i
+    double oji = fj > 1.0 ? xji / fj : xji;
     double fa = oji / ci.w;
     double vb0 = fa * alp[0] * xij, vb1 = fa * alp[1] * xij, vb2 = fa * alp[2] * xij;
     double vc0 = 0.0, vc1 = 0.0, vc2 = 0.0;
     if (r.t > tlow) {
       double di, fac;
-      double dsw = dfsw_exact(r.t, eta);
       if (fj > 1.0) {
         di = 1.0 / fj;
         fac = di * xji;
@@ -1461,7 +1671,6 @@ __global__ void __launch_bounds__(128) k_forces(const YlmTables tb, const DevGeo
       vb0 += fb2 * xij * beta * sx;
       vb1 += fb2 * xij * beta * sy;
       vb2 += fb2 * xij * beta * sz;
-      // fdoga neighbour term: switch band and ui(n,j) > 0
       if (r.t < 1.0 && g.ui[pj] > 0.0) {
         int cidx = g.cavidx[pj];
         double ph = cidx >= 0 ? phi[cidx] : 0.0;
@@ -1475,19 +1684,6 @@ __global__ void __launch_bounds__(128) k_forces(const YlmTables tb, const DevGeo
     f1 += gn.w * (vb1 - vc1);
     f2 += gn.w * (vb2 - vc2);
   }
-  // fdoga point term: 0 < ui(n,i) < 1
-  for (int n = threadIdx.x; n < G; n += blockDim.x) {
-    const size_t p = (size_t)i * G + n;
-    double u = g.ui[p];
-    if (u > 0.0 && u < 1.0) {
-      double ph = phi[g.cavidx[p]];
-      double c = g.grid[n].w * ph * xs[p];
-      f0 -= c * g.zi[3 * p];
-      f1 -= c * g.zi[3 * p + 1];
-      f2 -= c * g.zi[3 * p + 2];
-    }
-  }
-  // block reduction in fixed order
   __shared__ double sh[3][4];
 #pragma unroll
   for (int o = 16; o >= 1; o >>= 1) {
@@ -1504,17 +1700,70 @@ __global__ void __launch_bounds__(128) k_forces(const YlmTables tb, const DevGeo
   if (threadIdx.x < 3) {
     double s = 0.0;
     for (int ww = 0; ww < nw; ++ww) s += sh[threadIdx.x][ww];
-    fx[3 * (size_t)i + threadIdx.x] = fep * s;
+    fxa[3 * (size_t)i + threadIdx.x] = s;
+  }
+}
+
+// Forces, kernel B: block per sphere j.  Sums the fdoka slots of j (its pair
+// lists, found through lsstart), the fdoga point term (0 < U < 1) and the
+// kernel-A part, in fixed order, and applies fep (forces_dd.f90:160-161).
+__global__ void __launch_bounds__(128) k_forces_b(const DevGeo g, const double* __restrict__ xs,
+                                                  const double* __restrict__ phi,
+                                                  const double* __restrict__ fxa,
+                                                  const double* __restrict__ fda,
+                                                  const int* __restrict__ lsstart, double fep,
+                                                  double* fx) {
+  const int j = blockIdx.x;
+  const int G = g.ngrid;
+  double f0 = 0.0, f1 = 0.0, f2 = 0.0;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int k = g.inl[j] + w; k < g.inl[j + 1]; k += nw) {
+    const int base = lsstart[k], cnt = g.pn_ptr[k + 1] - g.pn_ptr[k];
+    for (int t = lane; t < cnt; t += 32) {
+      const double* d = fda + 3 * (size_t)(base + t);
+      f0 += d[0];
+      f1 += d[1];
+      f2 += d[2];
+    }
+  }
+  for (int n = threadIdx.x; n < G; n += blockDim.x) {
+    const size_t p = (size_t)j * G + n;
+    double u = g.ui[p];
+    if (u > 0.0 && u < 1.0) {
+      double ph = phi[g.cavidx[p]];
+      double c = g.grid[n].w * ph * xs[p];
+      f0 -= c * g.zi[3 * p];
+      f1 -= c * g.zi[3 * p + 1];
+      f2 -= c * g.zi[3 * p + 2];
+    }
+  }
+  __shared__ double sh[3][4];
+#pragma unroll
+  for (int o = 16; o >= 1; o >>= 1) {
+    f0 += __shfl_xor_sync(0xffffffffu, f0, o);
+    f1 += __shfl_xor_sync(0xffffffffu, f1, o);
+    f2 += __shfl_xor_sync(0xffffffffu, f2, o);
+  }
+  if (lane == 0) {
+    sh[0][w] = f0;
+    sh[1][w] = f1;
+    sh[2][w] = f2;
+  }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    double s = fxa[3 * (size_t)j + threadIdx.x];
+    for (int ww = 0; ww < nw; ++ww) s += sh[threadIdx.x][ww];
+    fx[3 * (size_t)j + threadIdx.x] = fep * s;
   }
 }
 
 cudaError_t launch_forces(Launch L, const YlmTables& tb, const DevGeo& g, const double* sigma,
                           const double* s_xi, const double* u_chi, const double* phi,
-                          double fep, double* fx) {
+                          double fep, double* fx, double* fxa, double* fda) {
   if (g.nsph == 0) return cudaSuccess;
 #define CASE(LV)                                                                               \
   case LV:                                                                                     \
-    k_forces<LV><<<g.nsph, 128, 0, L.st>>>(tb, g, sigma, s_xi, u_chi, phi, fep, fx);           \
+    k_forces_a<LV><<<g.nsph, 128, 0, L.st>>>(tb, g, sigma, s_xi, u_chi, phi, fxa, fda);        \
     break;
   switch (tb.lmax) {
     DDC_LMAX_CASES(CASE)
@@ -1522,6 +1771,10 @@ cudaError_t launch_forces(Launch L, const YlmTables& tb, const DevGeo& g, const 
       return cudaErrorInvalidValue;
   }
 #undef CASE
+  ++*L.launches;
+  cudaError_t e = cudaGetLastError();
+  if (e) return e;
+  k_forces_b<<<g.nsph, 128, 0, L.st>>>(g, s_xi, phi, fxa, fda, g.lsstart, fep, fx);
   ++*L.launches;
   return cudaGetLastError();
 }
@@ -1675,80 +1928,22 @@ __device__ __forceinline__ float ylm_dot_f(const YlmTables& tb, const AnglesF& a
   return acc;
 }
 
-template <int LMAX>
-__global__ void __launch_bounds__(128) k_lx_pot_f(const YlmTables tb, const DevGeo g,
-                                                  const double* __restrict__ X, float* pot) {
-  constexpr int NLM = (LMAX + 1) * (LMAX + 2) / 2;
-  constexpr int NW = 4;
-  extern __shared__ float smf[];
-  const int G = g.ngrid;
-  float* acc = smf;                                          // [NW][G]
-  float2* xs = reinterpret_cast<float2*>(smf + ((NW * G + 1) & ~1));  // [NW][NLM]
-  const int i = blockIdx.x, w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int q = threadIdx.x; q < NW * G; q += blockDim.x) acc[q] = 0.f;
-  __syncthreads();
-  const double4 ci = g.sph[i];
-  const float ri = (float)ci.w;
-  const float eta = (float)tb.eta, flow = 1.f - eta;
-  const float fa = 15.f * eta - 12.f, fb = 10.f * eta * eta - 15.f * eta + 6.f;
-  const float ie5 = (float)(1.0 / (tb.eta * tb.eta * tb.eta * tb.eta * tb.eta));
-  float* myacc = acc + w * G;
-  float2* myxs = xs + w * NLM;
-  const int k0 = g.inl[i], k1 = g.inl[i + 1];
-  for (int k = k0 + w; k < k1; k += NW) {
-    const int j = g.nl[k];
-    const double* Xj = X + (size_t)j * g.nylm;
-    __syncwarp();
-    for (int e = lane; e < NLM; e += 32) {
-      int l = 0;
-      while (lmi(l + 1, 0) <= e) ++l;
-      int m = e - lmi(l, 0);
-      int ind = l * l + l;
-      double kk = tb.K[e];
-      myxs[e] = make_float2((float)(kk * Xj[ind + m]), m ? (float)(kk * Xj[ind - m]) : 0.f);
-    }
-    __syncwarp();
-    const double4 cj = g.sph[j];
-    const float dx = (float)(ci.x - cj.x), dy = (float)(ci.y - cj.y), dz = (float)(ci.z - cj.z);
-    const float irj = (float)(1.0 / cj.w);
-    const int q0 = g.pn_ptr[k], q1 = g.pn_ptr[k + 1];
-    for (int q = q0 + lane; q < q1; q += 32) {
-      const int n = g.pn[q];
-      const float4 gn = g.gridf[n];
-      float vx = fmaf(ri, gn.x, dx), vy = fmaf(ri, gn.y, dy), vz = fmaf(ri, gn.z, dz);
-      float r2 = vx * vx + vy * vy + vz * vz;
-      float rinv = rsqrtf(r2);
-      float t = r2 * rinv * irj;
-      AnglesF a = angles_of_f(vx * rinv, vy * rinv, vz * rinv);
-      float chi = fsw_f(t, eta, flow, fa, fb, ie5);
-      float f = (float)g.fi[(size_t)i * G + n];
-      float W = f > 1.f ? chi / f : chi;
-      myacc[n] += W * ylm_dot_f<LMAX>(tb, a, t, myxs);
-    }
-  }
-  __syncthreads();
-  for (int n = threadIdx.x; n < G; n += blockDim.x) {
-    float s = acc[n];
-#pragma unroll
-    for (int ww = 1; ww < NW; ++ww) s += acc[ww * G + n];
-    pot[(size_t)i * G + n] = s;
-  }
-}
-
 cudaError_t launch_lx_pot_f32(Launch L, const YlmTables& tb, const DevGeo& g, const double* X,
-                              float* pot) {
+                              float* pot, void* xk) {
   if (g.nsph == 0) return cudaSuccess;
-  const int NW = 4;
-  int nlm = (tb.lmax + 1) * (tb.lmax + 2) / 2;
-  size_t sm = sizeof(float) * (((size_t)NW * g.ngrid + 1) & ~(size_t)1) + sizeof(float2) * NW * nlm;
-  cudaError_t e = cudaSuccess;
+  size_t sm = lx2_smem<float>(g.ngrid, g.maxnb);
+  const long long nk = (long long)g.nsph * ((tb.lmax + 1) * (tb.lmax + 2) / 2);
+  float2* XK = static_cast<float2*>(xk);
+  k_xk<float><<<(unsigned)((nk + 255) / 256), 256, 0, L.st>>>(tb, g.nsph, X, XK);
+  ++*L.launches;
+  cudaError_t e = cudaGetLastError();
+  if (e) return e;
 #define CASE(LV)                                                                              \
   case LV: {                                                                                  \
-    if (sm > 48 * 1024)                                                                       \
-      if ((e = cudaFuncSetAttribute(k_lx_pot_f<LV>,                                           \
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)))   \
-        return e;                                                                             \
-    k_lx_pot_f<LV><<<g.nsph, 128, sm, L.st>>>(tb, g, X, pot);                                 \
+    if ((e = cudaFuncSetAttribute(k_lx2<LV, false, float>,                                    \
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)))     \
+      return e;                                                                               \
+    k_lx2<LV, false, float><<<g.nsph, 128, sm, L.st>>>(tb, g, XK, pot);                       \
     break;                                                                                    \
   }
   switch (tb.lmax) {
@@ -1767,7 +1962,8 @@ __global__ void __launch_bounds__(32 * ls_nroles(LMAX)) k_lstarx_f(const YlmTabl
                                                                     const float* __restrict__ xi,
                                                                     double* y) {
   constexpr int NR = ls_nroles(LMAX);
-  constexpr int CH = 32 * NR;
+  constexpr int NT = 32 * NR;
+  constexpr int CH = NT;
   constexpr int NVM = ls_max_nvals(LMAX);
   extern __shared__ float shf[];  // [NF][CH]
   const int i = blockIdx.x;
@@ -1784,8 +1980,8 @@ __global__ void __launch_bounds__(32 * ls_nroles(LMAX)) k_lstarx_f(const YlmTabl
   const int q0 = g.ls_ptr[i], q1 = g.ls_ptr[i + 1];
   for (int c0 = q0; c0 < q1; c0 += CH) {
     const int chunk = min(CH, q1 - c0);
-    const int q = c0 + threadIdx.x;
-    if (threadIdx.x < chunk) {
+    for (int tt = threadIdx.x; tt < chunk; tt += NT) {
+      const int q = c0 + tt;
       const int2 jn = g.ls[q];
       const int j = jn.x, n = jn.y;
       const double4 cj = g.sph[j];
@@ -1803,7 +1999,7 @@ __global__ void __launch_bounds__(32 * ls_nroles(LMAX)) k_lstarx_f(const YlmTabl
       float f = (float)g.fi[pj];
       float W = f > 1.f ? chi / f : chi;
       const float st = a.s * t;
-      float* col = shf + threadIdx.x;
+      float* col = shf + tt;
       col[0] = a.c * t;
       col[CH] = t * t;
       float pmm = gn.w * xi[pj] * W;
