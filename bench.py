@@ -224,6 +224,38 @@ def _oracle_fixture():
         return None
 
 
+def measure_batch(dev, stream):
+    """The batched workload: 256 uneven globules solved in one library call
+    (FP64, per-molecule Jacobi/DIIS).  One warm-up call, one timed call."""
+    import torch
+    from ddpcm_b200 import molecules as M
+    from ddpcm_b200.ddcosmo import DDCosmo
+    bc = M.BATCH_CONFIG
+    mols = [M.to_bohr(m) for m in M.batch_molecules(bc["count"], bc["lo"], bc["hi"], bc["seed"])]
+    with DDCosmo(lmax=bc["lmax"], ngrid=bc["ngrid"], iconv=bc["iconv"], eps=bc["eps"],
+                 eta=bc["eta"], stream=stream.cuda_stream) as db:
+        db.batch_energy_forces(mols)
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        out = db.batch_energy_forces(mols)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        ms = e0.elapsed_time(e1)
+    it = out["iters"]
+    sizes = [len(m["q"]) for m in mols]
+    return {"workload": f"{bc['count']} globules, N log-uniform [{bc['lo']}, {bc['hi']}] "
+                        f"(total {sum(sizes)} spheres), lmax={bc['lmax']} ngrid={bc['ngrid']} "
+                        f"eta={bc['eta']} tol=1e-{bc['iconv']}, energy+forces, FP64",
+            "solves_per_s": bc["count"] / (ms * 1e-3), "ms_per_batch": ms,
+            "iterations_direct": {"min": int(it[:, 0].min()), "median": float(np.median(it[:, 0])),
+                                  "max": int(it[:, 0].max())},
+            "iterations_adjoint": {"min": int(it[:, 1].min()),
+                                   "median": float(np.median(it[:, 1])),
+                                   "max": int(it[:, 1].max())},
+            "host_arrays": True}
+
+
 def run_ours(args):
     import torch
 
@@ -316,6 +348,10 @@ def run_ours(args):
         for v in variants.values():
             v["speedup_vs_fp64_zero_guess"] = base / v["ms_per_solve"]
 
+    batch = None
+    if not args.no_batch and world == 1:
+        batch = measure_batch(dev, stream)
+
     if args.no_e2e:
         dd.close()
         if rank == 0:
@@ -389,7 +425,7 @@ def run_ours(args):
             "sizes": {k: info[k] for k in ("nsph", "ncav", "nylm", "ngrid", "ntriples",
                                            "npairs")},
             "esolv_hartree": info["esolv"], "error_vs_fp64_oracle": acc_head,
-            "variants": variants,
+            "variants": variants, "batch": batch,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e / args.steps},
             "gpu_launches": launches, "stage_ms_per_step": stage_ms,
@@ -529,6 +565,8 @@ def main():
                     help="molecule configuration (2: the benchmark workload)")
     ap.add_argument("--no-variants", action="store_true",
                     help="skip the comparison variants (plain FP64, zero guess)")
+    ap.add_argument("--no-batch", action="store_true",
+                    help="skip the batched-molecules measurement")
     ap.add_argument("--no-e2e", action="store_true",
                     help="time only the device-resident step (profiling runs)")
     args = ap.parse_args()

@@ -146,6 +146,14 @@ struct ddc_ctx {
   // geometry
   DBuf sph, grid, basis, bw, fi, ui, zi, inl, nl, rev, pn_ptr, pn, pn_pair, ls_ptr, ls, ntri_pt;
   DBuf lsstart, fxa, fda, xk;
+  // batched molecules: partition, per-target N-body ranges, per-molecule DIIS state
+  int nmol = 1;
+  bool batch_init = false;  // set while ddc_batch_energy_forces initialises
+  bool capturing = false;   // stream capture in progress: no stage events
+  std::vector<int> h_off;
+  DBuf d_off, mrange, tr_cav, tr_nuc, b_nmat, b_slot, b_B, b_status, b_iters, b_restarts, b_norm,
+      b_out;
+  const int2* mrange_ptr() const { return nmol > 1 ? mrange.as<int2>() : nullptr; }
   int maxnb = 0;
   DBuf cavoff, cavidx, cavpt, ccav, cnt, scan_tmp;
   DBuf csph, cx, cy, cz;  // csph(3,n) and SoA centres
@@ -278,7 +286,7 @@ struct StageScope {
     return e;
   }
   StageScope(ddc_ctx* ctx, int s) : c(ctx), stage(s) {
-    if (!c->prm.timing) return;
+    if (!c->prm.timing || c->capturing) return;
     a = take();
     b = take();
     if (a && b) cudaEventRecord(a, c->st);
@@ -371,7 +379,8 @@ int do_init(ddc_ctx* ctx, int n, const std::vector<double4>* hsph, const double4
   CK(ctx->cnt.ensure(sizeof(int) * (scan_n + 1)));
   CK(ctx->inl.ensure(sizeof(int) * (N + 1)));
   CK(cudaMemsetAsync(ctx->cnt.p, 0, sizeof(int) * (N + 1), ctx->st));
-  if (N > 0) CK(launch_csr_count(L, N, ctx->sph.as<double4>(), ctx->cnt.as<int>()));
+  if (N > 0)
+    CK(launch_csr_count(L, N, ctx->sph.as<double4>(), ctx->cnt.as<int>(), ctx->mrange_ptr()));
   size_t tb_bytes = scan_temp_bytes(N);
   CK(ctx->scan_tmp.ensure(tb_bytes));
   CK(scan_exclusive(L, ctx->cnt.as<int>(), ctx->inl.as<int>(), N, ctx->scan_tmp.p, tb_bytes));
@@ -398,7 +407,8 @@ int do_init(ddc_ctx* ctx, int n, const std::vector<double4>* hsph, const double4
                                                 std::to_string(mx) + ")");
   }
   if (N > 0) {
-    CK(launch_csr_fill(L, N, ctx->sph.as<double4>(), ctx->inl.as<int>(), ctx->nl.as<int>()));
+    CK(launch_csr_fill(L, N, ctx->sph.as<double4>(), ctx->inl.as<int>(), ctx->nl.as<int>(),
+                       ctx->mrange_ptr()));
     CK(launch_csr_rev(L, N, ctx->inl.as<int>(), ctx->nl.as<int>(), ctx->rev.as<int>()));
   }
   // fi, ui, zi
@@ -854,6 +864,136 @@ int forces_dev(ddc_ctx* ctx, const double* phi, const double* sigma, const doubl
 
 }  // namespace
 
+// Batched Jacobi/DIIS: every molecule runs the reference's algorithm on its
+// own segment of the concatenated vectors (own history, Gram matrix,
+// restarts and convergence test); one fused kernel per iteration does the
+// Jacobi step, Gram row, bordered solve, extrapolation and norm for all
+// molecules, a converged molecule's block returns at once.  iters receives
+// the per-molecule iteration counts.
+int batch_solve(ddc_ctx* ctx, bool adjoint, const double* rhs, double* x, int* iters,
+                ddc_solve_info* inf) {
+  const double t0 = now_s();
+  const int nmol = ctx->nmol, nd = std::max(ctx->prm.ndiis, 11);
+  if (ctx->prm.ndiis == 0) return fail(ctx, DDC_ERR_UNSUPPORTED, "batched solves need DIIS");
+  std::vector<int> nmat(nmol, 1), slot((size_t)nmol * nd), zero(nmol, 0);
+  for (int k = 0; k < nmol; k++)
+    for (int j = 0; j < nd; j++) slot[(size_t)k * nd + j] = j;
+  std::vector<int> status(nmol, 0);
+  for (int k = 0; k < nmol; k++)
+    if (ctx->h_off[k + 1] == ctx->h_off[k]) status[k] = 1;  // empty molecule
+  const size_t lenb = nd + 1;
+  CK(ctx->b_nmat.ensure(sizeof(int) * nmol));
+  CK(ctx->b_slot.ensure(sizeof(int) * nmol * nd));
+  CK(ctx->b_B.ensure(sizeof(double) * nmol * lenb * lenb));
+  CK(ctx->b_status.ensure(sizeof(int) * nmol));
+  CK(ctx->b_iters.ensure(sizeof(int) * nmol));
+  CK(ctx->b_restarts.ensure(sizeof(int) * nmol));
+  CK(ctx->b_norm.ensure(sizeof(double) * nmol));
+  CK(cudaMemcpyAsync(ctx->b_nmat.p, nmat.data(), sizeof(int) * nmol, cudaMemcpyHostToDevice,
+                     ctx->st));
+  CK(cudaMemcpyAsync(ctx->b_slot.p, slot.data(), sizeof(int) * nmol * nd, cudaMemcpyHostToDevice,
+                     ctx->st));
+  CK(cudaMemsetAsync(ctx->b_B.p, 0, sizeof(double) * nmol * lenb * lenb, ctx->st));
+  CK(cudaMemcpyAsync(ctx->b_status.p, status.data(), sizeof(int) * nmol, cudaMemcpyHostToDevice,
+                     ctx->st));
+  CK(cudaMemsetAsync(ctx->b_iters.p, 0, sizeof(int) * nmol, ctx->st));
+  CK(cudaMemsetAsync(ctx->b_restarts.p, 0, sizeof(int) * nmol, ctx->st));
+  BatchState bs;
+  bs.nmol = nmol;
+  bs.ndiis = nd;
+  bs.max_iter = ctx->prm.max_iter;
+  bs.tol = std::pow(10.0, -(double)ctx->prm.iconv);
+  bs.n_total = (long long)ctx->nsph * ctx->nylm;
+  bs.off = ctx->d_off.as<int>();
+  bs.nmat = ctx->b_nmat.as<int>();
+  bs.slot = ctx->b_slot.as<int>();
+  bs.B = ctx->b_B.as<double>();
+  bs.status = ctx->b_status.as<int>();
+  bs.iters = ctx->b_iters.as<int>();
+  bs.restarts = ctx->b_restarts.as<int>();
+  bs.norm = ctx->b_norm.as<double>();
+  bs.hx = ctx->hist_x.as<double>();
+  bs.he = ctx->hist_e.as<double>();
+  OpFn op = adjoint ? op_lstarx : op_lx;
+  double* y = ctx->y.as<double>();
+  // CUDA graph of `check` sweeps (operator kernels + fused DIIS kernel),
+  // captured once and replayed until every molecule has stopped; a
+  // stopped molecule's DIIS block returns at once, so extra sweeps are
+  // harmless.
+  const int check = 4;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  CK(cudaStreamSynchronize(ctx->st));
+  ctx->capturing = true;
+  cudaError_t ce = cudaStreamBeginCapture(ctx->st, cudaStreamCaptureModeThreadLocal);
+  int orc = DDC_OK;
+  if (ce == cudaSuccess) {
+    for (int r = 0; r < check && orc == DDC_OK; r++) {
+      orc = op(ctx, x, y);
+      if (orc == DDC_OK && launch_batch_diis(ctx->L(), ctx->tb, bs, rhs, y, x) != cudaSuccess)
+        orc = DDC_ERR_CUDA;
+    }
+    cudaError_t ee = cudaStreamEndCapture(ctx->st, &graph);
+    if (ce == cudaSuccess) ce = ee;
+  }
+  ctx->capturing = false;
+  if (orc != DDC_OK) {
+    if (graph) cudaGraphDestroy(graph);
+    return orc;
+  }
+  CK(ce);
+  CK(cudaGraphInstantiate(&exec, graph, 0));
+  int it = 0, active = nmol;
+  cudaError_t ge = cudaSuccess;
+  while (it < ctx->prm.max_iter && active > 0) {
+    {
+      StageScope sc(ctx, ST_COMBINE);
+      ge = cudaGraphLaunch(exec, ctx->st);
+    }
+    if (ge != cudaSuccess) break;
+    it += check;
+    CK(cudaMemcpyAsync(status.data(), ctx->b_status.p, sizeof(int) * nmol, cudaMemcpyDeviceToHost,
+                       ctx->st));
+    CKI(sync(ctx));
+    active = 0;
+    for (int k = 0; k < nmol; k++) active += status[k] == 0;
+  }
+  cudaGraphExecDestroy(exec);
+  cudaGraphDestroy(graph);
+  CK(ge);
+  std::vector<int> its(nmol), rst(nmol);
+  std::vector<double> nrm(nmol);
+  CK(cudaMemcpyAsync(status.data(), ctx->b_status.p, sizeof(int) * nmol, cudaMemcpyDeviceToHost,
+                     ctx->st));
+  CK(cudaMemcpyAsync(its.data(), ctx->b_iters.p, sizeof(int) * nmol, cudaMemcpyDeviceToHost,
+                     ctx->st));
+  CK(cudaMemcpyAsync(rst.data(), ctx->b_restarts.p, sizeof(int) * nmol, cudaMemcpyDeviceToHost,
+                     ctx->st));
+  CK(cudaMemcpyAsync(nrm.data(), ctx->b_norm.p, sizeof(double) * nmol, cudaMemcpyDeviceToHost,
+                     ctx->st));
+  CKI(sync(ctx));
+  int maxit = 0, nfail = 0, restarts = 0;
+  double worst = 0.0;
+  for (int k = 0; k < nmol; k++) {
+    if (iters) iters[k] = its[k];
+    maxit = std::max(maxit, its[k]);
+    restarts += rst[k];
+    if (status[k] != 1) nfail++;
+    if (ctx->h_off[k + 1] > ctx->h_off[k]) worst = std::max(worst, nrm[k]);
+  }
+  if (inf) {
+    memset(inf, 0, sizeof(*inf));
+    inf->iterations = maxit;
+    inf->converged = nfail == 0;
+    inf->diis_restarts = restarts;
+    inf->final_norm = worst;
+    inf->seconds = now_s() - t0;
+  }
+  if (nfail)
+    return fail(ctx, DDC_ERR_NOCONV, std::to_string(nfail) + " molecule(s) did not converge");
+  return DDC_OK;
+}
+
 // ===========================================================================
 // C ABI
 // ===========================================================================
@@ -1015,6 +1155,7 @@ int ddc_init(ddc_ctx* ctx, int n, const double* x, const double* y, const double
   }
   for (int i = 0; i < n; i++)
     if (!(hs[i].w > 0.0)) return fail(ctx, DDC_ERR_PARAM, "radii must be positive");
+  if (!ctx->batch_init) ctx->nmol = 1;
   int rc;
   {
     StageScope sc(ctx, ST_INIT);
@@ -1084,7 +1225,7 @@ int ddc_mkrhs(ddc_ctx* ctx, int n, const double* charge, const double* x, const 
   double *dphi, *dpsi;
   CKI(out_ptr(ctx, phi, ncav, ctx->phi, &dphi));
   CKI(out_ptr(ctx, psi, (size_t)n * nylm, ctx->out1, &dpsi));
-  CK(launch_coulomb_pot(ctx->L(), n, dq, dx, dy, dz, ncav, dc, dphi));
+  CK(launch_coulomb_pot(ctx->L(), n, dq, dx, dy, dz, ncav, dc, dphi, nullptr));
   CK(launch_psi(ctx->L(), n, nylm, dq, dpsi));
   CKI(finish_out(ctx, phi, dphi, ncav));
   CKI(finish_out(ctx, psi, dpsi, (size_t)n * nylm));
@@ -1193,7 +1334,7 @@ int ddc_efld(ddc_ctx* ctx, int nsrc, const double* src, const double* csrc, int 
   int nchunk = efield_chunks(nsrc, ntrg);
   CK(ctx->ef_scratch.ensure(sizeof(double) * 3 * (size_t)std::max(ntrg, 1) * nchunk));
   CK(launch_efield(ctx->L(), nsrc, dsrc, dcs, ntrg, dct, def, ctx->ef_scratch.as<double>(),
-                   nchunk));
+                   nchunk, nullptr));
   CKI(finish_out(ctx, ef, def, 3 * (size_t)ntrg));
   return sync(ctx);
 }
@@ -1272,7 +1413,7 @@ int ddc_energy_forces(ddc_ctx* ctx, int n, const double* charge, const double* x
   {
   StageScope sc(ctx, ST_COULOMB);
   CK(launch_coulomb_pot(ctx->L(), N, dq, ctx->cx.as<double>(), ctx->cy.as<double>(),
-                        ctx->cz.as<double>(), NC, ctx->ccav.as<double>(), dphi));
+                        ctx->cz.as<double>(), NC, ctx->ccav.as<double>(), dphi, nullptr));
   CK(launch_psi(ctx->L(), N, ctx->nylm, dq, dpsi));
   }
   CKI(sync(ctx));
@@ -1312,7 +1453,7 @@ int ddc_energy_forces(ddc_ctx* ctx, int n, const double* charge, const double* x
     {
       StageScope sc(ctx, ST_EFIELD);
       CK(efield(ctx->L(), N, dq, ctx->csph.as<double>(), NC, ctx->ccav.as<double>(),
-                ctx->ef1.as<double>(), ctx->ef_scratch.as<double>(), ch1));
+                ctx->ef1.as<double>(), ctx->ef_scratch.as<double>(), ch1, nullptr));
     }
     {
       StageScope sc(ctx, ST_CONTRACT);
@@ -1324,7 +1465,7 @@ int ddc_energy_forces(ddc_ctx* ctx, int n, const double* charge, const double* x
       StageScope sc(ctx, ST_EFIELD);
       CK(efield(ctx->L(), NC, ctx->zeta.as<double>(), ctx->ccav.as<double>(), N,
                 ctx->csph.as<double>(), ctx->ef2.as<double>(), ctx->ef_scratch.as<double>(),
-                ch2));
+                ch2, nullptr));
     }
     {
       StageScope sc(ctx, ST_CONTRACT);
@@ -1339,6 +1480,146 @@ int ddc_energy_forces(ddc_ctx* ctx, int n, const double* charge, const double* x
     CKI(finish_out(ctx, fx, dfx, 3 * (size_t)N));
   }
   CKI(sync(ctx));
+  inf->nsph = N;
+  inf->ncav = NC;
+  inf->nylm = ctx->nylm;
+  inf->ngrid = ctx->ngrid;
+  inf->ntriples = ctx->ntri;
+  inf->npairs = ctx->npair;
+  return DDC_OK;
+}
+
+
+int ddc_batch_energy_forces(ddc_ctx* ctx, int nmol, const int* off, const double* charge,
+                            const double* x, const double* y, const double* z,
+                            const double* rvdw, double* esolv, double* fx, int* iters,
+                            ddc_run_info* info) {
+  if (!ctx || nmol <= 0 || !off || !esolv) return DDC_ERR_PARAM;
+  if (ctx->prm.precision != DDC_PREC_FP64)
+    return fail(ctx, DDC_ERR_UNSUPPORTED, "batched solves run in FP64");
+  cudaSetDevice(ctx->prm.device);
+  if (off[0] != 0) return fail(ctx, DDC_ERR_PARAM, "off[0] must be 0");
+  for (int k = 0; k < nmol; k++)
+    if (off[k + 1] < off[k]) return fail(ctx, DDC_ERR_PARAM, "offsets must not decrease");
+  const int N = off[nmol];
+  ddc_run_info loc{};
+  ddc_run_info* inf = info ? info : &loc;
+  memset(inf, 0, sizeof(*inf));
+  double t0 = now_s();
+  // molecule partition: per-sphere index range of its molecule
+  ctx->nmol = nmol;
+  ctx->h_off.assign(off, off + nmol + 1);
+  {
+    std::vector<int2> mr(std::max(N, 1));
+    for (int k = 0; k < nmol; k++)
+      for (int i = off[k]; i < off[k + 1]; i++) mr[i] = make_int2(off[k], off[k + 1]);
+    CK(ctx->mrange.ensure(sizeof(int2) * std::max(N, 1)));
+    CK(cudaMemcpyAsync(ctx->mrange.p, mr.data(), sizeof(int2) * std::max(N, 1),
+                       cudaMemcpyHostToDevice, ctx->st));
+    CK(ctx->d_off.ensure(sizeof(int) * (nmol + 1)));
+    CK(cudaMemcpyAsync(ctx->d_off.p, off, sizeof(int) * (nmol + 1), cudaMemcpyHostToDevice,
+                       ctx->st));
+  }
+  ctx->batch_init = true;
+  int rc = ddc_init(ctx, N, x, y, z, rvdw);
+  ctx->batch_init = false;
+  if (rc != DDC_OK) {
+    ctx->nmol = 1;
+    return rc;
+  }
+  ctx->nmol = nmol;
+  double t1 = now_s();
+  inf->t_init = t1 - t0;
+  const int NC = ctx->ncav;
+  const size_t nv = (size_t)N * ctx->nylm;
+  CK(ctx->tr_cav.ensure(sizeof(int2) * std::max(NC, 1)));
+  CK(ctx->tr_nuc.ensure(sizeof(int2) * std::max(N, 1)));
+  CK(launch_batch_ranges(ctx->L(), N, ctx->ngrid, NC, ctx->mrange.as<int2>(), ctx->cavpt.as<int>(),
+                         ctx->cavoff.as<int>(), ctx->tr_cav.as<int2>(), ctx->tr_nuc.as<int2>()));
+  const double* dq;
+  CKI(stage_in(ctx, charge, N, ctx->q, &dq));
+  CK(ctx->phi.ensure(sizeof(double) * std::max(NC, 1)));
+  double* dphi = ctx->phi.as<double>();
+  double* dpsi = ctx->psi.as<double>();
+  {
+    StageScope sc(ctx, ST_COULOMB);
+    CK(launch_coulomb_pot(ctx->L(), N, dq, ctx->cx.as<double>(), ctx->cy.as<double>(),
+                          ctx->cz.as<double>(), NC, ctx->ccav.as<double>(), dphi,
+                          ctx->tr_cav.as<int2>()));
+    CK(launch_psi(ctx->L(), N, ctx->nylm, dq, dpsi));
+  }
+  CKI(sync(ctx));
+  double t2 = now_s();
+  inf->t_mkrhs = t2 - t1;
+  double* dsig = ctx->sigma.as<double>();
+  double* ds = ctx->s.as<double>();
+  const long long n = (long long)nv;
+  // direct solve
+  {
+    double* rhs = ctx->rhs.as<double>();
+    CK(ctx->gbuf.ensure(sizeof(double) * std::max<long long>((long long)N * ctx->ngrid, 1)));
+    {
+      StageScope sc(ctx, ST_RHS);
+      CK(launch_wghpot(ctx->L(), ctx->geo(), dphi, ctx->gbuf.as<double>()));
+      CK(launch_dgemm(ctx->L(), false, ctx->nylm, N, ctx->ngrid, 1.0, ctx->bw.as<double>(),
+                      ctx->nylm, ctx->gbuf.as<double>(), ctx->ngrid, 0.0, rhs, ctx->nylm));
+    }
+    CK(launch_guess(ctx->L(), ctx->tb, n, rhs, dsig, ctx->prm.guess == DDC_GUESS_ZERO ? 1 : 0));
+    std::vector<int> it(nmol);
+    CKI(batch_solve(ctx, false, rhs, dsig, it.data(), &inf->direct));
+    if (iters)
+      for (int k = 0; k < nmol; k++) iters[2 * k] = it[k];
+  }
+  CK(ctx->b_out.ensure(sizeof(double) * nmol));
+  const double fep = 0.5 * ((ctx->prm.eps - 1.0) / ctx->prm.eps);
+  CK(launch_batch_dot(ctx->L(), nmol, ctx->d_off.as<int>(), ctx->nylm, dsig, dpsi, fep,
+                      ctx->b_out.as<double>()));
+  CK(cudaMemcpyAsync(esolv, ctx->b_out.p, sizeof(double) * nmol, cudaMemcpyDeviceToHost, ctx->st));
+  CKI(sync(ctx));
+  double t3 = now_s();
+  inf->t_direct = t3 - t2;
+  if (ctx->prm.igrad) {
+    CK(launch_guess(ctx->L(), ctx->tb, n, dpsi, ds, ctx->prm.guess == DDC_GUESS_ZERO ? 1 : 0));
+    std::vector<int> it(nmol);
+    CKI(batch_solve(ctx, true, dpsi, ds, it.data(), &inf->adjoint));
+    if (iters)
+      for (int k = 0; k < nmol; k++) iters[2 * k + 1] = it[k];
+    double t4 = now_s();
+    inf->t_adjoint = t4 - t3;
+    CK(ctx->fx.ensure(sizeof(double) * 3 * std::max(N, 1)));
+    double* dfx = ctx->fx.as<double>();
+    CKI(forces_dev(ctx, dphi, dsig, ds, dfx));
+    CK(ctx->zeta.ensure(sizeof(double) * std::max(NC, 1)));
+    {
+      StageScope sc(ctx, ST_ZETA);
+      CK(launch_mkxi(ctx->L(), ctx->tb, ctx->geo(), ctx->xig.as<double>(), fep,
+                     ctx->zeta.as<double>()));
+    }
+    CKI(sync(ctx));
+    double t5 = now_s();
+    inf->t_forces = t5 - t4;
+    CK(ctx->ef1.ensure(sizeof(double) * 3 * std::max(NC, 1)));
+    CK(ctx->ef2.ensure(sizeof(double) * 3 * std::max(N, 1)));
+    CK(ctx->ef_scratch.ensure(sizeof(double) * 3 * std::max((size_t)NC, (size_t)N)));
+    {
+      StageScope sc(ctx, ST_EFIELD);
+      CK(launch_efield(ctx->L(), N, dq, ctx->csph.as<double>(), NC, ctx->ccav.as<double>(),
+                       ctx->ef1.as<double>(), ctx->ef_scratch.as<double>(), 1,
+                       ctx->tr_cav.as<int2>()));
+      CK(launch_efield(ctx->L(), NC, ctx->zeta.as<double>(), ctx->ccav.as<double>(), N,
+                       ctx->csph.as<double>(), ctx->ef2.as<double>(),
+                       ctx->ef_scratch.as<double>(), 1, ctx->tr_nuc.as<int2>()));
+    }
+    {
+      StageScope sc(ctx, ST_CONTRACT);
+      CK(launch_zeta_efld_contract(ctx->L(), ctx->geo(), ctx->zeta.as<double>(),
+                                   ctx->ef1.as<double>(), dfx));
+      CK(launch_charge_efld_contract(ctx->L(), N, dq, ctx->ef2.as<double>(), dfx));
+    }
+    CKI(finish_out(ctx, fx, dfx, 3 * (size_t)N));
+    CKI(sync(ctx));
+    inf->t_efld = now_s() - t5;
+  }
   inf->nsph = N;
   inf->ncav = NC;
   inf->nylm = ctx->nylm;

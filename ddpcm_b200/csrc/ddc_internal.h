@@ -86,6 +86,23 @@ struct HistPtrs {
   int n;
 };
 
+// Per-molecule Jacobi/DIIS state of a batched solve (device arrays).
+struct BatchState {
+  int nmol, ndiis, max_iter;
+  double tol;
+  long long n_total;  // length of the concatenated vectors
+  const int* off;     // [nmol+1] sphere offsets
+  int* nmat;          // [nmol]
+  int* slot;          // [nmol][ndiis] logical -> physical history slot
+  double* B;          // [nmol][(ndiis+1)^2] column-major bordered Gram matrix
+  int* status;        // [nmol]: 0 active, 1 converged, 2 max_iter, 3 non-finite
+  int* iters;         // [nmol]
+  int* restarts;      // [nmol]
+  double* norm;       // [nmol] last increment norm
+  double* hx;         // [ndiis][n_total]
+  double* he;         // [ndiis][n_total]
+};
+
 // ---------------------------------------------------------------------------
 // Kernel launchers (ddc_kernels.cu).  All run on `st` and return the CUDA
 // error of the launch.  `launches` is incremented per kernel launched.
@@ -98,8 +115,11 @@ struct Launch {
 // init
 cudaError_t launch_basis(Launch L, const YlmTables& tb, const double4* grid, double* basis,
                          double* bw);
-cudaError_t launch_csr_count(Launch L, int nsph, const double4* sph, int* cnt);
-cudaError_t launch_csr_fill(Launch L, int nsph, const double4* sph, const int* inl, int* nl);
+// mrange: per sphere, the index range of its molecule (nullptr: one molecule)
+cudaError_t launch_csr_count(Launch L, int nsph, const double4* sph, int* cnt,
+                             const int2* mrange);
+cudaError_t launch_csr_fill(Launch L, int nsph, const double4* sph, const int* inl, int* nl,
+                            const int2* mrange);
 cudaError_t launch_csr_rev(Launch L, int nsph, const int* inl, const int* nl, int* rev);
 cudaError_t launch_fiui(Launch L, const YlmTables& tb, int nsph, const double4* sph,
                         const double4* grid, const int* inl, const int* nl, double* fi, double* ui,
@@ -173,18 +193,21 @@ cudaError_t launch_reduce_partials(Launch L, const double* partials, int nblk, i
 int reduce_blocks();
 
 // electrostatics
+// trange: per target, the source index range it sums over (nullptr: all)
 cudaError_t launch_coulomb_pot(Launch L, int nsrc, const double* q, const double* sx,
                                const double* sy, const double* sz, int ntrg, const double* ctrg,
-                               double* phi);
+                               double* phi, const int2* trange);
 cudaError_t launch_psi(Launch L, int n, int nylm, const double* q, double* psi);
 // field of sources (q at csrc(3,nsrc)) at targets ctrg(3,ntrg); partial sums
 // over `nchunk` source chunks go to scratch[nchunk][ntrg][3]
 cudaError_t launch_efield(Launch L, int nsrc, const double* q, const double* csrc, int ntrg,
-                          const double* ctrg, double* ef, double* scratch, int nchunk);
+                          const double* ctrg, double* ef, double* scratch, int nchunk,
+                          const int2* trange);
 int efield_chunks(int nsrc, int ntrg);
 // FP32 pair arithmetic, FP64 accumulation (mixed-precision force terms)
 cudaError_t launch_efield_f32(Launch L, int nsrc, const double* q, const double* csrc, int ntrg,
-                              const double* ctrg, double* ef, double* scratch, int nchunk);
+                              const double* ctrg, double* ef, double* scratch, int nchunk,
+                              const int2* trange);
 
 // forces
 // fxa (3,N) and fda (3,T) are scratch of the two force kernels
@@ -197,6 +220,14 @@ cudaError_t launch_zeta_efld_contract(Launch L, const DevGeo& g, const double* z
                                       const double* ef, double* fx);
 cudaError_t launch_charge_efld_contract(Launch L, int n, const double* q, const double* ef,
                                         double* fx);
+// batched solves
+cudaError_t launch_batch_diis(Launch L, const YlmTables& tb, const BatchState& bs,
+                              const double* rhs, const double* y, double* x);
+cudaError_t launch_batch_dot(Launch L, int nmol, const int* off, int nylm, const double* a,
+                             const double* b, double scale, double* out);
+cudaError_t launch_batch_ranges(Launch L, int nsph, int ngrid, int ncav, const int2* mrange,
+                                const int* cavpt, const int* cavoff, int2* tr_cav, int2* tr_nuc);
+
 // FP64 FMA throughput probe: each thread runs `iters` x 8 independent FMA chains
 cudaError_t launch_fp64_probe(Launch L, int blocks, int iters, double* out);
 

@@ -162,16 +162,18 @@ __device__ __forceinline__ bool is_nb(double4 a, double4 b) {
 
 template <bool FILL>
 __global__ void k_csr(int nsph, const double4* __restrict__ sph, int* cnt, const int* inl,
-                      int* nl) {
+                      int* nl, const int2* __restrict__ mrange) {
   int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (warp >= nsph) return;
   const int i = warp;
   const double4 ci = sph[i];
   int base = FILL ? inl[i] : 0;
-  for (int j0 = 0; j0 < nsph; j0 += 32) {
+  // candidates: the sphere's own molecule (all spheres for a single molecule)
+  const int jlo = mrange ? mrange[i].x : 0, jhi = mrange ? mrange[i].y : nsph;
+  for (int j0 = jlo; j0 < jhi; j0 += 32) {
     int j = j0 + lane;
     bool nb = false;
-    if (j < nsph && j != i) nb = is_nb(ci, sph[j]);
+    if (j < jhi && j != i) nb = is_nb(ci, sph[j]);
     unsigned mask = __ballot_sync(0xffffffffu, nb);
     if (FILL && nb) nl[base + __popc(mask & ((1u << lane) - 1u))] = j;
     base += __popc(mask);
@@ -179,13 +181,15 @@ __global__ void k_csr(int nsph, const double4* __restrict__ sph, int* cnt, const
   if (!FILL && lane == 0) cnt[i] = base;
 }
 
-cudaError_t launch_csr_count(Launch L, int nsph, const double4* sph, int* cnt) {
-  k_csr<false><<<(nsph + 7) / 8, 256, 0, L.st>>>(nsph, sph, cnt, nullptr, nullptr);
+cudaError_t launch_csr_count(Launch L, int nsph, const double4* sph, int* cnt,
+                             const int2* mrange) {
+  k_csr<false><<<(nsph + 7) / 8, 256, 0, L.st>>>(nsph, sph, cnt, nullptr, nullptr, mrange);
   ++*L.launches;
   return cudaGetLastError();
 }
-cudaError_t launch_csr_fill(Launch L, int nsph, const double4* sph, const int* inl, int* nl) {
-  k_csr<true><<<(nsph + 7) / 8, 256, 0, L.st>>>(nsph, sph, nullptr, inl, nl);
+cudaError_t launch_csr_fill(Launch L, int nsph, const double4* sph, const int* inl, int* nl,
+                            const int2* mrange) {
+  k_csr<true><<<(nsph + 7) / 8, 256, 0, L.st>>>(nsph, sph, nullptr, inl, nl, mrange);
   ++*L.launches;
   return cudaGetLastError();
 }
@@ -1018,10 +1022,120 @@ __global__ void __launch_bounds__(256) k_dgemm(int M, int N, int K, double alpha
       }
     }
 }
+// Register-tiled GEMM, column-major C[M x N] = alpha * op(A) * B, used for
+// the projection (M = nylm <= 128 rows in one tile) and for xi.  BM x BN
+// tile per block, BK deep, TM x TN outputs per thread, shared tiles double
+// buffered with the next tile prefetched into registers.  Acc is the
+// arithmetic/accumulation type; inputs are converted when staged.
+template <bool TA, class TAin, class TBin, class TC, class Acc, int BM, int BN, int BK, int TM,
+          int TN>
+__global__ void __launch_bounds__((BM / TM) * (BN / TN)) k_gemm2(int M, int N, int K, Acc alpha,
+                                                                 const TAin* __restrict__ A,
+                                                                 int lda,
+                                                                 const TBin* __restrict__ B,
+                                                                 int ldb, TC* C, int ldc) {
+  constexpr int NT = (BM / TM) * (BN / TN);
+  constexpr int NA = BM * BK / NT, NB = BK * BN / NT;  // staged elements per thread
+  __shared__ __align__(16) Acc As[2][BK][BM];
+  __shared__ __align__(16) Acc Bs[2][BK][BN];
+  const int tx = threadIdx.x % (BN / TN), ty = threadIdx.x / (BN / TN);
+  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+  Acc ra[NA], rb[NB];
+  auto fetch = [&](int k0) {
+#pragma unroll
+    for (int u = 0; u < NA; ++u) {
+      const int e = threadIdx.x + u * NT;
+      int mm, kk;
+      if (TA) { kk = e % BK; mm = e / BK; } else { mm = e % BM; kk = e / BM; }
+      const int m = m0 + mm, k = k0 + kk;
+      Acc v = 0;
+      if (m < M && k < K) v = (Acc)(TA ? A[(size_t)m * lda + k] : A[(size_t)k * lda + m]);
+      ra[u] = v;
+    }
+#pragma unroll
+    for (int u = 0; u < NB; ++u) {
+      const int e = threadIdx.x + u * NT;
+      const int kk = e % BK, nn = e / BK;
+      const int n = n0 + nn, k = k0 + kk;
+      rb[u] = (n < N && k < K) ? (Acc)B[(size_t)n * ldb + k] : Acc(0);
+    }
+  };
+  auto stash = [&](int buf) {
+#pragma unroll
+    for (int u = 0; u < NA; ++u) {
+      const int e = threadIdx.x + u * NT;
+      int mm, kk;
+      if (TA) { kk = e % BK; mm = e / BK; } else { mm = e % BM; kk = e / BM; }
+      As[buf][kk][mm] = ra[u];
+    }
+#pragma unroll
+    for (int u = 0; u < NB; ++u) {
+      const int e = threadIdx.x + u * NT;
+      Bs[buf][e % BK][e / BK] = rb[u];
+    }
+  };
+  Acc acc[TM][TN];
+#pragma unroll
+  for (int a = 0; a < TM; ++a)
+#pragma unroll
+    for (int b = 0; b < TN; ++b) acc[a][b] = 0;
+  fetch(0);
+  stash(0);
+  __syncthreads();
+  int buf = 0;
+  for (int k0 = 0; k0 < K; k0 += BK) {
+    const bool more = k0 + BK < K;
+    if (more) fetch(k0 + BK);
+#pragma unroll
+    for (int kk = 0; kk < BK; ++kk) {
+      Acc a[TM], b[TN];
+#pragma unroll
+      for (int r = 0; r < TM; ++r) a[r] = As[buf][kk][ty * TM + r];
+#pragma unroll
+      for (int c = 0; c < TN; ++c) b[c] = Bs[buf][kk][tx * TN + c];
+#pragma unroll
+      for (int r = 0; r < TM; ++r)
+#pragma unroll
+        for (int c = 0; c < TN; ++c) acc[r][c] = fma(a[r], b[c], acc[r][c]);
+    }
+    if (more) {
+      stash(buf ^ 1);
+      __syncthreads();
+      buf ^= 1;
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < TM; ++r)
+#pragma unroll
+    for (int c = 0; c < TN; ++c) {
+      const int m = m0 + ty * TM + r, n = n0 + tx * TN + c;
+      if (m < M && n < N) C[(size_t)n * ldc + m] = (TC)(alpha * acc[r][c]);
+    }
+}
+
+template <bool TA, class TAin, class TBin, class TC, class Acc>
+cudaError_t gemm2(Launch L, int M, int N, int K, Acc alpha, const TAin* A, int lda, const TBin* B,
+                  int ldb, TC* C, int ldc) {
+  if (M == 0 || N == 0) return cudaSuccess;
+  // FP32: 128x64 tiles, 8x4 per thread; FP64: 128x32 tiles, 8x2 per thread
+  constexpr bool D = sizeof(Acc) == 8;
+  constexpr int BM = 128, BN = D ? 32 : 64, TM = 8, TN = D ? 2 : 4, BK = D ? 8 : 16;
+  dim3 grid((M + BM - 1) / BM, (N + BN - 1) / BN);
+  k_gemm2<TA, TAin, TBin, TC, Acc, BM, BN, BK, TM, TN>
+      <<<grid, (BM / TM) * (BN / TN), 0, L.st>>>(M, N, K, alpha, A, lda, B, ldb, C, ldc);
+  ++*L.launches;
+  return cudaGetLastError();
+}
+
 cudaError_t launch_dgemm(Launch L, bool transA, int M, int N, int K, double alpha,
                          const double* A, int lda, const double* B, int ldb, double beta,
                          double* C, int ldc) {
   if (M == 0 || N == 0) return cudaSuccess;
+  if (beta == 0.0)
+    return transA ? gemm2<true, double, double, double, double>(L, M, N, K, alpha, A, lda, B, ldb,
+                                                                C, ldc)
+                  : gemm2<false, double, double, double, double>(L, M, N, K, alpha, A, lda, B,
+                                                                 ldb, C, ldc);
   dim3 grid((M + GBM - 1) / GBM, (N + GBN - 1) / GBN);
   if (transA)
     k_dgemm<true><<<grid, 256, 0, L.st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
@@ -1253,12 +1367,49 @@ cudaError_t launch_reduce_partials(Launch L, const double* partials, int nblk, i
 // with source tiles staged in shared memory, summed in source order.
 // ---------------------------------------------------------------------------
 constexpr int kNbTile = 256;
+// Source range of each thread's target ([0, nsrc) for one molecule; the
+// target's own molecule in a batch) and the union over the block.
+struct SrcRange {
+  int lo, hi, ulo, uhi;
+};
+__device__ __forceinline__ SrcRange block_src_range(const int2* trange, int t, int ntrg,
+                                                    int s0, int s1) {
+  __shared__ int b_lo, b_hi;
+  SrcRange r;
+  r.lo = s0;
+  r.hi = s1;
+  if (trange) {
+    if (t < ntrg) {
+      int2 v = trange[t];
+      r.lo = max(v.x, s0);
+      r.hi = min(v.y, s1);
+    } else {
+      r.lo = s1;
+      r.hi = s0;
+    }
+  }
+  if (threadIdx.x == 0) {
+    b_lo = s1;
+    b_hi = s0;
+  }
+  __syncthreads();
+  if (r.lo < r.hi) {
+    atomicMin(&b_lo, r.lo);
+    atomicMax(&b_hi, r.hi);
+  }
+  __syncthreads();
+  r.ulo = b_lo;
+  r.uhi = b_hi;
+  return r;
+}
+
 __global__ void __launch_bounds__(kNbTile) k_coulomb_pot(int nsrc, const double* __restrict__ q,
                                                          const double* __restrict__ sx,
                                                          const double* __restrict__ sy,
                                                          const double* __restrict__ sz,
                                                          int ntrg, const double* __restrict__ ctrg,
-                                                         double* phi) {
+                                                         double* phi,
+                                                         const int2* __restrict__ trange) {
   __shared__ double4 src[kNbTile];
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   double px = 0, py = 0, pz = 0;
@@ -1267,14 +1418,17 @@ __global__ void __launch_bounds__(kNbTile) k_coulomb_pot(int nsrc, const double*
     py = ctrg[3 * (size_t)t + 1];
     pz = ctrg[3 * (size_t)t + 2];
   }
+  const SrcRange rg = block_src_range(trange, t, ntrg, 0, nsrc);
   double v = 0.0;
-  for (int j0 = 0; j0 < nsrc; j0 += kNbTile) {
+  for (int j0 = rg.ulo; j0 < rg.uhi; j0 += kNbTile) {
     int j = j0 + threadIdx.x;
     __syncthreads();
-    src[threadIdx.x] = j < nsrc ? make_double4(sx[j], sy[j], sz[j], q[j]) : make_double4(0, 0, 0, 0);
+    src[threadIdx.x] = j < rg.uhi ? make_double4(sx[j], sy[j], sz[j], q[j])
+                                  : make_double4(0, 0, 0, 0);
     __syncthreads();
-    int cnt = min(kNbTile, nsrc - j0);
-    if (cnt == kNbTile) {
+    int cnt = min(kNbTile, rg.uhi - j0);
+    const int kb = max(rg.lo - j0, 0), ke = min(rg.hi - j0, cnt);
+    if (kb == 0 && ke == kNbTile) {
 #pragma unroll 8
       for (int k = 0; k < kNbTile; ++k) {
         double4 s = src[k];
@@ -1282,7 +1436,7 @@ __global__ void __launch_bounds__(kNbTile) k_coulomb_pot(int nsrc, const double*
         v = fma(s.w, rsqrt(dx * dx + dy * dy + dz * dz), v);
       }
     } else {
-      for (int k = 0; k < cnt; ++k) {
+      for (int k = kb; k < ke; ++k) {
         double4 s = src[k];
         double dx = px - s.x, dy = py - s.y, dz = pz - s.z;
         v = fma(s.w, rsqrt(dx * dx + dy * dy + dz * dz), v);
@@ -1293,10 +1447,10 @@ __global__ void __launch_bounds__(kNbTile) k_coulomb_pot(int nsrc, const double*
 }
 cudaError_t launch_coulomb_pot(Launch L, int nsrc, const double* q, const double* sx,
                                const double* sy, const double* sz, int ntrg, const double* ctrg,
-                               double* phi) {
+                               double* phi, const int2* trange) {
   if (ntrg == 0) return cudaSuccess;
   k_coulomb_pot<<<(ntrg + kNbTile - 1) / kNbTile, kNbTile, 0, L.st>>>(nsrc, q, sx, sy, sz, ntrg,
-                                                                       ctrg, phi);
+                                                                       ctrg, phi, trange);
   ++*L.launches;
   return cudaGetLastError();
 }
@@ -1324,7 +1478,8 @@ int efield_chunks(int nsrc, int ntrg) {
 __global__ void __launch_bounds__(kNbTile) k_efield(int nsrc, const double* __restrict__ q,
                                                     const double* __restrict__ csrc, int ntrg,
                                                     const double* __restrict__ ctrg, int chunk,
-                                                    double* out) {
+                                                    double* out,
+                                                    const int2* __restrict__ trange) {
   __shared__ double4 src[kNbTile];
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int c = blockIdx.y;
@@ -1335,17 +1490,18 @@ __global__ void __launch_bounds__(kNbTile) k_efield(int nsrc, const double* __re
     pz = ctrg[3 * (size_t)t + 2];
   }
   double ex = 0.0, ey = 0.0, ez = 0.0;
-  const int s0 = c * chunk, s1 = min(nsrc, s0 + chunk);
-  for (int j0 = s0; j0 < s1; j0 += kNbTile) {
+  const SrcRange rg = block_src_range(trange, t, ntrg, c * chunk, min(nsrc, c * chunk + chunk));
+  for (int j0 = rg.ulo; j0 < rg.uhi; j0 += kNbTile) {
     int j = j0 + threadIdx.x;
     __syncthreads();
-    src[threadIdx.x] = j < s1 ? make_double4(csrc[3 * (size_t)j], csrc[3 * (size_t)j + 1],
-                                             csrc[3 * (size_t)j + 2], q[j])
-                              : make_double4(0, 0, 0, 0);
+    src[threadIdx.x] = j < rg.uhi ? make_double4(csrc[3 * (size_t)j], csrc[3 * (size_t)j + 1],
+                                                 csrc[3 * (size_t)j + 2], q[j])
+                                  : make_double4(0, 0, 0, 0);
     __syncthreads();
-    int cnt = min(kNbTile, s1 - j0);
+    const int cnt = min(kNbTile, rg.uhi - j0);
+    const int kb = max(rg.lo - j0, 0), ke = min(rg.hi - j0, cnt);
 #pragma unroll 4
-    for (int k = 0; k < cnt; ++k) {
+    for (int k = kb; k < ke; ++k) {
       double4 s = src[k];
       double dx = px - s.x, dy = py - s.y, dz = pz - s.z;
       double r2 = dx * dx + dy * dy + dz * dz;
@@ -1378,7 +1534,8 @@ __global__ void k_efield_reduce(int ntrg, int nchunk, const double* __restrict__
 __global__ void __launch_bounds__(kNbTile) k_efield_f(int nsrc, const double* __restrict__ q,
                                                       const double* __restrict__ csrc, int ntrg,
                                                       const double* __restrict__ ctrg, int chunk,
-                                                      double* out) {
+                                                      double* out,
+                                                      const int2* __restrict__ trange) {
   __shared__ float4 src[kNbTile];
   __shared__ double org[3];
   int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1398,19 +1555,21 @@ __global__ void __launch_bounds__(kNbTile) k_efield_f(int nsrc, const double* __
     pz = (float)(ctrg[3 * (size_t)t + 2] - oz);
   }
   double ex = 0.0, ey = 0.0, ez = 0.0;
-  const int s0 = c * chunk, s1 = min(nsrc, s0 + chunk);
-  for (int j0 = s0; j0 < s1; j0 += kNbTile) {
+  const SrcRange rg = block_src_range(trange, t, ntrg, c * chunk, min(nsrc, c * chunk + chunk));
+  for (int j0 = rg.ulo; j0 < rg.uhi; j0 += kNbTile) {
     int j = j0 + threadIdx.x;
     __syncthreads();
-    src[threadIdx.x] = j < s1 ? make_float4((float)(csrc[3 * (size_t)j] - ox),
-                                            (float)(csrc[3 * (size_t)j + 1] - oy),
-                                            (float)(csrc[3 * (size_t)j + 2] - oz), (float)q[j])
-                              : make_float4(0.f, 0.f, 0.f, 0.f);
+    src[threadIdx.x] = j < rg.uhi ? make_float4((float)(csrc[3 * (size_t)j] - ox),
+                                                (float)(csrc[3 * (size_t)j + 1] - oy),
+                                                (float)(csrc[3 * (size_t)j + 2] - oz),
+                                                (float)q[j])
+                                  : make_float4(0.f, 0.f, 0.f, 0.f);
     __syncthreads();
-    int cnt = min(kNbTile, s1 - j0);
+    const int cnt = min(kNbTile, rg.uhi - j0);
+    const int kb = max(rg.lo - j0, 0), ke = min(rg.hi - j0, cnt);
     float fx = 0.f, fy = 0.f, fz = 0.f;
 #pragma unroll 8
-    for (int k = 0; k < cnt; ++k) {
+    for (int k = kb; k < ke; ++k) {
       float4 s = src[k];
       float dx = px - s.x, dy = py - s.y, dz = pz - s.z;
       float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
@@ -1432,14 +1591,15 @@ __global__ void __launch_bounds__(kNbTile) k_efield_f(int nsrc, const double* __
   }
 }
 cudaError_t launch_efield_f32(Launch L, int nsrc, const double* q, const double* csrc, int ntrg,
-                              const double* ctrg, double* ef, double* scratch, int nchunk) {
+                              const double* ctrg, double* ef, double* scratch, int nchunk,
+                              const int2* trange) {
   if (ntrg == 0) return cudaSuccess;
   int chunk = (nsrc + nchunk - 1) / max(nchunk, 1);
   chunk = ((chunk + kNbTile - 1) / kNbTile) * kNbTile;
   if (chunk == 0) chunk = kNbTile;
   dim3 grid((ntrg + kNbTile - 1) / kNbTile, nchunk);
   double* out = nchunk == 1 ? ef : scratch;
-  k_efield_f<<<grid, kNbTile, 0, L.st>>>(nsrc, q, csrc, ntrg, ctrg, chunk, out);
+  k_efield_f<<<grid, kNbTile, 0, L.st>>>(nsrc, q, csrc, ntrg, ctrg, chunk, out, trange);
   ++*L.launches;
   cudaError_t e = cudaGetLastError();
   if (e || nchunk == 1) return e;
@@ -1449,14 +1609,15 @@ cudaError_t launch_efield_f32(Launch L, int nsrc, const double* q, const double*
 }
 
 cudaError_t launch_efield(Launch L, int nsrc, const double* q, const double* csrc, int ntrg,
-                          const double* ctrg, double* ef, double* scratch, int nchunk) {
+                          const double* ctrg, double* ef, double* scratch, int nchunk,
+                          const int2* trange) {
   if (ntrg == 0) return cudaSuccess;
   int chunk = (nsrc + nchunk - 1) / max(nchunk, 1);
   chunk = ((chunk + kNbTile - 1) / kNbTile) * kNbTile;
   if (chunk == 0) chunk = kNbTile;
   dim3 grid((ntrg + kNbTile - 1) / kNbTile, nchunk);
   double* out = nchunk == 1 ? ef : scratch;
-  k_efield<<<grid, kNbTile, 0, L.st>>>(nsrc, q, csrc, ntrg, ctrg, chunk, out);
+  k_efield<<<grid, kNbTile, 0, L.st>>>(nsrc, q, csrc, ntrg, ctrg, chunk, out, trange);
   ++*L.launches;
   cudaError_t e = cudaGetLastError();
   if (e || nchunk == 1) return e;
@@ -2106,6 +2267,10 @@ __global__ void __launch_bounds__(256) k_sgemm(int M, int N, int K, float alpha,
 cudaError_t launch_sgemm(Launch L, bool transA, int M, int N, int K, float alpha, const float* A,
                          int lda, const float* B, int ldb, double* C, int ldc) {
   if (M == 0 || N == 0) return cudaSuccess;
+  return transA ? gemm2<true, float, float, double, float>(L, M, N, K, alpha, A, lda, B, ldb, C,
+                                                           ldc)
+                : gemm2<false, float, float, double, float>(L, M, N, K, alpha, A, lda, B, ldb, C,
+                                                            ldc);
   dim3 grid((M + GBM - 1) / GBM, (N + GBN - 1) / GBN);
   if (transA)
     k_sgemm<true, float, double><<<grid, 256, 0, L.st>>>(M, N, K, alpha, A, lda, B, ldb, C, ldc);
@@ -2117,6 +2282,7 @@ cudaError_t launch_sgemm(Launch L, bool transA, int M, int N, int K, float alpha
 cudaError_t launch_sgemm_xi(Launch L, int M, int N, int K, const float* A, int lda,
                             const double* B, int ldb, float* C, int ldc) {
   if (M == 0 || N == 0) return cudaSuccess;
+  return gemm2<true, float, double, float, float>(L, M, N, K, 1.f, A, lda, B, ldb, C, ldc);
   dim3 grid((M + GBM - 1) / GBM, (N + GBN - 1) / GBN);
   k_sgemm<true, double, float><<<grid, 256, 0, L.st>>>(M, N, K, 1.f, A, lda, B, ldb, C, ldc);
   ++*L.launches;
@@ -2168,6 +2334,297 @@ __global__ void k_axpy(long long n, double a, const double* __restrict__ x, doub
 cudaError_t launch_axpy(Launch L, long long n, double a, const double* x, double* y) {
   if (n == 0) return cudaSuccess;
   k_axpy<<<(unsigned)((n + 255) / 256), 256, 0, L.st>>>(n, a, x, y);
+  ++*L.launches;
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Batched solves: many molecules concatenated into one system.  The
+// operators act per sphere and need no change; the Jacobi/DIIS driver
+// (jacobi_diis.f90) runs per molecule, fused into one kernel per iteration
+// with one block per molecule.
+// ---------------------------------------------------------------------------
+// Gauss-Jordan with full pivoting (gjinv, jacobi_diis.f90:272-360), one warp,
+// lane j owns row j.  a is n x n column-major in shared memory, b the rhs.
+// Pivot: the first maximum of |a| over free rows/columns in the reference's
+// scan order (rows outer, columns inner).  Returns false when singular.
+__device__ bool gjinv_warp(int n, double* a, double* b, int* piv) {
+  const int lane = threadIdx.x & 31;
+  if (lane < n) piv[lane] = 0;
+  __syncwarp();
+  for (int i = 0; i < n; ++i) {
+    double bv = 0.0;
+    int bk = -1;
+    if (lane < n && piv[lane] != 1) {
+      for (int k = 0; k < n; ++k)
+        if (piv[k] == 0) {
+          double v = fabs(a[k * n + lane]);
+          if (v > bv) {
+            bv = v;
+            bk = k;
+          }
+        }
+    }
+    int bj = bk >= 0 ? lane : 1 << 30;
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) {
+      double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+      int oj = __shfl_xor_sync(0xffffffffu, bj, o);
+      int ok = __shfl_xor_sync(0xffffffffu, bk, o);
+      if (ov > bv || (ov == bv && oj < bj)) {
+        bv = ov;
+        bj = oj;
+        bk = ok;
+      }
+    }
+    if (bk < 0) return false;  // no non-zero free entry
+    const int irow = bj, icol = bk;
+    __syncwarp();
+    if (lane == 0) piv[icol] += 1;
+    __syncwarp();
+    if (piv[icol] > 1) return false;
+    if (irow != icol) {
+      for (int k = lane; k < n; k += 32) {
+        double t = a[k * n + irow];
+        a[k * n + irow] = a[k * n + icol];
+        a[k * n + icol] = t;
+      }
+      if (lane == 0) {
+        double t = b[irow];
+        b[irow] = b[icol];
+        b[icol] = t;
+      }
+    }
+    __syncwarp();
+    const double piv_v = a[icol * n + icol];
+    if (piv_v == 0.0) return false;
+    const double pinv = 1.0 / piv_v;
+    __syncwarp();
+    if (lane == 0) a[icol * n + icol] = 1.0;
+    __syncwarp();
+    for (int k = lane; k < n; k += 32) a[k * n + icol] *= pinv;
+    if (lane == 0) b[icol] *= pinv;
+    __syncwarp();
+    double dum = 0.0;
+    if (lane < n && lane != icol) dum = a[icol * n + lane];
+    __syncwarp();
+    if (lane < n && lane != icol) {
+      a[icol * n + lane] = 0.0;
+      for (int k = 0; k < n; ++k) a[k * n + lane] -= a[k * n + icol] * dum;
+      b[lane] -= b[icol] * dum;
+    }
+    __syncwarp();
+  }
+  return true;
+}
+
+__global__ void __launch_bounds__(256) k_batch_diis(const YlmTables tb, BatchState bs,
+                                                    const double* __restrict__ rhs,
+                                                    const double* __restrict__ y, double* x) {
+  const int k = blockIdx.x;
+  const int lenb = bs.ndiis + 1;
+  __shared__ int s_status, s_nm, s_new, s_shift, s_ok, s_nmold;
+  __shared__ int pm[kMaxHist];
+  __shared__ double row[kMaxHist + 1], coef[kMaxHist];
+  __shared__ double ga[(kMaxHist + 1) * (kMaxHist + 1)], gb[kMaxHist + 1];
+  __shared__ int gpiv[kMaxHist + 1];
+  if (threadIdx.x == 0) s_status = bs.status[k];
+  __syncthreads();
+  if (s_status != 0) return;
+  const int nd = bs.ndiis;
+  if (threadIdx.x == 0) {
+    const int nm = bs.nmat[k];
+    const int* sl = bs.slot + (size_t)k * nd;
+    s_new = sl[nm - 1];
+    s_nmold = nm;
+    if (nm >= nd) {  // drop the 10 oldest (jacobi_diis.f90:196-205)
+      for (int j = 0; j < nd; ++j) pm[j] = sl[(j + 10) % nd];
+      s_nm = nm - 10;
+      s_shift = 1;
+    } else {
+      for (int j = 0; j < nd; ++j) pm[j] = sl[j];
+      s_nm = nm;
+      s_shift = 0;
+    }
+  }
+  __syncthreads();
+  const int nm = s_nm, nh = nm - 1;
+  const long long N = bs.n_total;
+  const long long e0 = (long long)bs.off[k] * tb.nylm, e1 = (long long)bs.off[k + 1] * tb.nylm;
+  double* xnew = bs.hx + (size_t)s_new * N;
+  double* enew = bs.he + (size_t)s_new * N;
+  double d[kMaxHist + 1];
+#pragma unroll
+  for (int h = 0; h <= kMaxHist; ++h) d[h] = 0.0;
+  for (long long e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+    const int lm = (int)(e % tb.nylm);
+    const double xn = tb.facl[l_of(lm)] * (rhs[e] - y[e]);
+    const double ev = xn - x[e];
+    xnew[e] = xn;
+    enew[e] = ev;
+#pragma unroll
+    for (int h = 0; h < kMaxHist; ++h)
+      if (h < nh) d[h] = fma(ev, bs.he[(size_t)pm[h] * N + e], d[h]);
+    d[kMaxHist] = fma(ev, ev, d[kMaxHist]);
+  }
+  double v[kMaxHist + 1];
+#pragma unroll
+  for (int h = 0; h <= kMaxHist; ++h) v[h] = (h < nh) ? d[h] : (h == nh ? d[kMaxHist] : 0.0);
+  {  // block sums of v[0..nh] into row[]
+    __shared__ double sh[kMaxHist + 1][8];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int h = 0; h <= kMaxHist; ++h) {
+      if (h <= nh) {
+        double t = v[h];
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+        if (lane == 0) sh[h][w] = t;
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x <= nh) {
+      double t = 0.0;
+      for (int ww = 0; ww < (int)(blockDim.x >> 5); ++ww) t += sh[threadIdx.x][ww];
+      row[threadIdx.x] = t;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x < 32) {
+    double* B = bs.B + (size_t)k * lenb * lenb;
+    auto Bm = [&](int j, int kk) -> double& { return B[(size_t)(kk - 1) * lenb + (j - 1)]; };
+    if (threadIdx.x == 0) {
+      if (s_shift) {
+        const int old = s_nmold;
+        for (int j = 2; j <= old - 10; ++j)
+          for (int kk = 2; kk <= old - 10; ++kk) Bm(j, kk) = Bm(j + 10, kk + 10);
+      }
+      if (nm == 1) {  // makeb (jacobi_diis.f90:232-270)
+        Bm(1, 1) = 0.0;
+        Bm(1, 2) = 1.0;
+        Bm(2, 1) = 1.0;
+        Bm(2, 2) = row[0];
+      } else {
+        Bm(nm + 1, 1) = 1.0;
+        Bm(1, nm + 1) = 1.0;
+        for (int i = 1; i <= nm - 1; ++i) {
+          Bm(nm + 1, i + 1) = row[i - 1];
+          Bm(i + 1, nm + 1) = row[i - 1];
+        }
+        Bm(nm + 1, nm + 1) = row[nm - 1];
+      }
+      const int n1 = nm + 1;
+      for (int kk = 1; kk <= n1; ++kk)
+        for (int j = 1; j <= n1; ++j) ga[(kk - 1) * n1 + (j - 1)] = Bm(j, kk);
+      for (int j = 0; j < n1; ++j) gb[j] = 0.0;
+      gb[0] = 1.0;
+    }
+    __syncwarp();
+    const bool ok = gjinv_warp(nm + 1, ga, gb, gpiv);
+    if (threadIdx.x == 0) {
+      int* sl = bs.slot + (size_t)k * nd;
+      if (s_shift)
+        for (int j = 0; j < nd; ++j) sl[j] = pm[j];
+      if (ok) {
+        for (int h = 0; h < nm; ++h) coef[h] = gb[h + 1];
+        bs.nmat[k] = nm + 1;
+      } else {  // singular: restart the history (jacobi_diis.f90:214-217)
+        bs.nmat[k] = 1;
+        bs.restarts[k] += 1;
+      }
+      s_ok = ok ? 1 : 0;
+    }
+  }
+  __syncthreads();
+  // extrapolation, increment H-norm and update (diis :222-226, hnorm)
+  double acc = 0.0;
+  const bool ok = s_ok != 0;
+  for (long long e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+    double xo;
+    if (ok) {
+      xo = 0.0;
+      for (int h = 0; h < nm; ++h) xo = fma(coef[h], bs.hx[(size_t)pm[h] * N + e], xo);
+    } else {
+      xo = xnew[e];
+    }
+    const double dd = xo - x[e];
+    const int l = l_of((int)(e % tb.nylm));
+    acc = fma(dd * dd, 1.0 / (1.0 + l), acc);
+    x[e] = xo;
+  }
+  {
+    __shared__ double sh2[8];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) sh2[w] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int ww = 0; ww < (int)(blockDim.x >> 5); ++ww) t += sh2[ww];
+      const int nsph = bs.off[k + 1] - bs.off[k];
+      const double nrm = sqrt(t / (double)max(nsph, 1));
+      bs.norm[k] = nrm;
+      const int it = bs.iters[k] + 1;
+      bs.iters[k] = it;
+      bs.status[k] = (nrm < bs.tol) ? 1 : (it >= bs.max_iter ? 2 : (isfinite(nrm) ? 0 : 3));
+    }
+  }
+}
+cudaError_t launch_batch_diis(Launch L, const YlmTables& tb, const BatchState& bs,
+                              const double* rhs, const double* y, double* x) {
+  if (bs.nmol == 0) return cudaSuccess;
+  k_batch_diis<<<bs.nmol, 256, 0, L.st>>>(tb, bs, rhs, y, x);
+  ++*L.launches;
+  return cudaGetLastError();
+}
+
+// per-molecule <a, b> (energy: fep * <X, psi>, cosmo.f90:155)
+__global__ void k_batch_dot(const int* __restrict__ off, int nylm, const double* __restrict__ a,
+                            const double* __restrict__ b, double scale, double* out) {
+  const int k = blockIdx.x;
+  const long long e0 = (long long)off[k] * nylm, e1 = (long long)off[k + 1] * nylm;
+  double acc = 0.0;
+  for (long long e = e0 + threadIdx.x; e < e1; e += blockDim.x) acc = fma(a[e], b[e], acc);
+  __shared__ double sh[8];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o >= 1; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if (lane == 0) sh[w] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int ww = 0; ww < (int)(blockDim.x >> 5); ++ww) t += sh[ww];
+    out[k] = scale * t;
+  }
+}
+cudaError_t launch_batch_dot(Launch L, int nmol, const int* off, int nylm, const double* a,
+                             const double* b, double scale, double* out) {
+  if (nmol == 0) return cudaSuccess;
+  k_batch_dot<<<nmol, 256, 0, L.st>>>(off, nylm, a, b, scale, out);
+  ++*L.launches;
+  return cudaGetLastError();
+}
+
+// source ranges of the batched N-body sums: a cavity point sums over the
+// nuclei of its molecule, a nucleus over the cavity points of its molecule
+__global__ void k_batch_ranges(int nsph, int ngrid, int ncav, const int2* __restrict__ mrange,
+                               const int* __restrict__ cavpt, const int* __restrict__ cavoff,
+                               int2* tr_cav, int2* tr_nuc) {
+  long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e < ncav) tr_cav[e] = mrange[cavpt[e] / ngrid];
+  if (e < nsph) {
+    int2 r = mrange[e];
+    tr_nuc[e] = make_int2(cavoff[r.x], cavoff[r.y]);
+  }
+}
+cudaError_t launch_batch_ranges(Launch L, int nsph, int ngrid, int ncav, const int2* mrange,
+                                const int* cavpt, const int* cavoff, int2* tr_cav,
+                                int2* tr_nuc) {
+  long long n = max((long long)ncav, (long long)nsph);
+  if (n == 0) return cudaSuccess;
+  k_batch_ranges<<<(unsigned)((n + 255) / 256), 256, 0, L.st>>>(nsph, ngrid, ncav, mrange, cavpt,
+                                                                 cavoff, tr_cav, tr_nuc);
   ++*L.launches;
   return cudaGetLastError();
 }

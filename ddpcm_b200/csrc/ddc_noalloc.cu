@@ -70,7 +70,8 @@ extern "C" int ddc_efld_noalloc(int device, int nsrc, const double* src, const d
     if (nchunk > fit) nchunk = (int)fit;
     long long launches = 0;
     ddc::Launch L{static_cast<cudaStream_t>(stream), &launches};
-    if (ddc::launch_efield(L, nsrc, src, csrc, ntrg, ctrg, ef, scratch, nchunk) != cudaSuccess)
+    if (ddc::launch_efield(L, nsrc, src, csrc, ntrg, ctrg, ef, scratch, nchunk, nullptr) !=
+        cudaSuccess)
       rc = DDC_ERR_CUDA;
   }
   if (prev != device) cudaSetDevice(prev);

@@ -111,6 +111,9 @@ _SIGS = {
     "ddc_stage_times": [ctypes.c_void_p, _dp, ctypes.POINTER(ctypes.c_longlong)],
     "ddc_reset_stage_times": [ctypes.c_void_p],
     "ddc_fp64_peak": [ctypes.c_int, _dp],
+    "ddc_batch_energy_forces": [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+                               + [_dp] * 5 + [_dp, _dp, ctypes.POINTER(ctypes.c_int),
+                                              ctypes.POINTER(RunInfo)],
 }
 
 
@@ -356,6 +359,29 @@ class DDCosmo:
         d["esolv"] = es.value
         self.nsph, self.ncav, self.nylm, self.ngrid = d["nsph"], d["ncav"], d["nylm"], d["ngrid"]
         return d
+
+    def batch_energy_forces(self, mols):
+        """Energy and forces of several independent molecules in one library
+        call (each molecule as if solved alone).  mols: list of dicts with
+        q, x, y, z, r (bohr).  Returns dict(esolv[nmol], fx list, iters
+        (nmol, 2), info)."""
+        sizes = [len(m["q"]) for m in mols]
+        off = np.zeros(len(mols) + 1, dtype=np.int32)
+        off[1:] = np.cumsum(sizes)
+        cat = {k: _f64(np.concatenate([np.asarray(m[k], dtype=np.float64) for m in mols]))
+               for k in "qxyzr"}
+        nmol = len(mols)
+        es = np.zeros(nmol)
+        fx = np.zeros((int(off[-1]), 3))
+        iters = np.zeros((nmol, 2), dtype=np.int32)
+        info = RunInfo()
+        ip = ctypes.POINTER(ctypes.c_int)
+        self._check(self.L.ddc_batch_energy_forces(
+            self.h, nmol, off.ctypes.data_as(ip), _p(cat["q"]), _p(cat["x"]), _p(cat["y"]),
+            _p(cat["z"]), _p(cat["r"]), _p(es), _p(fx), iters.ctypes.data_as(ip),
+            ctypes.byref(info)))
+        return dict(esolv=es, fx=[fx[off[k]:off[k + 1]] for k in range(nmol)], iters=iters,
+                    info=info.as_dict(), off=off)
 
     def energy_forces(self, charge, x, y, z, rvdw):
         """The main.f90 flow (main.f90:164-265) in one library call.

@@ -102,6 +102,11 @@ CONFIGS = {
 }
 
 
+# batched workload: 256 globules of log-uniform size in [20, 2000] spheres
+BATCH_CONFIG = dict(count=256, lo=20, hi=2000, lmax=6, ngrid=302, eta=0.1, eps=78.3553, iconv=10,
+                    seed=3000)
+
+
 def config_molecule(k):
     c = CONFIGS[k]
     return make_molecule(c["n"], c["seed"], globule=c["globule"])

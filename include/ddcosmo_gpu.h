@@ -153,6 +153,20 @@ int ddc_energy_forces(ddc_ctx* ctx, int n, const double* charge, const double* x
                       const double* y, const double* z, const double* rvdw, double* esolv,
                       double* sigma, double* s, double* fx, ddc_run_info* info);
 
+/* Batched energy+forces for nmol independent molecules in one call.  No
+ * counterpart in the reference, which solves one molecule per process; the
+ * result for each molecule is that of ddc_energy_forces on it alone.  The
+ * spheres of all molecules are concatenated: molecule k owns spheres
+ * [off[k], off[k+1]) (off is a host array of nmol+1 offsets, off[0] = 0).
+ * Each molecule runs the reference's Jacobi/DIIS with its own history and
+ * convergence test; all molecules share each kernel launch.  Outputs:
+ * esolv[nmol] (host), fx(3, off[nmol]) (may be NULL), iters[2*nmol]
+ * (direct, adjoint per molecule; host, may be NULL).  FP64 only. */
+int ddc_batch_energy_forces(ddc_ctx* ctx, int nmol, const int* off, const double* charge,
+                            const double* x, const double* y, const double* z,
+                            const double* rvdw, double* esolv, double* fx, int* iters,
+                            ddc_run_info* info);
+
 /* The operators the solver iterates (matvec.f90): y = off-diagonal L x
  * (lx, :94), y = off-diagonal L* x (lstarx, :161), y = D^-1 x (ldm1x, :246)
  * and the increment norm hnorm (:281).  x, y are (nylm,nsph). */
