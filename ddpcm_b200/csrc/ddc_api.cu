@@ -1421,6 +1421,16 @@ int ddc_energy_forces(ddc_ctx* ctx, int n, const double* charge, const double* x
   inf->t_mkrhs = t2 - t1;
   double* dsig = ctx->sigma.as<double>();
   double* ds = ctx->s.as<double>();
+  if (ctx->prm.guess == DDC_GUESS_USER) {
+    // sigma (and s) carry the initial guesses in, e.g. the previous frame's
+    // solutions (the sigma slot of cosmo.f90:136-138, 174-176)
+    if (!sigma || (ctx->prm.igrad && !s))
+      return fail(ctx, DDC_ERR_PARAM, "user guess needs sigma and s on entry");
+    const cudaMemcpyKind k =
+        ctx->prm.device_pointers ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    CK(cudaMemcpyAsync(dsig, sigma, sizeof(double) * nv, k, ctx->st));
+    if (ctx->prm.igrad) CK(cudaMemcpyAsync(ds, s, sizeof(double) * nv, k, ctx->st));
+  }
   CKI(cosmo_dev(ctx, 0, 1, dphi, nullptr, dpsi, dsig, esolv, &inf->direct));
   double t3 = now_s();
   inf->t_direct = t3 - t2;

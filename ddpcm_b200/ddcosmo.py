@@ -22,6 +22,7 @@ import numpy as np
 from .build import LIB
 
 DDC_OK = 0
+DDC_ERR_PARAM = 1
 DDC_ERR_NOCONV = 5
 PREC_FP64, PREC_MIXED = 0, 1
 GUESS_REFERENCE, GUESS_ZERO, GUESS_USER = 0, 1, 2
@@ -383,15 +384,16 @@ class DDCosmo:
         return dict(esolv=es, fx=[fx[off[k]:off[k + 1]] for k in range(nmol)], iters=iters,
                     info=info.as_dict(), off=off)
 
-    def energy_forces(self, charge, x, y, z, rvdw):
-        """The main.f90 flow (main.f90:164-265) in one library call.
-        Returns dict(esolv, sigma, s, fx, info)."""
+    def energy_forces(self, charge, x, y, z, rvdw, sigma0=None, s0=None):
+        """The main.f90 flow (main.f90:164-265) in one library call.  With
+        guess=GUESS_USER, sigma0 and s0 (n, nylm) are the initial guesses of
+        the direct and adjoint solves.  Returns dict(esolv, sigma, s, fx, info)."""
         q, x, y, z, r = map(_f64, (charge, x, y, z, rvdw))
         n = len(q)
         nylm = (self.lmax + 1) ** 2
         es = ctypes.c_double()
-        sig = np.zeros((n, nylm))
-        s = np.zeros((n, nylm))
+        sig = np.zeros((n, nylm)) if sigma0 is None else np.array(sigma0, dtype=np.float64, order="C")
+        s = np.zeros((n, nylm)) if s0 is None else np.array(s0, dtype=np.float64, order="C")
         fx = np.zeros((n, 3))
         info = RunInfo()
         self._check(self.L.ddc_energy_forces(self.h, n, _p(q), _p(x), _p(y), _p(z), _p(r),

@@ -119,6 +119,22 @@ def batch_molecules(count=256, lo=20, hi=2000, seed=3000):
     return [make_molecule(int(s), seed + 1 + i) for i, s in enumerate(sizes)]
 
 
+def trajectory(mol, frames, sigma=0.05, seed=0):
+    """A synthetic trajectory from ``mol`` (angstrom): each frame moves every
+    centre of the previous frame by a Gaussian displacement of ``sigma``
+    angstrom per coordinate.  Returns a list of ``frames`` molecules, the first
+    being ``mol`` itself; charges and radii do not change."""
+    rng = np.random.default_rng(seed)
+    out = [dict(mol)]
+    for _ in range(frames - 1):
+        prev = out[-1]
+        nxt = dict(prev)
+        for k in "xyz":
+            nxt[k] = np.asarray(prev[k], dtype=np.float64) + rng.normal(0.0, sigma, size=len(prev[k]))
+        out.append(nxt)
+    return out
+
+
 def write_input(path, mol, lmax, ngrid, iconv, eps, eta, igrad=1, iprint=1, nproc=1):
     """Write a reference-format Input.txt (angstrom)."""
     with open(path, "w") as f:

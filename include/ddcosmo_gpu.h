@@ -148,7 +148,10 @@ int ddc_efld(ddc_ctx* ctx, int nsrc, const double* src, const double* csrc, int 
  * mkrhs, direct solve, energy, adjoint solve, forces_dd, ddmkzeta and the two
  * efld contractions.  Inputs: charges and bohr coordinates/radii; outputs
  * esolv (Hartree), sigma = X and s = S (nylm,n), fx(3,n) total forces
- * (Hartree/bohr; any of sigma, s, fx may be NULL).  info may be NULL. */
+ * (Hartree/bohr; any of sigma, s, fx may be NULL).  info may be NULL.
+ * With guess = DDC_GUESS_USER, sigma and s are in/out: on entry they hold the
+ * initial guesses of the direct and adjoint solves (e.g. the previous
+ * frame's solutions of a trajectory) and must not be NULL. */
 int ddc_energy_forces(ddc_ctx* ctx, int n, const double* charge, const double* x,
                       const double* y, const double* z, const double* rvdw, double* esolv,
                       double* sigma, double* s, double* fx, ddc_run_info* info);

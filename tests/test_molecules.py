@@ -39,3 +39,15 @@ def test_batch_sizes():
     mols = M.batch_molecules(count=16, lo=20, hi=200, seed=5)
     ns = [m["n"] for m in mols]
     assert min(ns) >= 20 and max(ns) <= 200 and len(set(ns)) > 4
+
+
+def test_trajectory_displacements():
+    m = M.make_molecule(200, 5)
+    tr = M.trajectory(m, 4, sigma=0.05, seed=9)
+    assert len(tr) == 4 and tr[0]["x"] is m["x"]
+    for a, b in zip(tr[:-1], tr[1:]):
+        d = np.concatenate([b[k] - a[k] for k in "xyz"])
+        assert abs(d.std() - 0.05) < 0.01
+        assert np.array_equal(a["q"], b["q"]) and np.array_equal(a["r"], b["r"])
+    again = M.trajectory(m, 4, sigma=0.05, seed=9)
+    assert np.array_equal(again[3]["z"], tr[3]["z"])
