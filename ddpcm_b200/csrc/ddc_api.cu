@@ -163,6 +163,9 @@ struct ddc_ctx {
   DBuf in1, in2, in3, in4, out1;  // staging for host-pointer calls
   // mixed precision: FP32 grid/basis copies, FP32 grid fields, refinement vectors
   DBuf gridf, basis_f, bw_f, pot_f, xi_f, rres, dres, eres;
+  // second solve set (direct and adjoint solved together) and the fused
+  // operator's per-triple lx values
+  DBuf y2, xn2, hist_x2, hist_e2, rres2, dres2, eres2, tval;
 
   Launch L() { return Launch{st, &launches}; }
   DevGeo geo() const {
@@ -207,12 +210,16 @@ int fail(ddc_ctx* c, int code, const std::string& msg) {
   return code;
 }
 
+// On failure the runtime's last-error state is cleared as well, so that a
+// rejected launch configuration does not resurface in a later call.
 #define CK(expr)                                                                          \
   do {                                                                                    \
     cudaError_t _e = (expr);                                                              \
-    if (_e != cudaSuccess)                                                                \
+    if (_e != cudaSuccess) {                                                              \
+      cudaGetLastError();                                                                 \
       return fail(ctx, _e == cudaErrorMemoryAllocation ? DDC_ERR_NOMEM : DDC_ERR_CUDA,    \
                   std::string(#expr) + ": " + cudaGetErrorString(_e));                    \
+    }                                                                                     \
   } while (0)
 
 #define CKI(expr)                  \
@@ -326,10 +333,29 @@ void build_tables(ddc_ctx* c) {
       }
     }
   }
+  for (int m = 0; m <= lmax; m++) {
+    double gm2 = 1.0, gm1 = 1.0;  // gam_{l-2}, gam_{l-1}
+    for (int l = m; l <= lmax; l++) {
+      const int e = l * (l + 1) / 2 + m;
+      double gam;
+      if (l == m) {
+        gam = 1.0;
+      } else if (l == m + 1) {
+        gam = 2.0 * m + 1.0;
+      } else {
+        gam = tb.A[e] * gm1;
+        tb.Bn[e] = tb.B[e] * gm2 / gam;
+      }
+      tb.Kg[e] = tb.K[e] * gam;
+      gm2 = gm1;
+      gm1 = gam;
+    }
+  }
   for (int e = 0; e < DDC_NLM_CAP; e++) {
     tb.Kf[e] = (float)tb.K[e];
     tb.Af[e] = (float)tb.A[e];
     tb.Bf[e] = (float)tb.B[e];
+    tb.Bnf[e] = (float)tb.Bn[e];
   }
   tb.eta = c->prm.eta;
   tb.lmax = lmax;
@@ -337,12 +363,14 @@ void build_tables(ddc_ctx* c) {
   tb.ngrid = c->ngrid;
 }
 
-// deterministic reduction of `nvals` partial columns into red[0..nvals-1], copied to host
-int reduce_to_host(ddc_ctx* ctx, int nvals, double* host) {
+// deterministic reduction of `nvals` partial columns into red[0..nvals-1], copied to host.
+// stride: the partial row length of the producing kernel (kMaxHist + 1 for the
+// Jacobi step's Gram row, whatever its current length; 1 for single sums).
+int reduce_to_host(ddc_ctx* ctx, int nvals, double* host, int stride = 1) {
   {
     StageScope sc(ctx, ST_REDUCE);
     CK(launch_reduce_partials(ctx->L(), ctx->partials.as<double>(), reduce_blocks(), nvals,
-                            ctx->red.as<double>()));
+                              stride, ctx->red.as<double>()));
   }
   CK(cudaMemcpyAsync(host, ctx->red.p, sizeof(double) * nvals, cudaMemcpyDeviceToHost, ctx->st));
   return sync(ctx);
@@ -504,6 +532,17 @@ int do_init(ddc_ctx* ctx, int n, const std::vector<double4>* hsph, const double4
     for (DBuf* b : {&ctx->rres, &ctx->dres, &ctx->eres})
       CK(b->ensure(sizeof(double) * std::max(nv, (size_t)1)));
   }
+  if (ctx->prm.igrad && ctx->prm.pair_solves) {
+    for (DBuf* b : {&ctx->y2, &ctx->xn2})
+      CK(b->ensure(sizeof(double) * std::max(nv, (size_t)1)));
+    CK(ctx->hist_x2.ensure(sizeof(double) * std::max(nv, (size_t)1) * nd));
+    CK(ctx->hist_e2.ensure(sizeof(double) * std::max(nv, (size_t)1) * nd));
+    if (ctx->prm.precision == DDC_PREC_MIXED)
+      for (DBuf* b : {&ctx->rres2, &ctx->dres2, &ctx->eres2})
+        CK(b->ensure(sizeof(double) * std::max(nv, (size_t)1)));
+    // FP64 values: the mixed path also takes FP64 pair steps (refinement)
+    CK(ctx->tval.ensure(sizeof(double) * std::max<long long>(ctx->ntri, 1)));
+  }
   CKI(sync(ctx));
   ctx->ready = true;
   return DDC_OK;
@@ -560,6 +599,46 @@ int op_lstarx_f32(ddc_ctx* ctx, const double* x, double* y) {
   return DDC_OK;
 }
 
+// y = L x and z = L* s (off-diagonal parts) from one pass over the triples
+int op_pair(ddc_ctx* ctx, const double* x, double* y, const double* s, double* z) {
+  DevGeo g = ctx->geo();
+  CKI(op_xi(ctx, s, ctx->xig.as<double>()));
+  {
+    StageScope sc(ctx, ST_LXS);
+    CK(launch_lxs(ctx->L(), ctx->tb, g, x, ctx->xig.as<double>(), ctx->xk.p,
+                  ctx->tval.as<double>(), z));
+  }
+  {
+    StageScope sc(ctx, ST_GATHER);
+    CK(launch_lx_gather(ctx->L(), g, ctx->tval.as<double>(), ctx->pot.as<double>()));
+  }
+  StageScope sc(ctx, ST_PROJ);
+  CK(launch_dgemm(ctx->L(), false, ctx->nylm, ctx->nsph, ctx->ngrid, -1.0, ctx->bw.as<double>(),
+                  ctx->nylm, ctx->pot.as<double>(), ctx->ngrid, 0.0, y, ctx->nylm));
+  return DDC_OK;
+}
+int op_pair_f32(ddc_ctx* ctx, const double* x, double* y, const double* s, double* z) {
+  DevGeo g = ctx->geo();
+  {
+    StageScope sc(ctx, ST_XI);
+    CK(launch_sgemm_xi(ctx->L(), ctx->ngrid, ctx->nsph, ctx->nylm, ctx->basis_f.as<float>(),
+                       ctx->nylm, s, ctx->nylm, ctx->xi_f.as<float>(), ctx->ngrid));
+  }
+  {
+    StageScope sc(ctx, ST_LXS);
+    CK(launch_lxs_f32(ctx->L(), ctx->tb, g, x, ctx->xi_f.as<float>(), ctx->xk.p,
+                      ctx->tval.as<float>(), z));
+  }
+  {
+    StageScope sc(ctx, ST_GATHER);
+    CK(launch_lx_gather_f32(ctx->L(), g, ctx->tval.as<float>(), ctx->pot_f.as<float>()));
+  }
+  StageScope sc(ctx, ST_PROJ);
+  CK(launch_sgemm(ctx->L(), false, ctx->nylm, ctx->nsph, ctx->ngrid, -1.f, ctx->bw_f.as<float>(),
+                  ctx->nylm, ctx->pot_f.as<float>(), ctx->ngrid, y, ctx->nylm));
+  return DDC_OK;
+}
+
 // gjinv (jacobi_diis.f90:272-360): Gauss-Jordan, full pivoting, one rhs.
 bool gjinv(int n, std::vector<double>& a, std::vector<double>& b) {
   std::vector<int> indxc(n + 1), indxr(n + 1), piv(n + 1, 0);
@@ -605,124 +684,165 @@ bool gjinv(int n, std::vector<double>& a, std::vector<double>& b) {
 
 typedef int (*OpFn)(ddc_ctx*, const double*, double*);
 
-// jacobi_diis (jacobi_diis.f90:1-176), norm mode 4 (hnorm).  x holds the
-// initial guess on entry and the solution on exit (device).  The log of
-// increment norms continues at inf->norms[*logpos].
-int jacobi_diis(ddc_ctx* ctx, OpFn op, const double* rhs, double* x, double tol, int max_iter,
-                ddc_solve_info* inf, int* logpos, int* iters_done, int* restarts_out,
-                double* last_norm) {
+// Work vectors of one solve: set 0 is the context's, set 1 the second set
+// used when the direct and adjoint systems are solved together.
+struct SolveBufs {
+  double *y, *xn, *hx, *he, *r, *d, *e;
+};
+SolveBufs solve_bufs(ddc_ctx* ctx, int set) {
+  if (set == 0)
+    return SolveBufs{ctx->y.as<double>(),      ctx->xn.as<double>(),   ctx->hist_x.as<double>(),
+                     ctx->hist_e.as<double>(), ctx->rres.as<double>(), ctx->dres.as<double>(),
+                     ctx->eres.as<double>()};
+  return SolveBufs{ctx->y2.as<double>(),      ctx->xn2.as<double>(),   ctx->hist_x2.as<double>(),
+                   ctx->hist_e2.as<double>(), ctx->rres2.as<double>(), ctx->dres2.as<double>(),
+                   ctx->eres2.as<double>()};
+}
+
+// jacobi_diis (jacobi_diis.f90:1-176), norm mode 4 (hnorm), as a resumable
+// state: the caller applies the operator to x into y, then jd_step performs
+// the rest of the iteration (Jacobi step, DIIS extrapolation, increment
+// norm and convergence test).  x holds the initial guess on entry and the
+// solution on exit (device).  The log of increment norms continues at
+// inf->norms[*logpos].
+struct JDState {
+  const double* rhs = nullptr;
+  double* x = nullptr;
+  double tol = 0.0;
+  int max_iter = 0;
+  double *y = nullptr, *hx = nullptr, *he = nullptr, *xjac = nullptr;
+  std::vector<double> B;
+  std::vector<int> map;
+  int lenb = 0, nmat = 1, it = 0, restarts = 0;
+  double rms = 0.0;
+  bool done = false, ok = false;
+  ddc_solve_info* inf = nullptr;
+  int* logpos = nullptr;
+};
+
+void jd_begin(ddc_ctx* ctx, JDState& s, const double* rhs, double* x, double tol, int max_iter,
+              const SolveBufs& b, ddc_solve_info* inf, int* logpos) {
+  const int ndiis = ctx->prm.ndiis;
+  s.rhs = rhs;
+  s.x = x;
+  s.tol = tol;
+  s.max_iter = max_iter;
+  s.y = b.y;
+  s.hx = b.hx;
+  s.he = b.he;
+  s.xjac = b.xn;
+  s.lenb = ndiis + 1;
+  s.B.assign((size_t)s.lenb * s.lenb, 0.0);
+  s.map.resize(std::max(ndiis, 1));
+  for (int k = 0; k < (int)s.map.size(); k++) s.map[k] = k;
+  s.nmat = 1;
+  s.it = 0;
+  s.restarts = 0;
+  s.rms = 0.0;
+  s.ok = false;
+  s.done = max_iter <= 0;
+  s.inf = inf;
+  s.logpos = logpos;
+}
+
+// one iteration after y = op(x) (jacobi_diis.f90:120-160 with diis :183-230)
+int jd_step(ddc_ctx* ctx, JDState& s) {
   const long long n = (long long)ctx->nsph * ctx->nylm;
   const int ndiis = ctx->prm.ndiis;
-  const bool dodiis = ndiis != 0;
   const int nblk = reduce_blocks();
-  double* y = ctx->y.as<double>();
-  double* hx = ctx->hist_x.as<double>();
-  double* he = ctx->hist_e.as<double>();
-  double* xjac = ctx->xn.as<double>();
-  const int lenb = ndiis + 1;
-  std::vector<double> B((size_t)lenb * lenb, 0.0);
-  auto Bm = [&](int j, int k) -> double& { return B[(size_t)(k - 1) * lenb + (j - 1)]; };
-  std::vector<int> map(std::max(ndiis, 1));
-  for (int k = 0; k < (int)map.size(); k++) map[k] = k;
-  int nmat = 1, it = 0, restarts = 0;
-  bool ok = false;
-  double rms = 0.0;
-  std::vector<double> row(kMaxHist + 2);
-  for (it = 1; it <= max_iter; it++) {
-    CKI(op(ctx, x, y));
-    HistPtrs hist{};
-    HistPtrs comb{};
-    const double* xj = xjac;
-    if (dodiis) {
-      const int phys_new = map[nmat - 1];
-      int nm = nmat;
-      std::vector<int> pmap = map;
-      const bool shift = nmat >= ndiis;
-      if (shift) {  // drop the 10 oldest (jacobi_diis.f90:196-205)
-        std::vector<int> r(map.begin() + 10, map.end());
-        r.insert(r.end(), map.begin(), map.begin() + 10);
-        pmap = r;
-        nm = nmat - 10;
-      }
-      hist.n = nm - 1;
-      for (int k = 0; k < nm - 1; k++) hist.p[k] = he + (size_t)pmap[k] * n;
-      double* xnew = hx + (size_t)phys_new * n;
-      double* enew = he + (size_t)phys_new * n;
-      {
-        StageScope sc(ctx, ST_JACOBI);
-        CK(launch_jacobi_step(ctx->L(), ctx->tb, n, rhs, y, x, xnew, enew, hist,
-                            ctx->partials.as<double>(), nblk));
-      }
-      CKI(reduce_to_host(ctx, nm, row.data()));
-      if (shift) {
-        for (int j = 2; j <= nmat - 10; j++)
-          for (int k = 2; k <= nmat - 10; k++) Bm(j, k) = Bm(j + 10, k + 10);
-        map = pmap;
-      }
-      nmat = nm;
-      // makeb (jacobi_diis.f90:232-270)
-      if (nmat == 1) {
-        Bm(1, 1) = 0.0;
-        Bm(1, 2) = 1.0;
-        Bm(2, 1) = 1.0;
-        Bm(2, 2) = row[0];
-      } else {
-        Bm(nmat + 1, 1) = 1.0;
-        Bm(1, nmat + 1) = 1.0;
-        for (int i = 1; i <= nmat - 1; i++) {
-          Bm(nmat + 1, i + 1) = row[i - 1];
-          Bm(i + 1, nmat + 1) = row[i - 1];
-        }
-        Bm(nmat + 1, nmat + 1) = row[nmat - 1];
-      }
-      const int nmat1 = nmat + 1;
-      std::vector<double> bloc((size_t)nmat1 * nmat1), cex(nmat1, 0.0);
-      for (int k = 1; k <= nmat1; k++)
-        for (int j = 1; j <= nmat1; j++) bloc[(size_t)(k - 1) * nmat1 + (j - 1)] = Bm(j, k);
-      cex[0] = 1.0;
-      if (gjinv(nmat1, bloc, cex)) {
-        comb.n = nmat;
-        for (int k = 0; k < nmat; k++) {
-          comb.p[k] = hx + (size_t)map[k] * n;
-          comb.c[k] = cex[k + 1];
-        }
-        nmat = nmat + 1;
-      } else {  // singular: restart the history (jacobi_diis.f90:214-217)
-        nmat = 1;
-        restarts++;
-        comb.n = 0;
-      }
-      xj = xnew;
-    } else {
-      hist.n = 0;
-      StageScope sc(ctx, ST_JACOBI);
-      CK(launch_jacobi_step(ctx->L(), ctx->tb, n, rhs, y, x, hx, he, hist,
-                            ctx->partials.as<double>(), nblk));
-      comb.n = 0;
-      xj = hx;
+  const int lenb = s.lenb;
+  auto Bm = [&](int j, int k) -> double& { return s.B[(size_t)(k - 1) * lenb + (j - 1)]; };
+  ++s.it;
+  HistPtrs hist{};
+  HistPtrs comb{};
+  const double* xj = s.xjac;
+  if (ndiis != 0) {
+    std::vector<double> row(kMaxHist + 2);
+    const int phys_new = s.map[s.nmat - 1];
+    int nm = s.nmat;
+    std::vector<int> pmap = s.map;
+    const bool shift = s.nmat >= ndiis;
+    if (shift) {  // drop the 10 oldest (jacobi_diis.f90:196-205)
+      std::vector<int> r(s.map.begin() + 10, s.map.end());
+      r.insert(r.end(), s.map.begin(), s.map.begin() + 10);
+      pmap = r;
+      nm = s.nmat - 10;
     }
+    hist.n = nm - 1;
+    for (int k = 0; k < nm - 1; k++) hist.p[k] = s.he + (size_t)pmap[k] * n;
+    double* xnew = s.hx + (size_t)phys_new * n;
+    double* enew = s.he + (size_t)phys_new * n;
     {
-      StageScope sc(ctx, ST_COMBINE);
-      CK(launch_diis_combine(ctx->L(), ctx->tb, n, comb, xj, x, ctx->partials.as<double>(),
-                             nblk));
+      StageScope sc(ctx, ST_JACOBI);
+      CK(launch_jacobi_step(ctx->L(), ctx->tb, n, s.rhs, s.y, s.x, xnew, enew, hist,
+                            ctx->partials.as<double>(), nblk));
     }
-    double ss = 0.0;
-    CKI(reduce_to_host(ctx, 1, &ss));
-    rms = std::sqrt(ss / (double)std::max(ctx->nsph, 1));
-    if (*logpos < 256) inf->norms[*logpos] = rms;
-    ++*logpos;
-    if (ctx->prm.iprint > 0) printf("  iter=%4d residual norm: %14.4E\n", *logpos, rms);
-    if (!std::isfinite(rms)) {
-      *iters_done = it;
-      return fail(ctx, DDC_ERR_NUMERIC, "non-finite increment norm");
+    CKI(reduce_to_host(ctx, nm, row.data(), kMaxHist + 1));
+    if (shift) {
+      for (int j = 2; j <= s.nmat - 10; j++)
+        for (int k = 2; k <= s.nmat - 10; k++) Bm(j, k) = Bm(j + 10, k + 10);
+      s.map = pmap;
     }
-    ok = rms < tol;
-    if (ok) break;
+    s.nmat = nm;
+    // makeb (jacobi_diis.f90:232-270)
+    if (s.nmat == 1) {
+      Bm(1, 1) = 0.0;
+      Bm(1, 2) = 1.0;
+      Bm(2, 1) = 1.0;
+      Bm(2, 2) = row[0];
+    } else {
+      Bm(s.nmat + 1, 1) = 1.0;
+      Bm(1, s.nmat + 1) = 1.0;
+      for (int i = 1; i <= s.nmat - 1; i++) {
+        Bm(s.nmat + 1, i + 1) = row[i - 1];
+        Bm(i + 1, s.nmat + 1) = row[i - 1];
+      }
+      Bm(s.nmat + 1, s.nmat + 1) = row[s.nmat - 1];
+    }
+    const int nmat1 = s.nmat + 1;
+    std::vector<double> bloc((size_t)nmat1 * nmat1), cex(nmat1, 0.0);
+    for (int k = 1; k <= nmat1; k++)
+      for (int j = 1; j <= nmat1; j++) bloc[(size_t)(k - 1) * nmat1 + (j - 1)] = Bm(j, k);
+    cex[0] = 1.0;
+    if (gjinv(nmat1, bloc, cex)) {
+      comb.n = s.nmat;
+      for (int k = 0; k < s.nmat; k++) {
+        comb.p[k] = s.hx + (size_t)s.map[k] * n;
+        comb.c[k] = cex[k + 1];
+      }
+      s.nmat = s.nmat + 1;
+    } else {  // singular: restart the history (jacobi_diis.f90:214-217)
+      s.nmat = 1;
+      s.restarts++;
+      comb.n = 0;
+    }
+    xj = xnew;
+  } else {
+    hist.n = 0;
+    StageScope sc(ctx, ST_JACOBI);
+    CK(launch_jacobi_step(ctx->L(), ctx->tb, n, s.rhs, s.y, s.x, s.hx, s.he, hist,
+                          ctx->partials.as<double>(), nblk));
+    comb.n = 0;
+    xj = s.hx;
   }
-  *iters_done = ok ? it : max_iter;
-  *restarts_out += restarts;
-  *last_norm = rms;
-  return ok ? DDC_OK : DDC_ERR_NOCONV;
+  {
+    StageScope sc(ctx, ST_COMBINE);
+    CK(launch_diis_combine(ctx->L(), ctx->tb, n, comb, xj, s.x, ctx->partials.as<double>(),
+                           nblk));
+  }
+  double ss = 0.0;
+  CKI(reduce_to_host(ctx, 1, &ss));
+  s.rms = std::sqrt(ss / (double)std::max(ctx->nsph, 1));
+  if (*s.logpos < 256) s.inf->norms[*s.logpos] = s.rms;
+  ++*s.logpos;
+  if (ctx->prm.iprint > 0) printf("  iter=%4d residual norm: %14.4E\n", *s.logpos, s.rms);
+  if (!std::isfinite(s.rms)) {
+    s.done = true;
+    return fail(ctx, DDC_ERR_NUMERIC, "non-finite increment norm");
+  }
+  s.ok = s.rms < s.tol;
+  s.done = s.ok || s.it >= s.max_iter;
+  return DDC_OK;
 }
 
 // FP64 solve: the reference's Jacobi/DIIS on the FP64 operator.
@@ -732,72 +852,164 @@ int jacobi_diis(ddc_ctx* ctx, OpFn op, const double* rhs, double* x, double tol,
 // the solve stops exactly when the FP64 Jacobi increment is below
 // 10^-iconv.  Otherwise the correction equation L e = r is solved with
 // Jacobi/DIIS on the FP32 operator (from e = d, to 1e-5 relative) and x += e.
-int solve(ddc_ctx* ctx, bool adjoint, const double* rhs, double* x, ddc_solve_info* info) {
-  const double t0 = now_s();
-  const double tol = std::pow(10.0, -(double)ctx->prm.iconv);
-  ddc_solve_info loc{};
-  ddc_solve_info* inf = info ? info : &loc;
+// A SolveTask is one such solve as a resumable state; solve_tasks advances
+// one or two of them, one operator application each per round.
+enum OpKind { OP_NONE = 0, OP_F64 = 1, OP_F32 = 2 };
+struct SolveTask {
+  bool adjoint = false, mixed = false;
+  const double* rhs = nullptr;
+  double* x = nullptr;
+  ddc_solve_info* inf = nullptr;
+  SolveBufs b{};
+  double tol = 0.0, t0 = 0.0, last = 0.0;
+  int phase = 0;  // mixed: 0 = FP64 residual at x next, 1 = inner solve running
+  JDState jd;
+  int logpos = 0, its = 0, restarts = 0, budget = 0, outer = 0;
+  bool done = false, ok = false;
+};
+
+void task_begin(ddc_ctx* ctx, SolveTask& t, bool adjoint, const double* rhs, double* x,
+                ddc_solve_info* inf, int set) {
+  t.adjoint = adjoint;
+  t.mixed = ctx->prm.precision == DDC_PREC_MIXED;
+  t.rhs = rhs;
+  t.x = x;
+  t.inf = inf;
   memset(inf, 0, sizeof(*inf));
-  int logpos = 0, its = 0, restarts = 0;
-  double last = 0.0;
-  int rc;
-  if (ctx->prm.precision != DDC_PREC_MIXED) {
-    rc = jacobi_diis(ctx, adjoint ? op_lstarx : op_lx, rhs, x, tol, ctx->prm.max_iter, inf,
-                     &logpos, &its, &restarts, &last);
-    if (rc != DDC_OK && rc != DDC_ERR_NOCONV) return rc;
-    inf->iterations = its;
-  } else {
-    const long long n = (long long)ctx->nsph * ctx->nylm;
-    const int nblk = reduce_blocks();
-    double* r = ctx->rres.as<double>();
-    double* d = ctx->dres.as<double>();
-    double* e = ctx->eres.as<double>();
-    OpFn op64 = adjoint ? op_lstarx : op_lx;
-    OpFn op32 = adjoint ? op_lstarx_f32 : op_lx_f32;
-    const double rho = 1e-5;
-    int budget = ctx->prm.max_iter, outer = 0;
-    rc = DDC_ERR_NOCONV;
-    while (outer < 64) {
-      ++outer;
-      CKI(op64(ctx, x, ctx->y.as<double>()));
-      {
-        StageScope sc(ctx, ST_JACOBI);
-        CK(launch_residual(ctx->L(), ctx->tb, n, rhs, ctx->y.as<double>(), x, r, d,
-                           ctx->partials.as<double>(), nblk));
-      }
-      double ss = 0.0;
-      CKI(reduce_to_host(ctx, 1, &ss));
-      last = std::sqrt(ss / (double)std::max(ctx->nsph, 1));
-      if (ctx->prm.iprint > 0) printf("  refinement %d: FP64 increment norm %14.4E\n", outer, last);
-      if (!std::isfinite(last)) return fail(ctx, DDC_ERR_NUMERIC, "non-finite increment norm");
-      if (last < tol) {
-        rc = DDC_OK;
-        break;
-      }
-      if (budget <= 0) break;
-      // correction: (D + O32) e = r from e = D^-1 r
-      CK(cudaMemcpyAsync(e, d, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx->st));
-      int done = 0;
-      double inner_last = 0.0;
-      const double itol = std::max(rho * last, 0.3 * tol);
-      int irc = jacobi_diis(ctx, op32, r, e, itol, budget, inf, &logpos, &done, &restarts,
-                            &inner_last);
-      if (irc != DDC_OK && irc != DDC_ERR_NOCONV) return irc;
-      its += done;
-      budget -= done;
-      CK(launch_axpy(ctx->L(), n, 1.0, e, x));
-    }
-    inf->iterations = its;
-    inf->refinements = outer;
+  t.b = solve_bufs(ctx, set);
+  t.tol = std::pow(10.0, -(double)ctx->prm.iconv);
+  t.t0 = now_s();
+  t.phase = 0;
+  t.logpos = t.its = t.restarts = t.outer = 0;
+  t.budget = ctx->prm.max_iter;
+  t.last = 0.0;
+  t.done = t.ok = false;
+  if (!t.mixed) jd_begin(ctx, t.jd, rhs, x, t.tol, ctx->prm.max_iter, t.b, inf, &t.logpos);
+  if (!t.mixed && t.jd.done) t.done = true;
+}
+
+// operator application the task needs next: kind, input, output
+OpKind task_next(const SolveTask& t, const double** in, double** out) {
+  if (t.done) return OP_NONE;
+  if (!t.mixed || t.phase == 1) {
+    *in = t.jd.x;
+    *out = t.jd.y;
+    return t.mixed ? OP_F32 : OP_F64;
   }
-  inf->converged = rc == DDC_OK ? 1 : 0;
-  inf->diis_restarts = restarts;
-  inf->final_norm = last;
-  inf->seconds = now_s() - t0;
-  if (rc == DDC_ERR_NOCONV)
-    return fail(ctx, DDC_ERR_NOCONV, adjoint ? "adjoint ddCOSMO did not converge"
-                                             : "ddCOSMO did not converge");
+  *in = t.x;
+  *out = t.b.y;
+  return OP_F64;
+}
+
+int task_after(ddc_ctx* ctx, SolveTask& t) {
+  if (!t.mixed) {
+    CKI(jd_step(ctx, t.jd));
+    if (t.jd.done) {
+      t.done = true;
+      t.ok = t.jd.ok;
+      t.its = t.jd.ok ? t.jd.it : ctx->prm.max_iter;
+      t.restarts += t.jd.restarts;
+      t.last = t.jd.rms;
+    }
+    return DDC_OK;
+  }
+  const long long n = (long long)ctx->nsph * ctx->nylm;
+  if (t.phase == 1) {
+    CKI(jd_step(ctx, t.jd));
+    if (t.jd.done) {
+      const int done = t.jd.ok ? t.jd.it : t.jd.max_iter;
+      t.its += done;
+      t.budget -= done;
+      t.restarts += t.jd.restarts;
+      CK(launch_axpy(ctx->L(), n, 1.0, t.b.e, t.x));
+      t.phase = 0;
+      if (t.outer >= 64) t.done = true;
+    }
+    return DDC_OK;
+  }
+  // phase 0: y = L x in FP64 is ready
+  ++t.outer;
+  {
+    StageScope sc(ctx, ST_JACOBI);
+    CK(launch_residual(ctx->L(), ctx->tb, n, t.rhs, t.b.y, t.x, t.b.r, t.b.d,
+                       ctx->partials.as<double>(), reduce_blocks()));
+  }
+  double ss = 0.0;
+  CKI(reduce_to_host(ctx, 1, &ss));
+  t.last = std::sqrt(ss / (double)std::max(ctx->nsph, 1));
+  if (ctx->prm.iprint > 0) printf("  refinement %d: FP64 increment norm %14.4E\n", t.outer, t.last);
+  if (!std::isfinite(t.last)) {
+    t.done = true;
+    return fail(ctx, DDC_ERR_NUMERIC, "non-finite increment norm");
+  }
+  if (t.last < t.tol) {
+    t.done = t.ok = true;
+    return DDC_OK;
+  }
+  if (t.budget <= 0) {
+    t.done = true;
+    return DDC_OK;
+  }
+  // correction: (D + O32) e = r from e = D^-1 r
+  CK(cudaMemcpyAsync(t.b.e, t.b.d, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx->st));
+  const double rho = 1e-5;
+  const double itol = std::max(rho * t.last, 0.3 * t.tol);
+  jd_begin(ctx, t.jd, t.b.r, t.b.e, itol, t.budget, t.b, t.inf, &t.logpos);
+  t.phase = 1;
   return DDC_OK;
+}
+
+int op_single(ddc_ctx* ctx, OpKind k, bool adjoint, const double* in, double* out) {
+  if (k == OP_F64) return adjoint ? op_lstarx(ctx, in, out) : op_lx(ctx, in, out);
+  return adjoint ? op_lstarx_f32(ctx, in, out) : op_lx_f32(ctx, in, out);
+}
+
+// Advance the tasks in lockstep.  When a direct and an adjoint task need an
+// operator of the same precision in the same round, both come from one
+// fused pass over the triples (op_pair / op_pair_f32).
+int solve_tasks(ddc_ctx* ctx, SolveTask* t, int nt) {
+  for (;;) {
+    const double* in[2] = {nullptr, nullptr};
+    double* out[2] = {nullptr, nullptr};
+    OpKind k[2] = {OP_NONE, OP_NONE};
+    int active = 0;
+    for (int q = 0; q < nt; q++) {
+      k[q] = task_next(t[q], &in[q], &out[q]);
+      if (k[q] != OP_NONE) active++;
+    }
+    if (!active) break;
+    if (nt == 2 && k[0] != OP_NONE && k[0] == k[1] && t[0].adjoint != t[1].adjoint) {
+      const int dq = t[0].adjoint ? 1 : 0, aq = 1 - dq;
+      if (k[0] == OP_F64) CKI(op_pair(ctx, in[dq], out[dq], in[aq], out[aq]));
+      else CKI(op_pair_f32(ctx, in[dq], out[dq], in[aq], out[aq]));
+    } else {
+      for (int q = 0; q < nt; q++)
+        if (k[q] != OP_NONE) CKI(op_single(ctx, k[q], t[q].adjoint, in[q], out[q]));
+    }
+    for (int q = 0; q < nt; q++)
+      if (k[q] != OP_NONE) CKI(task_after(ctx, t[q]));
+  }
+  int rc = DDC_OK;
+  for (int q = 0; q < nt; q++) {
+    ddc_solve_info* inf = t[q].inf;
+    inf->iterations = t[q].its;
+    inf->refinements = t[q].mixed ? t[q].outer : 0;
+    inf->converged = t[q].ok ? 1 : 0;
+    inf->diis_restarts = t[q].restarts;
+    inf->final_norm = t[q].last;
+    inf->seconds = now_s() - t[q].t0;
+    if (!t[q].ok && rc == DDC_OK)
+      rc = fail(ctx, DDC_ERR_NOCONV, t[q].adjoint ? "adjoint ddCOSMO did not converge"
+                                                  : "ddCOSMO did not converge");
+  }
+  return rc;
+}
+
+int solve(ddc_ctx* ctx, bool adjoint, const double* rhs, double* x, ddc_solve_info* info) {
+  ddc_solve_info loc{};
+  SolveTask t;
+  task_begin(ctx, t, adjoint, rhs, x, info ? info : &loc, 0);
+  return solve_tasks(ctx, &t, 1);
 }
 
 int need_ready(ddc_ctx* ctx) {
@@ -812,6 +1024,17 @@ int dot_dev(ddc_ctx* ctx, long long n, const double* a, const double* b, double*
   return reduce_to_host(ctx, 1, out);
 }
 
+// right-hand side of the direct solve from the cavity potential: wghpot and
+// intrhs (cosmo.f90:104-117)
+int direct_rhs(ddc_ctx* ctx, const double* phi, double* rhs) {
+  CK(ctx->gbuf.ensure(sizeof(double) * std::max<long long>((long long)ctx->nsph * ctx->ngrid, 1)));
+  StageScope sc(ctx, ST_RHS);
+  CK(launch_wghpot(ctx->L(), ctx->geo(), phi, ctx->gbuf.as<double>()));
+  CK(launch_dgemm(ctx->L(), false, ctx->nylm, ctx->nsph, ctx->ngrid, 1.0, ctx->bw.as<double>(),
+                  ctx->nylm, ctx->gbuf.as<double>(), ctx->ngrid, 0.0, rhs, ctx->nylm));
+  return DDC_OK;
+}
+
 // cosmo on device vectors: phi (ncav) or glm -> sigma
 int cosmo_dev(ddc_ctx* ctx, int star, int cart, const double* phi, const double* glm,
               const double* psi, double* sigma, double* esolv, ddc_solve_info* info) {
@@ -820,11 +1043,7 @@ int cosmo_dev(ddc_ctx* ctx, int star, int cart, const double* phi, const double*
   if (!star) {
     double* rhs = ctx->rhs.as<double>();
     if (cart) {
-      CK(ctx->gbuf.ensure(sizeof(double) * std::max<long long>((long long)ctx->nsph * ctx->ngrid, 1)));
-      StageScope sc(ctx, ST_RHS);
-      CK(launch_wghpot(ctx->L(), ctx->geo(), phi, ctx->gbuf.as<double>()));
-      CK(launch_dgemm(ctx->L(), false, ctx->nylm, ctx->nsph, ctx->ngrid, 1.0, ctx->bw.as<double>(),
-                      ctx->nylm, ctx->gbuf.as<double>(), ctx->ngrid, 0.0, rhs, ctx->nylm));
+      CKI(direct_rhs(ctx, phi, rhs));
     } else {
       CK(cudaMemcpyAsync(rhs, glm, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx->st));
     }
@@ -1015,6 +1234,7 @@ int ddc_default_params(ddc_params* p) {
   p->guess = DDC_GUESS_REFERENCE;
   p->device = 0;
   p->device_pointers = 0;
+  p->pair_solves = 1;
   return DDC_OK;
 }
 
@@ -1083,7 +1303,8 @@ const char* ddc_stage_name(int k) {
   static const char* names[ST_N] = {"init",    "coulomb_pot", "rhs",       "lx_pot",
                                     "proj_gemm", "xi_gemm",   "lstarx",    "jacobi_step",
                                     "diis_combine", "reduce", "uchi_pot",  "forces",
-                                    "zeta",    "efield",      "contract"};
+                                    "zeta",    "efield",      "contract",  "lx_lstarx",
+                                    "lx_gather"};
   return (k >= 0 && k < ST_N) ? names[k] : "";
 }
 int ddc_stage_times(ddc_ctx* c, double* ms, long long* calls) {
@@ -1103,7 +1324,10 @@ int ddc_reset_stage_times(ddc_ctx* c) {
   return DDC_OK;
 }
 
-int ddc_fp64_peak(int device, double* gflops) {
+}  // extern "C"
+
+// FMA throughput probe: 8 dependent chains per thread, 8 blocks of 256 per SM
+static int fma_peak(int device, bool fp32, double* gflops) {
   if (!gflops) return DDC_ERR_PARAM;
   if (cudaSetDevice(device) != cudaSuccess) return DDC_ERR_CUDA;
   cudaDeviceProp pr;
@@ -1117,10 +1341,14 @@ int ddc_fp64_peak(int device, double* gflops) {
   cudaMalloc(&out, sizeof(double));
   cudaEventCreate(&a);
   cudaEventCreate(&b);
-  const int blocks = pr.multiProcessorCount * 8, iters = 4096;
-  launch_fp64_probe(L, blocks, 64, out);  // warm up
+  const int blocks = pr.multiProcessorCount * 8, iters = fp32 ? 8192 : 4096;
+  auto run = [&](int it) {
+    if (fp32) launch_fp32_probe(L, blocks, it, reinterpret_cast<float*>(out));
+    else launch_fp64_probe(L, blocks, it, out);
+  };
+  run(64);  // warm up
   cudaEventRecord(a, st);
-  launch_fp64_probe(L, blocks, iters, out);
+  run(iters);
   cudaEventRecord(b, st);
   cudaError_t e = cudaStreamSynchronize(st);
   float ms = 0.f;
@@ -1134,6 +1362,10 @@ int ddc_fp64_peak(int device, double* gflops) {
   *gflops = flops / (ms * 1e-3) / 1e9;
   return DDC_OK;
 }
+
+extern "C" {
+int ddc_fp64_peak(int device, double* gflops) { return fma_peak(device, false, gflops); }
+int ddc_fp32_peak(int device, double* gflops) { return fma_peak(device, true, gflops); }
 
 int ddc_init(ddc_ctx* ctx, int n, const double* x, const double* y, const double* z,
              const double* r) {
@@ -1363,6 +1595,28 @@ int ddc_lstarx(ddc_ctx* ctx, const double* x, double* y) {
   CKI(finish_out(ctx, y, dy, nv));
   return sync(ctx);
 }
+int ddc_lx_lstarx(ddc_ctx* ctx, const double* x, double* y, const double* s, double* z) {
+  CKI(need_ready(ctx));
+  cudaSetDevice(ctx->prm.device);
+  const size_t nv = (size_t)ctx->nsph * ctx->nylm;
+  CK(ctx->tval.ensure(sizeof(double) * std::max<long long>(ctx->ntri, 1)));
+  const double *dx, *ds;
+  CKI(stage_in(ctx, x, nv, ctx->in1, &dx));
+  CKI(stage_in(ctx, s, nv, ctx->in2, &ds));
+  double *dy, *dz;
+  CKI(out_ptr(ctx, y, nv, ctx->out1, &dy));
+  if (ctx->prm.device_pointers) {
+    dz = z;
+  } else {
+    CK(ctx->in3.ensure(sizeof(double) * std::max(nv, (size_t)1)));
+    dz = ctx->in3.as<double>();
+  }
+  if (!dz) return fail(ctx, DDC_ERR_PARAM, "null output array");
+  CKI(op_pair(ctx, dx, dy, ds, dz));
+  CKI(finish_out(ctx, y, dy, nv));
+  CKI(finish_out(ctx, z, dz, nv));
+  return sync(ctx);
+}
 int ddc_ldm1x(ddc_ctx* ctx, const double* x, double* y) {
   CKI(need_ready(ctx));
   cudaSetDevice(ctx->prm.device);
@@ -1431,12 +1685,32 @@ int ddc_energy_forces(ddc_ctx* ctx, int n, const double* charge, const double* x
     CK(cudaMemcpyAsync(dsig, sigma, sizeof(double) * nv, k, ctx->st));
     if (ctx->prm.igrad) CK(cudaMemcpyAsync(ds, s, sizeof(double) * nv, k, ctx->st));
   }
-  CKI(cosmo_dev(ctx, 0, 1, dphi, nullptr, dpsi, dsig, esolv, &inf->direct));
+  const bool paired = ctx->prm.igrad && ctx->prm.pair_solves;
+  if (paired) {
+    // both systems at once: the adjoint right-hand side psi is known before
+    // the direct solve, and each round applies L and L* in one fused pass
+    double* rhs = ctx->rhs.as<double>();
+    CKI(direct_rhs(ctx, dphi, rhs));
+    if (ctx->prm.guess != DDC_GUESS_USER) {
+      const int gmode = ctx->prm.guess == DDC_GUESS_ZERO ? 1 : 0;
+      CK(launch_guess(ctx->L(), ctx->tb, (long long)nv, rhs, dsig, gmode));
+      CK(launch_guess(ctx->L(), ctx->tb, (long long)nv, dpsi, ds, gmode));
+    }
+    SolveTask task[2];
+    task_begin(ctx, task[0], false, rhs, dsig, &inf->direct, 0);
+    task_begin(ctx, task[1], true, dpsi, ds, &inf->adjoint, 1);
+    CKI(solve_tasks(ctx, task, 2));
+    double d = 0.0;
+    CKI(dot_dev(ctx, (long long)nv, dsig, dpsi, &d));
+    *esolv = 0.5 * ((ctx->prm.eps - 1.0) / ctx->prm.eps) * d;
+  } else {
+    CKI(cosmo_dev(ctx, 0, 1, dphi, nullptr, dpsi, dsig, esolv, &inf->direct));
+  }
   double t3 = now_s();
   inf->t_direct = t3 - t2;
   double* dfx = nullptr;
   if (ctx->prm.igrad) {
-    CKI(cosmo_dev(ctx, 1, 0, nullptr, nullptr, dpsi, ds, nullptr, &inf->adjoint));
+    if (!paired) CKI(cosmo_dev(ctx, 1, 0, nullptr, nullptr, dpsi, ds, nullptr, &inf->adjoint));
     double t4 = now_s();
     inf->t_adjoint = t4 - t3;
     CK(ctx->fx.ensure(sizeof(double) * 3 * std::max(N, 1)));

@@ -39,6 +39,11 @@ struct YlmTables {
   double A[DDC_NLM_CAP];          // (2l-1)/(l-m): Legendre recurrence
   double B[DDC_NLM_CAP];          // (l+m-1)/(l-m)
   float Kf[DDC_NLM_CAP], Af[DDC_NLM_CAP], Bf[DDC_NLM_CAP];  // FP32 copies (mixed path)
+  // normalised recurrence of the fused L / L* kernel: Pt_l^m = gam_lm Q_l^m with
+  // Q_m = Pt_m^m, Q_{m+1} = c t Q_m, Q_l = c t Q_{l-1} - beta_lm t^2 Q_{l-2};
+  // Kg = K * gam folds the scale into the contractions
+  double Bn[DDC_NLM_CAP], Kg[DDC_NLM_CAP];
+  float Bnf[DDC_NLM_CAP];
   double eta;
   int lmax, nylm, ngrid;
 };
@@ -75,7 +80,8 @@ struct DevGeo {
 // Stages timed with CUDA events when ddc_params.timing = 1.
 enum Stage {
   ST_INIT = 0, ST_COULOMB, ST_RHS, ST_LX_POT, ST_PROJ, ST_XI, ST_LSTARX, ST_JACOBI,
-  ST_COMBINE, ST_REDUCE, ST_UCHI, ST_FORCES, ST_ZETA, ST_EFIELD, ST_CONTRACT, ST_N
+  ST_COMBINE, ST_REDUCE, ST_UCHI, ST_FORCES, ST_ZETA, ST_EFIELD, ST_CONTRACT, ST_LXS,
+  ST_GATHER, ST_N
 };
 
 // History of DIIS vectors for the fused Jacobi step / extrapolation.
@@ -152,6 +158,13 @@ cudaError_t launch_lstarx_acc(Launch L, const YlmTables& tb, const DevGeo& g, co
 // FP32 operator variants (mixed precision): pot/xi in FP32, y in FP64
 cudaError_t launch_lx_pot_f32(Launch L, const YlmTables& tb, const DevGeo& g, const double* X,
                               float* pot, void* xk);
+// fused L / L*: val (one lx value per triple, gather-list order) and y = L* rows
+cudaError_t launch_lxs(Launch L, const YlmTables& tb, const DevGeo& g, const double* X,
+                       const double* xi, void* xk, double* val, double* y);
+cudaError_t launch_lxs_f32(Launch L, const YlmTables& tb, const DevGeo& g, const double* X,
+                           const float* xi, void* xk, float* val, double* y);
+cudaError_t launch_lx_gather(Launch L, const DevGeo& g, const double* val, double* pot);
+cudaError_t launch_lx_gather_f32(Launch L, const DevGeo& g, const float* val, float* pot);
 cudaError_t launch_lstarx_acc_f32(Launch L, const YlmTables& tb, const DevGeo& g,
                                   const float* xi, double* y);
 // C[M x N] = alpha * op(A) * B in FP32 arithmetic, A float, B float or double, C float/double
@@ -187,9 +200,10 @@ cudaError_t launch_hnorm_partial(Launch L, const YlmTables& tb, long long n, con
                                  double* partials, int nblk);
 cudaError_t launch_dot_partial(Launch L, long long n, const double* a, const double* b,
                                double* partials, int nblk);
-// out[k] = sum_b partials[b*nvals + k], fixed order
+// out[k] = sum_b partials[b*stride + k], k < nvals, fixed order; stride is
+// the row length the producing kernel stores (block_sum_store's NV)
 cudaError_t launch_reduce_partials(Launch L, const double* partials, int nblk, int nvals,
-                                   double* out);
+                                   int stride, double* out);
 int reduce_blocks();
 
 // electrostatics
@@ -230,6 +244,7 @@ cudaError_t launch_batch_ranges(Launch L, int nsph, int ngrid, int ncav, const i
 
 // FP64 FMA throughput probe: each thread runs `iters` x 8 independent FMA chains
 cudaError_t launch_fp64_probe(Launch L, int blocks, int iters, double* out);
+cudaError_t launch_fp32_probe(Launch L, int blocks, int iters, float* out);
 
 cudaError_t launch_csph_pack(Launch L, int n, const double4* sph, double* csph, double* sx,
                              double* sy, double* sz);

@@ -689,7 +689,7 @@ __global__ void __launch_bounds__(128) k_lx2(const YlmTables tb, const DevGeo g,
 }
 
 // K-scaled copy of X in (X_{l,m}, X_{l,-m}) pair layout, [N][NLM]
-template <class Rl>
+template <class Rl, bool GAM = false>
 __global__ void k_xk(const YlmTables tb, int nsph, const double* __restrict__ X,
                      typename RT<Rl>::V2* XK) {
   const int nlm = (tb.lmax + 1) * (tb.lmax + 2) / 2;
@@ -700,7 +700,7 @@ __global__ void k_xk(const YlmTables tb, int nsph, const double* __restrict__ X,
   while (lmi(l + 1, 0) <= le) ++l;
   const int m = le - lmi(l, 0), ind = l * l + l;
   const double* Xi = X + (size_t)i * tb.nylm;
-  const double kk = tb.K[le];
+  const double kk = GAM ? tb.Kg[le] : tb.K[le];
   XK[e] = mk2<Rl>((Rl)(kk * Xi[ind + m]), m ? (Rl)(kk * Xi[ind - m]) : Rl(0));
 }
 
@@ -792,17 +792,19 @@ __device__ __forceinline__ void ls_column(const YlmTables& tb, Rl ct, Rl t2, Rl 
   }
 }
 
-template <int LMAX, int M, int OFF, class Rl>
+// GAM: accumulators of the normalised recurrence (scale Kg instead of K)
+template <int LMAX, int M, int OFF, class Rl, bool GAM = false>
 __device__ __forceinline__ void ls_store(const YlmTables& tb, const Rl* acc, double* yi,
                                          int lane) {
 #pragma unroll
   for (int l = M; l <= LMAX; ++l) {
     const int ind = l * l + l;
+    const double k = GAM ? tb.Kg[lmi(l, M)] : tb.K[lmi(l, M)];
     if (M == 0) {
-      if (lane == 0) yi[ind] = -tb.K[lmi(l, 0)] * (double)acc[OFF + (l - M)];
+      if (lane == 0) yi[ind] = -k * (double)acc[OFF + (l - M)];
     } else if (lane == 0) {
-      yi[ind + M] = -tb.K[lmi(l, M)] * (double)acc[OFF + (l - M)];
-      yi[ind - M] = -tb.K[lmi(l, M)] * (double)acc[OFF + (LMAX + 1 - M) + (l - M)];
+      yi[ind + M] = -k * (double)acc[OFF + (l - M)];
+      yi[ind - M] = -k * (double)acc[OFF + (LMAX + 1 - M) + (l - M)];
     }
   }
 }
@@ -823,7 +825,7 @@ __device__ __forceinline__ void ls_role(const YlmTables& tb, const Rl* sh, int s
   }
 }
 
-template <int LMAX, int R, class Rl>
+template <int LMAX, int R, class Rl, bool GAM = false>
 __device__ __forceinline__ void ls_role_finish(const YlmTables& tb, Rl* acc, double* yi,
                                                int lane) {
   constexpr int NV = ls_role_nvals(LMAX, R);
@@ -832,9 +834,9 @@ __device__ __forceinline__ void ls_role_finish(const YlmTables& tb, Rl* acc, dou
 #pragma unroll
     for (int o = 16; o >= 1; o >>= 1) acc[v] += __shfl_xor_sync(0xffffffffu, acc[v], o);
   }
-  ls_store<LMAX, R, 0, Rl>(tb, acc, yi, lane);
+  ls_store<LMAX, R, 0, Rl, GAM>(tb, acc, yi, lane);
   if constexpr (ls_has2(LMAX, R))
-    ls_store<LMAX, LMAX - R, ls_nvals_m(LMAX, R), Rl>(tb, acc, yi, lane);
+    ls_store<LMAX, LMAX - R, ls_nvals_m(LMAX, R), Rl, GAM>(tb, acc, yi, lane);
 }
 
 // dispatch a runtime role index to the compile-time role code
@@ -848,15 +850,15 @@ __device__ __forceinline__ void ls_run_role(int role, const YlmTables& tb, const
   if constexpr (R + 1 < ls_nroles(LMAX))
     ls_run_role<LMAX, R + 1, Rl>(role, tb, sh, stride, count, lane, acc);
 }
-template <int LMAX, int R, class Rl>
+template <int LMAX, int R, class Rl, bool GAM = false>
 __device__ __forceinline__ void ls_finish_role(int role, const YlmTables& tb, Rl* acc,
                                                double* yi, int lane) {
   if (role == R) {
-    ls_role_finish<LMAX, R, Rl>(tb, acc, yi, lane);
+    ls_role_finish<LMAX, R, Rl, GAM>(tb, acc, yi, lane);
     return;
   }
   if constexpr (R + 1 < ls_nroles(LMAX))
-    ls_finish_role<LMAX, R + 1, Rl>(role, tb, acc, yi, lane);
+    ls_finish_role<LMAX, R + 1, Rl, GAM>(role, tb, acc, yi, lane);
 }
 
 __host__ __device__ constexpr int ls_max_nvals(int L) {
@@ -1354,9 +1356,8 @@ __global__ void k_reduce_partials(const double* __restrict__ partials, int nblk,
   if (threadIdx.x == 0) out[k] = sh[0];
 }
 cudaError_t launch_reduce_partials(Launch L, const double* partials, int nblk, int nvals,
-                                   double* out) {
-  // partial rows are laid out with the stride of the producing kernel
-  int stride = nvals <= 1 ? 1 : kMaxHist + 1;
+                                   int stride, double* out) {
+  if (nvals > stride) return cudaErrorInvalidValue;
   k_reduce_partials<<<nvals, 256, 0, L.st>>>(partials, nblk, stride, out);
   ++*L.launches;
   return cudaGetLastError();
@@ -2211,6 +2212,366 @@ cudaError_t launch_lstarx_acc_f32(Launch L, const YlmTables& tb, const DevGeo& g
   return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// Fused application of L and L* (lx matvec.f90:94-148 with calcv
+// ddcosmo.f90:1671-1746; lstarx matvec.f90:161-235 with adjrhs
+// ddcosmo.f90:1301-1384).  Both operators run over the same triples
+// (a, n, b): grid point n of sphere a inside sphere b (t < 1).  They share
+// the weight W = chi(t) / f_a(n) and the values t^l Y_lm(s), s the unit
+// vector from c_b to c_a + r_a s_n:
+//   lx     (output a):  pot_a(n) += W sum_lm K_lm t^l Y_lm(s) X_b,lm
+//   lstarx (output b):  y_b,lm   -= K_lm w_n xi_a(n) W t^l Y_lm(s)
+// Block per sphere b over its gather list (the lstarx layout), in chunks
+// of one triple per thread, software pipelined over two shared buffers:
+// every thread issues the global loads of its triple of chunk k+1, then the
+// role warps (as in k_lstarx: a role owns the Legendre columns m and
+// lmax-m) run the normalised recurrence over chunk k and feed each value to
+// both contractions (registers accumulate the L* rows, the role's share of
+// each triple's lx value goes to shared memory), then the thread turns its
+// loaded inputs into chunk k+1's fields (prefix Q_m^m with W folded in,
+// cos m phi, sin m phi) in the other buffer.  One barrier per chunk; the
+// load latency hides behind the recurrences.  X_b (K-scaled pairs) sits in
+// the roles' registers.  The lx value of each triple (the roles' shares
+// summed in role order) goes to val[q] in gather-list order; k_lx_gather
+// then sums the triples of each point (a, n).  No atomics: the results are
+// bit-reproducible.
+// ---------------------------------------------------------------------------
+// shared fields per triple: ct, t2, c = w_n xi_a(n), then q0[m] (W and
+// t^m folded in), cos[m], sin[m]
+__host__ __device__ constexpr int lxs_nfields(int L) { return 3 + 3 * (L + 1); }
+
+template <class Rl> __device__ __forceinline__ Rl cBn(const YlmTables& tb, int e);
+template <> __device__ __forceinline__ double cBn<double>(const YlmTables& tb, int e) { return tb.Bn[e]; }
+template <> __device__ __forceinline__ float cBn<float>(const YlmTables& tb, int e) { return tb.Bnf[e]; }
+
+template <int LMAX, int M, int OFF, class Rl>
+__device__ __forceinline__ Rl lxs_column(const YlmTables& tb, Rl ct, Rl t2, Rl q0, Rl cm, Rl sm,
+                                         Rl c, Rl* acc, const Rl* xr) {
+  constexpr int NM = LMAX + 1 - M;
+  Rl q1 = 0, dc = 0, ds = 0;
+  const Rl cmc = cm * c, smc = sm * c;
+#pragma unroll
+  for (int l = M; l <= LMAX; ++l) {
+    Rl Q;
+    if (l == M) {
+      Q = q0;
+    } else if (l == M + 1) {
+      q1 = ct * q0;
+      Q = q1;
+    } else {
+      Q = fma(ct, q1, -(cBn<Rl>(tb, lmi(l, M)) * t2) * q0);
+      q0 = q1;
+      q1 = Q;
+    }
+    if (M == 0) {
+      acc[OFF + l] = fma(Q, c, acc[OFF + l]);
+      dc = fma(Q, xr[OFF + l], dc);
+    } else {
+      acc[OFF + (l - M)] = fma(Q, cmc, acc[OFF + (l - M)]);
+      acc[OFF + NM + (l - M)] = fma(Q, smc, acc[OFF + NM + (l - M)]);
+      dc = fma(Q, xr[OFF + (l - M)], dc);
+      ds = fma(Q, xr[OFF + NM + (l - M)], ds);
+    }
+  }
+  if (M == 0) return dc;
+  return fma(cm, dc, sm * ds);
+}
+
+template <int LMAX, int M, int OFF, class Rl>
+__device__ __forceinline__ void lxs_load_col(const typename RT<Rl>::V2* __restrict__ xb, Rl* xr) {
+  constexpr int NM = LMAX + 1 - M;
+#pragma unroll
+  for (int l = M; l <= LMAX; ++l) {
+    const typename RT<Rl>::V2 v = xb[lmi(l, M)];
+    xr[OFF + (l - M)] = v.x;
+    if (M > 0) xr[OFF + NM + (l - M)] = v.y;
+  }
+}
+
+template <int LMAX, int R, class Rl>
+__device__ __forceinline__ void lxs_load_role(int role, const typename RT<Rl>::V2* xb, Rl* xr) {
+  if (role == R) {
+    lxs_load_col<LMAX, R, 0, Rl>(xb, xr);
+    if constexpr (ls_has2(LMAX, R)) lxs_load_col<LMAX, LMAX - R, ls_nvals_m(LMAX, R), Rl>(xb, xr);
+    return;
+  }
+  if constexpr (R + 1 < ls_nroles(LMAX)) lxs_load_role<LMAX, R + 1, Rl>(role, xb, xr);
+}
+
+// fields stored [field][CH]; lanes take triples q < count
+template <int LMAX, int R, class Rl>
+__device__ __forceinline__ void lxs_role(const YlmTables& tb, const Rl* sh, int count, int lane,
+                                         Rl* acc, const Rl* xr, Rl* lxp) {
+  constexpr int CH = 32 * ls_nroles(LMAX);
+  constexpr int M1 = R, M2 = LMAX - R;
+  for (int q = lane; q < count; q += 32) {
+    const Rl ct = sh[q], t2 = sh[CH + q], c = sh[2 * CH + q];
+    Rl part = lxs_column<LMAX, M1, 0, Rl>(tb, ct, t2, sh[(3 + 3 * M1) * CH + q],
+                                          sh[(4 + 3 * M1) * CH + q], sh[(5 + 3 * M1) * CH + q],
+                                          c, acc, xr);
+    if constexpr (ls_has2(LMAX, R))
+      part += lxs_column<LMAX, M2, ls_nvals_m(LMAX, M1), Rl>(
+          tb, ct, t2, sh[(3 + 3 * M2) * CH + q], sh[(4 + 3 * M2) * CH + q],
+          sh[(5 + 3 * M2) * CH + q], c, acc, xr);
+    lxp[R * CH + q] = part;
+  }
+}
+template <int LMAX, int R, class Rl>
+__device__ __forceinline__ void lxs_run_role(int role, const YlmTables& tb, const Rl* sh,
+                                             int count, int lane, Rl* acc, const Rl* xr,
+                                             Rl* lxp) {
+  if (role == R) {
+    lxs_role<LMAX, R, Rl>(tb, sh, count, lane, acc, xr, lxp);
+    return;
+  }
+  if constexpr (R + 1 < ls_nroles(LMAX))
+    lxs_run_role<LMAX, R + 1, Rl>(role, tb, sh, count, lane, acc, xr, lxp);
+}
+
+// the inputs of one triple's shared fields, loaded one chunk ahead
+template <class Rl>
+struct LxsIn {
+  double4 ca;
+  GP<Rl> gn;
+  double f;
+  Rl xv;
+};
+template <class Rl>
+__device__ __forceinline__ LxsIn<Rl> lxs_load(const DevGeo& g, const Rl* __restrict__ xi, int q) {
+  const int2 an = g.ls[q];
+  const size_t pa = (size_t)an.x * g.ngrid + an.y;
+  LxsIn<Rl> in;
+  in.ca = g.sph[an.x];
+  in.gn = grid_pt(g, an.y, (Rl*)nullptr);
+  in.f = g.fi[pa];
+  in.xv = xi[pa];
+  return in;
+}
+// the shared fields of one triple from its inputs (column col of the buffer)
+template <int LMAX, class Rl>
+__device__ __forceinline__ void lxs_fields(const YlmTables& tb, const LxsIn<Rl>& in, double4 cb,
+                                           Rl irb, Rl* col) {
+  constexpr bool D = sizeof(Rl) == 8;
+  constexpr int CH = 32 * ls_nroles(LMAX);
+  const Rl eta = (Rl)tb.eta, flow = Rl(1) - eta;
+  const Rl fa = Rl(15) * eta - Rl(12), fb = Rl(10) * eta * eta - Rl(15) * eta + Rl(6);
+  const double4 ca = in.ca;
+  const GP<Rl> gn = in.gn;
+  Rl vx, vy, vz;
+  if constexpr (D) {
+    vx = fma(ca.w, gn.x, ca.x) - cb.x;
+    vy = fma(ca.w, gn.y, ca.y) - cb.y;
+    vz = fma(ca.w, gn.z, ca.z) - cb.z;
+  } else {
+    const float ra = (float)ca.w;
+    vx = fmaf(ra, gn.x, (float)(ca.x - cb.x));
+    vy = fmaf(ra, gn.y, (float)(ca.y - cb.y));
+    vz = fmaf(ra, gn.z, (float)(ca.z - cb.z));
+  }
+  const Rl r2 = vx * vx + vy * vy + vz * vz;
+  const Rl rinv = rsqrt_t(r2);
+  const Rl t = r2 * rinv * irb;
+  const Rl sz = vz * rinv;
+  const Rl sth = sqrt_t(fmax(Rl(0), Rl(1) - sz * sz));
+  Rl cp = 1, sp = 0;  // pole: only m = 0 survives
+  if (sth != Rl(0)) {
+    const Rl rs = Rl(1) / sth;
+    cp = vx * rinv * rs;
+    sp = vy * rinv * rs;
+  }
+  Rl chi;
+  if (t >= Rl(1)) chi = 0;
+  else if (t <= flow) chi = 1;
+  else {
+    const Rl xm = t - Rl(1);
+    const Rl ie5 = (Rl)(1.0 / (tb.eta * tb.eta * tb.eta * tb.eta * tb.eta));
+    chi = (xm * xm * (Rl(1) - t)) * ((Rl(6) * t + fa) * t + fb) * ie5;
+  }
+  const Rl f = (Rl)in.f;
+  const Rl W = f > Rl(1) ? chi / f : chi;
+  const Rl st = sth * t;
+  col[0] = sz * t;
+  col[CH] = t * t;
+  col[2 * CH] = gn.w * in.xv;
+  Rl pmm = W, cm = 1, sm = 0, cmm1 = 1, smm1 = 0;
+#pragma unroll
+  for (int m = 0; m <= LMAX; ++m) {
+    if (m == 1) {
+      cm = cp;
+      sm = sp;
+    } else if (m >= 2) {
+      const Rl cn = Rl(2) * cp * cm - cmm1, sn = Rl(2) * cp * sm - smm1;
+      cmm1 = cm; smm1 = sm; cm = cn; sm = sn;
+    }
+    col[(3 + 3 * m) * CH] = pmm;
+    col[(4 + 3 * m) * CH] = cm;
+    col[(5 + 3 * m) * CH] = sm;
+    pmm = -pmm * Rl(2 * m + 1) * st;
+  }
+}
+
+template <int LMAX, class Rl>
+__global__ void __launch_bounds__(32 * ls_nroles(LMAX))
+    k_lxs(const YlmTables tb, const DevGeo g, const typename RT<Rl>::V2* __restrict__ XK,
+          const Rl* __restrict__ xi, Rl* __restrict__ val, double* __restrict__ y) {
+  constexpr int NR = ls_nroles(LMAX);
+  constexpr int CH = 32 * NR;  // triples per chunk = threads per block
+  constexpr int NF = lxs_nfields(LMAX);
+  constexpr int NVM = ls_max_nvals(LMAX);
+  constexpr int NLM = (LMAX + 1) * (LMAX + 2) / 2;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  Rl* fld = reinterpret_cast<Rl*>(smraw);  // [2][NF][CH]
+  Rl* lxp = fld + 2 * NF * CH;             // [2][NR][CH]
+  const int b = blockIdx.x, tid = threadIdx.x;
+  const int role = tid >> 5, lane = tid & 31;
+  const int q0 = g.ls_ptr[b], q1 = g.ls_ptr[b + 1];
+  const int nch = (q1 - q0 + CH - 1) / CH;
+  const double4 cb = g.sph[b];
+  const Rl irb = (Rl)(1.0 / cb.w);
+  Rl acc[NVM], xr[NVM];
+#pragma unroll
+  for (int v = 0; v < NVM; ++v) acc[v] = xr[v] = 0;
+  lxs_load_role<LMAX, 0, Rl>(role, XK + (size_t)b * NLM, xr);
+  if (nch > 0 && tid < min(CH, q1 - q0))
+    lxs_fields<LMAX, Rl>(tb, lxs_load<Rl>(g, xi, q0 + tid), cb, irb, fld + tid);
+  __syncthreads();
+  // chunk k: loads of chunk k+1 in flight while the roles work on chunk k,
+  // then chunk k+1's fields go to the other buffer; one barrier per chunk
+  for (int k = 0; k < nch; ++k) {
+    const int c0 = q0 + k * CH, cnt = min(CH, q1 - c0);
+    const int n1 = k + 1 < nch ? min(CH, q1 - c0 - CH) : 0;
+    LxsIn<Rl> nxt;
+    if (tid < n1) nxt = lxs_load<Rl>(g, xi, c0 + CH + tid);
+    lxs_run_role<LMAX, 0, Rl>(role, tb, fld + (k & 1) * NF * CH, cnt, lane, acc, xr,
+                              lxp + (k & 1) * NR * CH);
+    if (tid < n1) lxs_fields<LMAX, Rl>(tb, nxt, cb, irb, fld + ((k + 1) & 1) * NF * CH + tid);
+    __syncthreads();
+    // lx values of chunk k: the roles' shares in role order (buffer k&1 of
+    // lxp is next written two chunks on, after the next barrier)
+    if (tid < cnt) {
+      const Rl* lp = lxp + (k & 1) * NR * CH;
+      Rl sv = lp[tid];
+#pragma unroll
+      for (int r = 1; r < NR; ++r) sv += lp[r * CH + tid];
+      val[c0 + tid] = sv;
+    }
+  }
+  ls_finish_role<LMAX, 0, Rl, true>(role, tb, acc, y + (size_t)b * tb.nylm, lane);
+}
+
+// pot_a(n) = sum over a's CSR pairs (a, b) of the lx values of the triples
+// (a, n, b), read from b's gather list (pair slot lsstart).  Block per
+// sphere a; warp w takes the pairs p = w, w + NW, ... in order and adds into
+// its own shared row, lanes over the pair's points (distinct within a pair,
+// so no two lanes of a warp touch one entry).  Four strided loads per lane
+// are issued before their adds.  The rows are summed in row order at the
+// end: a fixed summation order, no atomics.
+constexpr int kGatherWarps = 8;  // at most; fewer when NW rows of ngrid do not fit
+template <class Rl>
+__global__ void __launch_bounds__(32 * kGatherWarps)
+    k_lx_gather(const DevGeo g, const Rl* __restrict__ val, Rl* pot) {
+  constexpr int U = 4;
+  const int NW = blockDim.x >> 5;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int G = g.ngrid;
+  const int mb = (g.maxnb + 3) & ~3;
+  int* pst = reinterpret_cast<int*>(smraw);  // [maxnb+1]: pn_ptr of the pairs
+  int* dl = pst + mb + 4;                    // [maxnb]: lsstart - pn_ptr
+  Rl* acc = reinterpret_cast<Rl*>(dl + mb);  // [NW][G]
+  const int a = blockIdx.x, tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
+  const int k0 = g.inl[a], nn = g.inl[a + 1] - k0;
+  for (int k = tid; k <= nn; k += 32 * NW) pst[k] = g.pn_ptr[k0 + k];
+  for (int k = tid; k < nn; k += 32 * NW) dl[k] = g.lsstart[k0 + k] - g.pn_ptr[k0 + k];
+  for (int q = tid; q < NW * G; q += 32 * NW) acc[q] = 0;
+  __syncthreads();
+  Rl* myacc = acc + w * G;
+  for (int p = w; p < nn; p += NW) {
+    const int q0 = pst[p], q1 = pst[p + 1], d = dl[p];
+    for (int base = q0 + lane; base < q1; base += 32 * U) {
+      int n[U];
+      Rl v[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int q = base + 32 * u;
+        n[u] = q < q1 ? (int)g.pn[q] : -1;
+        v[u] = q < q1 ? val[q + d] : Rl(0);
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+        if (n[u] >= 0) myacc[n[u]] += v[u];
+    }
+  }
+  __syncthreads();
+  for (int n = tid; n < G; n += 32 * NW) {
+    Rl sum = acc[n];
+    for (int ww = 1; ww < NW; ++ww) sum += acc[ww * G + n];
+    pot[(size_t)a * G + n] = sum;
+  }
+}
+
+template <class Rl>
+static cudaError_t lxs_launch(Launch L, const YlmTables& tb, const DevGeo& g, const double* X,
+                              const Rl* xi, void* xk, Rl* val, double* y) {
+  if (g.nsph == 0) return cudaSuccess;
+  typedef typename RT<Rl>::V2 V2;
+  const long long nk = (long long)g.nsph * ((tb.lmax + 1) * (tb.lmax + 2) / 2);
+  V2* XK = static_cast<V2*>(xk);
+  k_xk<Rl, true><<<(unsigned)((nk + 255) / 256), 256, 0, L.st>>>(tb, g.nsph, X, XK);
+  ++*L.launches;
+  cudaError_t e = cudaGetLastError();
+  if (e) return e;
+#define CASE(LV)                                                                              \
+  case LV: {                                                                                  \
+    constexpr int NR = ls_nroles(LV);                                                         \
+    const size_t sm = sizeof(Rl) * 2 * (lxs_nfields(LV) + NR) * 32 * NR;                      \
+    if (sm > 48 * 1024)                                                                       \
+      if ((e = cudaFuncSetAttribute(k_lxs<LV, Rl>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                    (int)sm)))                                                \
+        return e;                                                                             \
+    k_lxs<LV, Rl><<<g.nsph, 32 * NR, sm, L.st>>>(tb, g, XK, xi, val, y);                      \
+    break;                                                                                    \
+  }
+  switch (tb.lmax) {
+    DDC_LMAX_CASES(CASE)
+    default:
+      return cudaErrorInvalidValue;
+  }
+#undef CASE
+  ++*L.launches;
+  return cudaGetLastError();
+}
+template <class Rl>
+static cudaError_t gather_launch(Launch L, const DevGeo& g, const Rl* val, Rl* pot) {
+  if (g.nsph == 0) return cudaSuccess;
+  const int mb = (g.maxnb + 3) & ~3;
+  const size_t idx = sizeof(int) * (2 * mb + 4), row = sizeof(Rl) * g.ngrid;
+  const size_t cap = 200 * 1024;  // within the 227 KB opt-in limit
+  const int nw = (int)std::max<size_t>(1, std::min<size_t>(kGatherWarps, (cap - idx) / row));
+  const size_t sm = idx + row * nw;
+  cudaError_t e;
+  if (sm > 48 * 1024)
+    if ((e = cudaFuncSetAttribute(k_lx_gather<Rl>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)sm)))
+      return e;
+  k_lx_gather<Rl><<<g.nsph, 32 * nw, sm, L.st>>>(g, val, pot);
+  ++*L.launches;
+  return cudaGetLastError();
+}
+cudaError_t launch_lxs(Launch L, const YlmTables& tb, const DevGeo& g, const double* X,
+                       const double* xi, void* xk, double* val, double* y) {
+  return lxs_launch<double>(L, tb, g, X, xi, xk, val, y);
+}
+cudaError_t launch_lxs_f32(Launch L, const YlmTables& tb, const DevGeo& g, const double* X,
+                           const float* xi, void* xk, float* val, double* y) {
+  return lxs_launch<float>(L, tb, g, X, xi, xk, val, y);
+}
+cudaError_t launch_lx_gather(Launch L, const DevGeo& g, const double* val, double* pot) {
+  return gather_launch<double>(L, g, val, pot);
+}
+cudaError_t launch_lx_gather_f32(Launch L, const DevGeo& g, const float* val, float* pot) {
+  return gather_launch<float>(L, g, val, pot);
+}
+
 // FP32 GEMM, column-major, 64x64 tiles, 256 threads x 4x4 outputs.
 // TB: float or double input for B (converted when staged), TC: output type.
 template <bool TA, class TB, class TC>
@@ -2630,22 +2991,28 @@ cudaError_t launch_batch_ranges(Launch L, int nsph, int ngrid, int ncav, const i
 }
 
 // FP64 peak probe: 8 independent FMA chains per thread, register resident.
-__global__ void __launch_bounds__(256) k_fp64_probe(int iters, double* out) {
-  double a[8];
+template <class T>
+__global__ void __launch_bounds__(256) k_fma_probe(int iters, T* out) {
+  T a[8];
 #pragma unroll
-  for (int k = 0; k < 8; ++k) a[k] = 1.0 + 1e-9 * (threadIdx.x + k);
-  const double b = 0.999999999, c = 1e-12;
+  for (int k = 0; k < 8; ++k) a[k] = T(1) + T(1e-6) * T(threadIdx.x + k);
+  const T b = T(0.999999), c = T(1e-7);
   for (int it = 0; it < iters; ++it) {
 #pragma unroll
     for (int k = 0; k < 8; ++k) a[k] = fma(a[k], b, c);
   }
-  double s = 0.0;
+  T s = 0;
 #pragma unroll
   for (int k = 0; k < 8; ++k) s += a[k];
-  if (s == 12345.0) out[0] = s;  // keeps the chains live
+  if (s == T(12345)) out[0] = s;  // keeps the chains live
 }
 cudaError_t launch_fp64_probe(Launch L, int blocks, int iters, double* out) {
-  k_fp64_probe<<<blocks, 256, 0, L.st>>>(iters, out);
+  k_fma_probe<double><<<blocks, 256, 0, L.st>>>(iters, out);
+  ++*L.launches;
+  return cudaGetLastError();
+}
+cudaError_t launch_fp32_probe(Launch L, int blocks, int iters, float* out) {
+  k_fma_probe<float><<<blocks, 256, 0, L.st>>>(iters, out);
   ++*L.launches;
   return cudaGetLastError();
 }

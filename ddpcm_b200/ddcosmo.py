@@ -44,7 +44,7 @@ class Params(ctypes.Structure):
                 ("iprint", ctypes.c_int), ("max_iter", ctypes.c_int), ("ndiis", ctypes.c_int),
                 ("precision", ctypes.c_int), ("guess", ctypes.c_int), ("device", ctypes.c_int),
                 ("device_pointers", ctypes.c_int), ("stream", ctypes.c_void_p),
-                ("timing", ctypes.c_int)]
+                ("timing", ctypes.c_int), ("pair_solves", ctypes.c_int)]
 
 
 class SolveInfo(ctypes.Structure):
@@ -101,6 +101,7 @@ _SIGS = {
                          + [ctypes.POINTER(RunInfo)],
     "ddc_lx": [ctypes.c_void_p, _dp, _dp],
     "ddc_lstarx": [ctypes.c_void_p, _dp, _dp],
+    "ddc_lx_lstarx": [ctypes.c_void_p, _dp, _dp, _dp, _dp],
     "ddc_ldm1x": [ctypes.c_void_p, _dp, _dp],
     "ddc_hnorm": [ctypes.c_void_p, _dp, _dp],
     "ddc_rhs": [ctypes.c_void_p, _dp, _dp],
@@ -112,6 +113,7 @@ _SIGS = {
     "ddc_stage_times": [ctypes.c_void_p, _dp, ctypes.POINTER(ctypes.c_longlong)],
     "ddc_reset_stage_times": [ctypes.c_void_p],
     "ddc_fp64_peak": [ctypes.c_int, _dp],
+    "ddc_fp32_peak": [ctypes.c_int, _dp],
     "ddc_batch_energy_forces": [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
                                + [_dp] * 5 + [_dp, _dp, ctypes.POINTER(ctypes.c_int),
                                               ctypes.POINTER(RunInfo)],
@@ -153,6 +155,15 @@ def fp64_peak_gflops(device=0):
     return v.value
 
 
+def fp32_peak_gflops(device=0):
+    """Measured FP32 FMA throughput of the device (GFLOP/s)."""
+    v = ctypes.c_double()
+    st = load_library().ddc_fp32_peak(device, ctypes.byref(v))
+    if st != DDC_OK:
+        raise DDCosmoError(st, "fp32 probe failed")
+    return v.value
+
+
 def _p(a):
     if a is None:
         return None
@@ -170,12 +181,13 @@ class DDCosmo:
 
     Parameters mirror the Input.txt scalars (main.f90:129-136): lmax, ngrid,
     iconv, igrad, eps, eta, iprint; plus max_iter (200), ndiis (25),
-    precision, guess and device.
+    precision, guess, device and pair_solves (energy_forces solves the
+    direct and adjoint systems together with the fused L / L* pass).
     """
 
     def __init__(self, lmax=6, ngrid=110, iconv=7, igrad=1, eps=78.3553, eta=0.2, iprint=0,
                  max_iter=200, ndiis=25, precision=PREC_FP64, guess=GUESS_REFERENCE, device=0,
-                 device_pointers=0, stream=None, timing=0):
+                 device_pointers=0, stream=None, timing=0, pair_solves=1):
         self.L = load_library()
         p = Params()
         self.L.ddc_default_params(ctypes.byref(p))
@@ -184,6 +196,7 @@ class DDCosmo:
         p.max_iter, p.ndiis, p.precision, p.guess, p.device = (max_iter, ndiis, precision, guess,
                                                                 device)
         p.device_pointers, p.timing = int(device_pointers), int(timing)
+        p.pair_solves = int(pair_solves)
         p.stream = stream
         self.params = p
         h = ctypes.c_void_p()
@@ -332,6 +345,14 @@ class DDCosmo:
 
     def lstarx(self, x):        # matvec.f90:161
         return self._op(self.L.ddc_lstarx, x)
+
+    def lx_lstarx(self, x, s):
+        """(lx(x), lstarx(s)) from one fused pass over the triples."""
+        x, s = _f64(x), _f64(s)
+        y = np.zeros((self.nsph, self.nylm))
+        z = np.zeros((self.nsph, self.nylm))
+        self._check(self.L.ddc_lx_lstarx(self.h, _p(x), _p(y), _p(s), _p(z)))
+        return y, z
 
     def ldm1x(self, x):         # matvec.f90:246
         return self._op(self.L.ddc_ldm1x, x)

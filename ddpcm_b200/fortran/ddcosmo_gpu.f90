@@ -22,7 +22,7 @@ module ddcosmo_c
     real(c_double)  :: eps, eta
     integer(c_int)  :: iprint, max_iter, ndiis, precision, guess, device, device_pointers
     type(c_ptr)     :: stream
-    integer(c_int)  :: timing
+    integer(c_int)  :: timing, pair_solves
   end type ddc_params
   type, bind(c) :: ddc_solve_info
     integer(c_int)  :: iterations, converged, diis_restarts, refinements

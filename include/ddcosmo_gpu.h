@@ -64,6 +64,11 @@ typedef struct {
   int device_pointers; /* 0: host arrays, 1: device arrays */
   void* stream;        /* cudaStream_t to run on; NULL: the context's own */
   int timing;          /* 1: time each stage with CUDA events (ddc_stage_times) */
+  int pair_solves;     /* 1 (default): ddc_energy_forces solves the direct and
+                        * adjoint systems together, one fused pass over the
+                        * (sphere, point, neighbour) triples giving both L x
+                        * and L* s per iteration; 0: one after the other as in
+                        * the reference.  Same iterates either way. */
 } ddc_params;
 
 /* Solver report of one cosmo call (replaces the iprint log and the
@@ -88,7 +93,8 @@ typedef struct {
 } ddc_run_info;
 
 /* Defaults: lmax 6, ngrid 110, iconv 7, igrad 1, eps 78.3553, eta 0.2,
- * max_iter 200, ndiis 25, FP64, reference guess, device 0, host pointers. */
+ * max_iter 200, ndiis 25, FP64, reference guess, device 0, host pointers,
+ * paired solves. */
 int ddc_default_params(ddc_params* p);
 
 /* Create / destroy a context (module state; memfree ddcosmo.f90:491). */
@@ -178,6 +184,12 @@ int ddc_lstarx(ddc_ctx* ctx, const double* x, double* y);
 int ddc_ldm1x(ddc_ctx* ctx, const double* x, double* y);
 int ddc_hnorm(ddc_ctx* ctx, const double* x, double* norm);
 
+/* y = off-diagonal L x and z = off-diagonal L* s from one fused pass over the
+ * (sphere, point, neighbour) triples (the operator step of the paired
+ * solves).  No reference counterpart: it equals ddc_lx(x) and ddc_lstarx(s)
+ * (matvec.f90:94, :161) up to rounding.  FP64. */
+int ddc_lx_lstarx(ddc_ctx* ctx, const double* x, double* y, const double* s, double* z);
+
 /* RHS of the direct equation from phi (wghpot + intrhs, cosmo.f90:104-117). */
 int ddc_rhs(ddc_ctx* ctx, const double* phi, double* g);
 
@@ -198,6 +210,9 @@ int ddc_reset_stage_times(ddc_ctx* ctx);
  * reference counterpart: it is the roofline denominator of the FP64-bound
  * kernels. */
 int ddc_fp64_peak(int device, double* gflops);
+/* The same for FP32 FMA: the denominator of the FP32 operator kernels of the
+ * mixed-precision path. */
+int ddc_fp32_peak(int device, double* gflops);
 
 /* efld without any device allocation.  No counterpart in the reference: it
  * serves host programs that own all of the GPU's memory (a QM/MM or MD code
