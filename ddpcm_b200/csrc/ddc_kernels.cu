@@ -2236,9 +2236,16 @@ cudaError_t launch_lstarx_acc_f32(Launch L, const YlmTables& tb, const DevGeo& g
 // then sums the triples of each point (a, n).  No atomics: the results are
 // bit-reproducible.
 // ---------------------------------------------------------------------------
-// shared fields per triple: ct, t2, c = w_n xi_a(n), then q0[m] (W and
-// t^m folded in), cos[m], sin[m]
-__host__ __device__ constexpr int lxs_nfields(int L) { return 3 + 3 * (L + 1); }
+// Shared fields of a chunk, in units of Rl with CH triples: a 4-vector
+// (ct, t2, c = w_n xi_a(n), 0) per triple, then per column m the prefix
+// q0[m] (W and t^m folded in) and the pair (cos m phi, sin m phi).  A role
+// reads a triple with one 4-vector load plus two loads per column.
+__host__ __device__ constexpr int lxs_nfields(int L) { return 4 + 3 * (L + 1); }
+__host__ __device__ constexpr int lxs_q0(int CH, int m) { return 4 * CH + 3 * CH * m; }
+__host__ __device__ constexpr int lxs_cs(int CH, int m) { return 4 * CH + 3 * CH * m + CH; }
+template <class Rl> struct V4T;
+template <> struct V4T<float> { typedef float4 T; };
+template <> struct V4T<double> { typedef double4 T; };
 
 template <class Rl> __device__ __forceinline__ Rl cBn(const YlmTables& tb, int e);
 template <> __device__ __forceinline__ double cBn<double>(const YlmTables& tb, int e) { return tb.Bn[e]; }
@@ -2298,21 +2305,28 @@ __device__ __forceinline__ void lxs_load_role(int role, const typename RT<Rl>::V
   if constexpr (R + 1 < ls_nroles(LMAX)) lxs_load_role<LMAX, R + 1, Rl>(role, xb, xr);
 }
 
-// fields stored [field][CH]; lanes take triples q < count
+// lanes take triples q < count of the chunk's fields sh
 template <int LMAX, int R, class Rl>
 __device__ __forceinline__ void lxs_role(const YlmTables& tb, const Rl* sh, int count, int lane,
                                          Rl* acc, const Rl* xr, Rl* lxp) {
+  typedef typename RT<Rl>::V2 V2;
+  typedef typename V4T<Rl>::T V4;
   constexpr int CH = 32 * ls_nroles(LMAX);
   constexpr int M1 = R, M2 = LMAX - R;
+  const V4* hdr = reinterpret_cast<const V4*>(sh);
+  const Rl* q01 = sh + lxs_q0(CH, M1);
+  const V2* cs1 = reinterpret_cast<const V2*>(sh + lxs_cs(CH, M1));
+  const Rl* q02 = sh + lxs_q0(CH, M2);
+  const V2* cs2 = reinterpret_cast<const V2*>(sh + lxs_cs(CH, M2));
   for (int q = lane; q < count; q += 32) {
-    const Rl ct = sh[q], t2 = sh[CH + q], c = sh[2 * CH + q];
-    Rl part = lxs_column<LMAX, M1, 0, Rl>(tb, ct, t2, sh[(3 + 3 * M1) * CH + q],
-                                          sh[(4 + 3 * M1) * CH + q], sh[(5 + 3 * M1) * CH + q],
-                                          c, acc, xr);
-    if constexpr (ls_has2(LMAX, R))
-      part += lxs_column<LMAX, M2, ls_nvals_m(LMAX, M1), Rl>(
-          tb, ct, t2, sh[(3 + 3 * M2) * CH + q], sh[(4 + 3 * M2) * CH + q],
-          sh[(5 + 3 * M2) * CH + q], c, acc, xr);
+    const V4 h = hdr[q];
+    const V2 c1 = cs1[q];
+    Rl part = lxs_column<LMAX, M1, 0, Rl>(tb, h.x, h.y, q01[q], c1.x, c1.y, h.z, acc, xr);
+    if constexpr (ls_has2(LMAX, R)) {
+      const V2 c2 = cs2[q];
+      part += lxs_column<LMAX, M2, ls_nvals_m(LMAX, M1), Rl>(tb, h.x, h.y, q02[q], c2.x, c2.y,
+                                                             h.z, acc, xr);
+    }
     lxp[R * CH + q] = part;
   }
 }
@@ -2348,9 +2362,19 @@ __device__ __forceinline__ LxsIn<Rl> lxs_load(const DevGeo& g, const Rl* __restr
   return in;
 }
 // the shared fields of one triple from its inputs (column col of the buffer)
+// FP32 path: approximate reciprocal square root and division (about 2 ulp;
+// the FP32 operator only has to be accurate to ~1e-6 for the FP64
+// refinement); FP64 path: IEEE operations
+__device__ __forceinline__ double div_t(double a, double b) { return a / b; }
+__device__ __forceinline__ float div_t(float a, float b) { return __fdividef(a, b); }
+__device__ __forceinline__ double sin_from_cos(double c) { return sqrt(fmax(0.0, 1.0 - c * c)); }
+__device__ __forceinline__ float sin_from_cos(float c) {
+  const float u = 1.f - c * c;
+  return u > 0.f ? u * rsqrtf(u) : 0.f;
+}
 template <int LMAX, class Rl>
 __device__ __forceinline__ void lxs_fields(const YlmTables& tb, const LxsIn<Rl>& in, double4 cb,
-                                           Rl irb, Rl* col) {
+                                           Rl irb, Rl* sh, int tt) {
   constexpr bool D = sizeof(Rl) == 8;
   constexpr int CH = 32 * ls_nroles(LMAX);
   const Rl eta = (Rl)tb.eta, flow = Rl(1) - eta;
@@ -2372,12 +2396,12 @@ __device__ __forceinline__ void lxs_fields(const YlmTables& tb, const LxsIn<Rl>&
   const Rl rinv = rsqrt_t(r2);
   const Rl t = r2 * rinv * irb;
   const Rl sz = vz * rinv;
-  const Rl sth = sqrt_t(fmax(Rl(0), Rl(1) - sz * sz));
+  const Rl sth = sin_from_cos(sz);
   Rl cp = 1, sp = 0;  // pole: only m = 0 survives
   if (sth != Rl(0)) {
-    const Rl rs = Rl(1) / sth;
-    cp = vx * rinv * rs;
-    sp = vy * rinv * rs;
+    const Rl rs = div_t(rinv, sth);
+    cp = vx * rs;
+    sp = vy * rs;
   }
   Rl chi;
   if (t >= Rl(1)) chi = 0;
@@ -2388,11 +2412,16 @@ __device__ __forceinline__ void lxs_fields(const YlmTables& tb, const LxsIn<Rl>&
     chi = (xm * xm * (Rl(1) - t)) * ((Rl(6) * t + fa) * t + fb) * ie5;
   }
   const Rl f = (Rl)in.f;
-  const Rl W = f > Rl(1) ? chi / f : chi;
+  const Rl W = f > Rl(1) ? div_t(chi, f) : chi;
   const Rl st = sth * t;
-  col[0] = sz * t;
-  col[CH] = t * t;
-  col[2 * CH] = gn.w * in.xv;
+  typedef typename RT<Rl>::V2 V2;
+  typedef typename V4T<Rl>::T V4;
+  V4 h;
+  h.x = sz * t;
+  h.y = t * t;
+  h.z = gn.w * in.xv;
+  h.w = 0;
+  reinterpret_cast<V4*>(sh)[tt] = h;
   Rl pmm = W, cm = 1, sm = 0, cmm1 = 1, smm1 = 0;
 #pragma unroll
   for (int m = 0; m <= LMAX; ++m) {
@@ -2403,15 +2432,18 @@ __device__ __forceinline__ void lxs_fields(const YlmTables& tb, const LxsIn<Rl>&
       const Rl cn = Rl(2) * cp * cm - cmm1, sn = Rl(2) * cp * sm - smm1;
       cmm1 = cm; smm1 = sm; cm = cn; sm = sn;
     }
-    col[(3 + 3 * m) * CH] = pmm;
-    col[(4 + 3 * m) * CH] = cm;
-    col[(5 + 3 * m) * CH] = sm;
+    sh[lxs_q0(CH, m) + tt] = pmm;
+    V2 c2;
+    c2.x = cm;
+    c2.y = sm;
+    reinterpret_cast<V2*>(sh + lxs_cs(CH, m))[tt] = c2;
     pmm = -pmm * Rl(2 * m + 1) * st;
   }
 }
 
+// FP32 up to lmax 10: three blocks per SM (caps the registers at 112)
 template <int LMAX, class Rl>
-__global__ void __launch_bounds__(32 * ls_nroles(LMAX))
+__global__ void __launch_bounds__(32 * ls_nroles(LMAX), sizeof(Rl) == 4 && LMAX <= 10 ? 3 : 1)
     k_lxs(const YlmTables tb, const DevGeo g, const typename RT<Rl>::V2* __restrict__ XK,
           const Rl* __restrict__ xi, Rl* __restrict__ val, double* __restrict__ y) {
   constexpr int NR = ls_nroles(LMAX);
@@ -2433,7 +2465,7 @@ __global__ void __launch_bounds__(32 * ls_nroles(LMAX))
   for (int v = 0; v < NVM; ++v) acc[v] = xr[v] = 0;
   lxs_load_role<LMAX, 0, Rl>(role, XK + (size_t)b * NLM, xr);
   if (nch > 0 && tid < min(CH, q1 - q0))
-    lxs_fields<LMAX, Rl>(tb, lxs_load<Rl>(g, xi, q0 + tid), cb, irb, fld + tid);
+    lxs_fields<LMAX, Rl>(tb, lxs_load<Rl>(g, xi, q0 + tid), cb, irb, fld, tid);
   __syncthreads();
   // chunk k: loads of chunk k+1 in flight while the roles work on chunk k,
   // then chunk k+1's fields go to the other buffer; one barrier per chunk
@@ -2444,7 +2476,7 @@ __global__ void __launch_bounds__(32 * ls_nroles(LMAX))
     if (tid < n1) nxt = lxs_load<Rl>(g, xi, c0 + CH + tid);
     lxs_run_role<LMAX, 0, Rl>(role, tb, fld + (k & 1) * NF * CH, cnt, lane, acc, xr,
                               lxp + (k & 1) * NR * CH);
-    if (tid < n1) lxs_fields<LMAX, Rl>(tb, nxt, cb, irb, fld + ((k + 1) & 1) * NF * CH + tid);
+    if (tid < n1) lxs_fields<LMAX, Rl>(tb, nxt, cb, irb, fld + ((k + 1) & 1) * NF * CH, tid);
     __syncthreads();
     // lx values of chunk k: the roles' shares in role order (buffer k&1 of
     // lxp is next written two chunks on, after the next barrier)
@@ -2524,10 +2556,14 @@ static cudaError_t lxs_launch(Launch L, const YlmTables& tb, const DevGeo& g, co
   case LV: {                                                                                  \
     constexpr int NR = ls_nroles(LV);                                                         \
     const size_t sm = sizeof(Rl) * 2 * (lxs_nfields(LV) + NR) * 32 * NR;                      \
-    if (sm > 48 * 1024)                                                                       \
+    if (sm > 48 * 1024) {                                                                     \
       if ((e = cudaFuncSetAttribute(k_lxs<LV, Rl>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
                                     (int)sm)))                                                \
         return e;                                                                             \
+      if ((e = cudaFuncSetAttribute(k_lxs<LV, Rl>,                                            \
+                                    cudaFuncAttributePreferredSharedMemoryCarveout, 100)))    \
+        return e;                                                                             \
+    }                                                                                         \
     k_lxs<LV, Rl><<<g.nsph, 32 * NR, sm, L.st>>>(tb, g, XK, xi, val, y);                      \
     break;                                                                                    \
   }
