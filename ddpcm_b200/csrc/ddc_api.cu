@@ -716,12 +716,17 @@ struct JDState {
   int lenb = 0, nmat = 1, it = 0, restarts = 0;
   double rms = 0.0;
   bool done = false, ok = false;
+  bool f32 = false;  // history vectors in FP32 (inner solves of the mixed path)
   ddc_solve_info* inf = nullptr;
   int* logpos = nullptr;
+  // history slot k of hx / he in the history precision
+  void* slot(double* base, int k, long long n) const {
+    return reinterpret_cast<char*>(base) + (size_t)k * n * (f32 ? sizeof(float) : sizeof(double));
+  }
 };
 
 void jd_begin(ddc_ctx* ctx, JDState& s, const double* rhs, double* x, double tol, int max_iter,
-              const SolveBufs& b, ddc_solve_info* inf, int* logpos) {
+              const SolveBufs& b, ddc_solve_info* inf, int* logpos, bool f32 = false) {
   const int ndiis = ctx->prm.ndiis;
   s.rhs = rhs;
   s.x = x;
@@ -741,6 +746,7 @@ void jd_begin(ddc_ctx* ctx, JDState& s, const double* rhs, double* x, double tol
   s.rms = 0.0;
   s.ok = false;
   s.done = max_iter <= 0;
+  s.f32 = f32;
   s.inf = inf;
   s.logpos = logpos;
 }
@@ -755,7 +761,7 @@ int jd_step(ddc_ctx* ctx, JDState& s) {
   ++s.it;
   HistPtrs hist{};
   HistPtrs comb{};
-  const double* xj = s.xjac;
+  const void* xj = s.xjac;
   if (ndiis != 0) {
     std::vector<double> row(kMaxHist + 2);
     const int phys_new = s.map[s.nmat - 1];
@@ -769,13 +775,13 @@ int jd_step(ddc_ctx* ctx, JDState& s) {
       nm = s.nmat - 10;
     }
     hist.n = nm - 1;
-    for (int k = 0; k < nm - 1; k++) hist.p[k] = s.he + (size_t)pmap[k] * n;
-    double* xnew = s.hx + (size_t)phys_new * n;
-    double* enew = s.he + (size_t)phys_new * n;
+    for (int k = 0; k < nm - 1; k++) hist.p[k] = s.slot(s.he, pmap[k], n);
+    void* xnew = s.slot(s.hx, phys_new, n);
+    void* enew = s.slot(s.he, phys_new, n);
     {
       StageScope sc(ctx, ST_JACOBI);
       CK(launch_jacobi_step(ctx->L(), ctx->tb, n, s.rhs, s.y, s.x, xnew, enew, hist,
-                            ctx->partials.as<double>(), nblk));
+                            ctx->partials.as<double>(), nblk, s.f32));
     }
     CKI(reduce_to_host(ctx, nm, row.data(), kMaxHist + 1));
     if (shift) {
@@ -807,7 +813,7 @@ int jd_step(ddc_ctx* ctx, JDState& s) {
     if (gjinv(nmat1, bloc, cex)) {
       comb.n = s.nmat;
       for (int k = 0; k < s.nmat; k++) {
-        comb.p[k] = s.hx + (size_t)s.map[k] * n;
+        comb.p[k] = s.slot(s.hx, s.map[k], n);
         comb.c[k] = cex[k + 1];
       }
       s.nmat = s.nmat + 1;
@@ -821,14 +827,14 @@ int jd_step(ddc_ctx* ctx, JDState& s) {
     hist.n = 0;
     StageScope sc(ctx, ST_JACOBI);
     CK(launch_jacobi_step(ctx->L(), ctx->tb, n, s.rhs, s.y, s.x, s.hx, s.he, hist,
-                          ctx->partials.as<double>(), nblk));
+                          ctx->partials.as<double>(), nblk, s.f32));
     comb.n = 0;
     xj = s.hx;
   }
   {
     StageScope sc(ctx, ST_COMBINE);
     CK(launch_diis_combine(ctx->L(), ctx->tb, n, comb, xj, s.x, ctx->partials.as<double>(),
-                           nblk));
+                           nblk, s.f32));
   }
   double ss = 0.0;
   CKI(reduce_to_host(ctx, 1, &ss));
@@ -954,7 +960,8 @@ int task_after(ddc_ctx* ctx, SolveTask& t) {
   CK(cudaMemcpyAsync(t.b.e, t.b.d, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx->st));
   const double rho = 1e-5;
   const double itol = std::max(rho * t.last, 0.3 * t.tol);
-  jd_begin(ctx, t.jd, t.b.r, t.b.e, itol, t.budget, t.b, t.inf, &t.logpos);
+  // the correction is wanted to ~1e-5 relative: FP32 history vectors suffice
+  jd_begin(ctx, t.jd, t.b.r, t.b.e, itol, t.budget, t.b, t.inf, &t.logpos, true);
   t.phase = 1;
   return DDC_OK;
 }

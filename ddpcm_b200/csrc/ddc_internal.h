@@ -86,8 +86,9 @@ enum Stage {
 
 // History of DIIS vectors for the fused Jacobi step / extrapolation.
 constexpr int kMaxHist = 32;
+// The vectors are FP64, or FP32 for the inner solves of the mixed path.
 struct HistPtrs {
-  const double* p[kMaxHist];
+  const void* p[kMaxHist];
   double c[kMaxHist];
   int n;
 };
@@ -189,13 +190,15 @@ cudaError_t launch_guess(Launch L, const YlmTables& tb, long long n, const doubl
                          double* x, int mode);
 
 // solver
-// xnew = facl*(rhs - y); e = xnew - x; partial dots e.h_k (k < hist.n) and e.e
+// xnew = facl*(rhs - y); e = xnew - x; partial dots e.h_k (k < hist.n) and e.e.
+// xnew, e and the history are FP32 when f32 (mixed-path inner solves), else FP64.
 cudaError_t launch_jacobi_step(Launch L, const YlmTables& tb, long long n, const double* rhs,
-                               const double* y, const double* x, double* xnew, double* e,
-                               const HistPtrs& hist, double* partials, int nblk);
+                               const double* y, const double* x, void* xnew, void* e,
+                               const HistPtrs& hist, double* partials, int nblk, bool f32);
 // xout = sum c_k p_k (or xjac if hist.n == 0); partial of sum_l 1/(l+1) (xout-x)^2; x = xout
 cudaError_t launch_diis_combine(Launch L, const YlmTables& tb, long long n, const HistPtrs& hist,
-                                const double* xjac, double* x, double* partials, int nblk);
+                                const void* xjac, double* x, double* partials, int nblk,
+                                bool f32);
 cudaError_t launch_hnorm_partial(Launch L, const YlmTables& tb, long long n, const double* x,
                                  double* partials, int nblk);
 cudaError_t launch_dot_partial(Launch L, long long n, const double* a, const double* b,

@@ -1173,6 +1173,24 @@ __device__ __forceinline__ int l_of(int lm) {
   return l;
 }
 
+// Grid-stride walk over the (nylm, nsph) vectors that keeps the harmonic
+// index lm = q mod nylm incrementally (no 64-bit division per element).
+struct LmWalk {
+  long long q, stride;
+  int lm, dlm, nylm;
+  __device__ LmWalk(int nylm_) : nylm(nylm_) {
+    q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    stride = (long long)gridDim.x * blockDim.x;
+    lm = (int)(q % nylm);
+    dlm = (int)(stride % nylm);
+  }
+  __device__ void next() {
+    q += stride;
+    lm += dlm;
+    if (lm >= nylm) lm -= nylm;
+  }
+};
+
 __global__ void k_ldm1x(const YlmTables tb, long long n, const double* __restrict__ x, double* y) {
   long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= n) return;
@@ -1235,27 +1253,27 @@ __device__ __forceinline__ void block_sum_store(double (&v)[NV], int nv, double*
 
 // Jacobi step + DIIS Gram row: xnew = D^-1 (rhs - Ox) (jacobi_diis.f90:105-110),
 // e = xnew - x (:117), dots e.h_k for the history and e.e (makeb :232-270).
+template <class H>
 __global__ void __launch_bounds__(256) k_jacobi_step(const YlmTables tb, long long n,
                                                      const double* __restrict__ rhs,
                                                      const double* __restrict__ y,
-                                                     const double* __restrict__ x, double* xnew,
-                                                     double* e, const HistPtrs hist,
+                                                     const double* __restrict__ x, H* xnew,
+                                                     H* e, const HistPtrs hist,
                                                      double* partials) {
   double d[kMaxHist + 1];
 #pragma unroll
   for (int k = 0; k <= kMaxHist; ++k) d[k] = 0.0;
   const int nh = hist.n;
-  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n;
-       q += (long long)gridDim.x * blockDim.x) {
-    int lm = (int)(q % tb.nylm);
-    double xn = tb.facl[l_of(lm)] * (rhs[q] - y[q]);
-    double ev = xn - x[q];
-    xnew[q] = xn;
+  for (LmWalk w(tb.nylm); w.q < n; w.next()) {
+    const long long q = w.q;
+    double xn = tb.facl[l_of(w.lm)] * (rhs[q] - y[q]);
+    const H hx = (H)xn, ev = (H)(xn - x[q]);
+    xnew[q] = hx;
     e[q] = ev;
 #pragma unroll
     for (int k = 0; k < kMaxHist; ++k)
-      if (k < nh) d[k] = fma(ev, hist.p[k][q], d[k]);
-    d[kMaxHist] = fma(ev, ev, d[kMaxHist]);
+      if (k < nh) d[k] = fma((double)ev, (double)static_cast<const H*>(hist.p[k])[q], d[k]);
+    d[kMaxHist] = fma((double)ev, (double)ev, d[kMaxHist]);
   }
   // move e.e to slot nh so the partial row is [e.h_0 .. e.h_{nh-1}, e.e]
   double v[kMaxHist + 1];
@@ -1264,33 +1282,40 @@ __global__ void __launch_bounds__(256) k_jacobi_step(const YlmTables tb, long lo
   block_sum_store<kMaxHist + 1>(v, nh + 1, partials);
 }
 cudaError_t launch_jacobi_step(Launch L, const YlmTables& tb, long long n, const double* rhs,
-                               const double* y, const double* x, double* xnew, double* e,
-                               const HistPtrs& hist, double* partials, int nblk) {
-  k_jacobi_step<<<nblk, 256, 0, L.st>>>(tb, n, rhs, y, x, xnew, e, hist, partials);
+                               const double* y, const double* x, void* xnew, void* e,
+                               const HistPtrs& hist, double* partials, int nblk, bool f32) {
+  if (f32)
+    k_jacobi_step<float><<<nblk, 256, 0, L.st>>>(tb, n, rhs, y, x, static_cast<float*>(xnew),
+                                                 static_cast<float*>(e), hist, partials);
+  else
+    k_jacobi_step<double><<<nblk, 256, 0, L.st>>>(tb, n, rhs, y, x, static_cast<double*>(xnew),
+                                                  static_cast<double*>(e), hist, partials);
   ++*L.launches;
   return cudaGetLastError();
 }
 
 // DIIS extrapolation (jacobi_diis.f90:222-226) + increment norm (hnorm,
 // matvec.f90:281-323: sum over spheres of sum_l 1/(l+1) |u_l|^2) + update.
+template <class H>
 __global__ void __launch_bounds__(256) k_diis_combine(const YlmTables tb, long long n,
                                                       const HistPtrs hist,
-                                                      const double* __restrict__ xjac, double* x,
+                                                      const H* __restrict__ xjac, double* x,
                                                       double* partials) {
   double acc = 0.0;
   const int nh = hist.n;
-  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n;
-       q += (long long)gridDim.x * blockDim.x) {
+  for (LmWalk w(tb.nylm); w.q < n; w.next()) {
+    const long long q = w.q;
     double xo;
     if (nh == 0) {
       xo = xjac[q];
     } else {
       xo = 0.0;
 #pragma unroll 4
-      for (int k = 0; k < nh; ++k) xo = fma(hist.c[k], hist.p[k][q], xo);
+      for (int k = 0; k < nh; ++k)
+        xo = fma(hist.c[k], (double)static_cast<const H*>(hist.p[k])[q], xo);
     }
     double d = xo - x[q];
-    int l = l_of((int)(q % tb.nylm));
+    int l = l_of(w.lm);
     acc = fma(d * d, 1.0 / (1.0 + l), acc);
     x[q] = xo;
   }
@@ -1298,8 +1323,14 @@ __global__ void __launch_bounds__(256) k_diis_combine(const YlmTables tb, long l
   block_sum_store<1>(v, 1, partials);
 }
 cudaError_t launch_diis_combine(Launch L, const YlmTables& tb, long long n, const HistPtrs& hist,
-                                const double* xjac, double* x, double* partials, int nblk) {
-  k_diis_combine<<<nblk, 256, 0, L.st>>>(tb, n, hist, xjac, x, partials);
+                                const void* xjac, double* x, double* partials, int nblk,
+                                bool f32) {
+  if (f32)
+    k_diis_combine<float><<<nblk, 256, 0, L.st>>>(tb, n, hist, static_cast<const float*>(xjac),
+                                                  x, partials);
+  else
+    k_diis_combine<double><<<nblk, 256, 0, L.st>>>(tb, n, hist,
+                                                   static_cast<const double*>(xjac), x, partials);
   ++*L.launches;
   return cudaGetLastError();
 }
@@ -1591,6 +1622,74 @@ __global__ void __launch_bounds__(kNbTile) k_efield_f(int nsrc, const double* __
     o[2] = ez;
   }
 }
+// One molecule: two targets per thread (targets t and t + kNbTile of a
+// 2*kNbTile block), so each broadcast source read serves both.  Same
+// arithmetic per pair and the same summation order per target as k_efield_f.
+__global__ void __launch_bounds__(kNbTile) k_efield_f2(int nsrc, const double* __restrict__ q,
+                                                       const double* __restrict__ csrc, int ntrg,
+                                                       const double* __restrict__ ctrg,
+                                                       int chunk, double* out) {
+  __shared__ float4 src[kNbTile];
+  const int tb0 = blockIdx.x * 2 * kNbTile;
+  const int c = blockIdx.y;
+  const double ox = ctrg[3 * (size_t)tb0], oy = ctrg[3 * (size_t)tb0 + 1],
+               oz = ctrg[3 * (size_t)tb0 + 2];
+  float p[2][3];
+  int tt[2];
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int t = tb0 + h * kNbTile + threadIdx.x;
+    tt[h] = t;
+    p[h][0] = p[h][1] = p[h][2] = 0.f;
+    if (t < ntrg) {
+      p[h][0] = (float)(ctrg[3 * (size_t)t] - ox);
+      p[h][1] = (float)(ctrg[3 * (size_t)t + 1] - oy);
+      p[h][2] = (float)(ctrg[3 * (size_t)t + 2] - oz);
+    }
+  }
+  double e[2][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
+  const int s0 = c * chunk, s1 = min(nsrc, c * chunk + chunk);
+  for (int j0 = s0; j0 < s1; j0 += kNbTile) {
+    const int j = j0 + threadIdx.x;
+    __syncthreads();
+    src[threadIdx.x] = j < s1 ? make_float4((float)(csrc[3 * (size_t)j] - ox),
+                                            (float)(csrc[3 * (size_t)j + 1] - oy),
+                                            (float)(csrc[3 * (size_t)j + 2] - oz), (float)q[j])
+                              : make_float4(0.f, 0.f, 0.f, 0.f);
+    __syncthreads();
+    const int cnt = min(kNbTile, s1 - j0);
+    float f[2][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
+#pragma unroll 4
+    for (int k = 0; k < cnt; ++k) {
+      const float4 sv = src[k];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const float dx = p[h][0] - sv.x, dy = p[h][1] - sv.y, dz = p[h][2] - sv.z;
+        const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+        const float ri = rsqrtf(r2);
+        const float w = sv.w * (ri * ri * ri);
+        f[h][0] = fmaf(w, dx, f[h][0]);
+        f[h][1] = fmaf(w, dy, f[h][1]);
+        f[h][2] = fmaf(w, dz, f[h][2]);
+      }
+    }
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      e[h][0] += f[h][0];
+      e[h][1] += f[h][1];
+      e[h][2] += f[h][2];
+    }
+  }
+#pragma unroll
+  for (int h = 0; h < 2; ++h)
+    if (tt[h] < ntrg) {
+      double* o = out + ((size_t)c * ntrg + tt[h]) * 3;
+      o[0] = e[h][0];
+      o[1] = e[h][1];
+      o[2] = e[h][2];
+    }
+}
+
 cudaError_t launch_efield_f32(Launch L, int nsrc, const double* q, const double* csrc, int ntrg,
                               const double* ctrg, double* ef, double* scratch, int nchunk,
                               const int2* trange) {
@@ -1598,9 +1697,15 @@ cudaError_t launch_efield_f32(Launch L, int nsrc, const double* q, const double*
   int chunk = (nsrc + nchunk - 1) / max(nchunk, 1);
   chunk = ((chunk + kNbTile - 1) / kNbTile) * kNbTile;
   if (chunk == 0) chunk = kNbTile;
-  dim3 grid((ntrg + kNbTile - 1) / kNbTile, nchunk);
   double* out = nchunk == 1 ? ef : scratch;
-  k_efield_f<<<grid, kNbTile, 0, L.st>>>(nsrc, q, csrc, ntrg, ctrg, chunk, out, trange);
+  const int tiles2 = (ntrg + 2 * kNbTile - 1) / (2 * kNbTile);
+  if (!trange && (long long)tiles2 * nchunk >= 148 * 8) {  // enough blocks to fill the GPU
+    dim3 grid2(tiles2, nchunk);
+    k_efield_f2<<<grid2, kNbTile, 0, L.st>>>(nsrc, q, csrc, ntrg, ctrg, chunk, out);
+  } else {
+    dim3 grid((ntrg + kNbTile - 1) / kNbTile, nchunk);
+    k_efield_f<<<grid, kNbTile, 0, L.st>>>(nsrc, q, csrc, ntrg, ctrg, chunk, out, trange);
+  }
   ++*L.launches;
   cudaError_t e = cudaGetLastError();
   if (e || nchunk == 1) return e;
@@ -2704,9 +2809,9 @@ __global__ void __launch_bounds__(256) k_residual(const YlmTables tb, long long 
                                                   const double* __restrict__ x, double* r,
                                                   double* d, double* partials) {
   double acc = 0.0;
-  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n;
-       q += (long long)gridDim.x * blockDim.x) {
-    int l = l_of((int)(q % tb.nylm));
+  for (LmWalk w(tb.nylm); w.q < n; w.next()) {
+    const long long q = w.q;
+    int l = l_of(w.lm);
     double fl = tb.facl[l];
     double rv = rhs[q] - y[q] - x[q] / fl;
     double dv = fl * rv;
