@@ -1230,7 +1230,9 @@ cudaError_t launch_guess(Launch L, const YlmTables& tb, long long n, const doubl
 
 int reduce_blocks() { return 148 * 4; }
 
-template <int NV>
+// block sums of v[0..nv) into partials[blockIdx.x * STRIDE + k] (blocks of
+// at most 256 threads)
+template <int NV, int STRIDE = NV>
 __device__ __forceinline__ void block_sum_store(double (&v)[NV], int nv, double* partials) {
   __shared__ double sh[NV][8];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -1247,49 +1249,110 @@ __device__ __forceinline__ void block_sum_store(double (&v)[NV], int nv, double*
   if (threadIdx.x < nv) {
     double s = 0.0;
     for (int ww = 0; ww < (int)(blockDim.x >> 5); ++ww) s += sh[threadIdx.x][ww];
-    partials[(size_t)blockIdx.x * NV + threadIdx.x] = s;
+    partials[(size_t)blockIdx.x * STRIDE + threadIdx.x] = s;
   }
+}
+
+// Element tiles of the solver kernels: a block takes 4 x 256 consecutive
+// elements per step, thread t the elements t, t+256, t+512, t+768, so that
+// each thread has four independent loads of every vector in flight.
+constexpr int kSolU = 4, kSolT = 256;
+__device__ __forceinline__ int lm_first(long long q, int nylm) { return (int)(q % nylm); }
+__device__ __forceinline__ int lm_add(int lm, int d, int nylm) {
+  lm += d;
+  return lm >= nylm ? lm - nylm : lm;
 }
 
 // Jacobi step + DIIS Gram row: xnew = D^-1 (rhs - Ox) (jacobi_diis.f90:105-110),
 // e = xnew - x (:117), dots e.h_k for the history and e.e (makeb :232-270).
-template <class H>
-__global__ void __launch_bounds__(256) k_jacobi_step(const YlmTables tb, long long n,
-                                                     const double* __restrict__ rhs,
-                                                     const double* __restrict__ y,
-                                                     const double* __restrict__ x, H* xnew,
-                                                     H* e, const HistPtrs hist,
-                                                     double* partials) {
-  double d[kMaxHist + 1];
+// NB >= hist.n bounds the accumulators (bucketed at launch); the partial row
+// keeps the stride kMaxHist + 1 that the host-side reduction expects.
+template <class H, int NB>
+__global__ void __launch_bounds__(kSolT) k_jacobi_step(const YlmTables tb, long long n,
+                                                       const double* __restrict__ rhs,
+                                                       const double* __restrict__ y,
+                                                       const double* __restrict__ x, H* xnew,
+                                                       H* e, const HistPtrs hist,
+                                                       double* partials) {
+  constexpr int U = 2 * kSolU;  // eight elements per thread and step
+  double d[NB + 1];
 #pragma unroll
-  for (int k = 0; k <= kMaxHist; ++k) d[k] = 0.0;
-  const int nh = hist.n;
-  for (LmWalk w(tb.nylm); w.q < n; w.next()) {
-    const long long q = w.q;
-    double xn = tb.facl[l_of(w.lm)] * (rhs[q] - y[q]);
-    const H hx = (H)xn, ev = (H)(xn - x[q]);
-    xnew[q] = hx;
-    e[q] = ev;
+  for (int k = 0; k <= NB; ++k) d[k] = 0.0;
+  const int nh = hist.n, nylm = tb.nylm;
+  const int dt = kSolT % nylm;
+  const int nn = (int)n;  // vectors hold fewer than 2^31 elements (checked at launch)
+  for (int b0 = blockIdx.x * U * kSolT; b0 < nn; b0 += gridDim.x * U * kSolT) {
+    const int q0 = b0 + threadIdx.x;
+    H ev[U];
+    {
+      double rv[U], yv[U], xv[U];
 #pragma unroll
-    for (int k = 0; k < kMaxHist; ++k)
-      if (k < nh) d[k] = fma((double)ev, (double)static_cast<const H*>(hist.p[k])[q], d[k]);
-    d[kMaxHist] = fma((double)ev, (double)ev, d[kMaxHist]);
+      for (int u = 0; u < U; ++u) {
+        const int q = q0 + u * kSolT;
+        rv[u] = q < nn ? rhs[q] : 0.0;
+        yv[u] = q < nn ? y[q] : 0.0;
+        xv[u] = q < nn ? x[q] : 0.0;
+      }
+      int lm = lm_first(q0, nylm);
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int q = q0 + u * kSolT;
+        const double xn = tb.facl[l_of(lm)] * (rv[u] - yv[u]);
+        ev[u] = q < nn ? (H)(xn - xv[u]) : H(0);
+        if (q < nn) {
+          xnew[q] = (H)xn;
+          e[q] = ev[u];
+        }
+        lm = lm_add(lm, dt, nylm);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < NB; ++k) {
+      if (k < nh) {
+        const H* hk = static_cast<const H*>(hist.p[k]);
+        H hv[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const int q = q0 + u * kSolT;
+          hv[u] = q < nn ? hk[q] : H(0);
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) d[k] = fma((double)ev[u], (double)hv[u], d[k]);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) d[NB] = fma((double)ev[u], (double)ev[u], d[NB]);
   }
-  // move e.e to slot nh so the partial row is [e.h_0 .. e.h_{nh-1}, e.e]
-  double v[kMaxHist + 1];
+  // partial row [e.h_0 .. e.h_{nh-1}, e.e]
+  double v[NB + 1];
 #pragma unroll
-  for (int k = 0; k <= kMaxHist; ++k) v[k] = (k < nh) ? d[k] : (k == nh ? d[kMaxHist] : 0.0);
-  block_sum_store<kMaxHist + 1>(v, nh + 1, partials);
+  for (int k = 0; k <= NB; ++k) v[k] = (k < nh) ? d[k] : (k == nh ? d[NB] : 0.0);
+  block_sum_store<NB + 1, kMaxHist + 1>(v, nh + 1, partials);
+}
+template <class H>
+static void jacobi_launch(Launch L, const YlmTables& tb, long long n, const double* rhs,
+                          const double* y, const double* x, H* xnew, H* e, const HistPtrs& hist,
+                          double* partials, int nblk) {
+  const int nh = hist.n;
+#define JB(NB) k_jacobi_step<H, NB><<<nblk, kSolT, 0, L.st>>>(tb, n, rhs, y, x, xnew, e, hist, partials)
+  if (nh <= 1) JB(1);
+  else if (nh <= 4) JB(4);
+  else if (nh <= 8) JB(8);
+  else if (nh <= 16) JB(16);
+  else if (nh <= 24) JB(24);
+  else JB(kMaxHist);
+#undef JB
 }
 cudaError_t launch_jacobi_step(Launch L, const YlmTables& tb, long long n, const double* rhs,
                                const double* y, const double* x, void* xnew, void* e,
                                const HistPtrs& hist, double* partials, int nblk, bool f32) {
+  if (hist.n > kMaxHist - 1 || n >= (1LL << 31)) return cudaErrorInvalidValue;
   if (f32)
-    k_jacobi_step<float><<<nblk, 256, 0, L.st>>>(tb, n, rhs, y, x, static_cast<float*>(xnew),
-                                                 static_cast<float*>(e), hist, partials);
+    jacobi_launch<float>(L, tb, n, rhs, y, x, static_cast<float*>(xnew), static_cast<float*>(e),
+                         hist, partials, nblk);
   else
-    k_jacobi_step<double><<<nblk, 256, 0, L.st>>>(tb, n, rhs, y, x, static_cast<double*>(xnew),
-                                                  static_cast<double*>(e), hist, partials);
+    jacobi_launch<double>(L, tb, n, rhs, y, x, static_cast<double*>(xnew),
+                          static_cast<double*>(e), hist, partials, nblk);
   ++*L.launches;
   return cudaGetLastError();
 }
@@ -1297,27 +1360,50 @@ cudaError_t launch_jacobi_step(Launch L, const YlmTables& tb, long long n, const
 // DIIS extrapolation (jacobi_diis.f90:222-226) + increment norm (hnorm,
 // matvec.f90:281-323: sum over spheres of sum_l 1/(l+1) |u_l|^2) + update.
 template <class H>
-__global__ void __launch_bounds__(256) k_diis_combine(const YlmTables tb, long long n,
-                                                      const HistPtrs hist,
-                                                      const H* __restrict__ xjac, double* x,
-                                                      double* partials) {
+__global__ void __launch_bounds__(kSolT) k_diis_combine(const YlmTables tb, long long n,
+                                                        const HistPtrs hist,
+                                                        const H* __restrict__ xjac, double* x,
+                                                        double* partials) {
   double acc = 0.0;
-  const int nh = hist.n;
-  for (LmWalk w(tb.nylm); w.q < n; w.next()) {
-    const long long q = w.q;
-    double xo;
-    if (nh == 0) {
-      xo = xjac[q];
-    } else {
-      xo = 0.0;
-#pragma unroll 4
-      for (int k = 0; k < nh; ++k)
-        xo = fma(hist.c[k], (double)static_cast<const H*>(hist.p[k])[q], xo);
+  const int nh = hist.n, nylm = tb.nylm;
+  const int dt = kSolT % nylm;
+  const long long tile = (long long)kSolU * kSolT;
+  for (long long b0 = (long long)blockIdx.x * tile; b0 < n; b0 += (long long)gridDim.x * tile) {
+    long long q[kSolU];
+    bool ok[kSolU];
+    double xo[kSolU], xold[kSolU];
+#pragma unroll
+    for (int u = 0; u < kSolU; ++u) {
+      q[u] = b0 + u * kSolT + threadIdx.x;
+      ok[u] = q[u] < n;
+      xold[u] = ok[u] ? x[q[u]] : 0.0;
+      xo[u] = 0.0;
     }
-    double d = xo - x[q];
-    int l = l_of(w.lm);
-    acc = fma(d * d, 1.0 / (1.0 + l), acc);
-    x[q] = xo;
+    if (nh == 0) {
+#pragma unroll
+      for (int u = 0; u < kSolU; ++u) xo[u] = ok[u] ? (double)xjac[q[u]] : 0.0;
+    } else {
+#pragma unroll 2
+      for (int k = 0; k < nh; ++k) {
+        const H* hk = static_cast<const H*>(hist.p[k]);
+        const double ck = hist.c[k];
+        H hv[kSolU];
+#pragma unroll
+        for (int u = 0; u < kSolU; ++u) hv[u] = ok[u] ? hk[q[u]] : H(0);
+#pragma unroll
+        for (int u = 0; u < kSolU; ++u) xo[u] = fma(ck, (double)hv[u], xo[u]);
+      }
+    }
+    int lm = lm_first(b0 + threadIdx.x, nylm);
+#pragma unroll
+    for (int u = 0; u < kSolU; ++u) {
+      if (ok[u]) {
+        const double dd = xo[u] - xold[u];
+        acc = fma(dd * dd, 1.0 / (1.0 + l_of(lm)), acc);
+        x[q[u]] = xo[u];
+      }
+      lm = lm_add(lm, dt, nylm);
+    }
   }
   double v[1] = {acc};
   block_sum_store<1>(v, 1, partials);
@@ -1326,11 +1412,12 @@ cudaError_t launch_diis_combine(Launch L, const YlmTables& tb, long long n, cons
                                 const void* xjac, double* x, double* partials, int nblk,
                                 bool f32) {
   if (f32)
-    k_diis_combine<float><<<nblk, 256, 0, L.st>>>(tb, n, hist, static_cast<const float*>(xjac),
-                                                  x, partials);
+    k_diis_combine<float><<<nblk, kSolT, 0, L.st>>>(tb, n, hist, static_cast<const float*>(xjac),
+                                                    x, partials);
   else
-    k_diis_combine<double><<<nblk, 256, 0, L.st>>>(tb, n, hist,
-                                                   static_cast<const double*>(xjac), x, partials);
+    k_diis_combine<double><<<nblk, kSolT, 0, L.st>>>(tb, n, hist,
+                                                     static_cast<const double*>(xjac), x,
+                                                     partials);
   ++*L.launches;
   return cudaGetLastError();
 }
