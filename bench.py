@@ -187,7 +187,10 @@ def _stage_work(stage, info, c):
 
 
 def _traffic_from_profiles(kernel):
-    """DRAM bytes per launch of `kernel` from the committed ncu summary, if any."""
+    """DRAM bytes per launch of `kernel` from the committed ncu summary, if any
+    (the figures there are for the 20,000-sphere workload)."""
+    if WORKLOAD != 2:
+        return None
     path = os.path.join(ROOT, "profiles", "dram_traffic.txt")
     try:
         for ln in open(path):
