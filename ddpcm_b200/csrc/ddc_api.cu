@@ -985,6 +985,14 @@ int solve_tasks(ddc_ctx* ctx, SolveTask* t, int nt) {
       if (k[q] != OP_NONE) active++;
     }
     if (!active) break;
+    // A task that needs an FP64 step (mixed refinement) while the other
+    // runs FP32 inner iterations waits a round: the other reaches its own
+    // FP64 step or finishes, and the FP64 steps then share a fused pass.
+    // This only reorders the tasks' rounds; each keeps its own arithmetic.
+    if (nt == 2 && k[0] != OP_NONE && k[1] != OP_NONE && k[0] != k[1]) {
+      const int wait = k[0] == OP_F64 ? 0 : 1;
+      k[wait] = OP_NONE;
+    }
     if (nt == 2 && k[0] != OP_NONE && k[0] == k[1] && t[0].adjoint != t[1].adjoint) {
       const int dq = t[0].adjoint ? 1 : 0, aq = 1 - dq;
       if (k[0] == OP_F64) CKI(op_pair(ctx, in[dq], out[dq], in[aq], out[aq]));

@@ -2633,9 +2633,13 @@ __device__ __forceinline__ void lxs_fields(const YlmTables& tb, const LxsIn<Rl>&
   }
 }
 
-// FP32 up to lmax 10: three blocks per SM (caps the registers at 112)
+// FP32 chunks are double-buffered (software pipeline); FP64 chunks use one
+// buffer so that two blocks fit in shared memory
+template <class Rl> __host__ __device__ constexpr bool lxs_piped() { return sizeof(Rl) == 4; }
+// Up to lmax 10: three blocks per SM in FP32 (at most 112 registers), two in
+// FP64 (at most 168)
 template <int LMAX, class Rl>
-__global__ void __launch_bounds__(32 * ls_nroles(LMAX), sizeof(Rl) == 4 && LMAX <= 10 ? 3 : 1)
+__global__ void __launch_bounds__(32 * ls_nroles(LMAX), LMAX > 10 ? 1 : (sizeof(Rl) == 4 ? 3 : 2))
     k_lxs(const YlmTables tb, const DevGeo g, const typename RT<Rl>::V2* __restrict__ XK,
           const Rl* __restrict__ xi, Rl* __restrict__ val, double* __restrict__ y) {
   constexpr int NR = ls_nroles(LMAX);
@@ -2644,8 +2648,9 @@ __global__ void __launch_bounds__(32 * ls_nroles(LMAX), sizeof(Rl) == 4 && LMAX 
   constexpr int NVM = ls_max_nvals(LMAX);
   constexpr int NLM = (LMAX + 1) * (LMAX + 2) / 2;
   extern __shared__ __align__(16) unsigned char smraw[];
-  Rl* fld = reinterpret_cast<Rl*>(smraw);  // [2][NF][CH]
-  Rl* lxp = fld + 2 * NF * CH;             // [2][NR][CH]
+  constexpr int NBUF = lxs_piped<Rl>() ? 2 : 1;
+  Rl* fld = reinterpret_cast<Rl*>(smraw);  // [NBUF][NF][CH]
+  Rl* lxp = fld + NBUF * NF * CH;          // [NBUF][NR][CH]
   const int b = blockIdx.x, tid = threadIdx.x;
   const int role = tid >> 5, lane = tid & 31;
   const int q0 = g.ls_ptr[b], q1 = g.ls_ptr[b + 1];
@@ -2656,6 +2661,24 @@ __global__ void __launch_bounds__(32 * ls_nroles(LMAX), sizeof(Rl) == 4 && LMAX 
 #pragma unroll
   for (int v = 0; v < NVM; ++v) acc[v] = xr[v] = 0;
   lxs_load_role<LMAX, 0, Rl>(role, XK + (size_t)b * NLM, xr);
+  if constexpr (!lxs_piped<Rl>()) {
+    // FP64: one buffer (two blocks per SM fit), two barriers per chunk
+    for (int k = 0; k < nch; ++k) {
+      const int c0 = q0 + k * CH, cnt = min(CH, q1 - c0);
+      if (tid < cnt) lxs_fields<LMAX, Rl>(tb, lxs_load<Rl>(g, xi, c0 + tid), cb, irb, fld, tid);
+      __syncthreads();
+      lxs_run_role<LMAX, 0, Rl>(role, tb, fld, cnt, lane, acc, xr, lxp);
+      __syncthreads();
+      if (tid < cnt) {
+        Rl sv = lxp[tid];
+#pragma unroll
+        for (int r = 1; r < NR; ++r) sv += lxp[r * CH + tid];
+        val[c0 + tid] = sv;
+      }
+    }
+    ls_finish_role<LMAX, 0, Rl, true>(role, tb, acc, y + (size_t)b * tb.nylm, lane);
+    return;
+  }
   if (nch > 0 && tid < min(CH, q1 - q0))
     lxs_fields<LMAX, Rl>(tb, lxs_load<Rl>(g, xi, q0 + tid), cb, irb, fld, tid);
   __syncthreads();
@@ -2747,7 +2770,7 @@ static cudaError_t lxs_launch(Launch L, const YlmTables& tb, const DevGeo& g, co
 #define CASE(LV)                                                                              \
   case LV: {                                                                                  \
     constexpr int NR = ls_nroles(LV);                                                         \
-    const size_t sm = sizeof(Rl) * 2 * (lxs_nfields(LV) + NR) * 32 * NR;                      \
+    const size_t sm = sizeof(Rl) * (lxs_piped<Rl>() ? 2 : 1) * (lxs_nfields(LV) + NR) * 32 * NR; \
     if (sm > 48 * 1024) {                                                                     \
       if ((e = cudaFuncSetAttribute(k_lxs<LV, Rl>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
                                     (int)sm)))                                                \
