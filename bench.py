@@ -618,15 +618,13 @@ def run_reference(args):
 
 def _reference_iters():
     """Jacobi/DIIS iteration counts of the reference algorithm on this workload
-    (direct, adjoint), from the committed measurement, else a typical count."""
-    path = os.path.join(ROOT, "profiles", "workload_iterations.txt")
-    try:
-        for ln in open(path):
-            f = ln.split()
-            if len(f) >= 3 and f[0] == "fp64_reference_guess":
-                return int(f[1]), int(f[2])
-    except OSError:
-        pass
+    (direct, adjoint): those of the stored full-size oracle run
+    (tests/golden/config2_oracle.npz, the reference's algorithm in FP64 from
+    the reference guess); for other workloads a typical count."""
+    ref = _oracle_fixture()
+    if ref is not None:
+        it = ref["iters"]
+        return int(it[0]), int(it[1])
     return 45, 45
 
 
