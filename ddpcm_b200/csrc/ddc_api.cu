@@ -1104,56 +1104,121 @@ int forces_dev(ddc_ctx* ctx, const double* phi, const double* sigma, const doubl
 // Jacobi step, Gram row, bordered solve, extrapolation and norm for all
 // molecules, a converged molecule's block returns at once.  iters receives
 // the per-molecule iteration counts.
-int batch_solve(ddc_ctx* ctx, bool adjoint, const double* rhs, double* x, int* iters,
-                ddc_solve_info* inf) {
-  const double t0 = now_s();
+// One system of a batched solve: its right-hand side, iterate, operator
+// output and per-molecule Jacobi/DIIS state on the device.  The state arrays
+// of the two systems of a paired solve sit side by side in the same buffers
+// (set 0, set 1).
+struct BatchSys {
+  bool adjoint = false;
+  const double* rhs = nullptr;
+  double* x = nullptr;
+  double* y = nullptr;
+  BatchState bs{};
+  int* iters = nullptr;
+  ddc_solve_info* inf = nullptr;
+};
+
+int batch_setup(ddc_ctx* ctx, BatchSys& b, bool adjoint, const double* rhs, double* x,
+                int* iters, ddc_solve_info* inf, int set) {
   const int nmol = ctx->nmol, nd = std::max(ctx->prm.ndiis, 11);
   if (ctx->prm.ndiis == 0) return fail(ctx, DDC_ERR_UNSUPPORTED, "batched solves need DIIS");
-  std::vector<int> nmat(nmol, 1), slot((size_t)nmol * nd), zero(nmol, 0);
+  std::vector<int> nmat(nmol, 1), slot((size_t)nmol * nd);
   for (int k = 0; k < nmol; k++)
     for (int j = 0; j < nd; j++) slot[(size_t)k * nd + j] = j;
   std::vector<int> status(nmol, 0);
   for (int k = 0; k < nmol; k++)
     if (ctx->h_off[k + 1] == ctx->h_off[k]) status[k] = 1;  // empty molecule
-  const size_t lenb = nd + 1;
-  CK(ctx->b_nmat.ensure(sizeof(int) * nmol));
-  CK(ctx->b_slot.ensure(sizeof(int) * nmol * nd));
-  CK(ctx->b_B.ensure(sizeof(double) * nmol * lenb * lenb));
-  CK(ctx->b_status.ensure(sizeof(int) * nmol));
-  CK(ctx->b_iters.ensure(sizeof(int) * nmol));
-  CK(ctx->b_restarts.ensure(sizeof(int) * nmol));
-  CK(ctx->b_norm.ensure(sizeof(double) * nmol));
-  CK(cudaMemcpyAsync(ctx->b_nmat.p, nmat.data(), sizeof(int) * nmol, cudaMemcpyHostToDevice,
-                     ctx->st));
-  CK(cudaMemcpyAsync(ctx->b_slot.p, slot.data(), sizeof(int) * nmol * nd, cudaMemcpyHostToDevice,
-                     ctx->st));
-  CK(cudaMemsetAsync(ctx->b_B.p, 0, sizeof(double) * nmol * lenb * lenb, ctx->st));
-  CK(cudaMemcpyAsync(ctx->b_status.p, status.data(), sizeof(int) * nmol, cudaMemcpyHostToDevice,
-                     ctx->st));
-  CK(cudaMemsetAsync(ctx->b_iters.p, 0, sizeof(int) * nmol, ctx->st));
-  CK(cudaMemsetAsync(ctx->b_restarts.p, 0, sizeof(int) * nmol, ctx->st));
-  BatchState bs;
+  const size_t lenb = nd + 1, lb2 = lenb * lenb;
+  // room for both sets
+  CK(ctx->b_nmat.ensure(sizeof(int) * 2 * nmol));
+  CK(ctx->b_slot.ensure(sizeof(int) * 2 * nmol * nd));
+  CK(ctx->b_B.ensure(sizeof(double) * 2 * nmol * lb2));
+  CK(ctx->b_status.ensure(sizeof(int) * 2 * nmol));
+  CK(ctx->b_iters.ensure(sizeof(int) * 2 * nmol));
+  CK(ctx->b_restarts.ensure(sizeof(int) * 2 * nmol));
+  CK(ctx->b_norm.ensure(sizeof(double) * 2 * nmol));
+  BatchState& bs = b.bs;
   bs.nmol = nmol;
   bs.ndiis = nd;
   bs.max_iter = ctx->prm.max_iter;
   bs.tol = std::pow(10.0, -(double)ctx->prm.iconv);
   bs.n_total = (long long)ctx->nsph * ctx->nylm;
   bs.off = ctx->d_off.as<int>();
-  bs.nmat = ctx->b_nmat.as<int>();
-  bs.slot = ctx->b_slot.as<int>();
-  bs.B = ctx->b_B.as<double>();
-  bs.status = ctx->b_status.as<int>();
-  bs.iters = ctx->b_iters.as<int>();
-  bs.restarts = ctx->b_restarts.as<int>();
-  bs.norm = ctx->b_norm.as<double>();
-  bs.hx = ctx->hist_x.as<double>();
-  bs.he = ctx->hist_e.as<double>();
-  OpFn op = adjoint ? op_lstarx : op_lx;
-  double* y = ctx->y.as<double>();
-  // CUDA graph of `check` sweeps (operator kernels + fused DIIS kernel),
-  // captured once and replayed until every molecule has stopped; a
-  // stopped molecule's DIIS block returns at once, so extra sweeps are
-  // harmless.
+  bs.nmat = ctx->b_nmat.as<int>() + (size_t)set * nmol;
+  bs.slot = ctx->b_slot.as<int>() + (size_t)set * nmol * nd;
+  bs.B = ctx->b_B.as<double>() + (size_t)set * nmol * lb2;
+  bs.status = ctx->b_status.as<int>() + (size_t)set * nmol;
+  bs.iters = ctx->b_iters.as<int>() + (size_t)set * nmol;
+  bs.restarts = ctx->b_restarts.as<int>() + (size_t)set * nmol;
+  bs.norm = ctx->b_norm.as<double>() + (size_t)set * nmol;
+  const SolveBufs sb = solve_bufs(ctx, set);
+  bs.hx = sb.hx;
+  bs.he = sb.he;
+  CK(cudaMemcpyAsync(bs.nmat, nmat.data(), sizeof(int) * nmol, cudaMemcpyHostToDevice, ctx->st));
+  CK(cudaMemcpyAsync(bs.slot, slot.data(), sizeof(int) * nmol * nd, cudaMemcpyHostToDevice,
+                     ctx->st));
+  CK(cudaMemsetAsync(bs.B, 0, sizeof(double) * nmol * lb2, ctx->st));
+  CK(cudaMemcpyAsync(bs.status, status.data(), sizeof(int) * nmol, cudaMemcpyHostToDevice,
+                     ctx->st));
+  CK(cudaMemsetAsync(bs.iters, 0, sizeof(int) * nmol, ctx->st));
+  CK(cudaMemsetAsync(bs.restarts, 0, sizeof(int) * nmol, ctx->st));
+  b.adjoint = adjoint;
+  b.rhs = rhs;
+  b.x = x;
+  b.y = sb.y;
+  b.iters = iters;
+  b.inf = inf;
+  // the host copy of status must not be read before these copies land
+  CKI(sync(ctx));
+  return DDC_OK;
+}
+
+// Copies one system's per-molecule results back and fills its report.
+int batch_finish(ddc_ctx* ctx, const BatchSys& b, double t0) {
+  const int nmol = ctx->nmol;
+  std::vector<int> status(nmol), its(nmol), rst(nmol);
+  std::vector<double> nrm(nmol);
+  CK(cudaMemcpyAsync(status.data(), b.bs.status, sizeof(int) * nmol, cudaMemcpyDeviceToHost,
+                     ctx->st));
+  CK(cudaMemcpyAsync(its.data(), b.bs.iters, sizeof(int) * nmol, cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaMemcpyAsync(rst.data(), b.bs.restarts, sizeof(int) * nmol, cudaMemcpyDeviceToHost,
+                     ctx->st));
+  CK(cudaMemcpyAsync(nrm.data(), b.bs.norm, sizeof(double) * nmol, cudaMemcpyDeviceToHost,
+                     ctx->st));
+  CKI(sync(ctx));
+  int maxit = 0, nfail = 0, restarts = 0;
+  double worst = 0.0;
+  for (int k = 0; k < nmol; k++) {
+    if (b.iters) b.iters[k] = its[k];
+    maxit = std::max(maxit, its[k]);
+    restarts += rst[k];
+    if (status[k] != 1) nfail++;
+    if (ctx->h_off[k + 1] > ctx->h_off[k]) worst = std::max(worst, nrm[k]);
+  }
+  if (b.inf) {
+    memset(b.inf, 0, sizeof(*b.inf));
+    b.inf->iterations = maxit;
+    b.inf->converged = nfail == 0;
+    b.inf->diis_restarts = restarts;
+    b.inf->final_norm = worst;
+    b.inf->seconds = now_s() - t0;
+  }
+  if (nfail)
+    return fail(ctx, DDC_ERR_NOCONV,
+                std::to_string(nfail) + " molecule(s) did not converge" +
+                    (b.adjoint ? " (adjoint)" : ""));
+  return DDC_OK;
+}
+
+// Batched Jacobi/DIIS over one system, or over a direct and an adjoint
+// system together (one fused L / L* pass per sweep).  A CUDA graph of
+// `check` sweeps (operator kernels + the fused per-molecule DIIS kernels)
+// is captured once and replayed until every molecule of every system has
+// stopped; a stopped molecule's DIIS block returns at once, so extra sweeps
+// are harmless.
+int batch_run(ddc_ctx* ctx, BatchSys* sys, int ns) {
+  const double t0 = now_s();
+  const int nmol = ctx->nmol;
   const int check = 4;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -1163,9 +1228,16 @@ int batch_solve(ddc_ctx* ctx, bool adjoint, const double* rhs, double* x, int* i
   int orc = DDC_OK;
   if (ce == cudaSuccess) {
     for (int r = 0; r < check && orc == DDC_OK; r++) {
-      orc = op(ctx, x, y);
-      if (orc == DDC_OK && launch_batch_diis(ctx->L(), ctx->tb, bs, rhs, y, x) != cudaSuccess)
-        orc = DDC_ERR_CUDA;
+      if (ns == 2) {
+        const int dq = sys[0].adjoint ? 1 : 0, aq = 1 - dq;
+        orc = op_pair(ctx, sys[dq].x, sys[dq].y, sys[aq].x, sys[aq].y);
+      } else {
+        orc = sys[0].adjoint ? op_lstarx(ctx, sys[0].x, sys[0].y) : op_lx(ctx, sys[0].x, sys[0].y);
+      }
+      for (int q = 0; q < ns && orc == DDC_OK; q++)
+        if (launch_batch_diis(ctx->L(), ctx->tb, sys[q].bs, sys[q].rhs, sys[q].y, sys[q].x) !=
+            cudaSuccess)
+          orc = DDC_ERR_CUDA;
     }
     cudaError_t ee = cudaStreamEndCapture(ctx->st, &graph);
     if (ce == cudaSuccess) ce = ee;
@@ -1173,11 +1245,13 @@ int batch_solve(ddc_ctx* ctx, bool adjoint, const double* rhs, double* x, int* i
   ctx->capturing = false;
   if (orc != DDC_OK) {
     if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
     return orc;
   }
   CK(ce);
   CK(cudaGraphInstantiate(&exec, graph, 0));
-  int it = 0, active = nmol;
+  std::vector<int> status(nmol);
+  int it = 0, active = 1;
   cudaError_t ge = cudaSuccess;
   while (it < ctx->prm.max_iter && active > 0) {
     {
@@ -1186,46 +1260,23 @@ int batch_solve(ddc_ctx* ctx, bool adjoint, const double* rhs, double* x, int* i
     }
     if (ge != cudaSuccess) break;
     it += check;
-    CK(cudaMemcpyAsync(status.data(), ctx->b_status.p, sizeof(int) * nmol, cudaMemcpyDeviceToHost,
-                       ctx->st));
-    CKI(sync(ctx));
     active = 0;
-    for (int k = 0; k < nmol; k++) active += status[k] == 0;
+    for (int q = 0; q < ns; q++) {
+      CK(cudaMemcpyAsync(status.data(), sys[q].bs.status, sizeof(int) * nmol,
+                         cudaMemcpyDeviceToHost, ctx->st));
+      CKI(sync(ctx));
+      for (int k = 0; k < nmol; k++) active += status[k] == 0;
+    }
   }
   cudaGraphExecDestroy(exec);
   cudaGraphDestroy(graph);
   CK(ge);
-  std::vector<int> its(nmol), rst(nmol);
-  std::vector<double> nrm(nmol);
-  CK(cudaMemcpyAsync(status.data(), ctx->b_status.p, sizeof(int) * nmol, cudaMemcpyDeviceToHost,
-                     ctx->st));
-  CK(cudaMemcpyAsync(its.data(), ctx->b_iters.p, sizeof(int) * nmol, cudaMemcpyDeviceToHost,
-                     ctx->st));
-  CK(cudaMemcpyAsync(rst.data(), ctx->b_restarts.p, sizeof(int) * nmol, cudaMemcpyDeviceToHost,
-                     ctx->st));
-  CK(cudaMemcpyAsync(nrm.data(), ctx->b_norm.p, sizeof(double) * nmol, cudaMemcpyDeviceToHost,
-                     ctx->st));
-  CKI(sync(ctx));
-  int maxit = 0, nfail = 0, restarts = 0;
-  double worst = 0.0;
-  for (int k = 0; k < nmol; k++) {
-    if (iters) iters[k] = its[k];
-    maxit = std::max(maxit, its[k]);
-    restarts += rst[k];
-    if (status[k] != 1) nfail++;
-    if (ctx->h_off[k + 1] > ctx->h_off[k]) worst = std::max(worst, nrm[k]);
+  int rc = DDC_OK;
+  for (int q = 0; q < ns; q++) {
+    const int r = batch_finish(ctx, sys[q], t0);
+    if (r != DDC_OK && rc == DDC_OK) rc = r;
   }
-  if (inf) {
-    memset(inf, 0, sizeof(*inf));
-    inf->iterations = maxit;
-    inf->converged = nfail == 0;
-    inf->diis_restarts = restarts;
-    inf->final_norm = worst;
-    inf->seconds = now_s() - t0;
-  }
-  if (nfail)
-    return fail(ctx, DDC_ERR_NOCONV, std::to_string(nfail) + " molecule(s) did not converge");
-  return DDC_OK;
+  return rc;
 }
 
 // ===========================================================================
@@ -1853,7 +1904,8 @@ int ddc_batch_energy_forces(ddc_ctx* ctx, int nmol, const int* off, const double
   double* dsig = ctx->sigma.as<double>();
   double* ds = ctx->s.as<double>();
   const long long n = (long long)nv;
-  // direct solve
+  const bool paired = ctx->prm.igrad && ctx->prm.pair_solves;
+  // direct solve (and the adjoint with it when paired)
   {
     double* rhs = ctx->rhs.as<double>();
     CK(ctx->gbuf.ensure(sizeof(double) * std::max<long long>((long long)N * ctx->ngrid, 1)));
@@ -1864,10 +1916,21 @@ int ddc_batch_energy_forces(ddc_ctx* ctx, int nmol, const int* off, const double
                       ctx->nylm, ctx->gbuf.as<double>(), ctx->ngrid, 0.0, rhs, ctx->nylm));
     }
     CK(launch_guess(ctx->L(), ctx->tb, n, rhs, dsig, ctx->prm.guess == DDC_GUESS_ZERO ? 1 : 0));
-    std::vector<int> it(nmol);
-    CKI(batch_solve(ctx, false, rhs, dsig, it.data(), &inf->direct));
+    std::vector<int> it(nmol), ita(nmol);
+    BatchSys sys[2];
+    CKI(batch_setup(ctx, sys[0], false, rhs, dsig, it.data(), &inf->direct, 0));
+    if (paired) {
+      // the adjoint right-hand side psi is known already: both systems share
+      // each sweep's fused L / L* pass
+      CK(launch_guess(ctx->L(), ctx->tb, n, dpsi, ds, ctx->prm.guess == DDC_GUESS_ZERO ? 1 : 0));
+      CKI(batch_setup(ctx, sys[1], true, dpsi, ds, ita.data(), &inf->adjoint, 1));
+    }
+    CKI(batch_run(ctx, sys, paired ? 2 : 1));
     if (iters)
-      for (int k = 0; k < nmol; k++) iters[2 * k] = it[k];
+      for (int k = 0; k < nmol; k++) {
+        iters[2 * k] = it[k];
+        if (paired) iters[2 * k + 1] = ita[k];
+      }
   }
   CK(ctx->b_out.ensure(sizeof(double) * nmol));
   const double fep = 0.5 * ((ctx->prm.eps - 1.0) / ctx->prm.eps);
@@ -1878,11 +1941,15 @@ int ddc_batch_energy_forces(ddc_ctx* ctx, int nmol, const int* off, const double
   double t3 = now_s();
   inf->t_direct = t3 - t2;
   if (ctx->prm.igrad) {
-    CK(launch_guess(ctx->L(), ctx->tb, n, dpsi, ds, ctx->prm.guess == DDC_GUESS_ZERO ? 1 : 0));
-    std::vector<int> it(nmol);
-    CKI(batch_solve(ctx, true, dpsi, ds, it.data(), &inf->adjoint));
-    if (iters)
-      for (int k = 0; k < nmol; k++) iters[2 * k + 1] = it[k];
+    if (!paired) {
+      CK(launch_guess(ctx->L(), ctx->tb, n, dpsi, ds, ctx->prm.guess == DDC_GUESS_ZERO ? 1 : 0));
+      std::vector<int> it(nmol);
+      BatchSys sys;
+      CKI(batch_setup(ctx, sys, true, dpsi, ds, it.data(), &inf->adjoint, 0));
+      CKI(batch_run(ctx, &sys, 1));
+      if (iters)
+        for (int k = 0; k < nmol; k++) iters[2 * k + 1] = it[k];
+    }
     double t4 = now_s();
     inf->t_adjoint = t4 - t3;
     CK(ctx->fx.ensure(sizeof(double) * 3 * std::max(N, 1)));
