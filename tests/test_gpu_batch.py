@@ -47,3 +47,21 @@ def test_batch_uneven_globules(oracle):
         np.testing.assert_allclose(out["fx"][k], ref["fx"], rtol=0, atol=FORCE_ATOL)
     # per-molecule convergence: iteration counts differ between molecules
     assert len(set(out["iters"][:, 0].tolist())) > 1
+
+
+def test_batch_paired_equals_one_system_after_the_other():
+    """pair_solves=0: the direct batch solve, then the adjoint one, each with
+    its own operator; the paired default gives the same energies and forces
+    (each system keeps its own per-molecule DIIS path)."""
+    from ddpcm_b200 import molecules as M
+    from ddpcm_b200.ddcosmo import DDCosmo
+    mols = [M.to_bohr(m) for m in M.batch_molecules(count=6, lo=20, hi=200, seed=91)]
+    p = dict(lmax=6, ngrid=302, iconv=10, eps=78.3553, eta=0.1)
+    with DDCosmo(pair_solves=1, **p) as dd:
+        a = dd.batch_energy_forces(mols)
+    with DDCosmo(pair_solves=0, **p) as dd:
+        b = dd.batch_energy_forces(mols)
+    np.testing.assert_allclose(a["esolv"], b["esolv"], rtol=1e-9, atol=0)
+    for fa, fb in zip(a["fx"], b["fx"]):
+        np.testing.assert_allclose(fa, fb, rtol=0, atol=1e-9)
+    assert np.abs(a["iters"] - b["iters"]).max() <= 2
