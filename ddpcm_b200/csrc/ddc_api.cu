@@ -366,11 +366,13 @@ void build_tables(ddc_ctx* c) {
 // deterministic reduction of `nvals` partial columns into red[0..nvals-1], copied to host.
 // stride: the partial row length of the producing kernel (kMaxHist + 1 for the
 // Jacobi step's Gram row, whatever its current length; 1 for single sums).
-int reduce_to_host(ddc_ctx* ctx, int nvals, double* host, int stride = 1) {
+// nblk: the producing kernel's block count (partial rows).
+int reduce_to_host(ddc_ctx* ctx, int nvals, double* host, int stride = 1, int nblk = 0) {
   {
     StageScope sc(ctx, ST_REDUCE);
-    CK(launch_reduce_partials(ctx->L(), ctx->partials.as<double>(), reduce_blocks(), nvals,
-                              stride, ctx->red.as<double>()));
+    CK(launch_reduce_partials(ctx->L(), ctx->partials.as<double>(),
+                              nblk > 0 ? nblk : reduce_blocks(), nvals, stride,
+                              ctx->red.as<double>()));
   }
   CK(cudaMemcpyAsync(host, ctx->red.p, sizeof(double) * nvals, cudaMemcpyDeviceToHost, ctx->st));
   return sync(ctx);
@@ -762,6 +764,7 @@ int jd_step(ddc_ctx* ctx, JDState& s) {
   HistPtrs hist{};
   HistPtrs comb{};
   const void* xj = s.xjac;
+  int jblk = nblk;
   if (ndiis != 0) {
     std::vector<double> row(kMaxHist + 2);
     const int phys_new = s.map[s.nmat - 1];
@@ -781,9 +784,9 @@ int jd_step(ddc_ctx* ctx, JDState& s) {
     {
       StageScope sc(ctx, ST_JACOBI);
       CK(launch_jacobi_step(ctx->L(), ctx->tb, n, s.rhs, s.y, s.x, xnew, enew, hist,
-                            ctx->partials.as<double>(), nblk, s.f32));
+                            ctx->partials.as<double>(), nblk, s.f32, &jblk));
     }
-    CKI(reduce_to_host(ctx, nm, row.data(), kMaxHist + 1));
+    CKI(reduce_to_host(ctx, nm, row.data(), kMaxHist + 1, jblk));
     if (shift) {
       for (int j = 2; j <= s.nmat - 10; j++)
         for (int k = 2; k <= s.nmat - 10; k++) Bm(j, k) = Bm(j + 10, k + 10);
@@ -827,7 +830,7 @@ int jd_step(ddc_ctx* ctx, JDState& s) {
     hist.n = 0;
     StageScope sc(ctx, ST_JACOBI);
     CK(launch_jacobi_step(ctx->L(), ctx->tb, n, s.rhs, s.y, s.x, s.hx, s.he, hist,
-                          ctx->partials.as<double>(), nblk, s.f32));
+                          ctx->partials.as<double>(), nblk, s.f32, nullptr));
     comb.n = 0;
     xj = s.hx;
   }

@@ -194,7 +194,8 @@ cudaError_t launch_guess(Launch L, const YlmTables& tb, long long n, const doubl
 // xnew, e and the history are FP32 when f32 (mixed-path inner solves), else FP64.
 cudaError_t launch_jacobi_step(Launch L, const YlmTables& tb, long long n, const double* rhs,
                                const double* y, const double* x, void* xnew, void* e,
-                               const HistPtrs& hist, double* partials, int nblk, bool f32);
+                               const HistPtrs& hist, double* partials, int nblk, bool f32,
+                               int* nblk_used);  // blocks launched (<= nblk): partial rows
 // xout = sum c_k p_k (or xjac if hist.n == 0); partial of sum_l 1/(l+1) (xout-x)^2; x = xout
 cudaError_t launch_diis_combine(Launch L, const YlmTables& tb, long long n, const HistPtrs& hist,
                                 const void* xjac, double* x, double* partials, int nblk,

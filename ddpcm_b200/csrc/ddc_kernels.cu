@@ -1329,30 +1329,58 @@ __global__ void __launch_bounds__(kSolT) k_jacobi_step(const YlmTables tb, long 
   for (int k = 0; k <= NB; ++k) v[k] = (k < nh) ? d[k] : (k == nh ? d[NB] : 0.0);
   block_sum_store<NB + 1, kMaxHist + 1>(v, nh + 1, partials);
 }
+// One wave: as many blocks as fit on the device at once for this bucket's
+// register count (at most nblk, the partial-row capacity).
+template <class KFN>
+static int one_wave_blocks(KFN kfn, int nblk) {
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) sms = 0;
+  }
+  int per = 0;
+  if (sms <= 0 ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kfn, kSolT, 0) != cudaSuccess ||
+      per <= 0) {
+    cudaGetLastError();
+    return nblk;
+  }
+  return std::min(nblk, sms * per);
+}
 template <class H>
-static void jacobi_launch(Launch L, const YlmTables& tb, long long n, const double* rhs,
-                          const double* y, const double* x, H* xnew, H* e, const HistPtrs& hist,
-                          double* partials, int nblk) {
+static int jacobi_launch(Launch L, const YlmTables& tb, long long n, const double* rhs,
+                         const double* y, const double* x, H* xnew, H* e, const HistPtrs& hist,
+                         double* partials, int nblk) {
   const int nh = hist.n;
-#define JB(NB) k_jacobi_step<H, NB><<<nblk, kSolT, 0, L.st>>>(tb, n, rhs, y, x, xnew, e, hist, partials)
-  if (nh <= 1) JB(1);
-  else if (nh <= 4) JB(4);
-  else if (nh <= 8) JB(8);
-  else if (nh <= 16) JB(16);
-  else if (nh <= 24) JB(24);
-  else JB(kMaxHist);
+  int used = nblk;
+#define JB(NB)                                                                              \
+  {                                                                                         \
+    used = one_wave_blocks(k_jacobi_step<H, NB>, nblk);                                     \
+    k_jacobi_step<H, NB><<<used, kSolT, 0, L.st>>>(tb, n, rhs, y, x, xnew, e, hist, partials); \
+  }
+  if (nh <= 1) JB(1)
+  else if (nh <= 4) JB(4)
+  else if (nh <= 8) JB(8)
+  else if (nh <= 16) JB(16)
+  else if (nh <= 24) JB(24)
+  else JB(kMaxHist)
 #undef JB
+  return used;
 }
 cudaError_t launch_jacobi_step(Launch L, const YlmTables& tb, long long n, const double* rhs,
                                const double* y, const double* x, void* xnew, void* e,
-                               const HistPtrs& hist, double* partials, int nblk, bool f32) {
+                               const HistPtrs& hist, double* partials, int nblk, bool f32,
+                               int* nblk_used) {
   if (hist.n > kMaxHist - 1 || n >= (1LL << 31)) return cudaErrorInvalidValue;
+  int used;
   if (f32)
-    jacobi_launch<float>(L, tb, n, rhs, y, x, static_cast<float*>(xnew), static_cast<float*>(e),
-                         hist, partials, nblk);
+    used = jacobi_launch<float>(L, tb, n, rhs, y, x, static_cast<float*>(xnew),
+                                static_cast<float*>(e), hist, partials, nblk);
   else
-    jacobi_launch<double>(L, tb, n, rhs, y, x, static_cast<double*>(xnew),
-                          static_cast<double*>(e), hist, partials, nblk);
+    used = jacobi_launch<double>(L, tb, n, rhs, y, x, static_cast<double*>(xnew),
+                                 static_cast<double*>(e), hist, partials, nblk);
+  if (nblk_used) *nblk_used = used;
   ++*L.launches;
   return cudaGetLastError();
 }
