@@ -2738,14 +2738,14 @@ __global__ void __launch_bounds__(32 * ls_nroles(LMAX), LMAX > 10 ? 1 : (sizeof(
 // (a, n, b), read from b's gather list (pair slot lsstart).  Block per
 // sphere a; warp w takes the pairs p = w, w + NW, ... in order and adds into
 // its own shared row, lanes over the pair's points (distinct within a pair,
-// so no two lanes of a warp touch one entry).  Four strided loads per lane
+// so no two lanes of a warp touch one entry).  Eight strided loads per lane
 // are issued before their adds.  The rows are summed in row order at the
 // end: a fixed summation order, no atomics.
-constexpr int kGatherWarps = 8;  // at most; fewer when NW rows of ngrid do not fit
+constexpr int kGatherWarps = 4;  // at most; fewer when NW rows of ngrid do not fit
 template <class Rl>
 __global__ void __launch_bounds__(32 * kGatherWarps)
     k_lx_gather(const DevGeo g, const Rl* __restrict__ val, Rl* pot) {
-  constexpr int U = 4;
+  constexpr int U = 8;
   const int NW = blockDim.x >> 5;
   extern __shared__ __align__(16) unsigned char smraw[];
   const int G = g.ngrid;
