@@ -2,6 +2,7 @@
 // include/ddcosmo_gpu.h, the module state (context), the ddinit pipeline and
 // the Jacobi/DIIS driver.  All device work runs on the context's stream.
 #include <chrono>
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -378,6 +379,21 @@ int reduce_to_host(ddc_ctx* ctx, int nvals, double* host, int stride = 1, int nb
   return sync(ctx);
 }
 
+// The per-item counts that are about to be scanned into 32-bit offsets must
+// total less than 2^31: summed in 64 bits on the device first.
+int check_count_total(ddc_ctx* ctx, const int* cnt, int n, const char* what) {
+  if (n <= 0) return DDC_OK;
+  unsigned long long* d = reinterpret_cast<unsigned long long*>(ctx->red.p);
+  CK(launch_sum_counts(ctx->L(), cnt, n, d));
+  unsigned long long total = 0;
+  CK(cudaMemcpyAsync(&total, d, sizeof(total), cudaMemcpyDeviceToHost, ctx->st));
+  CKI(sync(ctx));
+  if (total >= (unsigned long long)INT_MAX)
+    return fail(ctx, DDC_ERR_UNSUPPORTED,
+                std::string("more than 2^31 - 1 ") + what + " (" + std::to_string(total) + ")");
+  return DDC_OK;
+}
+
 // ---------------------------------------------------------------------------
 // ddinit (ddcosmo.f90:159-483) on device buffers
 // ---------------------------------------------------------------------------
@@ -390,6 +406,10 @@ int do_init(ddc_ctx* ctx, int n, const std::vector<double4>* hsph, const double4
   if (!lebedev(ctx->ngrid, ctx->h_grid)) return fail(ctx, DDC_ERR_PARAM, "bad Lebedev size");
   const int N = n, G = ctx->ngrid, NY = ctx->nylm;
   const long long NP = (long long)N * G;
+  // grid fields, cavity and triple lists are indexed with 32-bit integers
+  if (NP >= (long long)INT_MAX)
+    return fail(ctx, DDC_ERR_UNSUPPORTED, "nsph * ngrid exceeds 2^31 - 1 grid points");
+  CK(ctx->red.ensure(sizeof(double) * (kMaxHist + 1)));  // also the count checks' scratch
   auto L = ctx->L();
   CK(ctx->sph.ensure(sizeof(double4) * std::max(N, 1)));
   if (hsph)
@@ -413,6 +433,7 @@ int do_init(ddc_ctx* ctx, int n, const std::vector<double4>* hsph, const double4
     CK(launch_csr_count(L, N, ctx->sph.as<double4>(), ctx->cnt.as<int>(), ctx->mrange_ptr()));
   size_t tb_bytes = scan_temp_bytes(N);
   CK(ctx->scan_tmp.ensure(tb_bytes));
+  CKI(check_count_total(ctx, ctx->cnt.as<int>(), N, "neighbour pairs"));
   CK(scan_exclusive(L, ctx->cnt.as<int>(), ctx->inl.as<int>(), N, ctx->scan_tmp.p, tb_bytes));
   int npair = 0;
   CK(cudaMemcpyAsync(&npair, ctx->inl.as<int>() + N, sizeof(int), cudaMemcpyDeviceToHost,
@@ -473,6 +494,7 @@ int do_init(ddc_ctx* ctx, int n, const std::vector<double4>* hsph, const double4
   CK(cudaMemsetAsync(ctx->cnt.p, 0, sizeof(int) * (npair + 1), ctx->st));
   CK(launch_pair_count(L, N, G, ctx->sph.as<double4>(), ctx->grid.as<double4>(),
                        ctx->inl.as<int>(), ctx->nl.as<int>(), ctx->cnt.as<int>()));
+  CKI(check_count_total(ctx, ctx->cnt.as<int>(), npair, "(sphere, point, neighbour) triples"));
   size_t tb2 = scan_temp_bytes(npair);
   CK(ctx->scan_tmp.ensure(std::max(tb_bytes, tb2)));
   CK(scan_exclusive(L, ctx->cnt.as<int>(), ctx->pn_ptr.as<int>(), npair, ctx->scan_tmp.p,

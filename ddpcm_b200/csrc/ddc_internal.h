@@ -149,6 +149,8 @@ cudaError_t launch_ls_fill(Launch L, int nsph, const int* inl, const int* nl, co
 cudaError_t scan_exclusive(Launch L, const int* in, int* out, int n, void* temp,
                            size_t temp_bytes);
 size_t scan_temp_bytes(int n);
+// *out = sum of cnt[0..n) in 64 bits (out: device memory, overwritten)
+cudaError_t launch_sum_counts(Launch L, const int* cnt, int n, unsigned long long* out);
 
 // operators
 // xk: scratch of N*(lmax+1)(lmax+2)/2 double2 (K-scaled X in pair layout)

@@ -435,6 +435,21 @@ cudaError_t launch_ls_fill(Launch L, int nsph, const int* inl, const int* nl, co
   return cudaGetLastError();
 }
 
+__global__ void k_sum_counts(const int* __restrict__ cnt, int n, unsigned long long* out) {
+  unsigned long long v = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    v += (unsigned long long)(unsigned)cnt[i];
+  for (int o = 16; o >= 1; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0 && v) atomicAdd(out, v);  // integer sum: order-free
+}
+cudaError_t launch_sum_counts(Launch L, const int* cnt, int n, unsigned long long* out) {
+  cudaError_t e = cudaMemsetAsync(out, 0, sizeof(unsigned long long), L.st);
+  if (e || n <= 0) return e;
+  k_sum_counts<<<std::min((n + 255) / 256, 148 * 4), 256, 0, L.st>>>(cnt, n, out);
+  ++*L.launches;
+  return cudaGetLastError();
+}
+
 size_t scan_temp_bytes(int n) {
   size_t b = 0;
   cub::DeviceScan::ExclusiveSum(nullptr, b, (const int*)nullptr, (int*)nullptr, n + 1);

@@ -28,7 +28,9 @@ extern "C" {
 #define DDC_ERR_CUDA 3         /* CUDA runtime error */
 #define DDC_ERR_NOMEM 4        /* device allocation failed */
 #define DDC_ERR_NOCONV 5       /* Jacobi/DIIS hit max_iter (cosmo.f90:188-200) */
-#define DDC_ERR_UNSUPPORTED 6  /* lmax outside the compiled range */
+#define DDC_ERR_UNSUPPORTED 6  /* lmax outside the compiled range, or a problem beyond
+                                * 32-bit indexing (nsph*ngrid or the triple count
+                                * at or above 2^31) */
 #define DDC_ERR_NUMERIC 7      /* NaN/Inf in a stage output */
 #define DDC_ERR_CAPACITY 8     /* problem larger than the fixed scratch of ddc_efld_noalloc */
 

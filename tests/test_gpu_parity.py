@@ -290,6 +290,19 @@ def test_errors_and_nonconvergence():
             dd.ddinit([0.0], [0.0], [0.0], [-1.0])  # negative radius
 
 
+def test_sizes_beyond_32bit_indexing_are_rejected():
+    """Grid fields and triple lists use 32-bit indices: nsph * ngrid at or
+    above 2^31 is refused with DDC_ERR_UNSUPPORTED before any allocation."""
+    from ddpcm_b200.ddcosmo import DDCosmoError
+    n = 369_700  # * 5810 points > 2^31
+    x = np.arange(n, dtype=np.float64) * 10.0
+    z = np.zeros(n)
+    with gpu_ctx(lmax=2, ngrid=5810) as dd:
+        with pytest.raises(DDCosmoError) as ei:
+            dd.ddinit(x, z, z, np.ones(n))
+        assert ei.value.status == 6
+
+
 def test_zero_guess_and_no_diis_converge_to_same_solution(oracle):
     g = load_golden("taxol")
     p, m = g["params"], g["mol"]
