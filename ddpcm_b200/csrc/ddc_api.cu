@@ -164,6 +164,9 @@ struct ddc_ctx {
   DBuf in1, in2, in3, in4, out1;  // staging for host-pointer calls
   // mixed precision: FP32 grid/basis copies, FP32 grid fields, refinement vectors
   DBuf gridf, basis_f, bw_f, pot_f, xi_f, rres, dres, eres;
+  // FP32 static geometry of the gather-list triples (mixed path)
+  DBuf tgeo4, tgeo2;
+  bool tgeo_on = false;
   // second solve set (direct and adjoint solved together) and the fused
   // operator's per-triple lx values
   DBuf y2, xn2, hist_x2, hist_e2, rres2, dres2, eres2, tval;
@@ -192,6 +195,8 @@ struct ddc_ctx {
     g.pn = pn.as<uint16_t>();
     g.pn_pair = pn_pair.as<uint8_t>();
     g.maxnb = maxnb;
+    g.tgeo4 = tgeo_on ? tgeo4.as<float4>() : nullptr;
+    g.tgeo2 = tgeo_on ? tgeo2.as<float2>() : nullptr;
     g.ls_ptr = ls_ptr.as<int>();
     g.ls = ls.as<int2>();
     g.lsstart = lsstart.as<int>();
@@ -399,6 +404,7 @@ int check_count_total(ddc_ctx* ctx, const int* cnt, int n, const char* what) {
 // ---------------------------------------------------------------------------
 int do_init(ddc_ctx* ctx, int n, const std::vector<double4>* hsph, const double4* dsph) {
   ctx->ready = false;
+  ctx->tgeo_on = false;
   ctx->nsph = n;
   ctx->nylm = (ctx->prm.lmax + 1) * (ctx->prm.lmax + 1);
   ctx->ngrid = snap_ngrid(ctx->prm.ngrid);
@@ -555,6 +561,13 @@ int do_init(ddc_ctx* ctx, int n, const std::vector<double4>* hsph, const double4
     CK(ctx->xi_f.ensure(sizeof(float) * std::max(NP, 1LL)));
     for (DBuf* b : {&ctx->rres, &ctx->dres, &ctx->eres})
       CK(b->ensure(sizeof(double) * std::max(nv, (size_t)1)));
+    // the FP32 fused pass reads each triple's static geometry instead of
+    // recomputing it every iteration (24 bytes per triple)
+    ctx->tgeo_on = false;
+    CK(ctx->tgeo4.ensure(sizeof(float4) * std::max<long long>(ctx->ntri, 1)));
+    CK(ctx->tgeo2.ensure(sizeof(float2) * std::max<long long>(ctx->ntri, 1)));
+    CK(launch_lxs_geo(L, ctx->tb, ctx->geo(), ctx->tgeo4.as<float4>(), ctx->tgeo2.as<float2>()));
+    ctx->tgeo_on = true;
   }
   if (ctx->prm.igrad && ctx->prm.pair_solves) {
     for (DBuf* b : {&ctx->y2, &ctx->xn2})

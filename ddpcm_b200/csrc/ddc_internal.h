@@ -52,6 +52,10 @@ struct YlmTables {
 struct DevGeo {
   int nsph, ngrid, nylm, ncav, npair;
   int maxnb;  // largest neighbour count of a sphere
+  // FP32 geometry of each gather-list triple (mixed path; null if absent):
+  // (t cos theta, t^2, t sin theta, W) and (cos phi, sin phi)
+  const float4* tgeo4;
+  const float2* tgeo2;
   long long ntri;
   const double4* sph;
   const double4* grid;
@@ -164,6 +168,8 @@ cudaError_t launch_lx_pot_f32(Launch L, const YlmTables& tb, const DevGeo& g, co
 // fused L / L*: val (one lx value per triple, gather-list order) and y = L* rows
 cudaError_t launch_lxs(Launch L, const YlmTables& tb, const DevGeo& g, const double* X,
                        const double* xi, void* xk, double* val, double* y);
+cudaError_t launch_lxs_geo(Launch L, const YlmTables& tb, const DevGeo& g, float4* tg4,
+                           float2* tg2);
 cudaError_t launch_lxs_f32(Launch L, const YlmTables& tb, const DevGeo& g, const double* X,
                            const float* xi, void* xk, float* val, double* y);
 cudaError_t launch_lx_gather(Launch L, const DevGeo& g, const double* val, double* pot);

@@ -8,6 +8,7 @@
 // reorder (values only), and every reduction has a fixed order, so results
 // are deterministic from run to run.
 #include <cub/cub.cuh>
+#include <type_traits>
 
 #include "ddc_internal.h"
 
@@ -2607,15 +2608,18 @@ __device__ __forceinline__ float sin_from_cos(float c) {
   const float u = 1.f - c * c;
   return u > 0.f ? u * rsqrtf(u) : 0.f;
 }
-template <int LMAX, class Rl>
-__device__ __forceinline__ void lxs_fields(const YlmTables& tb, const LxsIn<Rl>& in, double4 cb,
-                                           Rl irb, Rl* sh, int tt) {
+// The static geometry of one triple: t cos(theta), t^2, t sin(theta), the
+// weight W = chi(t) / f_a(n), cos(phi), sin(phi).
+template <class Rl>
+struct LxsGeo {
+  Rl ct, t2, st, W, cp, sp;
+};
+template <class Rl>
+__device__ __forceinline__ LxsGeo<Rl> lxs_geom(const YlmTables& tb, double4 ca, GP<Rl> gn,
+                                               double fd, double4 cb, Rl irb) {
   constexpr bool D = sizeof(Rl) == 8;
-  constexpr int CH = 32 * ls_nroles(LMAX);
   const Rl eta = (Rl)tb.eta, flow = Rl(1) - eta;
   const Rl fa = Rl(15) * eta - Rl(12), fb = Rl(10) * eta * eta - Rl(15) * eta + Rl(6);
-  const double4 ca = in.ca;
-  const GP<Rl> gn = in.gn;
   Rl vx, vy, vz;
   if constexpr (D) {
     vx = fma(ca.w, gn.x, ca.x) - cb.x;
@@ -2632,11 +2636,13 @@ __device__ __forceinline__ void lxs_fields(const YlmTables& tb, const LxsIn<Rl>&
   const Rl t = r2 * rinv * irb;
   const Rl sz = vz * rinv;
   const Rl sth = sin_from_cos(sz);
-  Rl cp = 1, sp = 0;  // pole: only m = 0 survives
+  LxsGeo<Rl> o;
+  o.cp = 1;  // pole: only m = 0 survives
+  o.sp = 0;
   if (sth != Rl(0)) {
     const Rl rs = div_t(rinv, sth);
-    cp = vx * rs;
-    sp = vy * rs;
+    o.cp = vx * rs;
+    o.sp = vy * rs;
   }
   Rl chi;
   if (t >= Rl(1)) chi = 0;
@@ -2646,18 +2652,28 @@ __device__ __forceinline__ void lxs_fields(const YlmTables& tb, const LxsIn<Rl>&
     const Rl ie5 = (Rl)(1.0 / (tb.eta * tb.eta * tb.eta * tb.eta * tb.eta));
     chi = (xm * xm * (Rl(1) - t)) * ((Rl(6) * t + fa) * t + fb) * ie5;
   }
-  const Rl f = (Rl)in.f;
-  const Rl W = f > Rl(1) ? div_t(chi, f) : chi;
-  const Rl st = sth * t;
+  const Rl f = (Rl)fd;
+  o.W = f > Rl(1) ? div_t(chi, f) : chi;
+  o.st = sth * t;
+  o.ct = sz * t;
+  o.t2 = t * t;
+  return o;
+}
+// the shared fields of one triple (column tt of the chunk's buffer) from its
+// geometry, grid weight and xi_a(n)
+template <int LMAX, class Rl>
+__device__ __forceinline__ void lxs_fields(const LxsGeo<Rl>& gm, Rl w, Rl xv, Rl* sh, int tt) {
+  constexpr int CH = 32 * ls_nroles(LMAX);
   typedef typename RT<Rl>::V2 V2;
   typedef typename V4T<Rl>::T V4;
   V4 h;
-  h.x = sz * t;
-  h.y = t * t;
-  h.z = gn.w * in.xv;
+  h.x = gm.ct;
+  h.y = gm.t2;
+  h.z = w * xv;
   h.w = 0;
   reinterpret_cast<V4*>(sh)[tt] = h;
-  Rl pmm = W, cm = 1, sm = 0, cmm1 = 1, smm1 = 0;
+  Rl pmm = gm.W, cm = 1, sm = 0, cmm1 = 1, smm1 = 0;
+  const Rl cp = gm.cp, sp = gm.sp, st = gm.st;
 #pragma unroll
   for (int m = 0; m <= LMAX; ++m) {
     if (m == 1) {
@@ -2675,13 +2691,65 @@ __device__ __forceinline__ void lxs_fields(const YlmTables& tb, const LxsIn<Rl>&
     pmm = -pmm * Rl(2 * m + 1) * st;
   }
 }
+template <int LMAX, class Rl>
+__device__ __forceinline__ void lxs_fields(const YlmTables& tb, const LxsIn<Rl>& in, double4 cb,
+                                           Rl irb, Rl* sh, int tt) {
+  lxs_fields<LMAX, Rl>(lxs_geom<Rl>(tb, in.ca, in.gn, in.f, cb, irb), in.gn.w, in.xv, sh, tt);
+}
+// FP32 path with the geometry precomputed at ddinit (DevGeo::tgeo4/tgeo2)
+struct LxsInP {
+  float4 g4;  // ct, t2, st, W
+  float2 g2;  // cp, sp
+  float w, xv;
+};
+__device__ __forceinline__ LxsInP lxs_load_pre(const DevGeo& g, const float* __restrict__ xi,
+                                               int q) {
+  const int2 an = g.ls[q];
+  LxsInP in;
+  in.g4 = g.tgeo4[q];
+  in.g2 = g.tgeo2[q];
+  in.w = g.gridf[an.y].w;
+  in.xv = xi[(size_t)an.x * g.ngrid + an.y];
+  return in;
+}
+template <int LMAX>
+__device__ __forceinline__ void lxs_fields_pre(const LxsInP& in, float* sh, int tt) {
+  LxsGeo<float> gm;
+  gm.ct = in.g4.x;
+  gm.t2 = in.g4.y;
+  gm.st = in.g4.z;
+  gm.W = in.g4.w;
+  gm.cp = in.g2.x;
+  gm.sp = in.g2.y;
+  lxs_fields<LMAX, float>(gm, in.w, in.xv, sh, tt);
+}
+// the FP32 geometry of every triple, block per sphere b over its gather list
+__global__ void k_lxs_geo(const YlmTables tb, const DevGeo g, float4* tg4, float2* tg2) {
+  const int b = blockIdx.x;
+  const double4 cb = g.sph[b];
+  const float irb = (float)(1.0 / cb.w);
+  for (int q = g.ls_ptr[b] + threadIdx.x; q < g.ls_ptr[b + 1]; q += blockDim.x) {
+    const int2 an = g.ls[q];
+    const LxsGeo<float> gm = lxs_geom<float>(tb, g.sph[an.x], grid_pt(g, an.y, (float*)nullptr),
+                                             g.fi[(size_t)an.x * g.ngrid + an.y], cb, irb);
+    tg4[q] = make_float4(gm.ct, gm.t2, gm.st, gm.W);
+    tg2[q] = make_float2(gm.cp, gm.sp);
+  }
+}
+cudaError_t launch_lxs_geo(Launch L, const YlmTables& tb, const DevGeo& g, float4* tg4,
+                           float2* tg2) {
+  if (g.nsph == 0) return cudaSuccess;
+  k_lxs_geo<<<g.nsph, 128, 0, L.st>>>(tb, g, tg4, tg2);
+  ++*L.launches;
+  return cudaGetLastError();
+}
 
 // FP32 chunks are double-buffered (software pipeline); FP64 chunks use one
 // buffer so that two blocks fit in shared memory
 template <class Rl> __host__ __device__ constexpr bool lxs_piped() { return sizeof(Rl) == 4; }
 // Up to lmax 10: three blocks per SM in FP32 (at most 112 registers), two in
 // FP64 (at most 168)
-template <int LMAX, class Rl>
+template <int LMAX, class Rl, bool PRE = false>
 __global__ void __launch_bounds__(32 * ls_nroles(LMAX), LMAX > 10 ? 1 : (sizeof(Rl) == 4 ? 3 : 2))
     k_lxs(const YlmTables tb, const DevGeo g, const typename RT<Rl>::V2* __restrict__ XK,
           const Rl* __restrict__ xi, Rl* __restrict__ val, double* __restrict__ y) {
@@ -2722,19 +2790,29 @@ __global__ void __launch_bounds__(32 * ls_nroles(LMAX), LMAX > 10 ? 1 : (sizeof(
     ls_finish_role<LMAX, 0, Rl, true>(role, tb, acc, y + (size_t)b * tb.nylm, lane);
     return;
   }
-  if (nch > 0 && tid < min(CH, q1 - q0))
-    lxs_fields<LMAX, Rl>(tb, lxs_load<Rl>(g, xi, q0 + tid), cb, irb, fld, tid);
+  // FP32 with precomputed geometry: only xi_a(n) and the grid weight are
+  // read per triple besides the two geometry vectors
+  typedef typename std::conditional<PRE, LxsInP, LxsIn<Rl>>::type In;
+  auto load = [&](int q) -> In {
+    if constexpr (PRE) return lxs_load_pre(g, reinterpret_cast<const float*>(xi), q);
+    else return lxs_load<Rl>(g, xi, q);
+  };
+  auto fields = [&](const In& in, Rl* buf) {
+    if constexpr (PRE) lxs_fields_pre<LMAX>(in, reinterpret_cast<float*>(buf), tid);
+    else lxs_fields<LMAX, Rl>(tb, in, cb, irb, buf, tid);
+  };
+  if (nch > 0 && tid < min(CH, q1 - q0)) fields(load(q0 + tid), fld);
   __syncthreads();
   // chunk k: loads of chunk k+1 in flight while the roles work on chunk k,
   // then chunk k+1's fields go to the other buffer; one barrier per chunk
   for (int k = 0; k < nch; ++k) {
     const int c0 = q0 + k * CH, cnt = min(CH, q1 - c0);
     const int n1 = k + 1 < nch ? min(CH, q1 - c0 - CH) : 0;
-    LxsIn<Rl> nxt;
-    if (tid < n1) nxt = lxs_load<Rl>(g, xi, c0 + CH + tid);
+    In nxt;
+    if (tid < n1) nxt = load(c0 + CH + tid);
     lxs_run_role<LMAX, 0, Rl>(role, tb, fld + (k & 1) * NF * CH, cnt, lane, acc, xr,
                               lxp + (k & 1) * NR * CH);
-    if (tid < n1) lxs_fields<LMAX, Rl>(tb, nxt, cb, irb, fld + ((k + 1) & 1) * NF * CH, tid);
+    if (tid < n1) fields(nxt, fld + ((k + 1) & 1) * NF * CH);
     __syncthreads();
     // lx values of chunk k: the roles' shares in role order (buffer k&1 of
     // lxp is next written two chunks on, after the next barrier)
@@ -2814,15 +2892,16 @@ static cudaError_t lxs_launch(Launch L, const YlmTables& tb, const DevGeo& g, co
   case LV: {                                                                                  \
     constexpr int NR = ls_nroles(LV);                                                         \
     const size_t sm = sizeof(Rl) * (lxs_piped<Rl>() ? 2 : 1) * (lxs_nfields(LV) + NR) * 32 * NR; \
+    auto kfn = (sizeof(Rl) == 4 && g.tgeo4) ? k_lxs<LV, Rl, sizeof(Rl) == 4> : k_lxs<LV, Rl>;  \
     if (sm > 48 * 1024) {                                                                     \
-      if ((e = cudaFuncSetAttribute(k_lxs<LV, Rl>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+      if ((e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize,         \
                                     (int)sm)))                                                \
         return e;                                                                             \
-      if ((e = cudaFuncSetAttribute(k_lxs<LV, Rl>,                                            \
-                                    cudaFuncAttributePreferredSharedMemoryCarveout, 100)))    \
+      if ((e = cudaFuncSetAttribute(kfn, cudaFuncAttributePreferredSharedMemoryCarveout,      \
+                                    100)))                                                    \
         return e;                                                                             \
     }                                                                                         \
-    k_lxs<LV, Rl><<<g.nsph, 32 * NR, sm, L.st>>>(tb, g, XK, xi, val, y);                      \
+    kfn<<<g.nsph, 32 * NR, sm, L.st>>>(tb, g, XK, xi, val, y);                                \
     break;                                                                                    \
   }
   switch (tb.lmax) {
