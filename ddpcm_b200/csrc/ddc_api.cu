@@ -167,6 +167,9 @@ struct ddc_ctx {
   // FP32 static geometry of the gather-list triples (mixed path)
   DBuf tgeo4, tgeo2;
   bool tgeo_on = false;
+  // FP64 static geometry of the gather-list triples (FP64 path)
+  DBuf tgeo4d, tgeo2d;
+  bool tgeo64_on = false;
   // second solve set (direct and adjoint solved together) and the fused
   // operator's per-triple lx values
   DBuf y2, xn2, hist_x2, hist_e2, rres2, dres2, eres2, tval;
@@ -197,6 +200,8 @@ struct ddc_ctx {
     g.maxnb = maxnb;
     g.tgeo4 = tgeo_on ? tgeo4.as<float4>() : nullptr;
     g.tgeo2 = tgeo_on ? tgeo2.as<float2>() : nullptr;
+    g.tgeo4d = tgeo64_on ? tgeo4d.as<double4>() : nullptr;
+    g.tgeo2d = tgeo64_on ? tgeo2d.as<double2>() : nullptr;
     g.ls_ptr = ls_ptr.as<int>();
     g.ls = ls.as<int2>();
     g.lsstart = lsstart.as<int>();
@@ -405,6 +410,7 @@ int check_count_total(ddc_ctx* ctx, const int* cnt, int n, const char* what) {
 int do_init(ddc_ctx* ctx, int n, const std::vector<double4>* hsph, const double4* dsph) {
   ctx->ready = false;
   ctx->tgeo_on = false;
+  ctx->tgeo64_on = false;
   ctx->nsph = n;
   ctx->nylm = (ctx->prm.lmax + 1) * (ctx->prm.lmax + 1);
   ctx->ngrid = snap_ngrid(ctx->prm.ngrid);
@@ -568,6 +574,15 @@ int do_init(ddc_ctx* ctx, int n, const std::vector<double4>* hsph, const double4
     CK(ctx->tgeo2.ensure(sizeof(float2) * std::max<long long>(ctx->ntri, 1)));
     CK(launch_lxs_geo(L, ctx->tb, ctx->geo(), ctx->tgeo4.as<float4>(), ctx->tgeo2.as<float2>()));
     ctx->tgeo_on = true;
+  }
+  if (ctx->prm.precision != DDC_PREC_MIXED && ctx->prm.pair_solves) {
+    // the FP64 fused pass of the paired solves reads each triple's static
+    // geometry (48 bytes per triple) instead of recomputing it
+    CK(ctx->tgeo4d.ensure(sizeof(double4) * std::max<long long>(ctx->ntri, 1)));
+    CK(ctx->tgeo2d.ensure(sizeof(double2) * std::max<long long>(ctx->ntri, 1)));
+    CK(launch_lxs_geo_f64(L, ctx->tb, ctx->geo(), ctx->tgeo4d.as<double4>(),
+                          ctx->tgeo2d.as<double2>()));
+    ctx->tgeo64_on = true;
   }
   if (ctx->prm.igrad && ctx->prm.pair_solves) {
     for (DBuf* b : {&ctx->y2, &ctx->xn2})

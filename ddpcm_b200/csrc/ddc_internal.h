@@ -56,6 +56,8 @@ struct DevGeo {
   // (t cos theta, t^2, t sin theta, W) and (cos phi, sin phi)
   const float4* tgeo4;
   const float2* tgeo2;
+  const double4* tgeo4d;  // the same in FP64 (FP64 path)
+  const double2* tgeo2d;
   long long ntri;
   const double4* sph;
   const double4* grid;
@@ -170,6 +172,8 @@ cudaError_t launch_lxs(Launch L, const YlmTables& tb, const DevGeo& g, const dou
                        const double* xi, void* xk, double* val, double* y);
 cudaError_t launch_lxs_geo(Launch L, const YlmTables& tb, const DevGeo& g, float4* tg4,
                            float2* tg2);
+cudaError_t launch_lxs_geo_f64(Launch L, const YlmTables& tb, const DevGeo& g, double4* tg4,
+                               double2* tg2);
 cudaError_t launch_lxs_f32(Launch L, const YlmTables& tb, const DevGeo& g, const double* X,
                            const float* xi, void* xk, float* val, double* y);
 cudaError_t launch_lx_gather(Launch L, const DevGeo& g, const double* val, double* pot);

@@ -2696,50 +2696,70 @@ __device__ __forceinline__ void lxs_fields(const YlmTables& tb, const LxsIn<Rl>&
                                            Rl irb, Rl* sh, int tt) {
   lxs_fields<LMAX, Rl>(lxs_geom<Rl>(tb, in.ca, in.gn, in.f, cb, irb), in.gn.w, in.xv, sh, tt);
 }
-// FP32 path with the geometry precomputed at ddinit (DevGeo::tgeo4/tgeo2)
+// the geometry precomputed at ddinit (DevGeo::tgeo4/tgeo2 in FP32,
+// tgeo4d/tgeo2d in FP64)
+template <class Rl>
 struct LxsInP {
-  float4 g4;  // ct, t2, st, W
-  float2 g2;  // cp, sp
-  float w, xv;
+  typename V4T<Rl>::T g4;  // ct, t2, st, W
+  typename RT<Rl>::V2 g2;  // cp, sp
+  Rl w, xv;
 };
-__device__ __forceinline__ LxsInP lxs_load_pre(const DevGeo& g, const float* __restrict__ xi,
-                                               int q) {
+__device__ __forceinline__ float4 tgeo4_of(const DevGeo& g, int q, float*) { return g.tgeo4[q]; }
+__device__ __forceinline__ double4 tgeo4_of(const DevGeo& g, int q, double*) { return g.tgeo4d[q]; }
+__device__ __forceinline__ float2 tgeo2_of(const DevGeo& g, int q, float*) { return g.tgeo2[q]; }
+__device__ __forceinline__ double2 tgeo2_of(const DevGeo& g, int q, double*) { return g.tgeo2d[q]; }
+template <class Rl>
+__device__ __forceinline__ LxsInP<Rl> lxs_load_pre(const DevGeo& g, const Rl* __restrict__ xi,
+                                                   int q) {
   const int2 an = g.ls[q];
-  LxsInP in;
-  in.g4 = g.tgeo4[q];
-  in.g2 = g.tgeo2[q];
-  in.w = g.gridf[an.y].w;
+  LxsInP<Rl> in;
+  in.g4 = tgeo4_of(g, q, (Rl*)nullptr);
+  in.g2 = tgeo2_of(g, q, (Rl*)nullptr);
+  in.w = grid_pt(g, an.y, (Rl*)nullptr).w;
   in.xv = xi[(size_t)an.x * g.ngrid + an.y];
   return in;
 }
-template <int LMAX>
-__device__ __forceinline__ void lxs_fields_pre(const LxsInP& in, float* sh, int tt) {
-  LxsGeo<float> gm;
+template <int LMAX, class Rl>
+__device__ __forceinline__ void lxs_fields_pre(const LxsInP<Rl>& in, Rl* sh, int tt) {
+  LxsGeo<Rl> gm;
   gm.ct = in.g4.x;
   gm.t2 = in.g4.y;
   gm.st = in.g4.z;
   gm.W = in.g4.w;
   gm.cp = in.g2.x;
   gm.sp = in.g2.y;
-  lxs_fields<LMAX, float>(gm, in.w, in.xv, sh, tt);
+  lxs_fields<LMAX, Rl>(gm, in.w, in.xv, sh, tt);
 }
-// the FP32 geometry of every triple, block per sphere b over its gather list
-__global__ void k_lxs_geo(const YlmTables tb, const DevGeo g, float4* tg4, float2* tg2) {
+// the geometry of every triple, block per sphere b over its gather list
+template <class Rl>
+__global__ void k_lxs_geo(const YlmTables tb, const DevGeo g, typename V4T<Rl>::T* tg4,
+                          typename RT<Rl>::V2* tg2) {
   const int b = blockIdx.x;
   const double4 cb = g.sph[b];
-  const float irb = (float)(1.0 / cb.w);
+  const Rl irb = (Rl)(1.0 / cb.w);
   for (int q = g.ls_ptr[b] + threadIdx.x; q < g.ls_ptr[b + 1]; q += blockDim.x) {
     const int2 an = g.ls[q];
-    const LxsGeo<float> gm = lxs_geom<float>(tb, g.sph[an.x], grid_pt(g, an.y, (float*)nullptr),
-                                             g.fi[(size_t)an.x * g.ngrid + an.y], cb, irb);
-    tg4[q] = make_float4(gm.ct, gm.t2, gm.st, gm.W);
-    tg2[q] = make_float2(gm.cp, gm.sp);
+    const LxsGeo<Rl> gm = lxs_geom<Rl>(tb, g.sph[an.x], grid_pt(g, an.y, (Rl*)nullptr),
+                                       g.fi[(size_t)an.x * g.ngrid + an.y], cb, irb);
+    tg4[q].x = gm.ct;
+    tg4[q].y = gm.t2;
+    tg4[q].z = gm.st;
+    tg4[q].w = gm.W;
+    tg2[q].x = gm.cp;
+    tg2[q].y = gm.sp;
   }
 }
 cudaError_t launch_lxs_geo(Launch L, const YlmTables& tb, const DevGeo& g, float4* tg4,
                            float2* tg2) {
   if (g.nsph == 0) return cudaSuccess;
-  k_lxs_geo<<<g.nsph, 128, 0, L.st>>>(tb, g, tg4, tg2);
+  k_lxs_geo<float><<<g.nsph, 128, 0, L.st>>>(tb, g, tg4, tg2);
+  ++*L.launches;
+  return cudaGetLastError();
+}
+cudaError_t launch_lxs_geo_f64(Launch L, const YlmTables& tb, const DevGeo& g, double4* tg4,
+                               double2* tg2) {
+  if (g.nsph == 0) return cudaSuccess;
+  k_lxs_geo<double><<<g.nsph, 128, 0, L.st>>>(tb, g, tg4, tg2);
   ++*L.launches;
   return cudaGetLastError();
 }
@@ -2772,11 +2792,22 @@ __global__ void __launch_bounds__(32 * ls_nroles(LMAX), LMAX > 10 ? 1 : (sizeof(
 #pragma unroll
   for (int v = 0; v < NVM; ++v) acc[v] = xr[v] = 0;
   lxs_load_role<LMAX, 0, Rl>(role, XK + (size_t)b * NLM, xr);
+  // with the geometry precomputed at ddinit only xi_a(n) and the grid weight
+  // are read per triple besides the two geometry vectors
+  typedef typename std::conditional<PRE, LxsInP<Rl>, LxsIn<Rl>>::type In;
+  auto load = [&](int q) -> In {
+    if constexpr (PRE) return lxs_load_pre<Rl>(g, xi, q);
+    else return lxs_load<Rl>(g, xi, q);
+  };
+  auto fields = [&](const In& in, Rl* buf) {
+    if constexpr (PRE) lxs_fields_pre<LMAX, Rl>(in, buf, tid);
+    else lxs_fields<LMAX, Rl>(tb, in, cb, irb, buf, tid);
+  };
   if constexpr (!lxs_piped<Rl>()) {
     // FP64: one buffer (two blocks per SM fit), two barriers per chunk
     for (int k = 0; k < nch; ++k) {
       const int c0 = q0 + k * CH, cnt = min(CH, q1 - c0);
-      if (tid < cnt) lxs_fields<LMAX, Rl>(tb, lxs_load<Rl>(g, xi, c0 + tid), cb, irb, fld, tid);
+      if (tid < cnt) fields(load(c0 + tid), fld);
       __syncthreads();
       lxs_run_role<LMAX, 0, Rl>(role, tb, fld, cnt, lane, acc, xr, lxp);
       __syncthreads();
@@ -2790,17 +2821,6 @@ __global__ void __launch_bounds__(32 * ls_nroles(LMAX), LMAX > 10 ? 1 : (sizeof(
     ls_finish_role<LMAX, 0, Rl, true>(role, tb, acc, y + (size_t)b * tb.nylm, lane);
     return;
   }
-  // FP32 with precomputed geometry: only xi_a(n) and the grid weight are
-  // read per triple besides the two geometry vectors
-  typedef typename std::conditional<PRE, LxsInP, LxsIn<Rl>>::type In;
-  auto load = [&](int q) -> In {
-    if constexpr (PRE) return lxs_load_pre(g, reinterpret_cast<const float*>(xi), q);
-    else return lxs_load<Rl>(g, xi, q);
-  };
-  auto fields = [&](const In& in, Rl* buf) {
-    if constexpr (PRE) lxs_fields_pre<LMAX>(in, reinterpret_cast<float*>(buf), tid);
-    else lxs_fields<LMAX, Rl>(tb, in, cb, irb, buf, tid);
-  };
   if (nch > 0 && tid < min(CH, q1 - q0)) fields(load(q0 + tid), fld);
   __syncthreads();
   // chunk k: loads of chunk k+1 in flight while the roles work on chunk k,
@@ -2892,7 +2912,8 @@ static cudaError_t lxs_launch(Launch L, const YlmTables& tb, const DevGeo& g, co
   case LV: {                                                                                  \
     constexpr int NR = ls_nroles(LV);                                                         \
     const size_t sm = sizeof(Rl) * (lxs_piped<Rl>() ? 2 : 1) * (lxs_nfields(LV) + NR) * 32 * NR; \
-    auto kfn = (sizeof(Rl) == 4 && g.tgeo4) ? k_lxs<LV, Rl, sizeof(Rl) == 4> : k_lxs<LV, Rl>;  \
+    const bool pre = sizeof(Rl) == 4 ? g.tgeo4 != nullptr : g.tgeo4d != nullptr;              \
+    auto kfn = pre ? k_lxs<LV, Rl, true> : k_lxs<LV, Rl, false>;                              \
     if (sm > 48 * 1024) {                                                                     \
       if ((e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize,         \
                                     (int)sm)))                                                \
