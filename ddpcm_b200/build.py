@@ -1,11 +1,13 @@
 """Build the sm_100a shared library ``ddpcm_b200/lib/libddcosmo_gpu.so``.
 
 The library is compiled in-tree with nvcc for ``compute_100a``/``sm_100a``
-(B200).  cudart is linked statically, so the .so depends only on the driver.
+(B200).  cudart is linked statically; the one dynamic CUDA library is
+cuBLAS (the operators' plain GEMMs), found through an rpath to the toolkit.
 Host code is compiled with ``-ffp-contract=off`` so that the Lebedev grid and
 the normalisation tables follow the written operation order.
 """
 import os
+import shutil
 import subprocess
 import sys
 
@@ -25,6 +27,12 @@ def nvcc():
     return "nvcc"
 
 
+def cuda_libdir():
+    """The toolkit's library directory beside nvcc (cuBLAS is linked from it)."""
+    root = os.path.dirname(os.path.dirname(os.path.realpath(shutil.which(nvcc()) or nvcc())))
+    return os.path.join(root, "lib64")
+
+
 def _stale():
     if not os.path.exists(LIB):
         return True
@@ -42,7 +50,8 @@ def build(force=False, verbose=False):
     cmd = [nvcc(), "-O3", "-std=c++17", *ARCH, "-lineinfo", "-shared",
            "-Xcompiler", "-fPIC,-ffp-contract=off", "-Xptxas", "-warn-spills" if verbose else "-O3",
            "-I", os.path.join(HERE, "..", "include"),
-           "-o", LIB + ".tmp", *[os.path.join(CSRC, s) for s in SOURCES]]
+           "-o", LIB + ".tmp", *[os.path.join(CSRC, s) for s in SOURCES],
+           "-L", cuda_libdir(), "-lcublas", "-Xlinker", "-rpath," + cuda_libdir()]
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True)

@@ -10,6 +10,8 @@
 #include <string>
 #include <vector>
 
+#include <cublas_v2.h>
+
 #include "ddc_internal.h"
 #include "lebedev_orbits.inc"
 
@@ -173,6 +175,12 @@ struct ddc_ctx {
   // second solve set (direct and adjoint solved together) and the fused
   // operator's per-triple lx values
   DBuf y2, xn2, hist_x2, hist_e2, rres2, dres2, eres2, tval;
+  // cuBLAS for the two plain GEMMs of every operator application (the
+  // projection onto the harmonics and the harmonics-to-grid expansion), on
+  // the context's stream with its own workspace; gemm_f is the FP32 operand
+  // or result of the mixed path's GEMMs (nylm x nsph)
+  cublasHandle_t blas = nullptr;
+  DBuf blas_ws, gemm_f;
 
   Launch L() { return Launch{st, &launches}; }
   DevGeo geo() const {
@@ -231,6 +239,14 @@ int fail(ddc_ctx* c, int code, const std::string& msg) {
       return fail(ctx, _e == cudaErrorMemoryAllocation ? DDC_ERR_NOMEM : DDC_ERR_CUDA,    \
                   std::string(#expr) + ": " + cudaGetErrorString(_e));                    \
     }                                                                                     \
+  } while (0)
+
+#define CKB(expr)                                                                       \
+  do {                                                                                  \
+    cublasStatus_t _s = (expr);                                                         \
+    if (_s != CUBLAS_STATUS_SUCCESS)                                                    \
+      return fail(ctx, _s == CUBLAS_STATUS_ALLOC_FAILED ? DDC_ERR_NOMEM : DDC_ERR_CUDA, \
+                  std::string(#expr) + ": cuBLAS status " + std::to_string((int)_s));   \
   } while (0)
 
 #define CKI(expr)                  \
@@ -553,7 +569,12 @@ int do_init(ddc_ctx* ctx, int n, const std::vector<double4>* hsph, const double4
   CK(ctx->hist_e.ensure(sizeof(double) * std::max(nv, (size_t)1) * nd));
   CK(ctx->partials.ensure(sizeof(double) * reduce_blocks() * (kMaxHist + 1)));
   CK(ctx->red.ensure(sizeof(double) * (kMaxHist + 1)));
+  // cuBLAS handle, created once per context and outside any graph capture;
+  // its workspace is a context buffer, so a captured GEMM allocates nothing
+  if (!ctx->blas) CKB(cublasCreate(&ctx->blas));
+  CK(ctx->blas_ws.ensure((size_t)32 << 20));
   if (ctx->prm.precision == DDC_PREC_MIXED) {
+    CK(ctx->gemm_f.ensure(sizeof(float) * std::max(nv, (size_t)1)));
     std::vector<float> gf(4 * (size_t)G);
     for (size_t k = 0; k < gf.size(); k++) gf[k] = (float)ctx->h_grid[k];
     CK(ctx->gridf.ensure(sizeof(float) * 4 * G));
@@ -601,6 +622,53 @@ int do_init(ddc_ctx* ctx, int n, const std::vector<double4>* hsph, const double4
 }
 
 // ---------------------------------------------------------------------------
+// the operators' two GEMMs (cuBLAS, column-major, on the context's stream)
+// ---------------------------------------------------------------------------
+int blas_bind(ddc_ctx* ctx) {
+  CKB(cublasSetStream(ctx->blas, ctx->st));
+  // setting the stream restores the default workspace: point it back at ours
+  CKB(cublasSetWorkspace(ctx->blas, ctx->blas_ws.p, ctx->blas_ws.bytes));
+  return DDC_OK;
+}
+// y(lm,i) = alpha sum_n bw(lm,n) pot(n,i): intrhs over every sphere
+// (matvec.f90:131-135, bw = w_n Y_lm(s_n))
+int gemm_proj(ddc_ctx* ctx, double alpha, const double* pot, double* y) {
+  CKI(blas_bind(ctx));
+  const double beta = 0.0;
+  CKB(cublasDgemm(ctx->blas, CUBLAS_OP_N, CUBLAS_OP_N, ctx->nylm, ctx->nsph, ctx->ngrid, &alpha,
+                  ctx->bw.as<double>(), ctx->nylm, pot, ctx->ngrid, &beta, y, ctx->nylm));
+  return DDC_OK;
+}
+// FP32 projection of an FP32 field, widened into the FP64 vector y
+int gemm_proj_f32(ddc_ctx* ctx, float alpha, const float* pot, double* y) {
+  CKI(blas_bind(ctx));
+  const float beta = 0.f;
+  float* yf = ctx->gemm_f.as<float>();
+  CKB(cublasSgemm(ctx->blas, CUBLAS_OP_N, CUBLAS_OP_N, ctx->nylm, ctx->nsph, ctx->ngrid, &alpha,
+                  ctx->bw_f.as<float>(), ctx->nylm, pot, ctx->ngrid, &beta, yf, ctx->nylm));
+  CK(launch_to_double(ctx->L(), (long long)ctx->nylm * ctx->nsph, yf, y));
+  return DDC_OK;
+}
+// xi(n,i) = sum_lm basis(lm,n) s(lm,i)   (matvec.f90:189-204)
+int gemm_xi(ddc_ctx* ctx, const double* s, double* xig) {
+  CKI(blas_bind(ctx));
+  const double one = 1.0, zero = 0.0;
+  CKB(cublasDgemm(ctx->blas, CUBLAS_OP_T, CUBLAS_OP_N, ctx->ngrid, ctx->nsph, ctx->nylm, &one,
+                  ctx->basis.as<double>(), ctx->nylm, s, ctx->nylm, &zero, xig, ctx->ngrid));
+  return DDC_OK;
+}
+// FP32 xi of the FP64 vector s (narrowed first)
+int gemm_xi_f32(ddc_ctx* ctx, const double* s, float* xig) {
+  float* sf = ctx->gemm_f.as<float>();
+  CK(launch_to_float(ctx->L(), (long long)ctx->nylm * ctx->nsph, s, sf));
+  CKI(blas_bind(ctx));
+  const float one = 1.f, zero = 0.f;
+  CKB(cublasSgemm(ctx->blas, CUBLAS_OP_T, CUBLAS_OP_N, ctx->ngrid, ctx->nsph, ctx->nylm, &one,
+                  ctx->basis_f.as<float>(), ctx->nylm, sf, ctx->nylm, &zero, xig, ctx->ngrid));
+  return DDC_OK;
+}
+
+// ---------------------------------------------------------------------------
 // operators on device vectors
 // ---------------------------------------------------------------------------
 int op_lx(ddc_ctx* ctx, const double* x, double* y) {
@@ -611,16 +679,12 @@ int op_lx(ddc_ctx* ctx, const double* x, double* y) {
   }
   StageScope sc(ctx, ST_PROJ);
   // y = -Bw pot   (intrhs then negate, matvec.f90:131-135)
-  CK(launch_dgemm(ctx->L(), false, ctx->nylm, ctx->nsph, ctx->ngrid, -1.0, ctx->bw.as<double>(),
-                  ctx->nylm, ctx->pot.as<double>(), ctx->ngrid, 0.0, y, ctx->nylm));
-  return DDC_OK;
+  return gemm_proj(ctx, -1.0, ctx->pot.as<double>(), y);
 }
 int op_xi(ddc_ctx* ctx, const double* x, double* xig) {
   // xi(n,i) = sum_lm basis(lm,n) x(lm,i)   (matvec.f90:189-204)
   StageScope sc(ctx, ST_XI);
-  CK(launch_dgemm(ctx->L(), true, ctx->ngrid, ctx->nsph, ctx->nylm, 1.0, ctx->basis.as<double>(),
-                  ctx->nylm, x, ctx->nylm, 0.0, xig, ctx->ngrid));
-  return DDC_OK;
+  return gemm_xi(ctx, x, xig);
 }
 int op_lstarx(ddc_ctx* ctx, const double* x, double* y) {
   CKI(op_xi(ctx, x, ctx->xig.as<double>()));
@@ -636,15 +700,12 @@ int op_lx_f32(ddc_ctx* ctx, const double* x, double* y) {
     CK(launch_lx_pot_f32(ctx->L(), ctx->tb, ctx->geo(), x, ctx->pot_f.as<float>(), ctx->xk.p));
   }
   StageScope sc(ctx, ST_PROJ);
-  CK(launch_sgemm(ctx->L(), false, ctx->nylm, ctx->nsph, ctx->ngrid, -1.f, ctx->bw_f.as<float>(),
-                  ctx->nylm, ctx->pot_f.as<float>(), ctx->ngrid, y, ctx->nylm));
-  return DDC_OK;
+  return gemm_proj_f32(ctx, -1.f, ctx->pot_f.as<float>(), y);
 }
 int op_lstarx_f32(ddc_ctx* ctx, const double* x, double* y) {
   {
     StageScope sc(ctx, ST_XI);
-    CK(launch_sgemm_xi(ctx->L(), ctx->ngrid, ctx->nsph, ctx->nylm, ctx->basis_f.as<float>(),
-                       ctx->nylm, x, ctx->nylm, ctx->xi_f.as<float>(), ctx->ngrid));
+    CKI(gemm_xi_f32(ctx, x, ctx->xi_f.as<float>()));
   }
   StageScope sc(ctx, ST_LSTARX);
   CK(launch_lstarx_acc_f32(ctx->L(), ctx->tb, ctx->geo(), ctx->xi_f.as<float>(), y));
@@ -665,16 +726,13 @@ int op_pair(ddc_ctx* ctx, const double* x, double* y, const double* s, double* z
     CK(launch_lx_gather(ctx->L(), g, ctx->tval.as<double>(), ctx->pot.as<double>()));
   }
   StageScope sc(ctx, ST_PROJ);
-  CK(launch_dgemm(ctx->L(), false, ctx->nylm, ctx->nsph, ctx->ngrid, -1.0, ctx->bw.as<double>(),
-                  ctx->nylm, ctx->pot.as<double>(), ctx->ngrid, 0.0, y, ctx->nylm));
-  return DDC_OK;
+  return gemm_proj(ctx, -1.0, ctx->pot.as<double>(), y);
 }
 int op_pair_f32(ddc_ctx* ctx, const double* x, double* y, const double* s, double* z) {
   DevGeo g = ctx->geo();
   {
     StageScope sc(ctx, ST_XI);
-    CK(launch_sgemm_xi(ctx->L(), ctx->ngrid, ctx->nsph, ctx->nylm, ctx->basis_f.as<float>(),
-                       ctx->nylm, s, ctx->nylm, ctx->xi_f.as<float>(), ctx->ngrid));
+    CKI(gemm_xi_f32(ctx, s, ctx->xi_f.as<float>()));
   }
   {
     StageScope sc(ctx, ST_LXS);
@@ -686,9 +744,7 @@ int op_pair_f32(ddc_ctx* ctx, const double* x, double* y, const double* s, doubl
     CK(launch_lx_gather_f32(ctx->L(), g, ctx->tval.as<float>(), ctx->pot_f.as<float>()));
   }
   StageScope sc(ctx, ST_PROJ);
-  CK(launch_sgemm(ctx->L(), false, ctx->nylm, ctx->nsph, ctx->ngrid, -1.f, ctx->bw_f.as<float>(),
-                  ctx->nylm, ctx->pot_f.as<float>(), ctx->ngrid, y, ctx->nylm));
-  return DDC_OK;
+  return gemm_proj_f32(ctx, -1.f, ctx->pot_f.as<float>(), y);
 }
 
 // gjinv (jacobi_diis.f90:272-360): Gauss-Jordan, full pivoting, one rhs.
@@ -1408,6 +1464,7 @@ int ddc_destroy(ddc_ctx* c) {
     cudaEventDestroy(pe.second.second);
   }
   for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
+  if (c->blas) cublasDestroy(c->blas);
   delete c;
   if (st) cudaStreamDestroy(st);
   return DDC_OK;

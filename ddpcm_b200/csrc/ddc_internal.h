@@ -180,12 +180,8 @@ cudaError_t launch_lx_gather(Launch L, const DevGeo& g, const double* val, doubl
 cudaError_t launch_lx_gather_f32(Launch L, const DevGeo& g, const float* val, float* pot);
 cudaError_t launch_lstarx_acc_f32(Launch L, const YlmTables& tb, const DevGeo& g,
                                   const float* xi, double* y);
-// C[M x N] = alpha * op(A) * B in FP32 arithmetic, A float, B float or double, C float/double
-cudaError_t launch_sgemm(Launch L, bool transA, int M, int N, int K, float alpha, const float* A,
-                         int lda, const float* B, int ldb, double* C, int ldc);
-cudaError_t launch_sgemm_xi(Launch L, int M, int N, int K, const float* A, int lda,
-                            const double* B, int ldb, float* C, int ldc);
 cudaError_t launch_to_float(Launch L, long long n, const double* x, float* y);
+cudaError_t launch_to_double(Launch L, long long n, const float* x, double* y);
 // r = rhs - y - x/facl ; d = facl*r (Jacobi increment at x), partial H-norm of d
 cudaError_t launch_residual(Launch L, const YlmTables& tb, long long n, const double* rhs,
                             const double* y, const double* x, double* r, double* d,

@@ -1041,7 +1041,8 @@ __global__ void __launch_bounds__(256) k_dgemm(int M, int N, int K, double alpha
     }
 }
 // Register-tiled GEMM, column-major C[M x N] = alpha * op(A) * B, used for
-// the projection (M = nylm <= 128 rows in one tile) and for xi.  BM x BN
+// the one-off right-hand-side projections (M = nylm <= 128 rows in one
+// tile); the operators' per-iteration GEMMs go through cuBLAS.  BM x BN
 // tile per block, BK deep, TM x TN outputs per thread, shared tiles double
 // buffered with the next tile prefetched into registers.  Acc is the
 // arithmetic/accumulation type; inputs are converted when staged.
@@ -2966,83 +2967,6 @@ cudaError_t launch_lx_gather_f32(Launch L, const DevGeo& g, const float* val, fl
   return gather_launch<float>(L, g, val, pot);
 }
 
-// FP32 GEMM, column-major, 64x64 tiles, 256 threads x 4x4 outputs.
-// TB: float or double input for B (converted when staged), TC: output type.
-template <bool TA, class TB, class TC>
-__global__ void __launch_bounds__(256) k_sgemm(int M, int N, int K, float alpha,
-                                               const float* __restrict__ A, int lda,
-                                               const TB* __restrict__ B, int ldb, TC* C,
-                                               int ldc) {
-  __shared__ float As[GBK][GBM + 4];
-  __shared__ float Bs[GBK][GBN + 4];
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  const int m0 = blockIdx.x * GBM, n0 = blockIdx.y * GBN;
-  float acc[4][4];
-#pragma unroll
-  for (int a = 0; a < 4; ++a)
-#pragma unroll
-    for (int b = 0; b < 4; ++b) acc[a][b] = 0.f;
-  for (int k0 = 0; k0 < K; k0 += GBK) {
-    for (int e = threadIdx.x; e < GBM * GBK; e += 256) {
-      int mm, kk;
-      if (TA) { kk = e % GBK; mm = e / GBK; } else { mm = e % GBM; kk = e / GBM; }
-      int m = m0 + mm, k = k0 + kk;
-      float v = 0.f;
-      if (m < M && k < K) v = TA ? A[(size_t)m * lda + k] : A[(size_t)k * lda + m];
-      As[kk][mm] = v;
-    }
-    for (int e = threadIdx.x; e < GBK * GBN; e += 256) {
-      int kk = e % GBK, nn = e / GBK;
-      int n = n0 + nn, k = k0 + kk;
-      Bs[kk][nn] = (n < N && k < K) ? (float)B[(size_t)n * ldb + k] : 0.f;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int kk = 0; kk < GBK; ++kk) {
-      float a[4], b[4];
-#pragma unroll
-      for (int r = 0; r < 4; ++r) a[r] = As[kk][ty + 16 * r];
-#pragma unroll
-      for (int c = 0; c < 4; ++c) b[c] = Bs[kk][tx + 16 * c];
-#pragma unroll
-      for (int r = 0; r < 4; ++r)
-#pragma unroll
-        for (int c = 0; c < 4; ++c) acc[r][c] = fmaf(a[r], b[c], acc[r][c]);
-    }
-    __syncthreads();
-  }
-#pragma unroll
-  for (int r = 0; r < 4; ++r)
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      int m = m0 + ty + 16 * r, n = n0 + tx + 16 * c;
-      if (m < M && n < N) C[(size_t)n * ldc + m] = (TC)(alpha * acc[r][c]);
-    }
-}
-cudaError_t launch_sgemm(Launch L, bool transA, int M, int N, int K, float alpha, const float* A,
-                         int lda, const float* B, int ldb, double* C, int ldc) {
-  if (M == 0 || N == 0) return cudaSuccess;
-  return transA ? gemm2<true, float, float, double, float>(L, M, N, K, alpha, A, lda, B, ldb, C,
-                                                           ldc)
-                : gemm2<false, float, float, double, float>(L, M, N, K, alpha, A, lda, B, ldb, C,
-                                                            ldc);
-  dim3 grid((M + GBM - 1) / GBM, (N + GBN - 1) / GBN);
-  if (transA)
-    k_sgemm<true, float, double><<<grid, 256, 0, L.st>>>(M, N, K, alpha, A, lda, B, ldb, C, ldc);
-  else
-    k_sgemm<false, float, double><<<grid, 256, 0, L.st>>>(M, N, K, alpha, A, lda, B, ldb, C, ldc);
-  ++*L.launches;
-  return cudaGetLastError();
-}
-cudaError_t launch_sgemm_xi(Launch L, int M, int N, int K, const float* A, int lda,
-                            const double* B, int ldb, float* C, int ldc) {
-  if (M == 0 || N == 0) return cudaSuccess;
-  return gemm2<true, float, double, float, float>(L, M, N, K, 1.f, A, lda, B, ldb, C, ldc);
-  dim3 grid((M + GBM - 1) / GBM, (N + GBN - 1) / GBN);
-  k_sgemm<true, double, float><<<grid, 256, 0, L.st>>>(M, N, K, 1.f, A, lda, B, ldb, C, ldc);
-  ++*L.launches;
-  return cudaGetLastError();
-}
 __global__ void k_to_float(long long n, const double* __restrict__ x, float* y) {
   long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (e < n) y[e] = (float)x[e];
@@ -3050,6 +2974,16 @@ __global__ void k_to_float(long long n, const double* __restrict__ x, float* y) 
 cudaError_t launch_to_float(Launch L, long long n, const double* x, float* y) {
   if (n == 0) return cudaSuccess;
   k_to_float<<<(unsigned)((n + 255) / 256), 256, 0, L.st>>>(n, x, y);
+  ++*L.launches;
+  return cudaGetLastError();
+}
+__global__ void k_to_double(long long n, const float* __restrict__ x, double* y) {
+  long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e < n) y[e] = (double)x[e];
+}
+cudaError_t launch_to_double(Launch L, long long n, const float* x, double* y) {
+  if (n == 0) return cudaSuccess;
+  k_to_double<<<(unsigned)((n + 255) / 256), 256, 0, L.st>>>(n, x, y);
   ++*L.launches;
   return cudaGetLastError();
 }
