@@ -181,6 +181,8 @@ struct ddc_ctx {
   // or result of the mixed path's GEMMs (nylm x nsph)
   cublasHandle_t blas = nullptr;
   DBuf blas_ws, gemm_f;
+  // pinned landing buffer of the small device-to-host reads (reduced sums)
+  double* hred = nullptr;
 
   Launch L() { return Launch{st, &launches}; }
   DevGeo geo() const {
@@ -289,8 +291,10 @@ int finish_out(ddc_ctx* ctx, double* p, const double* dev, size_t count) {
                        ctx->st));
   return DDC_OK;
 }
-int sync(ddc_ctx* ctx) {
-  CK(cudaStreamSynchronize(ctx->st));
+// Stage-timer events are turned into times in batches: resolving them at
+// every synchronisation would put that host work between a solver step's
+// reduction and its next launch.
+void resolve_timers(ddc_ctx* ctx) {
   for (auto& pe : ctx->ev_pending) {
     float ms = 0.f;
     if (cudaEventElapsedTime(&ms, pe.second.first, pe.second.second) == cudaSuccess) {
@@ -301,6 +305,11 @@ int sync(ddc_ctx* ctx) {
     ctx->ev_pool.push_back(pe.second.second);
   }
   ctx->ev_pending.clear();
+}
+
+int sync(ddc_ctx* ctx) {
+  CK(cudaStreamSynchronize(ctx->st));
+  if (ctx->ev_pending.size() >= 1024) resolve_timers(ctx);
   return DDC_OK;
 }
 
@@ -401,8 +410,11 @@ int reduce_to_host(ddc_ctx* ctx, int nvals, double* host, int stride = 1, int nb
                               nblk > 0 ? nblk : reduce_blocks(), nvals, stride,
                               ctx->red.as<double>()));
   }
-  CK(cudaMemcpyAsync(host, ctx->red.p, sizeof(double) * nvals, cudaMemcpyDeviceToHost, ctx->st));
-  return sync(ctx);
+  CK(cudaMemcpyAsync(ctx->hred, ctx->red.p, sizeof(double) * nvals, cudaMemcpyDeviceToHost,
+                     ctx->st));
+  CKI(sync(ctx));
+  memcpy(host, ctx->hred, sizeof(double) * nvals);
+  return DDC_OK;
 }
 
 // The per-item counts that are about to be scanned into 32-bit offsets must
@@ -572,6 +584,7 @@ int do_init(ddc_ctx* ctx, int n, const std::vector<double4>* hsph, const double4
   // cuBLAS handle, created once per context and outside any graph capture;
   // its workspace is a context buffer, so a captured GEMM allocates nothing
   if (!ctx->blas) CKB(cublasCreate(&ctx->blas));
+  if (!ctx->hred) CK(cudaMallocHost(&ctx->hred, sizeof(double) * (kMaxHist + 1)));
   CK(ctx->blas_ws.ensure((size_t)32 << 20));
   if (ctx->prm.precision == DDC_PREC_MIXED) {
     CK(ctx->gemm_f.ensure(sizeof(float) * std::max(nv, (size_t)1)));
@@ -1465,6 +1478,7 @@ int ddc_destroy(ddc_ctx* c) {
   }
   for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
   if (c->blas) cublasDestroy(c->blas);
+  if (c->hred) cudaFreeHost(c->hred);
   delete c;
   if (st) cudaStreamDestroy(st);
   return DDC_OK;
@@ -1485,6 +1499,11 @@ const char* ddc_stage_name(int k) {
 }
 int ddc_stage_times(ddc_ctx* c, double* ms, long long* calls) {
   if (!c) return DDC_ERR_PARAM;
+  cudaSetDevice(c->prm.device);
+  if (!c->ev_pending.empty()) {
+    if (cudaStreamSynchronize(c->st) != cudaSuccess) return DDC_ERR_CUDA;
+    resolve_timers(c);
+  }
   for (int k = 0; k < ST_N; k++) {
     if (ms) ms[k] = c->st_ms[k];
     if (calls) calls[k] = c->st_calls[k];
@@ -1493,6 +1512,11 @@ int ddc_stage_times(ddc_ctx* c, double* ms, long long* calls) {
 }
 int ddc_reset_stage_times(ddc_ctx* c) {
   if (!c) return DDC_ERR_PARAM;
+  cudaSetDevice(c->prm.device);
+  if (!c->ev_pending.empty()) {
+    if (cudaStreamSynchronize(c->st) != cudaSuccess) return DDC_ERR_CUDA;
+    resolve_timers(c);
+  }
   for (int k = 0; k < ST_N; k++) {
     c->st_ms[k] = 0.0;
     c->st_calls[k] = 0;

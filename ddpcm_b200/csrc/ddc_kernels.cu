@@ -567,6 +567,18 @@ __device__ __forceinline__ GP<float> grid_pt(const DevGeo& g, int n, float*) {
 }
 __device__ __forceinline__ double rsqrt_t(double x) { return rsqrt(x); }
 __device__ __forceinline__ float rsqrt_t(float x) { return rsqrtf(x); }
+// 1/sqrt(x) for a positive normal x (a squared distance between distinct
+// points) in the N-body sums: the hardware estimate rsqrt.approx.ftz.f64,
+// then one third-order Householder step y (1 + h/2 + 3h^2/8), h = 1 - x y^2
+// (the binomial series of (1 - h)^(-1/2) to second order).  The step cubes
+// the estimate's relative error, so the result carries only the rounding of
+// its five FP64 operations; no special-value handling is needed for such x.
+__device__ __forceinline__ double rsqrt_pos(double x) {
+  double y;
+  asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+  const double h = fma(-x, y * y, 1.0);
+  return fma(y * h, fma(h, 0.375, 0.5), y);
+}
 __device__ __forceinline__ double sqrt_t(double x) { return sqrt(x); }
 __device__ __forceinline__ float sqrt_t(float x) { return sqrtf(x); }
 
@@ -1597,13 +1609,13 @@ __global__ void __launch_bounds__(kNbTile) k_coulomb_pot(int nsrc, const double*
       for (int k = 0; k < kNbTile; ++k) {
         double4 s = src[k];
         double dx = px - s.x, dy = py - s.y, dz = pz - s.z;
-        v = fma(s.w, rsqrt(dx * dx + dy * dy + dz * dz), v);
+        v = fma(s.w, rsqrt_pos(dx * dx + dy * dy + dz * dz), v);
       }
     } else {
       for (int k = kb; k < ke; ++k) {
         double4 s = src[k];
         double dx = px - s.x, dy = py - s.y, dz = pz - s.z;
-        v = fma(s.w, rsqrt(dx * dx + dy * dy + dz * dz), v);
+        v = fma(s.w, rsqrt_pos(dx * dx + dy * dy + dz * dz), v);
       }
     }
   }
@@ -1669,7 +1681,7 @@ __global__ void __launch_bounds__(kNbTile) k_efield(int nsrc, const double* __re
       double4 s = src[k];
       double dx = px - s.x, dy = py - s.y, dz = pz - s.z;
       double r2 = dx * dx + dy * dy + dz * dz;
-      double ri = rsqrt(r2);
+      double ri = rsqrt_pos(r2);
       double f = s.w * (ri * ri * ri);
       ex = fma(f, dx, ex);
       ey = fma(f, dy, ey);
