@@ -13,8 +13,10 @@ solves per second.
 * ``e2e``: the same through the C ABI with host arrays: the host->device copy
   of the inputs and the device->host copy of Esolv and the forces are inside
   the timed region.
-* ``roofline``: the dominant kernel of the step, timed live with the
-  library's CUDA-event stage timers.
+* ``roofline``: the dominant kernel of the step, timed live inside the timed
+  region with the library's CUDA-event stage timers (only that stage is
+  timed there; ``stage_ms_per_step`` comes from one untimed step after the
+  warm-up with every stage timed).
 * ``cpu_baseline``: the CPU oracle (restatement of the reference, OpenMP over
   all host cores) on a bounded sample of the same workload, scaled to one
   solve.
@@ -385,8 +387,23 @@ def run_ours(args):
     # headline: mixed precision (FP32 operator in FP64 refinement), reference guess
     names = list(VARIANTS)
     prec, guess, paired = VARIANTS[names[0]]
+    # After the warm-up, one untimed step with every stage timed gives the
+    # stage breakdown and the dominant stage; the timed region then records
+    # events around the dominant stage only (its live launch times feed the
+    # roofline), which keeps the other stages' event records off the host
+    # path between a solver step's reductions and its next launches.
     dd = make(prec, guess, device_pointers=1, timing=1, pair_solves=paired)
-    ms, info, launches, clk = timed(dd, dev_step(dd), args.warmup, args.steps, clocks=True)
+    step = dev_step(dd)
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    dd.reset_stage_times()
+    step()
+    profile_stages = dd.stage_times()
+    per = {k: v for k, v in profile_stages.items() if v[1] > 0 and k != "init"}
+    dom = max(per, key=lambda k: per[k][0])
+    dd.set_timed_stages([dom])
+    ms, info, launches, clk = timed(dd, step, 0, args.steps, clocks=True)
     stages = dd.stage_times()
     acc_head = accuracy(info)
     ms_step = ms / args.steps
@@ -425,8 +442,8 @@ def run_ours(args):
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
                               "ms_per_step": ms_step, "profile_run": True,
-                              "stage_ms_per_step": {k: round(v[0] / args.steps, 3)
-                                                    for k, v in dd_stages(stages).items()},
+                              "stage_ms_per_step": {k: round(v[0], 3) for k, v in
+                                                    dd_stages(profile_stages).items()},
                               "variants": variants,
                               "info": {k: info[k] for k in ("nsph", "ncav", "ntriples",
                                                             "npairs")}}), flush=True)
@@ -461,10 +478,8 @@ def run_ours(args):
     h2d = 5 * N * 8
     d2h = 3 * N * 8 + 8
 
-    # dominant kernel and its roofline
-    per = {k: v for k, v in stages.items() if v[1] > 0 and k != "init"}
-    dom = max(per, key=lambda k: per[k][0])
-    dom_ms, dom_calls = per[dom]
+    # dominant kernel and its roofline (its events in the timed region)
+    dom_ms, dom_calls = stages[dom]
     work = _stage_work(dom, info, c)
     fp64 = fp64_peak_gflops(local) if rank == 0 else None
     fp32 = fp32_peak_gflops(local) if rank == 0 else None
@@ -488,7 +503,7 @@ def run_ours(args):
                         "applications (6*nylm per triple each)")
     if roof["achieved"] and roof["peak"]:
         roof["frac"] = roof["achieved"] / roof["peak"]
-    stage_ms = {k: round(v[0] / args.steps, 3) for k, v in stages.items() if v[1] > 0}
+    stage_ms = {k: round(v[0], 3) for k, v in profile_stages.items() if v[1] > 0}
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
@@ -505,6 +520,7 @@ def run_ours(args):
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e / args.steps},
             "gpu_launches": launches, "stage_ms_per_step": stage_ms,
+            "stage_ms_note": "one untimed step after the warm-up with every stage timed",
             "roofline": roof, "clocks": clk.summary(),
             "peaks": {"fp64_gflops_measured": fp64, "fp32_gflops_measured": fp32,
                       "hbm_gbs": hbm, "hbm_source": hbm_src}}

@@ -183,6 +183,7 @@ struct ddc_ctx {
   DBuf blas_ws, gemm_f;
   // pinned landing buffer of the small device-to-host reads (reduced sums)
   double* hred = nullptr;
+  unsigned int stage_mask = ~0u;  // stages timed when prm.timing is set
 
   Launch L() { return Launch{st, &launches}; }
   DevGeo geo() const {
@@ -329,7 +330,7 @@ struct StageScope {
     return e;
   }
   StageScope(ddc_ctx* ctx, int s) : c(ctx), stage(s) {
-    if (!c->prm.timing || c->capturing) return;
+    if (!c->prm.timing || c->capturing || !((c->stage_mask >> s) & 1u)) return;
     a = take();
     b = take();
     if (a && b) cudaEventRecord(a, c->st);
@@ -1508,6 +1509,11 @@ int ddc_stage_times(ddc_ctx* c, double* ms, long long* calls) {
     if (ms) ms[k] = c->st_ms[k];
     if (calls) calls[k] = c->st_calls[k];
   }
+  return DDC_OK;
+}
+int ddc_set_timed_stages(ddc_ctx* c, unsigned int mask) {
+  if (!c) return DDC_ERR_PARAM;
+  c->stage_mask = mask;
   return DDC_OK;
 }
 int ddc_reset_stage_times(ddc_ctx* c) {

@@ -2864,14 +2864,15 @@ __global__ void __launch_bounds__(32 * ls_nroles(LMAX), LMAX > 10 ? 1 : (sizeof(
 // (a, n, b), read from b's gather list (pair slot lsstart).  Block per
 // sphere a; warp w takes the pairs p = w, w + NW, ... in order and adds into
 // its own shared row, lanes over the pair's points (distinct within a pair,
-// so no two lanes of a warp touch one entry).  Eight strided loads per lane
-// are issued before their adds.  The rows are summed in row order at the
-// end: a fixed summation order, no atomics.
+// so no two lanes of a warp touch one entry).  Four strided loads per lane
+// are issued before their adds, and the next pair's first loads before the
+// current pair's adds (two pairs in flight per warp).  The rows are summed
+// in row order at the end: a fixed summation order, no atomics.
 constexpr int kGatherWarps = 4;  // at most; fewer when NW rows of ngrid do not fit
 template <class Rl>
 __global__ void __launch_bounds__(32 * kGatherWarps)
     k_lx_gather(const DevGeo g, const Rl* __restrict__ val, Rl* pot) {
-  constexpr int U = 8;
+  constexpr int U = 4;
   const int NW = blockDim.x >> 5;
   extern __shared__ __align__(16) unsigned char smraw[];
   const int G = g.ngrid;
@@ -2886,20 +2887,43 @@ __global__ void __launch_bounds__(32 * kGatherWarps)
   for (int q = tid; q < NW * G; q += 32 * NW) acc[q] = 0;
   __syncthreads();
   Rl* myacc = acc + w * G;
+  // the first 32*U points of the warp's next pair are loaded before the
+  // current pair's values are added, so two pairs' loads are in flight
+  auto load = [&](int base, int q1, int d, int* n, Rl* v) {
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int q = base + 32 * u;
+      n[u] = q < q1 ? (int)g.pn[q] : -1;
+      v[u] = q < q1 ? val[q + d] : Rl(0);
+    }
+  };
+  auto add = [&](const int* n, const Rl* v) {
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+      if (n[u] >= 0) myacc[n[u]] += v[u];
+  };
+  int cn[U];
+  Rl cv[U];
+  if (w < nn) load(pst[w] + lane, pst[w + 1], dl[w], cn, cv);
   for (int p = w; p < nn; p += NW) {
     const int q0 = pst[p], q1 = pst[p + 1], d = dl[p];
-    for (int base = q0 + lane; base < q1; base += 32 * U) {
-      int n[U];
-      Rl v[U];
+    int nn1[U];
+    Rl nv1[U];
+    const bool more = p + NW < nn;
+    if (more) load(pst[p + NW] + lane, pst[p + NW + 1], dl[p + NW], nn1, nv1);
+    add(cn, cv);
+    for (int base = q0 + lane + 32 * U; base < q1; base += 32 * U) {
+      int n2[U];
+      Rl v2[U];
+      load(base, q1, d, n2, v2);
+      add(n2, v2);
+    }
+    if (more) {
 #pragma unroll
       for (int u = 0; u < U; ++u) {
-        const int q = base + 32 * u;
-        n[u] = q < q1 ? (int)g.pn[q] : -1;
-        v[u] = q < q1 ? val[q + d] : Rl(0);
+        cn[u] = nn1[u];
+        cv[u] = nv1[u];
       }
-#pragma unroll
-      for (int u = 0; u < U; ++u)
-        if (n[u] >= 0) myacc[n[u]] += v[u];
     }
   }
   __syncthreads();

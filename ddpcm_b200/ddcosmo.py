@@ -112,6 +112,7 @@ _SIGS = {
     "ddc_stage_name": [ctypes.c_int],
     "ddc_stage_times": [ctypes.c_void_p, _dp, ctypes.POINTER(ctypes.c_longlong)],
     "ddc_reset_stage_times": [ctypes.c_void_p],
+    "ddc_set_timed_stages": [ctypes.c_void_p, ctypes.c_uint],
     "ddc_fp64_peak": [ctypes.c_int, _dp],
     "ddc_fp32_peak": [ctypes.c_int, _dp],
     "ddc_batch_energy_forces": [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
@@ -244,6 +245,17 @@ class DDCosmo:
 
     def reset_stage_times(self):
         self._check(self.L.ddc_reset_stage_times(self.h))
+
+    def set_timed_stages(self, names=None):
+        """Time only the named stages (None: every stage)."""
+        if names is None:
+            mask = 0xFFFFFFFF
+        else:
+            idx = {self.L.ddc_stage_name(k).decode(): k for k in range(self.L.ddc_stage_count())}
+            mask = 0
+            for n in names:
+                mask |= 1 << idx[n]
+        self._check(self.L.ddc_set_timed_stages(self.h, mask))
 
     # ddinit (ddcosmo.f90:159): coordinates and radii in bohr
     def ddinit(self, x, y, z, rvdw):

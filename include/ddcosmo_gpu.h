@@ -206,6 +206,11 @@ int ddc_stage_count(void);
 const char* ddc_stage_name(int k);
 int ddc_stage_times(ddc_ctx* ctx, double* ms, long long* calls);
 int ddc_reset_stage_times(ddc_ctx* ctx);
+/* Restrict the stage timers to the stages whose bit (1 << k) is set in mask
+ * (default: every stage).  Each timed stage records two events per call, so
+ * timing only the stage of interest keeps the host work between a solver
+ * step's reductions and its next launches small. */
+int ddc_set_timed_stages(ddc_ctx* ctx, unsigned int mask);
 
 /* Measured FP64 FMA throughput of the device (GFLOP/s, 2 flops per FMA),
  * from a register-resident FMA kernel timed with CUDA events.  No
