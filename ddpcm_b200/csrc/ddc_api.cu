@@ -148,7 +148,7 @@ struct ddc_ctx {
   std::vector<double> h_grid;  // x,y,z,w per point
   // geometry
   DBuf sph, grid, basis, bw, fi, ui, zi, inl, nl, rev, pn_ptr, pn, pn_pair, ls_ptr, ls, ntri_pt;
-  DBuf lsstart, fxa, fda, xk;
+  DBuf lsstart, fxa, fda, fvec, xk;
   // batched molecules: partition, per-target N-body ranges, per-molecule DIIS state
   int nmol = 1;
   bool batch_init = false;  // set while ddc_batch_energy_forces initialises
@@ -1212,10 +1212,12 @@ int forces_dev(ddc_ctx* ctx, const double* phi, const double* sigma, const doubl
   const double fep = 0.5 * (ctx->prm.eps - 1.0) / ctx->prm.eps;
   CK(ctx->fxa.ensure(sizeof(double) * 3 * std::max(ctx->nsph, 1)));
   CK(ctx->fda.ensure(sizeof(double) * 3 * std::max<long long>(ctx->ntri, 1)));
+  const int nlm = (ctx->prm.lmax + 1) * (ctx->prm.lmax + 2) / 2;
+  CK(ctx->fvec.ensure(sizeof(double2) * 4 * nlm * std::max(ctx->nsph, 1)));
   StageScope sc(ctx, ST_FORCES);
   CK(launch_forces(ctx->L(), ctx->tb, ctx->geo(), sigma, ctx->xig.as<double>(),
                    ctx->uchi.as<double>(), phi, fep, fx, ctx->fxa.as<double>(),
-                   ctx->fda.as<double>()));
+                   ctx->fda.as<double>(), ctx->fvec.as<double2>()));
   return DDC_OK;
 }
 

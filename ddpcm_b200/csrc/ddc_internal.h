@@ -236,10 +236,11 @@ cudaError_t launch_efield_f32(Launch L, int nsrc, const double* q, const double*
                               const int2* trange);
 
 // forces
-// fxa (3,N) and fda (3,T) are scratch of the two force kernels
+// fxa (3,N), fda (3,T) and fv (4 (lmax+1)(lmax+2)/2 pairs per sphere) are
+// scratch of the force kernels
 cudaError_t launch_forces(Launch L, const YlmTables& tb, const DevGeo& g, const double* sigma,
                           const double* s_xi, const double* u_chi, const double* phi,
-                          double fep, double* fx, double* fxa, double* fda);
+                          double fep, double* fx, double* fxa, double* fda, double2* fv);
 cudaError_t launch_mkxi(Launch L, const YlmTables& tb, const DevGeo& g, const double* xi_grid,
                         double scale, double* out);
 cudaError_t launch_zeta_efld_contract(Launch L, const DevGeo& g, const double* zeta,

@@ -1995,6 +1995,140 @@ __device__ void dbasis_contract(const YlmTables& tb, double sx, double sy, doubl
   }
 }
 
+// The same alp and beta from the recurrence of the fused L / L* pass.  With
+// u = v / r_i (|u| = t, u / |u| = s) and the real solid harmonics
+// R_lm(u) = t^l Y_lm(s), the contraction above is
+//   beta  = sum_lm w_lm R_lm(u),   alp_k = sum_lm w_lm d_k R_lm(u),
+// w = sigma / facl, and d_k R_lm is a harmonic polynomial of degree l - 1,
+// so alp_k = sum_{l'm'} G^k_{l'm'} R_{l'm'}(u) with l' = l - 1.  G follows
+// from the ladder relations of the complex solid harmonics without the
+// Condon-Shortley phase, S_l^m = |u|^l Pt_l^m(cos theta) e^{i m phi}:
+//   d_z S_l^m = (l+m) S_{l-1}^m,   (d_x + i d_y) S_l^m = -S_{l-1}^{m+1},
+//   (d_x - i d_y) S_l^m = (l+m)(l+m-1) S_{l-1}^{m-1}   (m >= 1),
+//   (d_x - i d_y) S_l^0 = -conj(S_{l-1}^1),
+// with R_{l,+m} = nu_lm Re S_l^m, R_{l,-m} = nu_lm Im S_l^m, nu_lm = |facs_lm|.
+// k_force_vec writes per sphere the four vectors (beta, G^x, G^y, G^z) in
+// the (l, m >= 0) pair layout, scaled by Kg facl so that they contract the
+// normalised recurrence values Q_l^m (prefix 1) times cos / sin m phi.
+template <int LMAX>
+__global__ void k_force_vec(const YlmTables tb, int nsph, const double* __restrict__ sigma,
+                            double2* __restrict__ fv) {
+  constexpr int NLM = (LMAX + 1) * (LMAX + 2) / 2;
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (long long)nsph * NLM) return;
+  const int i = (int)(e / NLM), le = (int)(e - (long long)i * NLM);
+  int lp = 0;
+  while (lmi(lp + 1, 0) <= le) ++lp;
+  const int m = le - lmi(lp, 0);
+  const double* sg = sigma + (size_t)i * tb.nylm;
+  auto nu = [&](int l, int mm) { return fabs(tb.facs[lmi(l, mm)]); };
+  auto wc = [&](int l, int mm) { return sg[l * l + l + mm] / tb.facl[l]; };
+  auto ws = [&](int l, int mm) { return sg[l * l + l - mm] / tb.facl[l]; };
+  double2* out = fv + 4 * (size_t)e;
+  out[0] = make_double2(tb.Kg[le] * sg[lp * lp + lp + m], m ? tb.Kg[le] * sg[lp * lp + lp - m] : 0.0);
+  double gxc = 0.0, gxs = 0.0, gyc = 0.0, gys = 0.0, gzc = 0.0, gzs = 0.0;
+  if (lp < LMAX) {
+    const int l = lp + 1;
+    gzc = (double)(l + m) * nu(l, m) * wc(l, m);
+    if (m >= 1) gzs = (double)(l + m) * nu(l, m) * ws(l, m);
+    if (m + 1 <= l) {  // lowering from m + 1
+      const double f = 0.5 * nu(l, m + 1) * ((double)(l + m + 1) * (double)(l + m));
+      gxc += f * wc(l, m + 1);
+      gyc += f * ws(l, m + 1);
+      if (m >= 1) {
+        gxs += f * ws(l, m + 1);
+        gys -= f * wc(l, m + 1);
+      }
+    }
+    if (m >= 2) {  // raising from m - 1
+      const double f = 0.5 * nu(l, m - 1);
+      gxc -= f * wc(l, m - 1);
+      gyc += f * ws(l, m - 1);
+      gxs -= f * ws(l, m - 1);
+      gys -= f * wc(l, m - 1);
+    } else if (m == 1) {  // raising from m = 0
+      gxc -= nu(l, 0) * wc(l, 0);
+      gys -= nu(l, 0) * wc(l, 0);
+    }
+    const double sc = tb.Kg[le] * tb.facl[lp] / nu(lp, m);
+    gxc *= sc; gxs *= sc; gyc *= sc; gys *= sc; gzc *= sc; gzs *= sc;
+  }
+  out[1] = make_double2(gxc, gxs);
+  out[2] = make_double2(gyc, gys);
+  out[3] = make_double2(gzc, gzs);
+}
+cudaError_t launch_force_vec(Launch L, const YlmTables& tb, int nsph, const double* sigma,
+                             double2* fv) {
+  const int nlm = (tb.lmax + 1) * (tb.lmax + 2) / 2;
+  const long long n = (long long)nsph * nlm;
+  if (n == 0) return cudaSuccess;
+#define CASE(LV)                                                                              \
+  case LV:                                                                                    \
+    k_force_vec<LV><<<(unsigned)((n + 127) / 128), 128, 0, L.st>>>(tb, nsph, sigma, fv);       \
+    break;
+  switch (tb.lmax) {
+    DDC_LMAX_CASES(CASE)
+    default:
+      return cudaErrorInvalidValue;
+  }
+#undef CASE
+  ++*L.launches;
+  return cudaGetLastError();
+}
+// beta and alp of one triple (s off the poles) from the vectors V of its
+// sphere: ct = t cos theta, t2 = t^2, st = t sin theta, (cp, sp) = (cos, sin)
+// phi.  The column loop is not unrolled (register pressure); (l, m) is warp
+// uniform, so the table and shared-memory reads are broadcasts.
+template <int LMAX>
+__device__ __forceinline__ void force_contract(const YlmTables& tb, double ct, double t2,
+                                               double st, double cp, double sp,
+                                               const double2* V, double alp[3], double& beta) {
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  double pmm = 1.0, cm = 1.0, sm = 0.0, cmm1 = 1.0, smm1 = 0.0;
+#pragma unroll 1
+  for (int m = 0; m <= LMAX; ++m) {
+    if (m == 1) {
+      cm = cp;
+      sm = sp;
+    } else if (m >= 2) {
+      const double cn = 2.0 * cp * cm - cmm1, sn = 2.0 * cp * sm - smm1;
+      cmm1 = cm; smm1 = sm; cm = cn; sm = sn;
+    }
+    double dc[4] = {0.0, 0.0, 0.0, 0.0}, ds[4] = {0.0, 0.0, 0.0, 0.0};
+    // value Q of degree l: beta for every l, the gradient vectors below lmax
+    auto add = [&](double Q, int l) {
+      const double2* v = V + 4 * lmi(l, m);
+      const int nv = l < LMAX ? 4 : 1;
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        if (k < nv) {
+          const double2 c = v[k];
+          dc[k] = fma(Q, c.x, dc[k]);
+          ds[k] = fma(Q, c.y, ds[k]);
+        }
+    };
+    double q0 = pmm, q1 = ct * pmm;
+    add(q0, m);
+    if (m < LMAX) {
+      add(q1, m + 1);
+#pragma unroll 2
+      for (int l = m + 2; l <= LMAX; ++l) {
+        const double Q = fma(ct, q1, -(tb.Bn[lmi(l, m)] * t2) * q0);
+        q0 = q1;
+        q1 = Q;
+        add(Q, l);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) acc[k] = fma(cm, dc[k], fma(sm, ds[k], acc[k]));
+    pmm = -pmm * (double)(2 * m + 1) * st;
+  }
+  beta = acc[0];
+  alp[0] = acc[1];
+  alp[1] = acc[2];
+  alp[2] = acc[3];
+}
+
 // Forces, kernel A: block per sphere i over its gather list, i.e. the
 // triples (j, n, i) with point n of neighbour j inside i.  fdoka(j)
 // (ddcosmo.f90:1436-1504) and fdokb(i) (:1511-1607) both contract
@@ -2003,14 +2137,21 @@ __device__ void dbasis_contract(const YlmTables& tb, double sx, double sy, doubl
 // fxa(:,i), the fdoka term of sphere j goes to the per-triple slot fda(:,q).
 // fdokb's inner loop over k in N_j (:1575-1590) is u_chi(j,n) - chi_ji*beta
 // with u_chi = sum_k chi_jk intmlp_k (an extra k_lx pass on sigma).
+// alp and beta come from force_contract off the poles and from the
+// reference's dbasis restatement at them.
 template <int LMAX>
 __global__ void __launch_bounds__(128) k_forces_a(const YlmTables tb, const DevGeo g,
                                                   const double* __restrict__ sigma,
+                                                  const double2* __restrict__ fv,
                                                   const double* __restrict__ xs,
                                                   const double* __restrict__ uchi,
                                                   const double* __restrict__ phi, double* fxa,
                                                   double* fda) {
+  constexpr int NLM = (LMAX + 1) * (LMAX + 2) / 2;
+  __shared__ double2 sv[4 * NLM];
   const int i = blockIdx.x;
+  for (int k = threadIdx.x; k < 4 * NLM; k += blockDim.x) sv[k] = fv[4 * (size_t)i * NLM + k];
+  __syncthreads();
   const int G = g.ngrid, NY = g.nylm;
   const double4 ci = g.sph[i];
   const double eta = tb.eta, tlow = 1.0 - eta;
@@ -2026,7 +2167,12 @@ __global__ void __launch_bounds__(128) k_forces_a(const YlmTables tb, const DevG
     Rel r = rel_exact(cj, gn, ci);
     double sx = r.vx / r.vv, sy = r.vy / r.vv, sz = r.vz / r.vv;
     double alp[3], beta;
-    dbasis_contract<LMAX>(tb, sx, sy, sz, r.t, si, alp, beta);
+    const double sthe = sqrt(fmax(0.0, 1.0 - sz * sz));
+    if (sthe != 0.0)
+      force_contract<LMAX>(tb, r.t * sz, r.t * r.t, r.t * sthe, sx / sthe, sy / sthe, sv, alp,
+                           beta);
+    else
+      dbasis_contract<LMAX>(tb, sx, sy, sz, r.t, si, alp, beta);
     double xji = fsw_exact(r.t, eta), fj = g.fi[pj];
     double xij = xs[pj];
     double dsw = (r.t > tlow) ? dfsw_exact(r.t, eta) : 0.0;
@@ -2170,11 +2316,13 @@ __global__ void __launch_bounds__(128) k_forces_b(const DevGeo g, const double* 
 
 cudaError_t launch_forces(Launch L, const YlmTables& tb, const DevGeo& g, const double* sigma,
                           const double* s_xi, const double* u_chi, const double* phi,
-                          double fep, double* fx, double* fxa, double* fda) {
+                          double fep, double* fx, double* fxa, double* fda, double2* fv) {
   if (g.nsph == 0) return cudaSuccess;
+  cudaError_t e0 = launch_force_vec(L, tb, g.nsph, sigma, fv);
+  if (e0) return e0;
 #define CASE(LV)                                                                               \
   case LV:                                                                                     \
-    k_forces_a<LV><<<g.nsph, 128, 0, L.st>>>(tb, g, sigma, s_xi, u_chi, phi, fxa, fda);        \
+    k_forces_a<LV><<<g.nsph, 128, 0, L.st>>>(tb, g, sigma, fv, s_xi, u_chi, phi, fxa, fda);    \
     break;
   switch (tb.lmax) {
     DDC_LMAX_CASES(CASE)
