@@ -1871,11 +1871,19 @@ int ddc_energy_forces(ddc_ctx* ctx, int n, const double* charge, const double* x
   CK(ctx->phi.ensure(sizeof(double) * std::max(NC, 1)));
   double* dphi = ctx->phi.as<double>();
   double* dpsi = ctx->psi.as<double>();
-  // mkrhs (mkrhs.f90:102-120) with the context's own centres and cavity
+  // mkrhs (mkrhs.f90:102-120) with the context's own centres and cavity; with
+  // forces, the solute field at the cavity (main.f90:241-253) comes from the
+  // same pass over the pairs
+  if (ctx->prm.igrad) CK(ctx->ef1.ensure(sizeof(double) * 3 * std::max(NC, 1)));
   {
   StageScope sc(ctx, ST_COULOMB);
-  CK(launch_coulomb_pot(ctx->L(), N, dq, ctx->cx.as<double>(), ctx->cy.as<double>(),
-                        ctx->cz.as<double>(), NC, ctx->ccav.as<double>(), dphi, nullptr));
+  if (ctx->prm.igrad)
+    CK(launch_coulomb_pot_field(ctx->L(), N, dq, ctx->cx.as<double>(), ctx->cy.as<double>(),
+                                ctx->cz.as<double>(), NC, ctx->ccav.as<double>(), dphi,
+                                ctx->ef1.as<double>(), nullptr));
+  else
+    CK(launch_coulomb_pot(ctx->L(), N, dq, ctx->cx.as<double>(), ctx->cy.as<double>(),
+                          ctx->cz.as<double>(), NC, ctx->ccav.as<double>(), dphi, nullptr));
   CK(launch_psi(ctx->L(), N, ctx->nylm, dq, dpsi));
   }
   CKI(sync(ctx));
@@ -1934,19 +1942,13 @@ int ddc_energy_forces(ddc_ctx* ctx, int n, const double* charge, const double* x
     CKI(sync(ctx));
     double t5 = now_s();
     inf->t_forces = t5 - t4;
-    // solute field at the cavity times zeta (main.f90:241-253)
-    CK(ctx->ef1.ensure(sizeof(double) * 3 * std::max(NC, 1)));
+    // solute field at the cavity (from the mkrhs pass) times zeta
+    // (main.f90:241-253)
     CK(ctx->ef2.ensure(sizeof(double) * 3 * std::max(N, 1)));
-    int ch1 = efield_chunks(N, NC), ch2 = efield_chunks(NC, N);
-    CK(ctx->ef_scratch.ensure(sizeof(double) * 3 *
-                              std::max((size_t)ch1 * NC, (size_t)ch2 * N + 1)));
-    // in mixed precision the two force-only field sums use FP32 pair arithmetic
+    const int ch2 = efield_chunks(NC, N);
+    CK(ctx->ef_scratch.ensure(sizeof(double) * 3 * ((size_t)ch2 * N + 1)));
+    // in mixed precision the force-only field of zeta uses FP32 pair arithmetic
     auto efield = ctx->prm.precision == DDC_PREC_MIXED ? launch_efield_f32 : launch_efield;
-    {
-      StageScope sc(ctx, ST_EFIELD);
-      CK(efield(ctx->L(), N, dq, ctx->csph.as<double>(), NC, ctx->ccav.as<double>(),
-                ctx->ef1.as<double>(), ctx->ef_scratch.as<double>(), ch1, nullptr));
-    }
     {
       StageScope sc(ctx, ST_CONTRACT);
       CK(launch_zeta_efld_contract(ctx->L(), ctx->geo(), ctx->zeta.as<double>(),
@@ -2033,11 +2035,19 @@ int ddc_batch_energy_forces(ddc_ctx* ctx, int nmol, const int* off, const double
   CK(ctx->phi.ensure(sizeof(double) * std::max(NC, 1)));
   double* dphi = ctx->phi.as<double>();
   double* dpsi = ctx->psi.as<double>();
+  // the potential and (with forces) the solute field at the cavity, each
+  // molecule's points from its own nuclei
+  if (ctx->prm.igrad) CK(ctx->ef1.ensure(sizeof(double) * 3 * std::max(NC, 1)));
   {
     StageScope sc(ctx, ST_COULOMB);
-    CK(launch_coulomb_pot(ctx->L(), N, dq, ctx->cx.as<double>(), ctx->cy.as<double>(),
-                          ctx->cz.as<double>(), NC, ctx->ccav.as<double>(), dphi,
-                          ctx->tr_cav.as<int2>()));
+    if (ctx->prm.igrad)
+      CK(launch_coulomb_pot_field(ctx->L(), N, dq, ctx->cx.as<double>(), ctx->cy.as<double>(),
+                                  ctx->cz.as<double>(), NC, ctx->ccav.as<double>(), dphi,
+                                  ctx->ef1.as<double>(), ctx->tr_cav.as<int2>()));
+    else
+      CK(launch_coulomb_pot(ctx->L(), N, dq, ctx->cx.as<double>(), ctx->cy.as<double>(),
+                            ctx->cz.as<double>(), NC, ctx->ccav.as<double>(), dphi,
+                            ctx->tr_cav.as<int2>()));
     CK(launch_psi(ctx->L(), N, ctx->nylm, dq, dpsi));
   }
   CKI(sync(ctx));
@@ -2106,14 +2116,10 @@ int ddc_batch_energy_forces(ddc_ctx* ctx, int nmol, const int* off, const double
     CKI(sync(ctx));
     double t5 = now_s();
     inf->t_forces = t5 - t4;
-    CK(ctx->ef1.ensure(sizeof(double) * 3 * std::max(NC, 1)));
     CK(ctx->ef2.ensure(sizeof(double) * 3 * std::max(N, 1)));
     CK(ctx->ef_scratch.ensure(sizeof(double) * 3 * std::max((size_t)NC, (size_t)N)));
     {
       StageScope sc(ctx, ST_EFIELD);
-      CK(launch_efield(ctx->L(), N, dq, ctx->csph.as<double>(), NC, ctx->ccav.as<double>(),
-                       ctx->ef1.as<double>(), ctx->ef_scratch.as<double>(), 1,
-                       ctx->tr_cav.as<int2>()));
       CK(launch_efield(ctx->L(), NC, ctx->zeta.as<double>(), ctx->ccav.as<double>(), N,
                        ctx->csph.as<double>(), ctx->ef2.as<double>(),
                        ctx->ef_scratch.as<double>(), 1, ctx->tr_nuc.as<int2>()));

@@ -220,6 +220,11 @@ int reduce_blocks();
 
 // electrostatics
 // trange: per target, the source index range it sums over (nullptr: all)
+// launch_coulomb_pot plus the field of the same sources at the targets, ef (3, ntrg)
+cudaError_t launch_coulomb_pot_field(Launch L, int nsrc, const double* q, const double* sx,
+                                     const double* sy, const double* sz, int ntrg,
+                                     const double* ctrg, double* phi, double* ef,
+                                     const int2* trange);
 cudaError_t launch_coulomb_pot(Launch L, int nsrc, const double* q, const double* sx,
                                const double* sy, const double* sz, int ntrg, const double* ctrg,
                                double* phi, const int2* trange);

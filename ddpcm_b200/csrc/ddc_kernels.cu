@@ -1621,6 +1621,64 @@ __global__ void __launch_bounds__(kNbTile) k_coulomb_pot(int nsrc, const double*
   }
   if (t < ntrg) phi[t] = v;
 }
+// The potential and, for the forces, the solute's field at the same targets
+// (efld.f90:97-114 with the nuclei as sources) from one pass over the pairs:
+// per pair the field adds q r^-3 (p - s) to the potential's q r^-1.
+__global__ void __launch_bounds__(kNbTile) k_coulomb_pot_field(
+    int nsrc, const double* __restrict__ q, const double* __restrict__ sx,
+    const double* __restrict__ sy, const double* __restrict__ sz, int ntrg,
+    const double* __restrict__ ctrg, double* phi, double* ef, const int2* __restrict__ trange) {
+  __shared__ double4 src[kNbTile];
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  double px = 0, py = 0, pz = 0;
+  if (t < ntrg) {
+    px = ctrg[3 * (size_t)t];
+    py = ctrg[3 * (size_t)t + 1];
+    pz = ctrg[3 * (size_t)t + 2];
+  }
+  const SrcRange rg = block_src_range(trange, t, ntrg, 0, nsrc);
+  double v = 0.0, ex = 0.0, ey = 0.0, ez = 0.0;
+  auto pair = [&](const double4& s) {
+    const double dx = px - s.x, dy = py - s.y, dz = pz - s.z;
+    const double ri = rsqrt_pos(dx * dx + dy * dy + dz * dz);
+    v = fma(s.w, ri, v);
+    const double f = s.w * (ri * ri * ri);
+    ex = fma(f, dx, ex);
+    ey = fma(f, dy, ey);
+    ez = fma(f, dz, ez);
+  };
+  for (int j0 = rg.ulo; j0 < rg.uhi; j0 += kNbTile) {
+    int j = j0 + threadIdx.x;
+    __syncthreads();
+    src[threadIdx.x] = j < rg.uhi ? make_double4(sx[j], sy[j], sz[j], q[j])
+                                  : make_double4(0, 0, 0, 0);
+    __syncthreads();
+    int cnt = min(kNbTile, rg.uhi - j0);
+    const int kb = max(rg.lo - j0, 0), ke = min(rg.hi - j0, cnt);
+    if (kb == 0 && ke == kNbTile) {
+#pragma unroll 4
+      for (int k = 0; k < kNbTile; ++k) pair(src[k]);
+    } else {
+      for (int k = kb; k < ke; ++k) pair(src[k]);
+    }
+  }
+  if (t < ntrg) {
+    phi[t] = v;
+    ef[3 * (size_t)t] = ex;
+    ef[3 * (size_t)t + 1] = ey;
+    ef[3 * (size_t)t + 2] = ez;
+  }
+}
+cudaError_t launch_coulomb_pot_field(Launch L, int nsrc, const double* q, const double* sx,
+                                     const double* sy, const double* sz, int ntrg,
+                                     const double* ctrg, double* phi, double* ef,
+                                     const int2* trange) {
+  if (ntrg == 0) return cudaSuccess;
+  k_coulomb_pot_field<<<(ntrg + kNbTile - 1) / kNbTile, kNbTile, 0, L.st>>>(
+      nsrc, q, sx, sy, sz, ntrg, ctrg, phi, ef, trange);
+  ++*L.launches;
+  return cudaGetLastError();
+}
 cudaError_t launch_coulomb_pot(Launch L, int nsrc, const double* q, const double* sx,
                                const double* sy, const double* sz, int ntrg, const double* ctrg,
                                double* phi, const int2* trange) {
