@@ -1294,72 +1294,108 @@ __device__ __forceinline__ int lm_add(int lm, int d, int nylm) {
 
 // Jacobi step + DIIS Gram row: xnew = D^-1 (rhs - Ox) (jacobi_diis.f90:105-110),
 // e = xnew - x (:117), dots e.h_k for the history and e.e (makeb :232-270).
-// NB >= hist.n bounds the accumulators (bucketed at launch); the partial row
-// keeps the stride kMaxHist + 1 that the host-side reduction expects.
-template <class H, int NB>
-__global__ void __launch_bounds__(kSolT) k_jacobi_step(const YlmTables tb, long long n,
+// A block takes tiles of 8 x 256 consecutive elements: each thread forms
+// eight elements of xnew and e and leaves e in shared memory; then warp w
+// takes the history vectors k = w, w + 8, ... and reads the tile of h_k
+// (sixteen loads per lane in flight) against e from shared memory.  Per
+// history vector a lane accumulates in FP64 over the tiles in order, and the
+// warp's shuffle tree gives the block's partial, so the row is reproducible.
+// The partial row keeps the stride kMaxHist + 1 that the host-side
+// reduction expects.
+template <class H>
+__global__ void __launch_bounds__(kSolT, 4) k_jacobi_step(const YlmTables tb, long long n,
                                                        const double* __restrict__ rhs,
                                                        const double* __restrict__ y,
                                                        const double* __restrict__ x, H* xnew,
                                                        H* e, const HistPtrs hist,
                                                        double* partials) {
-  constexpr int U = 2 * kSolU;  // eight elements per thread and step
-  double d[NB + 1];
+  constexpr int U = 2 * kSolU;  // eight elements per thread and tile
+  constexpr int TILE = U * kSolT;
+  constexpr int NW = kSolT / 32;
+  constexpr int KS = (kMaxHist + NW - 1) / NW;  // history vectors per warp
+  constexpr int HL = 16;                        // loads per lane in flight
+  __shared__ H es[TILE];
+  __shared__ double red[kMaxHist + 1 + NW];
+  double d[KS];
 #pragma unroll
-  for (int k = 0; k <= NB; ++k) d[k] = 0.0;
+  for (int s = 0; s < KS; ++s) d[s] = 0.0;
+  double ee = 0.0;
   const int nh = hist.n, nylm = tb.nylm;
   const int dt = kSolT % nylm;
   const int nn = (int)n;  // vectors hold fewer than 2^31 elements (checked at launch)
-  for (int b0 = blockIdx.x * U * kSolT; b0 < nn; b0 += gridDim.x * U * kSolT) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int b0 = blockIdx.x * TILE; b0 < nn; b0 += gridDim.x * TILE) {
     const int q0 = b0 + threadIdx.x;
-    H ev[U];
-    {
-      double rv[U], yv[U], xv[U];
+    int lm = lm_first(q0, nylm);
 #pragma unroll
-      for (int u = 0; u < U; ++u) {
-        const int q = q0 + u * kSolT;
+    for (int h = 0; h < U; h += kSolU) {  // two halves of four elements
+      double rv[kSolU], yv[kSolU], xv[kSolU];
+#pragma unroll
+      for (int u = 0; u < kSolU; ++u) {
+        const int q = q0 + (h + u) * kSolT;
         rv[u] = q < nn ? rhs[q] : 0.0;
         yv[u] = q < nn ? y[q] : 0.0;
         xv[u] = q < nn ? x[q] : 0.0;
       }
-      int lm = lm_first(q0, nylm);
 #pragma unroll
-      for (int u = 0; u < U; ++u) {
-        const int q = q0 + u * kSolT;
+      for (int u = 0; u < kSolU; ++u) {
+        const int q = q0 + (h + u) * kSolT;
         const double xn = tb.facl[l_of(lm)] * (rv[u] - yv[u]);
-        ev[u] = q < nn ? (H)(xn - xv[u]) : H(0);
+        const H ev = q < nn ? (H)(xn - xv[u]) : H(0);
         if (q < nn) {
           xnew[q] = (H)xn;
-          e[q] = ev[u];
+          e[q] = ev;
         }
+        es[threadIdx.x + (h + u) * kSolT] = ev;
+        ee = fma((double)ev, (double)ev, ee);
         lm = lm_add(lm, dt, nylm);
       }
     }
+    __syncthreads();
+    const int cnt = min(TILE, nn - b0);
 #pragma unroll
-    for (int k = 0; k < NB; ++k) {
+    for (int s = 0; s < KS; ++s) {
+      const int k = w + NW * s;
       if (k < nh) {
-        const H* hk = static_cast<const H*>(hist.p[k]);
-        H hv[U];
+        const H* hk = static_cast<const H*>(hist.p[k]) + b0;
+        for (int j0 = 0; j0 < TILE; j0 += 32 * HL) {
+          H hv[HL];
 #pragma unroll
-        for (int u = 0; u < U; ++u) {
-          const int q = q0 + u * kSolT;
-          hv[u] = q < nn ? hk[q] : H(0);
+          for (int u = 0; u < HL; ++u) {
+            const int j = j0 + u * 32 + lane;
+            hv[u] = j < cnt ? hk[j] : H(0);
+          }
+#pragma unroll
+          for (int u = 0; u < HL; ++u)
+            d[s] = fma((double)es[j0 + u * 32 + lane], (double)hv[u], d[s]);
         }
-#pragma unroll
-        for (int u = 0; u < U; ++u) d[k] = fma((double)ev[u], (double)hv[u], d[k]);
       }
     }
-#pragma unroll
-    for (int u = 0; u < U; ++u) d[NB] = fma((double)ev[u], (double)ev[u], d[NB]);
+    __syncthreads();
   }
   // partial row [e.h_0 .. e.h_{nh-1}, e.e]
-  double v[NB + 1];
 #pragma unroll
-  for (int k = 0; k <= NB; ++k) v[k] = (k < nh) ? d[k] : (k == nh ? d[NB] : 0.0);
-  block_sum_store<NB + 1, kMaxHist + 1>(v, nh + 1, partials);
+  for (int s = 0; s < KS; ++s) {
+    double v = d[s];
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int k = w + NW * s;
+    if (lane == 0 && k < nh) red[k] = v;
+  }
+#pragma unroll
+  for (int o = 16; o >= 1; o >>= 1) ee += __shfl_xor_sync(0xffffffffu, ee, o);
+  if (lane == 0) red[kMaxHist + 1 + w] = ee;
+  __syncthreads();
+  if (threadIdx.x < nh) {
+    partials[(size_t)blockIdx.x * (kMaxHist + 1) + threadIdx.x] = red[threadIdx.x];
+  } else if (threadIdx.x == nh) {
+    double t = 0.0;
+    for (int ww = 0; ww < NW; ++ww) t += red[kMaxHist + 1 + ww];
+    partials[(size_t)blockIdx.x * (kMaxHist + 1) + nh] = t;
+  }
 }
-// One wave: as many blocks as fit on the device at once for this bucket's
-// register count (at most nblk, the partial-row capacity).
+// One wave: as many blocks as fit on the device at once (at most nblk, the
+// partial-row capacity).
 template <class KFN>
 static int one_wave_blocks(KFN kfn, int nblk) {
   static int sms = 0;
@@ -1381,20 +1417,8 @@ template <class H>
 static int jacobi_launch(Launch L, const YlmTables& tb, long long n, const double* rhs,
                          const double* y, const double* x, H* xnew, H* e, const HistPtrs& hist,
                          double* partials, int nblk) {
-  const int nh = hist.n;
-  int used = nblk;
-#define JB(NB)                                                                              \
-  {                                                                                         \
-    used = one_wave_blocks(k_jacobi_step<H, NB>, nblk);                                     \
-    k_jacobi_step<H, NB><<<used, kSolT, 0, L.st>>>(tb, n, rhs, y, x, xnew, e, hist, partials); \
-  }
-  if (nh <= 1) JB(1)
-  else if (nh <= 4) JB(4)
-  else if (nh <= 8) JB(8)
-  else if (nh <= 16) JB(16)
-  else if (nh <= 24) JB(24)
-  else JB(kMaxHist)
-#undef JB
+  const int used = one_wave_blocks(k_jacobi_step<H>, nblk);
+  k_jacobi_step<H><<<used, kSolT, 0, L.st>>>(tb, n, rhs, y, x, xnew, e, hist, partials);
   return used;
 }
 cudaError_t launch_jacobi_step(Launch L, const YlmTables& tb, long long n, const double* rhs,
@@ -1440,7 +1464,7 @@ __global__ void __launch_bounds__(kSolT) k_diis_combine(const YlmTables tb, long
 #pragma unroll
       for (int u = 0; u < kSolU; ++u) xo[u] = ok[u] ? (double)xjac[q[u]] : 0.0;
     } else {
-#pragma unroll 2
+#pragma unroll 4
       for (int k = 0; k < nh; ++k) {
         const H* hk = static_cast<const H*>(hist.p[k]);
         const double ck = hist.c[k];
