@@ -2830,8 +2830,8 @@ struct LxsIn {
   Rl xv;
 };
 template <class Rl>
-__device__ __forceinline__ LxsIn<Rl> lxs_load(const DevGeo& g, const Rl* __restrict__ xi, int q) {
-  const int2 an = g.ls[q];
+__device__ __forceinline__ LxsIn<Rl> lxs_load(const DevGeo& g, const Rl* __restrict__ xi, int q,
+                                               int2 an) {
   const size_t pa = (size_t)an.x * g.ngrid + an.y;
   LxsIn<Rl> in;
   in.ca = g.sph[an.x];
@@ -2953,8 +2953,7 @@ __device__ __forceinline__ float2 tgeo2_of(const DevGeo& g, int q, float*) { ret
 __device__ __forceinline__ double2 tgeo2_of(const DevGeo& g, int q, double*) { return g.tgeo2d[q]; }
 template <class Rl>
 __device__ __forceinline__ LxsInP<Rl> lxs_load_pre(const DevGeo& g, const Rl* __restrict__ xi,
-                                                   int q) {
-  const int2 an = g.ls[q];
+                                                   int q, int2 an) {
   LxsInP<Rl> in;
   in.g4 = tgeo4_of(g, q, (Rl*)nullptr);
   in.g2 = tgeo2_of(g, q, (Rl*)nullptr);
@@ -3038,20 +3037,31 @@ __global__ void __launch_bounds__(32 * ls_nroles(LMAX), LMAX > 10 ? 1 : (sizeof(
   // with the geometry precomputed at ddinit only xi_a(n) and the grid weight
   // are read per triple besides the two geometry vectors
   typedef typename std::conditional<PRE, LxsInP<Rl>, LxsIn<Rl>>::type In;
-  auto load = [&](int q) -> In {
-    if constexpr (PRE) return lxs_load_pre<Rl>(g, xi, q);
-    else return lxs_load<Rl>(g, xi, q);
+  // an: the triple's gather-list entry (a, n), loaded a chunk earlier than
+  // the inputs that depend on it
+  auto load = [&](int q, int2 an) -> In {
+    if constexpr (PRE) return lxs_load_pre<Rl>(g, xi, q, an);
+    else return lxs_load<Rl>(g, xi, q, an);
   };
   auto fields = [&](const In& in, Rl* buf) {
     if constexpr (PRE) lxs_fields_pre<LMAX, Rl>(in, buf, tid);
     else lxs_fields<LMAX, Rl>(tb, in, cb, irb, buf, tid);
   };
   if constexpr (!lxs_piped<Rl>()) {
-    // FP64: one buffer (two blocks per SM fit), two barriers per chunk
+    // FP64: one buffer (two blocks per SM fit), two barriers per chunk; the
+    // inputs of chunk k+1 are loaded while the roles work on chunk k
+    In cur;
+    int2 an1 = make_int2(0, 0);
+    if (nch > 0 && tid < min(CH, q1 - q0)) cur = load(q0 + tid, g.ls[q0 + tid]);
+    if (nch > 1 && tid < min(CH, q1 - q0 - CH)) an1 = g.ls[q0 + CH + tid];
     for (int k = 0; k < nch; ++k) {
       const int c0 = q0 + k * CH, cnt = min(CH, q1 - c0);
-      if (tid < cnt) fields(load(c0 + tid), fld);
+      if (tid < cnt) fields(cur, fld);
       __syncthreads();
+      const int n1 = k + 1 < nch ? min(CH, q1 - c0 - CH) : 0;
+      const int n2 = k + 2 < nch ? min(CH, q1 - c0 - 2 * CH) : 0;
+      if (tid < n1) cur = load(c0 + CH + tid, an1);
+      if (tid < n2) an1 = g.ls[c0 + 2 * CH + tid];
       lxs_run_role<LMAX, 0, Rl>(role, tb, fld, cnt, lane, acc, xr, lxp);
       __syncthreads();
       if (tid < cnt) {
@@ -3064,15 +3074,21 @@ __global__ void __launch_bounds__(32 * ls_nroles(LMAX), LMAX > 10 ? 1 : (sizeof(
     ls_finish_role<LMAX, 0, Rl, true>(role, tb, acc, y + (size_t)b * tb.nylm, lane);
     return;
   }
-  if (nch > 0 && tid < min(CH, q1 - q0)) fields(load(q0 + tid), fld);
+  if (nch > 0 && tid < min(CH, q1 - q0)) fields(load(q0 + tid, g.ls[q0 + tid]), fld);
+  int2 an1 = make_int2(0, 0);
+  if (nch > 1 && tid < min(CH, q1 - q0 - CH)) an1 = g.ls[q0 + CH + tid];
   __syncthreads();
-  // chunk k: loads of chunk k+1 in flight while the roles work on chunk k,
-  // then chunk k+1's fields go to the other buffer; one barrier per chunk
+  // chunk k: loads of chunk k+1 (and the gather-list entries of chunk k+2)
+  // in flight while the roles work on chunk k, then chunk k+1's fields go to
+  // the other buffer; one barrier per chunk
   for (int k = 0; k < nch; ++k) {
     const int c0 = q0 + k * CH, cnt = min(CH, q1 - c0);
     const int n1 = k + 1 < nch ? min(CH, q1 - c0 - CH) : 0;
+    const int n2 = k + 2 < nch ? min(CH, q1 - c0 - 2 * CH) : 0;
     In nxt;
-    if (tid < n1) nxt = load(c0 + CH + tid);
+    if (tid < n1) nxt = load(c0 + CH + tid, an1);
+    int2 an2 = make_int2(0, 0);
+    if (tid < n2) an2 = g.ls[c0 + 2 * CH + tid];
     lxs_run_role<LMAX, 0, Rl>(role, tb, fld + (k & 1) * NF * CH, cnt, lane, acc, xr,
                               lxp + (k & 1) * NR * CH);
     if (tid < n1) fields(nxt, fld + ((k + 1) & 1) * NF * CH);
@@ -3086,6 +3102,7 @@ __global__ void __launch_bounds__(32 * ls_nroles(LMAX), LMAX > 10 ? 1 : (sizeof(
       for (int r = 1; r < NR; ++r) sv += lp[r * CH + tid];
       val[c0 + tid] = sv;
     }
+    an1 = an2;
   }
   ls_finish_role<LMAX, 0, Rl, true>(role, tb, acc, y + (size_t)b * tb.nylm, lane);
 }
