@@ -1945,10 +1945,11 @@ int ddc_energy_forces(ddc_ctx* ctx, int n, const double* charge, const double* x
     // solute field at the cavity (from the mkrhs pass) times zeta
     // (main.f90:241-253)
     CK(ctx->ef2.ensure(sizeof(double) * 3 * std::max(N, 1)));
-    const int ch2 = efield_chunks(NC, N);
+    const bool mixed = ctx->prm.precision == DDC_PREC_MIXED;
+    const int ch2 = mixed ? efield_chunks_f32(NC, N) : efield_chunks(NC, N);
     CK(ctx->ef_scratch.ensure(sizeof(double) * 3 * ((size_t)ch2 * N + 1)));
     // in mixed precision the force-only field of zeta uses FP32 pair arithmetic
-    auto efield = ctx->prm.precision == DDC_PREC_MIXED ? launch_efield_f32 : launch_efield;
+    auto efield = mixed ? launch_efield_f32 : launch_efield;
     {
       StageScope sc(ctx, ST_CONTRACT);
       CK(launch_zeta_efld_contract(ctx->L(), ctx->geo(), ctx->zeta.as<double>(),

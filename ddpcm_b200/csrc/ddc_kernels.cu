@@ -1732,6 +1732,14 @@ int efield_chunks(int nsrc, int ntrg) {
   int maxc = (nsrc + 4 * kNbTile - 1) / (4 * kNbTile);
   return max(1, min(want, max(maxc, 1)));
 }
+// source chunks for the FP32 field of one molecule: enough blocks of the
+// two-targets-per-thread kernel (k_efield_f2) to fill the device
+int efield_chunks_f32(int nsrc, int ntrg) {
+  int tiles2 = (ntrg + 2 * kNbTile - 1) / (2 * kNbTile);
+  int want = (148 * 8 + tiles2 - 1) / max(tiles2, 1);
+  int maxc = (nsrc + 4 * kNbTile - 1) / (4 * kNbTile);
+  return max(1, min(want, max(maxc, 1)));
+}
 
 __global__ void __launch_bounds__(kNbTile) k_efield(int nsrc, const double* __restrict__ q,
                                                     const double* __restrict__ csrc, int ntrg,
