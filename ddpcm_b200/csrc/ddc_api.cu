@@ -405,6 +405,8 @@ void build_tables(ddc_ctx* c) {
 // Jacobi step's Gram row, whatever its current length; 1 for single sums).
 // nblk: the producing kernel's block count (partial rows).
 int reduce_to_host(ddc_ctx* ctx, int nvals, double* host, int stride = 1, int nblk = 0) {
+  if (nvals > kMaxHist + 1 || !ctx->hred)
+    return fail(ctx, DDC_ERR_STATE, "reduction read beyond the pinned buffer");
   {
     StageScope sc(ctx, ST_REDUCE);
     CK(launch_reduce_partials(ctx->L(), ctx->partials.as<double>(),
