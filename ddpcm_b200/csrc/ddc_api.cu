@@ -183,6 +183,10 @@ struct ddc_ctx {
   DBuf blas_ws, gemm_f;
   // pinned landing buffer of the small device-to-host reads (reduced sums)
   double* hred = nullptr;
+  // second stream of the force tail: the field of zeta at the nuclei runs
+  // beside the force kernels (events: fork after zeta, join before its use)
+  cudaStream_t st2 = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   unsigned int stage_mask = ~0u;  // stages timed when prm.timing is set
 
   Launch L() { return Launch{st, &launches}; }
@@ -329,15 +333,17 @@ struct StageScope {
     }
     return e;
   }
-  StageScope(ddc_ctx* ctx, int s) : c(ctx), stage(s) {
+  cudaStream_t on;
+  StageScope(ddc_ctx* ctx, int s, cudaStream_t stream = nullptr)
+      : c(ctx), stage(s), on(stream ? stream : ctx->st) {
     if (!c->prm.timing || c->capturing || !((c->stage_mask >> s) & 1u)) return;
     a = take();
     b = take();
-    if (a && b) cudaEventRecord(a, c->st);
+    if (a && b) cudaEventRecord(a, on);
   }
   ~StageScope() {
     if (!a || !b) return;
-    cudaEventRecord(b, c->st);
+    cudaEventRecord(b, on);
     c->ev_pending.push_back({stage, {a, b}});
   }
 };
@@ -588,6 +594,11 @@ int do_init(ddc_ctx* ctx, int n, const std::vector<double4>* hsph, const double4
   // its workspace is a context buffer, so a captured GEMM allocates nothing
   if (!ctx->blas) CKB(cublasCreate(&ctx->blas));
   if (!ctx->hred) CK(cudaMallocHost(&ctx->hred, sizeof(double) * (kMaxHist + 1)));
+  if (ctx->prm.igrad && !ctx->st2) {
+    CK(cudaStreamCreateWithFlags(&ctx->st2, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming));
+  }
   CK(ctx->blas_ws.ensure((size_t)32 << 20));
   if (ctx->prm.precision == DDC_PREC_MIXED) {
     CK(ctx->gemm_f.ensure(sizeof(float) * std::max(nv, (size_t)1)));
@@ -1202,10 +1213,13 @@ int cosmo_dev(ddc_ctx* ctx, int star, int cart, const double* phi, const double*
 }
 
 // forces_dd on device vectors (forces_dd.f90:91-164)
-int forces_dev(ddc_ctx* ctx, const double* phi, const double* sigma, const double* s, double* fx) {
+// xi_ready: xig already holds xi of s (the energy+force flow forms it first
+// for zeta)
+int forces_dev(ddc_ctx* ctx, const double* phi, const double* sigma, const double* s, double* fx,
+               bool xi_ready = false) {
   if (!ctx->prm.igrad || !ctx->zi.p)
     return fail(ctx, DDC_ERR_STATE, "forces need igrad=1 at init (zi)");
-  CKI(op_xi(ctx, s, ctx->xig.as<double>()));
+  if (!xi_ready) CKI(op_xi(ctx, s, ctx->xig.as<double>()));
   {
     StageScope sc(ctx, ST_UCHI);
     CK(launch_lx_pot(ctx->L(), ctx->tb, ctx->geo(), sigma, ctx->uchi.as<double>(), true,
@@ -1484,6 +1498,10 @@ int ddc_destroy(ddc_ctx* c) {
   for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
   if (c->blas) cublasDestroy(c->blas);
   if (c->hred) cudaFreeHost(c->hred);
+  if (c->st2) cudaStreamSynchronize(c->st2);
+  if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+  if (c->ev_join) cudaEventDestroy(c->ev_join);
+  if (c->st2) cudaStreamDestroy(c->st2);
   delete c;
   if (st) cudaStreamDestroy(st);
   return DDC_OK;
@@ -1933,7 +1951,11 @@ int ddc_energy_forces(ddc_ctx* ctx, int n, const double* charge, const double* x
     inf->t_adjoint = t4 - t3;
     CK(ctx->fx.ensure(sizeof(double) * 3 * std::max(N, 1)));
     dfx = ctx->fx.as<double>();
-    CKI(forces_dev(ctx, dphi, dsig, ds, dfx));
+    // zeta first (ddmkzeta, ddcosmo.f90:1758-1806): the field of zeta at the
+    // nuclei (main.f90:259-265) then runs on the second stream beside the
+    // force kernels, which keep the FP64 pipe busy while it loads the FP32
+    // (or FP64) pipe
+    CKI(op_xi(ctx, ds, ctx->xig.as<double>()));
     CK(ctx->zeta.ensure(sizeof(double) * std::max(NC, 1)));
     double fep = 0.5 * ((ctx->prm.eps - 1.0) / ctx->prm.eps);
     {
@@ -1941,35 +1963,39 @@ int ddc_energy_forces(ddc_ctx* ctx, int n, const double* charge, const double* x
       CK(launch_mkxi(ctx->L(), ctx->tb, ctx->geo(), ctx->xig.as<double>(), fep,
                      ctx->zeta.as<double>()));
     }
-    CKI(sync(ctx));
-    double t5 = now_s();
-    inf->t_forces = t5 - t4;
-    // solute field at the cavity (from the mkrhs pass) times zeta
-    // (main.f90:241-253)
     CK(ctx->ef2.ensure(sizeof(double) * 3 * std::max(N, 1)));
     const bool mixed = ctx->prm.precision == DDC_PREC_MIXED;
     const int ch2 = mixed ? efield_chunks_f32(NC, N) : efield_chunks(NC, N);
     CK(ctx->ef_scratch.ensure(sizeof(double) * 3 * ((size_t)ch2 * N + 1)));
     // in mixed precision the force-only field of zeta uses FP32 pair arithmetic
     auto efield = mixed ? launch_efield_f32 : launch_efield;
+    CK(cudaEventRecord(ctx->ev_fork, ctx->st));
+    CK(cudaStreamWaitEvent(ctx->st2, ctx->ev_fork, 0));
+    {
+      StageScope sc(ctx, ST_EFIELD, ctx->st2);
+      CK(efield(Launch{ctx->st2, &ctx->launches}, NC, ctx->zeta.as<double>(),
+                ctx->ccav.as<double>(), N, ctx->csph.as<double>(), ctx->ef2.as<double>(),
+                ctx->ef_scratch.as<double>(), ch2, nullptr));
+    }
+    CK(cudaEventRecord(ctx->ev_join, ctx->st2));
+    CKI(forces_dev(ctx, dphi, dsig, ds, dfx, true));
+    // solute field at the cavity (from the mkrhs pass) times zeta
+    // (main.f90:241-253)
     {
       StageScope sc(ctx, ST_CONTRACT);
       CK(launch_zeta_efld_contract(ctx->L(), ctx->geo(), ctx->zeta.as<double>(),
                                    ctx->ef1.as<double>(), dfx));
     }
-    // field of zeta at the nuclei times the charges (main.f90:259-265)
-    {
-      StageScope sc(ctx, ST_EFIELD);
-      CK(efield(ctx->L(), NC, ctx->zeta.as<double>(), ctx->ccav.as<double>(), N,
-                ctx->csph.as<double>(), ctx->ef2.as<double>(), ctx->ef_scratch.as<double>(),
-                ch2, nullptr));
-    }
+    // the field of zeta at the nuclei times the charges, after the join
+    CK(cudaStreamWaitEvent(ctx->st, ctx->ev_join, 0));
     {
       StageScope sc(ctx, ST_CONTRACT);
       CK(launch_charge_efld_contract(ctx->L(), N, dq, ctx->ef2.as<double>(), dfx));
     }
     CKI(sync(ctx));
-    inf->t_efld = now_s() - t5;
+    const double t5 = now_s();
+    inf->t_forces = t5 - t4;  // forces and both field contractions, overlapped
+    inf->t_efld = 0.0;
   }
   CKI(finish_out(ctx, sigma, dsig, nv));
   if (ctx->prm.igrad) {

@@ -88,7 +88,9 @@ typedef struct {
 /* Report of the fused energy+forces flow. */
 typedef struct {
   ddc_solve_info direct, adjoint;
-  double t_init, t_mkrhs, t_direct, t_adjoint, t_forces, t_efld; /* seconds */
+  /* seconds; in ddc_energy_forces t_forces covers forces_dd and both field
+   * contractions (run side by side on two streams) and t_efld is 0 */
+  double t_init, t_mkrhs, t_direct, t_adjoint, t_forces, t_efld;
   int nsph, ncav, nylm, ngrid;
   long long ntriples;  /* (sphere, point, neighbour) triples with t < 1 */
   int npairs;          /* neighbour pairs in the CSR list */
