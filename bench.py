@@ -507,7 +507,8 @@ def run_ours(args):
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+f64 (FP32 operator inside FP64 refinement)",
             "data": "synthetic (seeded globule, PCG64)",
             "config": _config_json(c, world, {"precision": "mixed (FP32 operator, FP64 "
                                                             "refinement/DIIS/energy/forces)"}),
