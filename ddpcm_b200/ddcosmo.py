@@ -121,6 +121,20 @@ _SIGS = {
 }
 
 
+def stage_mask(L, names=None):
+    """Bit mask of ddc_set_timed_stages for the named stages (None: all);
+    an unknown name raises ValueError."""
+    if names is None:
+        return 0xFFFFFFFF
+    idx = {L.ddc_stage_name(k).decode(): k for k in range(L.ddc_stage_count())}
+    mask = 0
+    for n in names:
+        if n not in idx:
+            raise ValueError(f"unknown stage {n!r}; stages: {sorted(idx)}")
+        mask |= 1 << idx[n]
+    return mask
+
+
 def load_library(path=None):
     """Load libddcosmo_gpu.so (building it first when the sources changed and
     nvcc is present).  Raises DDCosmoError when the library is missing."""
@@ -248,14 +262,7 @@ class DDCosmo:
 
     def set_timed_stages(self, names=None):
         """Time only the named stages (None: every stage)."""
-        if names is None:
-            mask = 0xFFFFFFFF
-        else:
-            idx = {self.L.ddc_stage_name(k).decode(): k for k in range(self.L.ddc_stage_count())}
-            mask = 0
-            for n in names:
-                mask |= 1 << idx[n]
-        self._check(self.L.ddc_set_timed_stages(self.h, mask))
+        self._check(self.L.ddc_set_timed_stages(self.h, stage_mask(self.L, names)))
 
     # ddinit (ddcosmo.f90:159): coordinates and radii in bohr
     def ddinit(self, x, y, z, rvdw):

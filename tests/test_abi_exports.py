@@ -27,6 +27,21 @@ def test_status_strings_and_defaults_without_gpu():
     assert L.ddc_stage_count() >= 10
 
 
+def test_stage_mask_without_gpu():
+    import pytest
+    from ddpcm_b200.ddcosmo import load_library, stage_mask
+    L = load_library()
+    names = [L.ddc_stage_name(k).decode() for k in range(L.ddc_stage_count())]
+    assert len(set(names)) == len(names) and "lx_lstarx" in names
+    assert stage_mask(L) == 0xFFFFFFFF
+    assert stage_mask(L, []) == 0
+    assert stage_mask(L, ["lx_lstarx"]) == 1 << names.index("lx_lstarx")
+    assert stage_mask(L, ["init", "efield"]) == (1 << names.index("init")) | (
+        1 << names.index("efield"))
+    with pytest.raises(ValueError):
+        stage_mask(L, ["no_such_stage"])
+
+
 def test_product_does_not_import_oracle():
     pkg = os.path.join(ROOT, "ddpcm_b200")
     for dirpath, _, files in os.walk(pkg):
