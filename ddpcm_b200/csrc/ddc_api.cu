@@ -1978,13 +1978,25 @@ int ddc_energy_forces(ddc_ctx* ctx, int n, const double* charge, const double* x
                 ctx->ef_scratch.as<double>(), ch2, nullptr));
     }
     CK(cudaEventRecord(ctx->ev_join, ctx->st2));
-    CKI(forces_dev(ctx, dphi, dsig, ds, dfx, true));
-    // solute field at the cavity (from the mkrhs pass) times zeta
-    // (main.f90:241-253)
-    {
+    // forces and the zeta contraction on the main stream; whatever happens
+    // there, the second stream is joined before this call returns, so no
+    // later call can reuse ef2 / ef_scratch while the field is still running
+    int frc = forces_dev(ctx, dphi, dsig, ds, dfx, true);
+    if (frc == DDC_OK) {
+      // solute field at the cavity (from the mkrhs pass) times zeta
+      // (main.f90:241-253)
       StageScope sc(ctx, ST_CONTRACT);
-      CK(launch_zeta_efld_contract(ctx->L(), ctx->geo(), ctx->zeta.as<double>(),
-                                   ctx->ef1.as<double>(), dfx));
+      cudaError_t e = launch_zeta_efld_contract(ctx->L(), ctx->geo(), ctx->zeta.as<double>(),
+                                                ctx->ef1.as<double>(), dfx);
+      if (e != cudaSuccess) {
+        cudaGetLastError();
+        frc = fail(ctx, DDC_ERR_CUDA,
+                   std::string("launch_zeta_efld_contract: ") + cudaGetErrorString(e));
+      }
+    }
+    if (frc != DDC_OK) {
+      cudaStreamSynchronize(ctx->st2);
+      return frc;
     }
     // the field of zeta at the nuclei times the charges, after the join
     CK(cudaStreamWaitEvent(ctx->st, ctx->ev_join, 0));

@@ -235,6 +235,8 @@ cudaError_t launch_efield(Launch L, int nsrc, const double* q, const double* csr
                           const double* ctrg, double* ef, double* scratch, int nchunk,
                           const int2* trange);
 int efield_chunks(int nsrc, int ntrg);
+// load k_efield / k_efield_reduce on the current device (one-time set-up)
+cudaError_t preload_efield();
 int efield_chunks_f32(int nsrc, int ntrg);
 // FP32 pair arithmetic, FP64 accumulation (mixed-precision force terms)
 cudaError_t launch_efield_f32(Launch L, int nsrc, const double* q, const double* csrc, int ntrg,

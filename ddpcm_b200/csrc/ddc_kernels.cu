@@ -1965,6 +1965,14 @@ cudaError_t launch_efield(Launch L, int nsrc, const double* q, const double* csr
   ++*L.launches;
   return cudaGetLastError();
 }
+// Loads the FP64 field kernels' code onto the current device now, rather than
+// at their first launch (CUDA loads modules lazily by default).
+cudaError_t preload_efield() {
+  cudaFuncAttributes a;
+  cudaError_t e = cudaFuncGetAttributes(&a, k_efield);
+  if (e != cudaSuccess) return e;
+  return cudaFuncGetAttributes(&a, k_efield_reduce);
+}
 
 // ---------------------------------------------------------------------------
 // forces (fdoka ddcosmo.f90:1436-1504, fdokb :1511-1607, fdoga :1614-1650)

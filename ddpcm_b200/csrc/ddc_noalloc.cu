@@ -9,11 +9,15 @@
 // the inputs and the output, and the per-chunk partial sums of the field
 // kernel live in a fixed array compiled into this library.
 //
-// The scratch array below is allocated once per GPU when the library is
-// loaded and stays resident until the process exits.  Its device address is
-// looked up with cudaGetSymbolAddress on the first call made for a device
-// (with that device current); that first call therefore also does this
-// one-time set-up.  All calls share the array: two calls whose kernels
+// The scratch array below is part of this library's device code.  CUDA loads
+// a library's device code lazily by default, so the array (with the field
+// kernels that use it) is put on a GPU by the first call made for that
+// device, and stays there until the process exits.  That first call also
+// looks up the array's device address with cudaGetSymbolAddress (with the
+// device current).  A caller whose memory pool will take the whole GPU
+// therefore makes one call with ntrg = 0 at start-up, before the pool claims
+// the memory and outside any stream capture: it does this one-time set-up
+// and nothing else.  All calls share the array: two calls whose kernels
 // overlap on the GPU (different streams, or different host threads on the
 // same device) race on it, so callers must order them.  Nothing in the
 // array has to start at zero: every partial that the reduction reads is
@@ -55,24 +59,36 @@ extern "C" int ddc_efld_noalloc(int device, int nsrc, const double* src, const d
   if (ntrg > 0 && (!ctrg || !ef)) return DDC_ERR_PARAM;
   if (nsrc > 0 && (!src || !csrc)) return DDC_ERR_PARAM;
   if (3LL * ntrg > kScratchDoubles) return DDC_ERR_CAPACITY;
-  if (ntrg == 0) return DDC_OK;
   int prev = -1;
   if (cudaGetDevice(&prev) != cudaSuccess) return DDC_ERR_CUDA;
   if (prev != device && cudaSetDevice(device) != cudaSuccess) return DDC_ERR_CUDA;
   double* scratch = nullptr;
   int rc = DDC_OK;
-  if (scratch_for(device, &scratch) != cudaSuccess) {
+  // one-time set-up first, so that a call with ntrg = 0 does it: the scratch
+  // address and the field kernels' code on this device
+  if (scratch_for(device, &scratch) != cudaSuccess || ddc::preload_efield() != cudaSuccess) {
     rc = DDC_ERR_CUDA;
   } else {
-    // as many source chunks as the fixed scratch holds, up to what fills the GPU
-    long long fit = kScratchDoubles / (3LL * ntrg);
-    int nchunk = ddc::efield_chunks(nsrc, ntrg);
-    if (nchunk > fit) nchunk = (int)fit;
-    long long launches = 0;
-    ddc::Launch L{static_cast<cudaStream_t>(stream), &launches};
-    if (ddc::launch_efield(L, nsrc, src, csrc, ntrg, ctrg, ef, scratch, nchunk, nullptr) !=
-        cudaSuccess)
-      rc = DDC_ERR_CUDA;
+    // a stream of another device would make the launch fail and leave a
+    // sticky error behind; reject it up front
+    int sdev = -1;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (cudaStreamGetDevice(st, &sdev) != cudaSuccess) {
+      cudaGetLastError();
+      rc = DDC_ERR_PARAM;
+    } else if (sdev != device) {
+      rc = DDC_ERR_PARAM;
+    } else if (ntrg > 0) {
+      // as many source chunks as the fixed scratch holds, up to what fills the GPU
+      long long fit = kScratchDoubles / (3LL * ntrg);
+      int nchunk = ddc::efield_chunks(nsrc, ntrg);
+      if (nchunk > fit) nchunk = (int)fit;
+      long long launches = 0;
+      ddc::Launch L{st, &launches};
+      if (ddc::launch_efield(L, nsrc, src, csrc, ntrg, ctrg, ef, scratch, nchunk, nullptr) !=
+          cudaSuccess)
+        rc = DDC_ERR_CUDA;
+    }
   }
   if (prev != device) cudaSetDevice(prev);
   return rc;

@@ -11,7 +11,7 @@ the published Lebedev-Laikov constants (Lebedev & Laikov, Doklady Math. 59,
 ``Call GEN_OH`` line together with the current ``A``/``B``/``V`` values and
 writes them as a C table of ``{code, a, b, v}`` records, one block per grid
 size.  The orbit expansion itself (the point order inside an orbit) is
-implemented in ``lebedev.cpp``.
+``expand_orbit`` in ``ddc_api.cu``.
 
 The decimal literals are copied digit-for-digit (``D`` exponent replaced by
 ``e``), so that ``strtod`` rounds them to exactly the same doubles as the

@@ -233,10 +233,15 @@ int ddc_fp32_peak(int device, double* gflops);
  * the call returns without waiting; ef is valid once that stream reaches it.
  * Scratch is a fixed 8 MiB array compiled into the library (held on every GPU
  * that loads it until exit): ntrg is limited to 349,525 targets, larger
- * problems return DDC_ERR_CAPACITY (use ddc_efld).  The first call on a device
- * also resolves the array's device address (one-time set-up, done with that
- * device current).  All calls share the array, so calls whose work overlaps
- * on the GPU race; order them on one stream. */
+ * problems return DDC_ERR_CAPACITY (use ddc_efld).  `stream` must belong to
+ * `device` (else DDC_ERR_PARAM).  The first call on a device does a one-time
+ * set-up: CUDA loads this library's device code (the array included) lazily,
+ * so that call may allocate module memory on the device, and it resolves the
+ * array's device address.  Callers whose pool will take the whole GPU make
+ * that first call with ntrg = 0 at start-up, before the pool claims the
+ * memory and outside any stream capture; it does the set-up and nothing
+ * else.  All calls share the array, so calls whose work overlaps on the GPU
+ * race; order them on one stream. */
 int ddc_efld_noalloc(int device, int nsrc, const double* src, const double* csrc, int ntrg,
                      const double* ctrg, double* ef, void* stream);
 

@@ -162,7 +162,9 @@ def parse_log(path, params, n):
 
 
 def main():
-    src = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/tests"
+    if len(sys.argv) != 2:
+        sys.exit("usage: python make_golden.py <reference tests/ directory>")
+    src = sys.argv[1]
     here = os.path.dirname(os.path.abspath(__file__))
     for mol in MOLS:
         params, atoms = read_deck(os.path.join(src, mol + ".txt"))
