@@ -253,6 +253,23 @@ def measure_batch(dev, stream):
         ms = e0.elapsed_time(e1)
     it = out["iters"]
     sizes = [len(m["q"]) for m in mols]
+    err = None
+    try:
+        gold = np.load(os.path.join(ROOT, "tests", "golden", "config3_oracle.npz"))
+        e_rel, f_abs = [], []
+        for j, k in enumerate(gold["index"]):
+            k = int(k)
+            ref_e = float(gold["esolv"][j])
+            ref_f = gold["fx"][gold["off"][j]:gold["off"][j + 1]]
+            e_rel.append(abs(out["esolv"][k] - ref_e) / abs(ref_e))
+            f_abs.append(float(np.abs(out["fx"][k] - ref_f).max()))
+        err = {"esolv_rel_max": max(e_rel), "forces_max_abs": max(f_abs),
+               "molecules_checked": len(e_rel),
+               "largest_checked": int(gold["nsph"].max()),
+               "against": "FP64 CPU oracle, 16 of the 256 molecules incl. the six largest "
+                          "(tests/golden/config3_oracle.npz)"}
+    except OSError:
+        pass
     return {"workload": f"{bc['count']} globules, N log-uniform [{bc['lo']}, {bc['hi']}] "
                         f"(total {sum(sizes)} spheres), lmax={bc['lmax']} ngrid={bc['ngrid']} "
                         f"eta={bc['eta']} tol=1e-{bc['iconv']}, energy+forces, FP64",
@@ -262,7 +279,7 @@ def measure_batch(dev, stream):
             "iterations_adjoint": {"min": int(it[:, 1].min()),
                                    "median": float(np.median(it[:, 1])),
                                    "max": int(it[:, 1].max())},
-            "host_arrays": True}
+            "error": err, "host_arrays": True}
 
 
 def measure_previous_frame(make, timed, d_in, keys, c, dev):
@@ -542,12 +559,15 @@ def run_ours(args):
 ORACLE_ITERS = None  # filled from a measured run when available
 
 
-def cpu_sample(c, mol, iters, frac=64):
+def cpu_sample(c, mol, iters, frac=64, diis_iters=32):
     """Time the oracle (OpenMP, all host threads) on a bounded sample of one
     energy+force solve and scale it to one solve.  Sample: the full ddinit;
-    one lx and one lstarx application, scaled by the solve's iteration
+    one lx and one lstarx application and `diis_iters` iterations of the
+    reference's serial Jacobi/DIIS vector work (history copies, Gram row,
+    Gauss-Jordan, extrapolation, H-norm), each scaled by the solve's iteration
     counts; mkrhs on every frac-th cavity point; forces_dd on 1/frac of the
-    spheres; both efld calls on 1/frac of their targets."""
+    spheres in eight ranges spread over the molecule; both efld calls on
+    1/frac of their targets."""
     from oracle import oracle as O
     t = {}
     nthreads = O.num_threads()
@@ -569,36 +589,67 @@ def cpu_sample(c, mol, iters, frac=64):
     t0 = time.perf_counter()
     d.lstarx(x)
     t["lstarx"] = time.perf_counter() - t0
+    t["diis_per_iter"] = d.diis_sample(diis_iters) / diis_iters
     phi = rng.standard_normal(NC) * 1e-2
-    n1 = max(1, N // frac)
+    # the per-call set-up (xi and the expanded phi over the whole molecule)
+    # is timed alone and counted once; the per-sphere work is scaled
+    nr = 8 if N >= 8 * frac else 1
+    width = max(1, N // (frac * nr))
+    ranges = [((k * N) // nr, min(N, (k * N) // nr + width)) for k in range(nr)]
+    done = sum(b - a for a, b in ranges)
     t0 = time.perf_counter()
-    d.forces_dd_range(phi, x, x, 0, n1)
-    t["forces"] = (time.perf_counter() - t0) * N / n1
+    d.forces_dd_ranges(phi, x, x, [(0, 0)])
+    t_setup = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    d.forces_dd_ranges(phi, x, x, ranges)
+    t_rg = time.perf_counter() - t0
+    t["forces"] = t_setup + max(t_rg - t_setup, 0.0) * N / done
     csph = d.get("csph")
     t0 = time.perf_counter()
     O.efld(mol["q"], csph, sub)
     t["efld1"] = (time.perf_counter() - t0) * NC / max(len(sub), 1)
     zeta = rng.standard_normal(NC) * 1e-4
+    n1 = max(1, N // frac)
     t0 = time.perf_counter()
     O.efld(zeta, ccav, csph[:n1])
     t["efld2"] = (time.perf_counter() - t0) * N / n1
-    total = (t["init"] + t["mkrhs"] + iters[0] * t["lx"] + iters[1] * t["lstarx"] + t["forces"]
-             + t["efld1"] + t["efld2"])
+    total = (t["init"] + t["mkrhs"] + iters[0] * t["lx"] + iters[1] * t["lstarx"]
+             + (iters[0] + iters[1]) * t["diis_per_iter"] + t["forces"] + t["efld1"]
+             + t["efld2"])
     return total, t, nthreads
+
+
+def cpu_model_check():
+    """The sampling model against a full oracle run on the same host: the
+    600-sphere globule (lmax 8, 302 points) solved in full (energy, adjoint,
+    forces), and the model's estimate from a sample of it."""
+    from ddpcm_b200 import molecules as M
+    from oracle import oracle as O
+    c = M.CONFIGS[1]
+    mol = M.to_bohr(M.config_molecule(1))
+    t0 = time.perf_counter()
+    r = O.energy_forces(mol, c["lmax"], c["ngrid"], c["iconv"], c["eps"], c["eta"])
+    full = time.perf_counter() - t0
+    model, _, _ = cpu_sample(c, mol, r["iters"], frac=8, diis_iters=16)
+    return {"workload": "globule N=600 lmax=8 ngrid=302 (full oracle energy+forces)",
+            "full_s": full, "model_s": model, "model_error": model / full - 1.0}
 
 
 def cpu_baseline(variant, budget_s=None):
     c, mol = _workload_config()
-    iters = tuple(variant["iterations"])
+    iters = _reference_iters() if WORKLOAD == 2 else tuple(variant["iterations"])
     t0 = time.perf_counter()
     total, parts, nth = cpu_sample(c, mol, iters)
+    check = cpu_model_check()
     spent = time.perf_counter() - t0
     return {"value": 1.0 / total, "unit": UNIT, "cores": nth, "kind": "port",
             "sample": (f"oracle (C restatement of the reference, OpenMP {nth} threads): full "
-                       f"ddinit + one lx + one lstarx scaled by {iters[0]}/{iters[1]} "
-                       f"iterations + 1/64 of mkrhs, forces_dd and both efld, scaled to one "
-                       f"solve; {spent:.1f} s of CPU wall time"),
-            "seconds_per_solve": total, "parts_s": {k: round(v, 4) for k, v in parts.items()}}
+                       f"ddinit + one lx + one lstarx + 32 iterations of the serial Jacobi/DIIS "
+                       f"vector work, scaled by the reference's {iters[0]}/{iters[1]} "
+                       f"iterations, + 1/64 of mkrhs, forces_dd (8 spread ranges) and both "
+                       f"efld, scaled to one solve; {spent:.1f} s of CPU wall time"),
+            "seconds_per_solve": total, "parts_s": {k: round(v, 4) for k, v in parts.items()},
+            "model_check": check, "model_error": check["model_error"]}
 
 
 def run_reference(args):
@@ -624,10 +675,12 @@ def run_reference(args):
             "data": "synthetic (seeded globule, PCG64)", "impl": "reference",
             "config": _config_json(c, 1),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": nth, "kind": "port",
-                             "sample": (f"per step: full ddinit + one lx + one lstarx scaled by "
-                                        f"{iters[0]}/{iters[1]} iterations + 1/64 of mkrhs, "
-                                        f"forces_dd and both efld, scaled to one solve; "
-                                        f"{statistics.mean(spent):.1f} s CPU wall per step")},
+                             "sample": (f"per step: full ddinit + one lx + one lstarx + 32 "
+                                        f"iterations of the serial Jacobi/DIIS vector work, "
+                                        f"scaled by {iters[0]}/{iters[1]} iterations, + 1/64 of "
+                                        f"mkrhs, forces_dd (8 spread ranges) and both efld, "
+                                        f"scaled to one solve; {statistics.mean(spent):.1f} s "
+                                        f"CPU wall per step")},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)

@@ -1,8 +1,10 @@
 """Build the sm_100a shared library ``ddpcm_b200/lib/libddcosmo_gpu.so``.
 
 The library is compiled in-tree with nvcc for ``compute_100a``/``sm_100a``
-(B200).  cudart is linked statically; the one dynamic CUDA library is
-cuBLAS (the operators' plain GEMMs), found through an rpath to the toolkit.
+(B200).  cudart is linked statically and no other CUDA library is linked:
+every kernel, the dense contractions included, is this library's own (the
+driver's TMA descriptor encoder is reached through cudart's entry-point
+query).
 Host code is compiled with ``-ffp-contract=off`` so that the Lebedev grid and
 the normalisation tables follow the written operation order.
 """
@@ -15,7 +17,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libddcosmo_gpu.so")
-SOURCES = ["ddc_api.cu", "ddc_kernels.cu", "ddc_noalloc.cu"]
+SOURCES = ["ddc_api.cu", "ddc_kernels.cu", "ddc_tc.cu", "ddc_noalloc.cu"]
 HEADERS = ["ddc_internal.h", "lebedev_orbits.inc"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -50,8 +52,7 @@ def build(force=False, verbose=False):
     cmd = [nvcc(), "-O3", "-std=c++17", *ARCH, "-lineinfo", "-shared",
            "-Xcompiler", "-fPIC,-ffp-contract=off", "-Xptxas", "-warn-spills" if verbose else "-O3",
            "-I", os.path.join(HERE, "..", "include"),
-           "-o", LIB + ".tmp", *[os.path.join(CSRC, s) for s in SOURCES],
-           "-L", cuda_libdir(), "-lcublas", "-Xlinker", "-rpath," + cuda_libdir()]
+           "-o", LIB + ".tmp", *[os.path.join(CSRC, s) for s in SOURCES]]
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True)

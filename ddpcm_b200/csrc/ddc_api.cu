@@ -10,7 +10,6 @@
 #include <string>
 #include <vector>
 
-#include <cublas_v2.h>
 
 #include "ddc_internal.h"
 #include "lebedev_orbits.inc"
@@ -22,29 +21,6 @@ namespace {
 // ---------------------------------------------------------------------------
 // device buffer
 // ---------------------------------------------------------------------------
-struct DBuf {
-  void* p = nullptr;
-  size_t bytes = 0;
-  ~DBuf() { release(); }
-  void release() {
-    if (p) cudaFree(p);
-    p = nullptr;
-    bytes = 0;
-  }
-  cudaError_t ensure(size_t b) {
-    if (b <= bytes && p) return cudaSuccess;
-    release();
-    if (b == 0) b = 16;
-    cudaError_t e = cudaMalloc(&p, b);
-    if (e == cudaSuccess) bytes = b;
-    return e;
-  }
-  template <class T>
-  T* as() const {
-    return reinterpret_cast<T*>(p);
-  }
-};
-
 double now_s() {
   return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch())
       .count();
@@ -175,12 +151,13 @@ struct ddc_ctx {
   // second solve set (direct and adjoint solved together) and the fused
   // operator's per-triple lx values
   DBuf y2, xn2, hist_x2, hist_e2, rres2, dres2, eres2, tval;
-  // cuBLAS for the two plain GEMMs of every operator application (the
-  // projection onto the harmonics and the harmonics-to-grid expansion), on
-  // the context's stream with its own workspace; gemm_f is the FP32 operand
-  // or result of the mixed path's GEMMs (nylm x nsph)
-  cublasHandle_t blas = nullptr;
-  DBuf blas_ws, gemm_f;
+  // the two dense contractions of every operator application (projection
+  // onto the harmonics, expansion to the grid): basisT[Y][G] is the basis
+  // transposed for the FP64 expansion; tc plans the tensor-core kernels of
+  // the mixed path, whose FP32 grid field pot_f has rows ldp_f floats apart
+  DBuf basisT;
+  TcPlan tc;
+  int ldp_f = 0;
   // pinned landing buffer of the small device-to-host reads (reduced sums)
   double* hred = nullptr;
   // second stream of the force tail: the field of zeta at the nuclei runs
@@ -248,14 +225,6 @@ int fail(ddc_ctx* c, int code, const std::string& msg) {
     }                                                                                     \
   } while (0)
 
-#define CKB(expr)                                                                       \
-  do {                                                                                  \
-    cublasStatus_t _s = (expr);                                                         \
-    if (_s != CUBLAS_STATUS_SUCCESS)                                                    \
-      return fail(ctx, _s == CUBLAS_STATUS_ALLOC_FAILED ? DDC_ERR_NOMEM : DDC_ERR_CUDA, \
-                  std::string(#expr) + ": cuBLAS status " + std::to_string((int)_s));   \
-  } while (0)
-
 #define CKI(expr)                  \
   do {                             \
     int _r = (expr);               \
@@ -314,6 +283,12 @@ void resolve_timers(ddc_ctx* ctx) {
 
 int sync(ddc_ctx* ctx) {
   CK(cudaStreamSynchronize(ctx->st));
+  if (ctx->tc.err_h && *ctx->tc.err_h) {
+    const int code = *ctx->tc.err_h;
+    *ctx->tc.err_h = 0;
+    return fail(ctx, DDC_ERR_CUDA,
+                "tensor-core contraction gave up waiting (code " + std::to_string(code) + ")");
+  }
   if (ctx->ev_pending.size() >= 1024) resolve_timers(ctx);
   return DDC_OK;
 }
@@ -590,29 +565,37 @@ int do_init(ddc_ctx* ctx, int n, const std::vector<double4>* hsph, const double4
   CK(ctx->hist_e.ensure(sizeof(double) * std::max(nv, (size_t)1) * nd));
   CK(ctx->partials.ensure(sizeof(double) * reduce_blocks() * (kMaxHist + 1)));
   CK(ctx->red.ensure(sizeof(double) * (kMaxHist + 1)));
-  // cuBLAS handle, created once per context and outside any graph capture;
-  // its workspace is a context buffer, so a captured GEMM allocates nothing
-  if (!ctx->blas) CKB(cublasCreate(&ctx->blas));
+  // the basis transposed to [Y][G] for the FP64 expansion xi = basis^T s
+  CK(ctx->basisT.ensure(sizeof(double) * G * NY));
+  CK(launch_transpose(L, G, NY, ctx->basis.as<double>(), ctx->basisT.as<double>()));
   if (!ctx->hred) CK(cudaMallocHost(&ctx->hred, sizeof(double) * (kMaxHist + 1)));
   if (ctx->prm.igrad && !ctx->st2) {
     CK(cudaStreamCreateWithFlags(&ctx->st2, cudaStreamNonBlocking));
     CK(cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming));
   }
-  CK(ctx->blas_ws.ensure((size_t)32 << 20));
   if (ctx->prm.precision == DDC_PREC_MIXED) {
-    CK(ctx->gemm_f.ensure(sizeof(float) * std::max(nv, (size_t)1)));
     std::vector<float> gf(4 * (size_t)G);
     for (size_t k = 0; k < gf.size(); k++) gf[k] = (float)ctx->h_grid[k];
     CK(ctx->gridf.ensure(sizeof(float) * 4 * G));
     CK(cudaMemcpyAsync(ctx->gridf.p, gf.data(), sizeof(float) * 4 * G, cudaMemcpyHostToDevice,
                        ctx->st));
-    CK(ctx->basis_f.ensure(sizeof(float) * G * NY));
-    CK(ctx->bw_f.ensure(sizeof(float) * G * NY));
-    CK(launch_to_float(L, (long long)G * NY, ctx->basis.as<double>(), ctx->basis_f.as<float>()));
-    CK(launch_to_float(L, (long long)G * NY, ctx->bw.as<double>(), ctx->bw_f.as<float>()));
-    CK(ctx->pot_f.ensure(sizeof(float) * std::max(NP, 1LL)));
+    // the two contractions run on the tensor cores (split TF32) up to 128
+    // harmonics (lmax 10), else as FP32 SIMT GEMMs on FP32 copies of the basis
+    const bool tc = tc_supported(NY);
+    ctx->ldp_f = tc ? (G + 3) / 4 * 4 : G;
+    CK(ctx->pot_f.ensure(sizeof(float) * std::max<long long>((long long)N * ctx->ldp_f, 1LL)));
     CK(ctx->xi_f.ensure(sizeof(float) * std::max(NP, 1LL)));
+    if (tc) {
+      CK(tc_plan(L, ctx->tc, ctx->basis.as<double>(), ctx->bw.as<double>(), N, NY, G,
+                 ctx->pot_f.as<float>(), ctx->ldp_f));
+    } else {
+      ctx->tc.on = false;
+      CK(ctx->basis_f.ensure(sizeof(float) * G * NY));
+      CK(ctx->bw_f.ensure(sizeof(float) * G * NY));
+      CK(launch_to_float(L, (long long)G * NY, ctx->basis.as<double>(), ctx->basis_f.as<float>()));
+      CK(launch_to_float(L, (long long)G * NY, ctx->bw.as<double>(), ctx->bw_f.as<float>()));
+    }
     for (DBuf* b : {&ctx->rres, &ctx->dres, &ctx->eres})
       CK(b->ensure(sizeof(double) * std::max(nv, (size_t)1)));
     // the FP32 fused pass reads each triple's static geometry instead of
@@ -649,49 +632,37 @@ int do_init(ddc_ctx* ctx, int n, const std::vector<double4>* hsph, const double4
 }
 
 // ---------------------------------------------------------------------------
-// the operators' two GEMMs (cuBLAS, column-major, on the context's stream)
+// the operators' two dense contractions, on the context's stream
 // ---------------------------------------------------------------------------
-int blas_bind(ddc_ctx* ctx) {
-  CKB(cublasSetStream(ctx->blas, ctx->st));
-  // setting the stream restores the default workspace: point it back at ours
-  CKB(cublasSetWorkspace(ctx->blas, ctx->blas_ws.p, ctx->blas_ws.bytes));
-  return DDC_OK;
-}
 // y(lm,i) = alpha sum_n bw(lm,n) pot(n,i): intrhs over every sphere
 // (matvec.f90:131-135, bw = w_n Y_lm(s_n))
 int gemm_proj(ddc_ctx* ctx, double alpha, const double* pot, double* y) {
-  CKI(blas_bind(ctx));
-  const double beta = 0.0;
-  CKB(cublasDgemm(ctx->blas, CUBLAS_OP_N, CUBLAS_OP_N, ctx->nylm, ctx->nsph, ctx->ngrid, &alpha,
-                  ctx->bw.as<double>(), ctx->nylm, pot, ctx->ngrid, &beta, y, ctx->nylm));
+  CK(launch_dgemm_nn(ctx->L(), ctx->nylm, ctx->nsph, ctx->ngrid, alpha, ctx->bw.as<double>(),
+                     ctx->nylm, pot, ctx->ngrid, y, ctx->nylm));
   return DDC_OK;
 }
-// FP32 projection of an FP32 field, widened into the FP64 vector y
+// projection of the FP32 field (rows ldp_f apart) into the FP64 vector y
 int gemm_proj_f32(ddc_ctx* ctx, float alpha, const float* pot, double* y) {
-  CKI(blas_bind(ctx));
-  const float beta = 0.f;
-  float* yf = ctx->gemm_f.as<float>();
-  CKB(cublasSgemm(ctx->blas, CUBLAS_OP_N, CUBLAS_OP_N, ctx->nylm, ctx->nsph, ctx->ngrid, &alpha,
-                  ctx->bw_f.as<float>(), ctx->nylm, pot, ctx->ngrid, &beta, yf, ctx->nylm));
-  CK(launch_to_double(ctx->L(), (long long)ctx->nylm * ctx->nsph, yf, y));
+  if (ctx->tc.on)
+    CK(launch_proj_tc(ctx->L(), ctx->tc, alpha, y));
+  else
+    CK(launch_proj_f32_simt(ctx->L(), ctx->nylm, ctx->nsph, ctx->ngrid, alpha,
+                            ctx->bw_f.as<float>(), pot, ctx->ldp_f, y));
   return DDC_OK;
 }
 // xi(n,i) = sum_lm basis(lm,n) s(lm,i)   (matvec.f90:189-204)
 int gemm_xi(ddc_ctx* ctx, const double* s, double* xig) {
-  CKI(blas_bind(ctx));
-  const double one = 1.0, zero = 0.0;
-  CKB(cublasDgemm(ctx->blas, CUBLAS_OP_T, CUBLAS_OP_N, ctx->ngrid, ctx->nsph, ctx->nylm, &one,
-                  ctx->basis.as<double>(), ctx->nylm, s, ctx->nylm, &zero, xig, ctx->ngrid));
+  CK(launch_dgemm_nn(ctx->L(), ctx->ngrid, ctx->nsph, ctx->nylm, 1.0, ctx->basisT.as<double>(),
+                     ctx->ngrid, s, ctx->nylm, xig, ctx->ngrid));
   return DDC_OK;
 }
-// FP32 xi of the FP64 vector s (narrowed first)
+// FP32 xi of the FP64 vector s
 int gemm_xi_f32(ddc_ctx* ctx, const double* s, float* xig) {
-  float* sf = ctx->gemm_f.as<float>();
-  CK(launch_to_float(ctx->L(), (long long)ctx->nylm * ctx->nsph, s, sf));
-  CKI(blas_bind(ctx));
-  const float one = 1.f, zero = 0.f;
-  CKB(cublasSgemm(ctx->blas, CUBLAS_OP_T, CUBLAS_OP_N, ctx->ngrid, ctx->nsph, ctx->nylm, &one,
-                  ctx->basis_f.as<float>(), ctx->nylm, sf, ctx->nylm, &zero, xig, ctx->ngrid));
+  if (ctx->tc.on)
+    CK(launch_xi_tc(ctx->L(), ctx->tc, s, xig));
+  else
+    CK(launch_xi_f32_simt(ctx->L(), ctx->nylm, ctx->nsph, ctx->ngrid, ctx->basis_f.as<float>(),
+                          s, xig));
   return DDC_OK;
 }
 
@@ -724,7 +695,8 @@ int op_lstarx(ddc_ctx* ctx, const double* x, double* y) {
 int op_lx_f32(ddc_ctx* ctx, const double* x, double* y) {
   {
     StageScope sc(ctx, ST_LX_POT);
-    CK(launch_lx_pot_f32(ctx->L(), ctx->tb, ctx->geo(), x, ctx->pot_f.as<float>(), ctx->xk.p));
+    CK(launch_lx_pot_f32(ctx->L(), ctx->tb, ctx->geo(), x, ctx->pot_f.as<float>(), ctx->xk.p,
+                         ctx->ldp_f));
   }
   StageScope sc(ctx, ST_PROJ);
   return gemm_proj_f32(ctx, -1.f, ctx->pot_f.as<float>(), y);
@@ -768,7 +740,8 @@ int op_pair_f32(ddc_ctx* ctx, const double* x, double* y, const double* s, doubl
   }
   {
     StageScope sc(ctx, ST_GATHER);
-    CK(launch_lx_gather_f32(ctx->L(), g, ctx->tval.as<float>(), ctx->pot_f.as<float>()));
+    CK(launch_lx_gather_f32(ctx->L(), g, ctx->tval.as<float>(), ctx->pot_f.as<float>(),
+                            ctx->ldp_f));
   }
   StageScope sc(ctx, ST_PROJ);
   return gemm_proj_f32(ctx, -1.f, ctx->pot_f.as<float>(), y);
@@ -1181,8 +1154,8 @@ int direct_rhs(ddc_ctx* ctx, const double* phi, double* rhs) {
   CK(ctx->gbuf.ensure(sizeof(double) * std::max<long long>((long long)ctx->nsph * ctx->ngrid, 1)));
   StageScope sc(ctx, ST_RHS);
   CK(launch_wghpot(ctx->L(), ctx->geo(), phi, ctx->gbuf.as<double>()));
-  CK(launch_dgemm(ctx->L(), false, ctx->nylm, ctx->nsph, ctx->ngrid, 1.0, ctx->bw.as<double>(),
-                  ctx->nylm, ctx->gbuf.as<double>(), ctx->ngrid, 0.0, rhs, ctx->nylm));
+  CK(launch_dgemm_nn(ctx->L(), ctx->nylm, ctx->nsph, ctx->ngrid, 1.0, ctx->bw.as<double>(),
+                     ctx->nylm, ctx->gbuf.as<double>(), ctx->ngrid, rhs, ctx->nylm));
   return DDC_OK;
 }
 
@@ -1496,7 +1469,7 @@ int ddc_destroy(ddc_ctx* c) {
     cudaEventDestroy(pe.second.second);
   }
   for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
-  if (c->blas) cublasDestroy(c->blas);
+  tc_release(c->tc);
   if (c->hred) cudaFreeHost(c->hred);
   if (c->st2) cudaStreamSynchronize(c->st2);
   if (c->ev_fork) cudaEventDestroy(c->ev_fork);
@@ -1701,8 +1674,8 @@ int ddc_rhs(ddc_ctx* ctx, const double* phi, double* g) {
   CKI(out_ptr(ctx, g, (size_t)ctx->nsph * ctx->nylm, ctx->out1, &dg));
   CK(ctx->gbuf.ensure(sizeof(double) * std::max<long long>((long long)ctx->nsph * ctx->ngrid, 1)));
   CK(launch_wghpot(ctx->L(), ctx->geo(), dphi, ctx->gbuf.as<double>()));
-  CK(launch_dgemm(ctx->L(), false, ctx->nylm, ctx->nsph, ctx->ngrid, 1.0, ctx->bw.as<double>(),
-                  ctx->nylm, ctx->gbuf.as<double>(), ctx->ngrid, 0.0, dg, ctx->nylm));
+  CK(launch_dgemm_nn(ctx->L(), ctx->nylm, ctx->nsph, ctx->ngrid, 1.0, ctx->bw.as<double>(),
+                     ctx->nylm, ctx->gbuf.as<double>(), ctx->ngrid, dg, ctx->nylm));
   CKI(finish_out(ctx, g, dg, (size_t)ctx->nsph * ctx->nylm));
   return sync(ctx);
 }
@@ -1807,7 +1780,10 @@ int ddc_lx(ddc_ctx* ctx, const double* x, double* y) {
   CKI(stage_in(ctx, x, nv, ctx->in1, &dx));
   double* dy;
   CKI(out_ptr(ctx, y, nv, ctx->out1, &dy));
-  CKI(op_lx(ctx, dx, dy));
+  if (ctx->prm.precision == DDC_PREC_MIXED)
+    CKI(op_lx_f32(ctx, dx, dy));
+  else
+    CKI(op_lx(ctx, dx, dy));
   CKI(finish_out(ctx, y, dy, nv));
   return sync(ctx);
 }
@@ -1819,7 +1795,10 @@ int ddc_lstarx(ddc_ctx* ctx, const double* x, double* y) {
   CKI(stage_in(ctx, x, nv, ctx->in1, &dx));
   double* dy;
   CKI(out_ptr(ctx, y, nv, ctx->out1, &dy));
-  CKI(op_lstarx(ctx, dx, dy));
+  if (ctx->prm.precision == DDC_PREC_MIXED)
+    CKI(op_lstarx_f32(ctx, dx, dy));
+  else
+    CKI(op_lstarx(ctx, dx, dy));
   CKI(finish_out(ctx, y, dy, nv));
   return sync(ctx);
 }
@@ -1840,7 +1819,10 @@ int ddc_lx_lstarx(ddc_ctx* ctx, const double* x, double* y, const double* s, dou
     dz = ctx->in3.as<double>();
   }
   if (!dz) return fail(ctx, DDC_ERR_PARAM, "null output array");
-  CKI(op_pair(ctx, dx, dy, ds, dz));
+  if (ctx->prm.precision == DDC_PREC_MIXED)
+    CKI(op_pair_f32(ctx, dx, dy, ds, dz));
+  else
+    CKI(op_pair(ctx, dx, dy, ds, dz));
   CKI(finish_out(ctx, y, dy, nv));
   CKI(finish_out(ctx, z, dz, nv));
   return sync(ctx);
@@ -2105,8 +2087,8 @@ int ddc_batch_energy_forces(ddc_ctx* ctx, int nmol, const int* off, const double
     {
       StageScope sc(ctx, ST_RHS);
       CK(launch_wghpot(ctx->L(), ctx->geo(), dphi, ctx->gbuf.as<double>()));
-      CK(launch_dgemm(ctx->L(), false, ctx->nylm, N, ctx->ngrid, 1.0, ctx->bw.as<double>(),
-                      ctx->nylm, ctx->gbuf.as<double>(), ctx->ngrid, 0.0, rhs, ctx->nylm));
+      CK(launch_dgemm_nn(ctx->L(), ctx->nylm, N, ctx->ngrid, 1.0, ctx->bw.as<double>(),
+                         ctx->nylm, ctx->gbuf.as<double>(), ctx->ngrid, rhs, ctx->nylm));
     }
     CK(launch_guess(ctx->L(), ctx->tb, n, rhs, dsig, ctx->prm.guess == DDC_GUESS_ZERO ? 1 : 0));
     std::vector<int> it(nmol), ita(nmol);

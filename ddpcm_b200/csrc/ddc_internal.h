@@ -17,6 +17,7 @@
 //   cavoff[N+1], cavidx[N][G], cavpt[ncav], ccav[ncav][3]
 // Vectors X(nylm,nsph) live as X[i*nylm + lm], like the reference.
 #pragma once
+#include <cuda.h>  // CUtensorMap (type only; the driver is reached through cudart)
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -28,6 +29,46 @@
 #define DDC_NLM_CAP ((DDC_MAX_LMAX + 1) * (DDC_MAX_LMAX + 2) / 2)
 
 namespace ddc {
+
+// Device buffer owned by a context (freed with it).
+struct DBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  ~DBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  cudaError_t ensure(size_t b) {
+    if (b <= bytes && p) return cudaSuccess;
+    release();
+    if (b == 0) b = 16;
+    cudaError_t e = cudaMalloc(&p, b);
+    if (e == cudaSuccess) bytes = b;
+    return e;
+  }
+  template <class T>
+  T* as() const {
+    return reinterpret_cast<T*>(p);
+  }
+};
+
+// Plan of the tensor-core contractions of the mixed-precision operators
+// (ddc_tc.cu): tile widths, pipeline depths, the split images of the static
+// operands, the TMA descriptor of the FP32 grid field and an error flag in
+// mapped host memory that a kernel sets when one of its bounded waits runs out.
+struct TcPlan {
+  bool on = false;
+  int nsph = 0, nylm = 0, ngrid = 0;
+  int kc_proj = 0, bn_proj = 0, ns_proj = 0, smem_proj = 0;
+  int mt_xi = 0, kc_xi = 0, bn_xi = 0, ns_xi = 0, smem_xi = 0;
+  DBuf img_proj, img_xi;
+  alignas(64) CUtensorMap tm_pot;
+  float* pot_f = nullptr;
+  int* err_h = nullptr;
+  int* err_d = nullptr;
+};
 
 // Constants of the spherical-harmonic recurrences, indexed by (l, m >= 0)
 // packed as l*(l+1)/2 + m.  Passed by value to the kernels (parameter space
@@ -166,7 +207,7 @@ cudaError_t launch_lstarx_acc(Launch L, const YlmTables& tb, const DevGeo& g, co
                               double* y);
 // FP32 operator variants (mixed precision): pot/xi in FP32, y in FP64
 cudaError_t launch_lx_pot_f32(Launch L, const YlmTables& tb, const DevGeo& g, const double* X,
-                              float* pot, void* xk);
+                              float* pot, void* xk, int ldp);
 // fused L / L*: val (one lx value per triple, gather-list order) and y = L* rows
 cudaError_t launch_lxs(Launch L, const YlmTables& tb, const DevGeo& g, const double* X,
                        const double* xi, void* xk, double* val, double* y);
@@ -177,7 +218,10 @@ cudaError_t launch_lxs_geo_f64(Launch L, const YlmTables& tb, const DevGeo& g, d
 cudaError_t launch_lxs_f32(Launch L, const YlmTables& tb, const DevGeo& g, const double* X,
                            const float* xi, void* xk, float* val, double* y);
 cudaError_t launch_lx_gather(Launch L, const DevGeo& g, const double* val, double* pot);
-cudaError_t launch_lx_gather_f32(Launch L, const DevGeo& g, const float* val, float* pot);
+// FP32 field rows are ldp >= ngrid floats apart (the tensor-core projection
+// reads them with TMA, which wants 16-byte row strides)
+cudaError_t launch_lx_gather_f32(Launch L, const DevGeo& g, const float* val, float* pot,
+                                 int ldp);
 cudaError_t launch_lstarx_acc_f32(Launch L, const YlmTables& tb, const DevGeo& g,
                                   const float* xi, double* y);
 cudaError_t launch_to_float(Launch L, long long n, const double* x, float* y);
@@ -191,11 +235,31 @@ cudaError_t launch_axpy(Launch L, long long n, double a, const double* x, double
 cudaError_t launch_dgemm(Launch L, bool transA, int M, int N, int K, double alpha,
                          const double* A, int lda, const double* B, int ldb, double beta,
                          double* C, int ldc);
+// dst[c*rows + r] = src[r*cols + c] (FP64)
+cudaError_t launch_transpose(Launch L, int rows, int cols, const double* src, double* dst);
+// C[n*ldc + m] = alpha * sum_k A[k*lda + m] B[n*ldb + k] (FP64, pipelined)
+cudaError_t launch_dgemm_nn(Launch L, int M, int N, int K, double alpha, const double* A,
+                            int lda, const double* B, int ldb, double* C, int ldc);
+// FP32 SIMT projection / expansion (mixed path, more than 128 harmonics)
+cudaError_t launch_proj_f32_simt(Launch L, int nylm, int nsph, int ngrid, float alpha,
+                                 const float* bw_f, const float* pot, int ldp, double* y);
+cudaError_t launch_xi_f32_simt(Launch L, int nylm, int nsph, int ngrid, const float* basis_f,
+                               const double* s, float* xi);
 cudaError_t launch_wghpot(Launch L, const DevGeo& g, const double* phi, double* gbuf);
 cudaError_t launch_ldm1x(Launch L, const YlmTables& tb, long long n, const double* x, double* y);
 cudaError_t launch_scale(Launch L, long long n, double a, const double* x, double* y);
 cudaError_t launch_guess(Launch L, const YlmTables& tb, long long n, const double* rhs,
                          double* x, int mode);
+
+// tensor-core contractions of the mixed-precision operators (ddc_tc.cu):
+// projection y = alpha * bw pot (FP64 out) and expansion xi = basis^T s (FP32
+// out), split-TF32 on tcgen05 for nylm <= 128
+bool tc_supported(int nylm);
+cudaError_t tc_plan(Launch L, TcPlan& p, const double* basis, const double* bw, int nsph,
+                    int nylm, int ngrid, float* pot_f, int ldp);
+cudaError_t launch_proj_tc(Launch L, const TcPlan& p, double alpha, double* y);
+cudaError_t launch_xi_tc(Launch L, const TcPlan& p, const double* s, float* xi);
+void tc_release(TcPlan& p);
 
 // solver
 // xnew = facl*(rhs - y); e = xnew - x; partial dots e.h_k (k < hist.n) and e.e.

@@ -635,7 +635,7 @@ __device__ __forceinline__ Rl ylm_dot2(const YlmTables& tb, Rl sx, Rl sy, Rl sz,
 template <int LMAX, bool CHI, class Rl>
 __global__ void __launch_bounds__(128) k_lx2(const YlmTables tb, const DevGeo g,
                                              const typename RT<Rl>::V2* __restrict__ XK,
-                                             Rl* pot) {
+                                             Rl* pot, int ldp) {
   typedef typename RT<Rl>::V2 V2;
   constexpr int NLM = (LMAX + 1) * (LMAX + 2) / 2;
   constexpr int NW = 4;
@@ -712,7 +712,7 @@ __global__ void __launch_bounds__(128) k_lx2(const YlmTables tb, const DevGeo g,
     Rl sum = acc[n];
 #pragma unroll
     for (int ww = 1; ww < NW; ++ww) sum += acc[ww * G + n];
-    pot[(size_t)i * G + n] = sum;
+    pot[(size_t)i * ldp + n] = sum;
   }
 }
 
@@ -755,7 +755,7 @@ cudaError_t launch_lx_pot(Launch L, const YlmTables& tb, const DevGeo& g, const 
     auto kfn = chi_only ? k_lx2<LV, true, double> : k_lx2<LV, false, double>;                 \
     if ((e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm))) \
       return e;                                                                               \
-    kfn<<<g.nsph, 128, sm, L.st>>>(tb, g, XK, pot);                                           \
+    kfn<<<g.nsph, 128, sm, L.st>>>(tb, g, XK, pot, g.ngrid);                                  \
     break;                                                                                    \
   }
   switch (tb.lmax) {
@@ -1156,6 +1156,135 @@ cudaError_t gemm2(Launch L, int M, int N, int K, Acc alpha, const TAin* A, int l
       <<<grid, (BM / TM) * (BN / TN), 0, L.st>>>(M, N, K, alpha, A, lda, B, ldb, C, ldc);
   ++*L.launches;
   return cudaGetLastError();
+}
+
+// Pipelined FP64 GEMM of the operators' projection and expansion (FP64
+// path): C[n*ldc + m] = alpha * sum_k A[k*lda + m] B[n*ldb + k].  128 x 64
+// tiles, 16-deep k slabs copied to shared memory with cp.async (the next
+// slab in flight while the current one is used), 256 threads each
+// accumulating an 8 x 4 block from vector shared-memory reads.
+namespace dgp {
+constexpr int BM = 128, BN = 64, BK = 16;
+}
+__device__ __forceinline__ void cp_async8(void* sdst, const void* gsrc, bool valid) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(sdst);
+  const int n = valid ? 8 : 0;  // 0: nothing read, the destination is zero-filled
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(gsrc), "r"(n)
+               : "memory");
+}
+__global__ void __launch_bounds__(256) k_dgemm_cp(int M, int N, int K, double alpha,
+                                                  const double* __restrict__ A, int lda,
+                                                  const double* __restrict__ B, int ldb,
+                                                  double* __restrict__ C, int ldc) {
+  using namespace dgp;
+  __shared__ __align__(16) double As[2][BK][BM];
+  __shared__ __align__(16) double Bs[2][BK][BN];
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+  auto load = [&](int buf, int k0) {
+#pragma unroll
+    for (int u = 0; u < BM * BK / 256; ++u) {
+      const int e = tid + u * 256;
+      const int mm = e & (BM - 1), kk = e / BM;
+      const int m = m0 + mm, k = k0 + kk;
+      const bool ok = m < M && k < K;
+      cp_async8(&As[buf][kk][mm], ok ? A + (size_t)k * lda + m : A, ok);
+    }
+#pragma unroll
+    for (int u = 0; u < BN * BK / 256; ++u) {
+      const int e = tid + u * 256;
+      const int kk = e & (BK - 1), nn = e / BK;
+      const int n = n0 + nn, k = k0 + kk;
+      const bool ok = n < N && k < K;
+      cp_async8(&Bs[buf][kk][nn], ok ? B + (size_t)n * ldb + k : B, ok);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  double acc[8][4];
+#pragma unroll
+  for (int r = 0; r < 8; ++r)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) acc[r][c] = 0.0;
+  const int nk = (K + BK - 1) / BK;
+  load(0, 0);
+  for (int t = 0; t < nk; ++t) {
+    const int buf = t & 1;
+    if (t + 1 < nk) {
+      load(buf ^ 1, (t + 1) * BK);
+      asm volatile("cp.async.wait_group 1;" ::: "memory");
+    } else {
+      asm volatile("cp.async.wait_group 0;" ::: "memory");
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < BK; ++kk) {
+      const double2* ap = reinterpret_cast<const double2*>(&As[buf][kk][ty * 8]);
+      const double2* bp = reinterpret_cast<const double2*>(&Bs[buf][kk][tx * 4]);
+      double a[8], b[4];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const double2 v = ap[r];
+        a[2 * r] = v.x;
+        a[2 * r + 1] = v.y;
+      }
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+        const double2 v = bp[c];
+        b[2 * c] = v.x;
+        b[2 * c + 1] = v.y;
+      }
+#pragma unroll
+      for (int r = 0; r < 8; ++r)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) acc[r][c] = fma(a[r], b[c], acc[r][c]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    const int n = n0 + tx * 4 + c;
+    if (n >= N) continue;
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      const int m = m0 + ty * 8 + r;
+      if (m < M) C[(size_t)n * ldc + m] = alpha * acc[r][c];
+    }
+  }
+}
+// dst[c*rows + r] = src[r*cols + c]
+__global__ void k_transpose(int rows, int cols, const double* __restrict__ src, double* dst) {
+  long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (long long)rows * cols) return;
+  const int r = (int)(e / cols), c = (int)(e - (long long)r * cols);
+  dst[(size_t)c * rows + r] = src[e];
+}
+cudaError_t launch_transpose(Launch L, int rows, int cols, const double* src, double* dst) {
+  const long long n = (long long)rows * cols;
+  if (n == 0) return cudaSuccess;
+  k_transpose<<<(unsigned)((n + 255) / 256), 256, 0, L.st>>>(rows, cols, src, dst);
+  ++*L.launches;
+  return cudaGetLastError();
+}
+cudaError_t launch_dgemm_nn(Launch L, int M, int N, int K, double alpha, const double* A,
+                            int lda, const double* B, int ldb, double* C, int ldc) {
+  if (M == 0 || N == 0) return cudaSuccess;
+  dim3 grid((M + dgp::BM - 1) / dgp::BM, (N + dgp::BN - 1) / dgp::BN);
+  k_dgemm_cp<<<grid, 256, 0, L.st>>>(M, N, K, alpha, A, lda, B, ldb, C, ldc);
+  ++*L.launches;
+  return cudaGetLastError();
+}
+// FP32 SIMT contractions of the mixed path where the tensor-core kernels do
+// not apply (more than 128 harmonics): projection into FP64 y, and xi of the
+// FP64 vector s
+cudaError_t launch_proj_f32_simt(Launch L, int nylm, int nsph, int ngrid, float alpha,
+                                 const float* bw_f, const float* pot, int ldp, double* y) {
+  return gemm2<false, float, float, double, float>(L, nylm, nsph, ngrid, alpha, bw_f, nylm, pot,
+                                                   ldp, y, nylm);
+}
+cudaError_t launch_xi_f32_simt(Launch L, int nylm, int nsph, int ngrid, const float* basis_f,
+                               const double* s, float* xi) {
+  return gemm2<true, float, double, float, float>(L, ngrid, nsph, nylm, 1.f, basis_f, nylm, s,
+                                                  nylm, xi, ngrid);
 }
 
 cudaError_t launch_dgemm(Launch L, bool transA, int M, int N, int K, double alpha,
@@ -2586,7 +2715,7 @@ __device__ __forceinline__ float ylm_dot_f(const YlmTables& tb, const AnglesF& a
 }
 
 cudaError_t launch_lx_pot_f32(Launch L, const YlmTables& tb, const DevGeo& g, const double* X,
-                              float* pot, void* xk) {
+                              float* pot, void* xk, int ldp) {
   if (g.nsph == 0) return cudaSuccess;
   size_t sm = lx2_smem<float>(g.ngrid, g.maxnb);
   const long long nk = (long long)g.nsph * ((tb.lmax + 1) * (tb.lmax + 2) / 2);
@@ -2600,7 +2729,7 @@ cudaError_t launch_lx_pot_f32(Launch L, const YlmTables& tb, const DevGeo& g, co
     if ((e = cudaFuncSetAttribute(k_lx2<LV, false, float>,                                    \
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)))     \
       return e;                                                                               \
-    k_lx2<LV, false, float><<<g.nsph, 128, sm, L.st>>>(tb, g, XK, pot);                       \
+    k_lx2<LV, false, float><<<g.nsph, 128, sm, L.st>>>(tb, g, XK, pot, ldp);                  \
     break;                                                                                    \
   }
   switch (tb.lmax) {
@@ -3134,7 +3263,7 @@ __global__ void __launch_bounds__(32 * ls_nroles(LMAX), LMAX > 10 ? 1 : (sizeof(
 constexpr int kGatherWarps = 4;  // at most; fewer when NW rows of ngrid do not fit
 template <class Rl>
 __global__ void __launch_bounds__(32 * kGatherWarps)
-    k_lx_gather(const DevGeo g, const Rl* __restrict__ val, Rl* pot) {
+    k_lx_gather(const DevGeo g, const Rl* __restrict__ val, Rl* pot, int ldp) {
   constexpr int U = 4;
   const int NW = blockDim.x >> 5;
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -3193,7 +3322,7 @@ __global__ void __launch_bounds__(32 * kGatherWarps)
   for (int n = tid; n < G; n += 32 * NW) {
     Rl sum = acc[n];
     for (int ww = 1; ww < NW; ++ww) sum += acc[ww * G + n];
-    pot[(size_t)a * G + n] = sum;
+    pot[(size_t)a * ldp + n] = sum;
   }
 }
 
@@ -3235,7 +3364,7 @@ static cudaError_t lxs_launch(Launch L, const YlmTables& tb, const DevGeo& g, co
   return cudaGetLastError();
 }
 template <class Rl>
-static cudaError_t gather_launch(Launch L, const DevGeo& g, const Rl* val, Rl* pot) {
+static cudaError_t gather_launch(Launch L, const DevGeo& g, const Rl* val, Rl* pot, int ldp) {
   if (g.nsph == 0) return cudaSuccess;
   const int mb = (g.maxnb + 3) & ~3;
   const size_t idx = sizeof(int) * (2 * mb + 4), row = sizeof(Rl) * g.ngrid;
@@ -3247,7 +3376,7 @@ static cudaError_t gather_launch(Launch L, const DevGeo& g, const Rl* val, Rl* p
     if ((e = cudaFuncSetAttribute(k_lx_gather<Rl>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)sm)))
       return e;
-  k_lx_gather<Rl><<<g.nsph, 32 * nw, sm, L.st>>>(g, val, pot);
+  k_lx_gather<Rl><<<g.nsph, 32 * nw, sm, L.st>>>(g, val, pot, ldp);
   ++*L.launches;
   return cudaGetLastError();
 }
@@ -3260,10 +3389,11 @@ cudaError_t launch_lxs_f32(Launch L, const YlmTables& tb, const DevGeo& g, const
   return lxs_launch<float>(L, tb, g, X, xi, xk, val, y);
 }
 cudaError_t launch_lx_gather(Launch L, const DevGeo& g, const double* val, double* pot) {
-  return gather_launch<double>(L, g, val, pot);
+  return gather_launch<double>(L, g, val, pot, g.ngrid);
 }
-cudaError_t launch_lx_gather_f32(Launch L, const DevGeo& g, const float* val, float* pot) {
-  return gather_launch<float>(L, g, val, pot);
+cudaError_t launch_lx_gather_f32(Launch L, const DevGeo& g, const float* val, float* pot,
+                                 int ldp) {
+  return gather_launch<float>(L, g, val, pot, ldp);
 }
 
 __global__ void k_to_float(long long n, const double* __restrict__ x, float* y) {

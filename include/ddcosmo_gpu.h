@@ -182,7 +182,10 @@ int ddc_batch_energy_forces(ddc_ctx* ctx, int nmol, const int* off, const double
 
 /* The operators the solver iterates (matvec.f90): y = off-diagonal L x
  * (lx, :94), y = off-diagonal L* x (lstarx, :161), y = D^-1 x (ldm1x, :246)
- * and the increment norm hnorm (:281).  x, y are (nylm,nsph). */
+ * and the increment norm hnorm (:281).  x, y are (nylm,nsph).  In a
+ * DDC_PREC_MIXED context lx, lstarx and lx_lstarx apply the FP32 operators of
+ * the inner solves (FP32 sums, tensor-core split-TF32 projection and
+ * expansion), read and written as FP64; otherwise everything is FP64. */
 int ddc_lx(ddc_ctx* ctx, const double* x, double* y);
 int ddc_lstarx(ddc_ctx* ctx, const double* x, double* y);
 int ddc_ldm1x(ddc_ctx* ctx, const double* x, double* y);
@@ -191,7 +194,7 @@ int ddc_hnorm(ddc_ctx* ctx, const double* x, double* norm);
 /* y = off-diagonal L x and z = off-diagonal L* s from one fused pass over the
  * (sphere, point, neighbour) triples (the operator step of the paired
  * solves).  No reference counterpart: it equals ddc_lx(x) and ddc_lstarx(s)
- * (matvec.f90:94, :161) up to rounding.  FP64. */
+ * (matvec.f90:94, :161) up to rounding, in the context's precision. */
 int ddc_lx_lstarx(ddc_ctx* ctx, const double* x, double* y, const double* s, double* z);
 
 /* RHS of the direct equation from phi (wghpot + intrhs, cosmo.f90:104-117). */

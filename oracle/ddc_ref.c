@@ -860,6 +860,47 @@ static int jacobi_diis(ref_ctx *c, size_t n, double tol, const double *rhs, doub
   return ok;
 }
 
+/* Timing sample of the solver's vector work (CPU baseline only): the
+ * jacobi_diis loop above, run for `iters` iterations on a vector of the
+ * context's size, with the operator replaced by a cheap shift (y_k = 0.3 x_{k+1},
+ * which keeps the DIIS history non-degenerate) and a tolerance of zero so it
+ * never stops early.  Everything else -- D^-1, the history copies, the Gram
+ * row, the Gauss-Jordan solve, the extrapolation and the H-norm -- is the
+ * reference's serial per-iteration work (jacobi_diis.f90:102-176, 183-270).
+ * Returns the number of iterations run; *op_share is the fraction of them
+ * spent in the stand-in operator, measured separately. */
+static void shift_op(const ref_ctx *c, const double *x, double *y) {
+  size_t n = (size_t)c->nylm * c->nsph;
+  for (size_t k = 0; k + 1 < n; k++) y[k] = 0.3 * x[k + 1];
+  y[n - 1] = 0.3 * x[0];
+}
+int ref_diis_sample(ref_ctx *c, int iters, double *seconds, double *op_seconds) {
+  size_t n = (size_t)c->nylm * c->nsph;
+  if (n == 0) return 0;
+  double *rhs = malloc(sizeof(double) * n), *x = malloc(sizeof(double) * n);
+  for (size_t k = 0; k < n; k++) {
+    rhs[k] = 1.0 + 1e-3 * (double)(k % 97);
+    x[k] = 0.0;
+  }
+#ifdef _OPENMP
+  double t0 = omp_get_wtime();
+#endif
+  jacobi_diis(c, n, 0.0, rhs, x, iters, shift_op, NULL);
+#ifdef _OPENMP
+  double t1 = omp_get_wtime();
+  for (int it = 0; it < iters; it++) shift_op(c, x, rhs);
+  double t2 = omp_get_wtime();
+  *seconds = t1 - t0;
+  *op_seconds = t2 - t1;
+#else
+  *seconds = 0.0;
+  *op_seconds = 0.0;
+#endif
+  free(rhs);
+  free(x);
+  return iters;
+}
+
 /* wghpot (ddcosmo.f90:1187-1224). */
 static void wghpot(const ref_ctx *c, const double *phi, double *g) {
   int ic = 0;
@@ -1077,16 +1118,18 @@ static void fdoga(const ref_ctx *c, int isph, const double *xi, const double *ph
   }
 }
 
-/* forces_dd (forces_dd.f90:91-164) restricted to spheres [i0, i1): fx(3,n)
- * rows i0..i1-1 are overwritten (used to time a bounded sample). */
-int ref_forces_dd_range(const ref_ctx *c, const double *phi, const double *sigma, const double *s,
-                        double *fx, int i0, int i1);
+/* forces_dd (forces_dd.f90:91-164) restricted to the sphere ranges
+ * [rg[2r], rg[2r+1]), r < nrg: those rows of fx(3,n) are overwritten (the
+ * whole molecule, or a bounded timing sample). */
+int ref_forces_dd_ranges(const ref_ctx *c, const double *phi, const double *sigma,
+                         const double *s, double *fx, const int *rg, int nrg);
 int ref_forces_dd(const ref_ctx *c, const double *phi, const double *sigma, const double *s,
                   double *fx) {
-  return ref_forces_dd_range(c, phi, sigma, s, fx, 0, c->nsph);
+  int rg[2] = {0, c->nsph};
+  return ref_forces_dd_ranges(c, phi, sigma, s, fx, rg, 1);
 }
-int ref_forces_dd_range(const ref_ctx *c, const double *phi, const double *sigma, const double *s,
-                        double *fx, int i0, int i1) {
+int ref_forces_dd_ranges(const ref_ctx *c, const double *phi, const double *sigma,
+                         const double *s, double *fx, const int *rg, int nrg) {
   int nsph = c->nsph, ngrid = c->ngrid, nylm = c->nylm;
   if (!c->zi) return -1;
   double *xi = malloc(sizeof(double) * (size_t)ngrid * nsph);
@@ -1112,21 +1155,32 @@ int ref_forces_dd_range(const ref_ctx *c, const double *phi, const double *sigma
     ws.vsin = malloc(sizeof(double) * nv);
     /* each sphere writes only its own fx(:,isph): the parallel loop gives the
      * same result as the reference's serial loop (forces_dd.f90:132-136). */
+    for (int r = 0; r < nrg; r++) {
+      const int i0 = rg[2 * r], i1 = rg[2 * r + 1];
 #pragma omp for schedule(dynamic)
-    for (int isph = i0; isph < i1; isph++) {
-      double *f = fx + 3 * isph;
-      f[0] = f[1] = f[2] = 0.0;
-      fdoka(c, isph, sigma, xi + (size_t)isph * ngrid, &ws, f);
-      fdokb(c, isph, sigma, xi, &ws, f);
-      fdoga(c, isph, xi, phiexp, f);
+      for (int isph = i0; isph < i1; isph++) {
+        double *f = fx + 3 * isph;
+        f[0] = f[1] = f[2] = 0.0;
+        fdoka(c, isph, sigma, xi + (size_t)isph * ngrid, &ws, f);
+        fdokb(c, isph, sigma, xi, &ws, f);
+        fdoga(c, isph, xi, phiexp, f);
+      }
     }
     free(ws.basloc); free(ws.dbsloc); free(ws.vplm); free(ws.vcos); free(ws.vsin);
   }
   double fep = 0.5 * (c->eps - 1.0) / c->eps;
-  for (int k = 3 * i0; k < 3 * i1; k++) fx[k] = fep * fx[k];
+  for (int r = 0; r < nrg; r++)
+    for (int k = 3 * rg[2 * r]; k < 3 * rg[2 * r + 1]; k++) fx[k] = fep * fx[k];
   free(xi);
   free(phiexp);
   return 0;
+}
+
+/* forces_dd over spheres [i0, i1) only (timing samples). */
+int ref_forces_dd_range(const ref_ctx *c, const double *phi, const double *sigma, const double *s,
+                        double *fx, int i0, int i1) {
+  int rg[2] = {i0, i1};
+  return ref_forces_dd_ranges(c, phi, sigma, s, fx, rg, 1);
 }
 
 /* ddmkxi / ddmkzeta (ddcosmo.f90:1758-1806). */

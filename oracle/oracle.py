@@ -66,6 +66,8 @@ def lib():
         L.ref_forces_dd.argtypes = [ctypes.c_void_p, _dp, _dp, _dp, _dp]
         L.ref_forces_dd_range.argtypes = [ctypes.c_void_p, _dp, _dp, _dp, _dp, ctypes.c_int,
                                           ctypes.c_int]
+        L.ref_forces_dd_ranges.argtypes = [ctypes.c_void_p, _dp, _dp, _dp, _dp, _ip,
+                                           ctypes.c_int]
         L.ref_num_threads.restype = ctypes.c_int
         L.ref_mkxi.argtypes = [ctypes.c_void_p, _dp, _dp, ctypes.c_int]
         L.ref_mkrhs.argtypes = [ctypes.c_int, _dp, _dp, _dp, _dp, ctypes.c_int, _dp, _dp,
@@ -82,6 +84,8 @@ def lib():
         L.ref_dfsw.restype = ctypes.c_double
         L.ref_gjinv.argtypes = [ctypes.c_int, _dp, _dp]
         L.ref_gjinv.restype = ctypes.c_int
+        L.ref_diis_sample.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp]
+        L.ref_diis_sample.restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -178,6 +182,21 @@ class RefDD:
     def forces_dd_range(self, phi, sigma, s, i0, i1):
         fx = np.zeros((self.nsph, 3))
         self.L.ref_forces_dd_range(self.h, _p(_c(phi)), _p(_c(sigma)), _p(_c(s)), _p(fx), i0, i1)
+        return fx
+
+    def diis_sample(self, iters):
+        """Seconds of the reference's serial Jacobi/DIIS vector work over
+        `iters` iterations at this context's size (operator excluded)."""
+        sec, op = ctypes.c_double(0.0), ctypes.c_double(0.0)
+        self.L.ref_diis_sample(self.h, iters, ctypes.byref(sec), ctypes.byref(op))
+        return max(sec.value - op.value, 0.0)
+
+    def forces_dd_ranges(self, phi, sigma, s, ranges):
+        """forces_dd over several sphere ranges [(i0, i1), ...] in one call."""
+        fx = np.zeros((self.nsph, 3))
+        rg = np.ascontiguousarray(np.asarray(ranges, dtype=np.int32).reshape(-1))
+        self.L.ref_forces_dd_ranges(self.h, _p(_c(phi)), _p(_c(sigma)), _p(_c(s)), _p(fx),
+                                    rg.ctypes.data_as(_ip), len(rg) // 2)
         return fx
 
     def mkzeta(self, s):      # ddcosmo.f90:1787

@@ -65,3 +65,34 @@ def test_batch_paired_equals_one_system_after_the_other():
     for fa, fb in zip(a["fx"], b["fx"]):
         np.testing.assert_allclose(fa, fb, rtol=0, atol=1e-9)
     assert np.abs(a["iters"] - b["iters"]).max() <= 2
+
+
+def test_batch_full_size_workload_vs_oracle():
+    """The benchmarked batch itself: 256 globules of 20-1,952 spheres (107,332
+    in all) in one call, against the oracle's stored results for 16 of them
+    (the six largest and ten spread over the size order,
+    tests/golden/make_config3.py)."""
+    import os
+
+    from conftest import GOLDEN
+    from ddpcm_b200 import molecules as M
+    from ddpcm_b200.ddcosmo import DDCosmo
+    c = M.BATCH_CONFIG
+    mols = [M.to_bohr(m) for m in M.batch_molecules(count=c["count"], lo=c["lo"], hi=c["hi"],
+                                                     seed=c["seed"])]
+    gold = np.load(os.path.join(GOLDEN, "config3_oracle.npz"))
+    p = dict(lmax=c["lmax"], ngrid=c["ngrid"], iconv=c["iconv"], eps=c["eps"], eta=c["eta"])
+    with DDCosmo(**p) as dd:
+        out = dd.batch_energy_forces(mols)
+    assert out["info"]["direct"]["converged"] and out["info"]["adjoint"]["converged"]
+    assert max(len(m["x"]) for m in mols) == gold["nsph"].max()
+    for j, k in enumerate(gold["index"]):
+        k = int(k)
+        assert len(mols[k]["x"]) == gold["nsph"][j]
+        ref_e = float(gold["esolv"][j])
+        ref_f = gold["fx"][gold["off"][j]:gold["off"][j + 1]]
+        assert abs(out["esolv"][k] - ref_e) <= ESOLV_RTOL * abs(ref_e), k
+        np.testing.assert_allclose(out["fx"][k], ref_f, rtol=0, atol=FORCE_ATOL)
+        for col in (0, 1):
+            a, b = int(out["iters"][k, col]), int(gold["iters"][j][col])
+            assert abs(a - b) <= 1 + 0.2 * b, (k, col, a, b)
