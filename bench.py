@@ -282,6 +282,95 @@ def measure_batch(dev, stream):
             "error": err, "host_arrays": True}
 
 
+def measure_learned(dev, stream, weights=None, nmol=4, n=2000):
+    """Learned initial guess on held-out globules (the learned-guess
+    configuration): `nmol` globules of `n` spheres at lmax 6 / 302 points,
+    tol 1e-10, seeds outside the training set.  Each is solved by energy +
+    forces from the FP64 zero guess (the plain method, also the accuracy
+    reference), the reference guess, the learned guess (FP64 and mixed) and,
+    for frame 1 of a 0.05 angstrom trajectory from the molecule, frame 0's
+    solutions.  One warm-up and one timed call each, device arrays, CUDA
+    events on the library's stream."""
+    import torch
+    from ddpcm_b200 import molecules as M
+    from ddpcm_b200.ddcosmo import (GUESS_LEARNED, GUESS_REFERENCE, GUESS_USER, GUESS_ZERO,
+                                    DDCosmo, GuessModel)
+    from ddpcm_b200.train_guess import EVAL_SEEDS
+    weights = weights or os.path.join(ROOT, "ddpcm_b200", "guess_lmax6_g302.npz")
+    if not os.path.exists(weights):
+        return {"unavailable": f"no trained model at {os.path.relpath(weights, ROOT)}"}
+    model = GuessModel.load(weights, device=dev.index or 0)
+    p = dict(lmax=6, ngrid=302, iconv=10, eps=78.3553, eta=0.1, device=dev.index or 0)
+    keys = "qxyzr"
+    runs = {}
+    names = ("fp64_zero_guess", "fp64_ref_guess", "fp64_learned_guess", "mixed_learned_guess",
+             "mixed_ref_guess", "fp64_prev_frame_guess", "mixed_prev_frame_guess")
+    for k in range(nmol):
+        m0, m1 = (M.to_bohr(f) for f in M.trajectory(M.make_molecule(n, EVAL_SEEDS[k]), 2,
+                                                      sigma=0.05, seed=EVAL_SEEDS[k] + 77))
+        nylm = 49
+        d_in = {kk: torch.tensor(m1[kk], dtype=torch.float64, device=dev) for kk in keys}
+        d0 = {kk: torch.tensor(m0[kk], dtype=torch.float64, device=dev) for kk in keys}
+        sig = torch.zeros((n, nylm), dtype=torch.float64, device=dev)
+        ss = torch.zeros_like(sig)
+        fx = torch.zeros((n, 3), dtype=torch.float64, device=dev)
+        prev = {}
+        for prec in (0, 1):  # frame 0's solutions, the trajectory guess
+            with DDCosmo(precision=prec, guess=GUESS_REFERENCE, device_pointers=1,
+                         stream=stream.cuda_stream, **p) as dd:
+                dd.energy_forces_ptr(*(d0[kk].data_ptr() for kk in keys), n, sig.data_ptr(),
+                                     ss.data_ptr(), fx.data_ptr())
+                prev[prec] = (sig.clone(), ss.clone())
+        ref = None
+        for name in names:
+            prec = 1 if name.startswith("mixed") else 0
+            guess = (GUESS_ZERO if "zero" in name else GUESS_REFERENCE if "ref_" in name else
+                     GUESS_LEARNED if "learned" in name else GUESS_USER)
+            with DDCosmo(precision=prec, guess=guess, device_pointers=1,
+                         stream=stream.cuda_stream, **p) as dd:
+                if guess == GUESS_LEARNED:
+                    dd.set_guess_model(model)
+
+                def step():
+                    if guess == GUESS_USER:
+                        sig.copy_(prev[prec][0])
+                        ss.copy_(prev[prec][1])
+                    return dd.energy_forces_ptr(*(d_in[kk].data_ptr() for kk in keys), n,
+                                                sig.data_ptr(), ss.data_ptr(), fx.data_ptr())
+                step()
+                torch.cuda.synchronize(dev)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                info = step()
+                e1.record(stream)
+                torch.cuda.synchronize(dev)
+                ms = e0.elapsed_time(e1)
+            r = {"ms": ms, "iterations": [info["direct"]["iterations"],
+                                          info["adjoint"]["iterations"]],
+                 "esolv": info["esolv"], "fx": fx.cpu().numpy().copy()}
+            if ref is None:
+                ref = r
+            r["esolv_rel_err"] = abs(r["esolv"] - ref["esolv"]) / abs(ref["esolv"])
+            r["forces_max_abs_err"] = float(np.abs(r["fx"] - ref["fx"]).max())
+            runs.setdefault(name, []).append(r)
+    out = {"workload": f"{nmol} held-out globules of {n} spheres (seeds {EVAL_SEEDS[:nmol]}), "
+                       "lmax=6 ngrid=302 eta=0.1 tol=1e-10, energy+forces, frame 1 of a "
+                       "0.05 angstrom trajectory from each",
+           "model": os.path.relpath(weights, ROOT), "variants": {}}
+    base = sum(r["ms"] for r in runs["fp64_zero_guess"])
+    for name, rs in runs.items():
+        ms = sum(r["ms"] for r in rs)
+        out["variants"][name] = {
+            "ms_per_solve": ms / len(rs),
+            "iterations_direct": [r["iterations"][0] for r in rs],
+            "iterations_adjoint": [r["iterations"][1] for r in rs],
+            "speedup_vs_fp64_zero_guess": base / ms,
+            "esolv_rel_err_max": max(r["esolv_rel_err"] for r in rs),
+            "forces_max_abs_err": max(r["forces_max_abs_err"] for r in rs),
+            "against": "FP64 zero-guess GPU solve of the same frame"}
+    return out
+
+
 def measure_previous_frame(make, timed, d_in, keys, c, dev):
     """Trajectory guess: frame 1 of a trajectory (every centre of the workload
     moved by a Gaussian 0.05 angstrom per coordinate) solved with frame 0's
@@ -453,6 +542,9 @@ def run_ours(args):
     batch = None
     if not args.no_batch and world == 1:
         batch = measure_batch(dev, stream)
+    learned = None
+    if not args.no_variants and world == 1:
+        learned = measure_learned(dev, stream)
 
     if args.no_e2e:
         dd.close()
@@ -534,7 +626,7 @@ def run_ours(args):
             "sizes": {k: info[k] for k in ("nsph", "ncav", "nylm", "ngrid", "ntriples",
                                            "npairs")},
             "esolv_hartree": info["esolv"], "error_vs_fp64_oracle": acc_head,
-            "variants": variants, "batch": batch,
+            "variants": variants, "batch": batch, "learned_guess": learned,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e / args.steps},
             "gpu_launches": launches, "stage_ms_per_step": stage_ms,

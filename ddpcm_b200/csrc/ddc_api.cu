@@ -158,6 +158,12 @@ struct ddc_ctx {
   DBuf basisT;
   TcPlan tc;
   int ldp_f = 0;
+  // learned initial guess: the attached model, its feature rows, and flags
+  // for the flows (rhs/psi/sigma/s of the last flow are valid; the initial
+  // guesses are already in place)
+  ddc_guess* gmodel = nullptr;
+  DBuf gfeat;
+  bool have_flow = false, guess_preset = false;
   // pinned landing buffer of the small device-to-host reads (reduced sums)
   double* hred = nullptr;
   // second stream of the force tail: the field of zeta at the nuclei runs
@@ -582,13 +588,19 @@ int do_init(ddc_ctx* ctx, int n, const std::vector<double4>* hsph, const double4
                        ctx->st));
     // the two contractions run on the tensor cores (split TF32) up to 128
     // harmonics (lmax 10), else as FP32 SIMT GEMMs on FP32 copies of the basis
-    const bool tc = tc_supported(NY);
+    // DDC_TC_OFF=1 in the environment selects the SIMT contractions (a
+    // diagnostic switch: the tests compare the two paths' accuracy)
+    const char* tc_off = std::getenv("DDC_TC_OFF");
+    const bool tc = tc_supported(NY) && !(tc_off && tc_off[0] == '1');
     ctx->ldp_f = tc ? (G + 3) / 4 * 4 : G;
     CK(ctx->pot_f.ensure(sizeof(float) * std::max<long long>((long long)N * ctx->ldp_f, 1LL)));
     CK(ctx->xi_f.ensure(sizeof(float) * std::max(NP, 1LL)));
     if (tc) {
       CK(tc_plan(L, ctx->tc, ctx->basis.as<double>(), ctx->bw.as<double>(), N, NY, G,
                  ctx->pot_f.as<float>(), ctx->ldp_f));
+      // tile widths by measurement (x and y are free work vectors here)
+      CK(tc_autotune(L, ctx->tc, ctx->x.as<double>(), ctx->y.as<double>(),
+                     ctx->xi_f.as<float>()));
     } else {
       ctx->tc.on = false;
       CK(ctx->basis_f.ensure(sizeof(float) * G * NY));
@@ -1164,6 +1176,11 @@ int cosmo_dev(ddc_ctx* ctx, int star, int cart, const double* phi, const double*
               const double* psi, double* sigma, double* esolv, ddc_solve_info* info) {
   const long long n = (long long)ctx->nsph * ctx->nylm;
   const int gmode = ctx->prm.guess == DDC_GUESS_ZERO ? 1 : 0;
+  // the start is the caller's (USER) or was set by the energy+force flow
+  const bool keep = ctx->prm.guess == DDC_GUESS_USER || ctx->guess_preset;
+  if (ctx->prm.guess == DDC_GUESS_LEARNED && !ctx->guess_preset)
+    return fail(ctx, DDC_ERR_PARAM,
+                "the learned guess is formed by ddc_energy_forces / ddc_batch_energy_forces");
   if (!star) {
     double* rhs = ctx->rhs.as<double>();
     if (cart) {
@@ -1171,7 +1188,7 @@ int cosmo_dev(ddc_ctx* ctx, int star, int cart, const double* phi, const double*
     } else {
       CK(cudaMemcpyAsync(rhs, glm, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx->st));
     }
-    if (ctx->prm.guess != DDC_GUESS_USER) CK(launch_guess(ctx->L(), ctx->tb, n, rhs, sigma, gmode));
+    if (!keep) CK(launch_guess(ctx->L(), ctx->tb, n, rhs, sigma, gmode));
     CKI(solve(ctx, false, rhs, sigma, info));
     if (esolv) {
       double d = 0.0;
@@ -1179,9 +1196,22 @@ int cosmo_dev(ddc_ctx* ctx, int star, int cart, const double* phi, const double*
       *esolv = 0.5 * ((ctx->prm.eps - 1.0) / ctx->prm.eps) * d;
     }
   } else {
-    if (ctx->prm.guess != DDC_GUESS_USER) CK(launch_guess(ctx->L(), ctx->tb, n, psi, sigma, gmode));
+    if (!keep) CK(launch_guess(ctx->L(), ctx->tb, n, psi, sigma, gmode));
     CKI(solve(ctx, true, psi, sigma, info));
   }
+  return DDC_OK;
+}
+
+// learned initial guesses x (direct) and s (adjoint, may be NULL) from the
+// context's rhs g and psi: facl * rhs plus the model's correction
+int learned_guess(ddc_ctx* ctx, const double* g, const double* psi, double* x, double* s) {
+  ddc_guess* m = ctx->gmodel;
+  if (!m) return fail(ctx, DDC_ERR_STATE, "DDC_GUESS_LEARNED needs a model (ddc_set_guess_model)");
+  const int nin = guess_nfeat(m);
+  CK(ctx->gfeat.ensure(sizeof(float) * std::max<long long>((long long)ctx->nsph * nin, 1)));
+  CK(launch_guess_features(ctx->L(), ctx->nsph, ctx->nylm, nin, g, psi, ctx->sph.as<double4>(),
+                           ctx->mrange_ptr(), ctx->gfeat.as<float>()));
+  CK(guess_infer(ctx->L(), m, ctx->tb, ctx->nsph, ctx->gfeat.as<float>(), g, psi, x, s));
   return DDC_OK;
 }
 
@@ -1442,6 +1472,7 @@ int ddc_create(const ddc_params* p, ddc_ctx** out) {
       p->max_iter <= 0 || p->ndiis < 0 || p->ndiis > kMaxHist || (p->ndiis > 0 && p->ndiis <= 10))
     return DDC_ERR_PARAM;
   if (p->precision != DDC_PREC_FP64 && p->precision != DDC_PREC_MIXED) return DDC_ERR_PARAM;
+  if (p->guess < DDC_GUESS_REFERENCE || p->guess > DDC_GUESS_LEARNED) return DDC_ERR_PARAM;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return DDC_ERR_CUDA;
   if (p->device < 0 || p->device >= ndev) return DDC_ERR_PARAM;
@@ -1589,6 +1620,7 @@ int ddc_init(ddc_ctx* ctx, int n, const double* x, const double* y, const double
   for (int i = 0; i < n; i++)
     if (!(hs[i].w > 0.0)) return fail(ctx, DDC_ERR_PARAM, "radii must be positive");
   if (!ctx->batch_init) ctx->nmol = 1;
+  ctx->have_flow = false;
   int rc;
   {
     StageScope sc(ctx, ST_INIT);
@@ -1909,7 +1941,9 @@ int ddc_energy_forces(ddc_ctx* ctx, int n, const double* charge, const double* x
     // the direct solve, and each round applies L and L* in one fused pass
     double* rhs = ctx->rhs.as<double>();
     CKI(direct_rhs(ctx, dphi, rhs));
-    if (ctx->prm.guess != DDC_GUESS_USER) {
+    if (ctx->prm.guess == DDC_GUESS_LEARNED) {
+      CKI(learned_guess(ctx, rhs, dpsi, dsig, ds));
+    } else if (ctx->prm.guess != DDC_GUESS_USER) {
       const int gmode = ctx->prm.guess == DDC_GUESS_ZERO ? 1 : 0;
       CK(launch_guess(ctx->L(), ctx->tb, (long long)nv, rhs, dsig, gmode));
       CK(launch_guess(ctx->L(), ctx->tb, (long long)nv, dpsi, ds, gmode));
@@ -1922,13 +1956,26 @@ int ddc_energy_forces(ddc_ctx* ctx, int n, const double* charge, const double* x
     CKI(dot_dev(ctx, (long long)nv, dsig, dpsi, &d));
     *esolv = 0.5 * ((ctx->prm.eps - 1.0) / ctx->prm.eps) * d;
   } else {
-    CKI(cosmo_dev(ctx, 0, 1, dphi, nullptr, dpsi, dsig, esolv, &inf->direct));
+    if (ctx->prm.guess == DDC_GUESS_LEARNED) {
+      // both starts from the model before the solves (cosmo_dev recomputes
+      // the same rhs and keeps them)
+      CKI(direct_rhs(ctx, dphi, ctx->rhs.as<double>()));
+      CKI(learned_guess(ctx, ctx->rhs.as<double>(), dpsi, dsig, ctx->prm.igrad ? ds : nullptr));
+      ctx->guess_preset = true;
+    }
+    const int rc = cosmo_dev(ctx, 0, 1, dphi, nullptr, dpsi, dsig, esolv, &inf->direct);
+    if (rc != DDC_OK || !ctx->prm.igrad) ctx->guess_preset = false;
+    if (rc != DDC_OK) return rc;
   }
   double t3 = now_s();
   inf->t_direct = t3 - t2;
   double* dfx = nullptr;
   if (ctx->prm.igrad) {
-    if (!paired) CKI(cosmo_dev(ctx, 1, 0, nullptr, nullptr, dpsi, ds, nullptr, &inf->adjoint));
+    if (!paired) {
+      const int rc = cosmo_dev(ctx, 1, 0, nullptr, nullptr, dpsi, ds, nullptr, &inf->adjoint);
+      ctx->guess_preset = false;
+      if (rc != DDC_OK) return rc;
+    }
     double t4 = now_s();
     inf->t_adjoint = t4 - t3;
     CK(ctx->fx.ensure(sizeof(double) * 3 * std::max(N, 1)));
@@ -2003,6 +2050,7 @@ int ddc_energy_forces(ddc_ctx* ctx, int n, const double* charge, const double* x
   inf->ngrid = ctx->ngrid;
   inf->ntriples = ctx->ntri;
   inf->npairs = ctx->npair;
+  ctx->have_flow = true;
   return DDC_OK;
 }
 
@@ -2090,14 +2138,19 @@ int ddc_batch_energy_forces(ddc_ctx* ctx, int nmol, const int* off, const double
       CK(launch_dgemm_nn(ctx->L(), ctx->nylm, N, ctx->ngrid, 1.0, ctx->bw.as<double>(),
                          ctx->nylm, ctx->gbuf.as<double>(), ctx->ngrid, rhs, ctx->nylm));
     }
-    CK(launch_guess(ctx->L(), ctx->tb, n, rhs, dsig, ctx->prm.guess == DDC_GUESS_ZERO ? 1 : 0));
+    const bool learned = ctx->prm.guess == DDC_GUESS_LEARNED;
+    if (learned)
+      CKI(learned_guess(ctx, rhs, dpsi, dsig, ctx->prm.igrad ? ds : nullptr));
+    else
+      CK(launch_guess(ctx->L(), ctx->tb, n, rhs, dsig, ctx->prm.guess == DDC_GUESS_ZERO ? 1 : 0));
     std::vector<int> it(nmol), ita(nmol);
     BatchSys sys[2];
     CKI(batch_setup(ctx, sys[0], false, rhs, dsig, it.data(), &inf->direct, 0));
     if (paired) {
       // the adjoint right-hand side psi is known already: both systems share
       // each sweep's fused L / L* pass
-      CK(launch_guess(ctx->L(), ctx->tb, n, dpsi, ds, ctx->prm.guess == DDC_GUESS_ZERO ? 1 : 0));
+      if (!learned)
+        CK(launch_guess(ctx->L(), ctx->tb, n, dpsi, ds, ctx->prm.guess == DDC_GUESS_ZERO ? 1 : 0));
       CKI(batch_setup(ctx, sys[1], true, dpsi, ds, ita.data(), &inf->adjoint, 1));
     }
     CKI(batch_run(ctx, sys, paired ? 2 : 1));
@@ -2117,7 +2170,8 @@ int ddc_batch_energy_forces(ddc_ctx* ctx, int nmol, const int* off, const double
   inf->t_direct = t3 - t2;
   if (ctx->prm.igrad) {
     if (!paired) {
-      CK(launch_guess(ctx->L(), ctx->tb, n, dpsi, ds, ctx->prm.guess == DDC_GUESS_ZERO ? 1 : 0));
+      if (ctx->prm.guess != DDC_GUESS_LEARNED)
+        CK(launch_guess(ctx->L(), ctx->tb, n, dpsi, ds, ctx->prm.guess == DDC_GUESS_ZERO ? 1 : 0));
       std::vector<int> it(nmol);
       BatchSys sys;
       CKI(batch_setup(ctx, sys, true, dpsi, ds, it.data(), &inf->adjoint, 0));
@@ -2163,6 +2217,38 @@ int ddc_batch_energy_forces(ddc_ctx* ctx, int nmol, const int* off, const double
   inf->ngrid = ctx->ngrid;
   inf->ntriples = ctx->ntri;
   inf->npairs = ctx->npair;
+  ctx->have_flow = true;
+  return DDC_OK;
+}
+
+// training rows of the learned guess from the last flow (ddc_guess.cu)
+int ddc_guess_features(ddc_ctx* ctx, float* feat) {
+  if (!ctx || !feat) return DDC_ERR_PARAM;
+  if (!ctx->have_flow)
+    return fail(ctx, DDC_ERR_STATE, "guess features need a ddc_energy_forces or batch call first");
+  if (!ctx->gmodel) return fail(ctx, DDC_ERR_STATE, "no guess model (ddc_set_guess_model)");
+  cudaSetDevice(ctx->prm.device);
+  CK(launch_guess_features(ctx->L(), ctx->nsph, ctx->nylm, guess_nfeat(ctx->gmodel),
+                           ctx->rhs.as<double>(), ctx->psi.as<double>(), ctx->sph.as<double4>(),
+                           ctx->mrange_ptr(), feat));
+  return sync(ctx);
+}
+int ddc_guess_targets(ddc_ctx* ctx, float* target) {
+  if (!ctx || !target) return DDC_ERR_PARAM;
+  if (!ctx->have_flow || !ctx->prm.igrad)
+    return fail(ctx, DDC_ERR_STATE, "guess targets need an energy+force call (igrad=1) first");
+  if (!ctx->gmodel) return fail(ctx, DDC_ERR_STATE, "no guess model (ddc_set_guess_model)");
+  cudaSetDevice(ctx->prm.device);
+  CK(launch_guess_targets(ctx->L(), ctx->tb, ctx->nsph, guess_nout(ctx->gmodel),
+                          ctx->rhs.as<double>(), ctx->psi.as<double>(), ctx->sigma.as<double>(),
+                          ctx->s.as<double>(), target));
+  return sync(ctx);
+}
+int ddc_set_guess_model(ddc_ctx* ctx, ddc_guess* m) {
+  if (!ctx) return DDC_ERR_PARAM;
+  if (m && guess_lmax(m) != ctx->prm.lmax)
+    return fail(ctx, DDC_ERR_PARAM, "guess model was built for another lmax");
+  ctx->gmodel = m;
   return DDC_OK;
 }
 

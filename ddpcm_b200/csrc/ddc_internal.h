@@ -60,7 +60,10 @@ struct DBuf {
 // mapped host memory that a kernel sets when one of its bounded waits runs out.
 struct TcPlan {
   bool on = false;
-  int nsph = 0, nylm = 0, ngrid = 0;
+  bool tuned = false;        // tile widths measured for tune_key's shape
+  long long tune_key = 0;
+  float ms_proj = 0.f, ms_xi = 0.f;  // measured launch times of the chosen widths
+  int nsph = 0, nylm = 0, ngrid = 0, ldp = 0;
   int kc_proj = 0, bn_proj = 0, ns_proj = 0, smem_proj = 0;
   int mt_xi = 0, kc_xi = 0, bn_xi = 0, ns_xi = 0, smem_xi = 0;
   DBuf img_proj, img_xi;
@@ -257,9 +260,29 @@ cudaError_t launch_guess(Launch L, const YlmTables& tb, long long n, const doubl
 bool tc_supported(int nylm);
 cudaError_t tc_plan(Launch L, TcPlan& p, const double* basis, const double* bw, int nsph,
                     int nylm, int ngrid, float* pot_f, int ldp);
+// pick the tile widths of both kernels by timing the candidates (y, xi are
+// scratch; s is zeroed)
+cudaError_t tc_autotune(Launch L, TcPlan& p, const double* s, double* y, float* xi);
 cudaError_t launch_proj_tc(Launch L, const TcPlan& p, double alpha, double* y);
 cudaError_t launch_xi_tc(Launch L, const TcPlan& p, const double* s, float* xi);
 void tc_release(TcPlan& p);
+
+// learned initial guess (ddc_guess.cu)
+int guess_nfeat(const ddc_guess* m);
+int guess_nout(const ddc_guess* m);
+int guess_lmax(const ddc_guess* m);
+// raw per-sphere features [nsph][nin]: g (nylm), psi(00), radius, 16-bin
+// histogram of the distances to the other centres of the sphere's molecule
+cudaError_t launch_guess_features(Launch L, int nsph, int nylm, int nin, const double* g,
+                                  const double* psi, const double4* sph, const int2* mrange,
+                                  float* feat);
+// training targets [nsph][nout]: X - facl g and S - facl psi
+cudaError_t launch_guess_targets(Launch L, const YlmTables& tb, int nsph, int nout,
+                                 const double* g, const double* psi, const double* X,
+                                 const double* S, float* t);
+// x = facl g + model correction, s = facl psi + model correction
+cudaError_t guess_infer(Launch L, ddc_guess* m, const YlmTables& tb, int nsph, const float* feat,
+                        const double* g, const double* psi, double* x, double* s);
 
 // solver
 // xnew = facl*(rhs - y); e = xnew - x; partial dots e.h_k (k < hist.n) and e.e.

@@ -32,6 +32,7 @@
 #include <cuda.h>  // CUtensorMap
 
 #include <algorithm>
+#include <vector>
 
 #include "ddc_internal.h"
 
@@ -551,44 +552,76 @@ int pick_bn(int nsph, int cap) {
 
 bool tc_supported(int nylm) { return nylm <= 128; }
 
+namespace {
+
+// tile width bn of the projection: pipeline depth, shared memory and the TMA
+// box of the grid field (bn rows of 32 values)
+cudaError_t cfg_proj(TcPlan& p, int bn) {
+  const int sb = 2 * kChunk + 2 * bn * 128;
+  p.bn_proj = bn;
+  p.ns_proj = std::min(4, (kSmemCap - kSmemSlack) / sb);
+  if (p.ns_proj < 2) return cudaErrorInvalidValue;
+  // at least 120 KB: one CTA per SM, so tensor-memory allocations never wait
+  p.smem_proj = std::max(p.ns_proj * sb + kSmemSlack, 120 * 1024);
+  cuuint64_t dims[2] = {(cuuint64_t)p.ngrid, (cuuint64_t)p.nsph};
+  cuuint64_t strides[1] = {(cuuint64_t)p.ldp * 4};
+  cuuint32_t box[2] = {32, (cuuint32_t)bn};
+  cuuint32_t es[2] = {1, 1};
+  CUresult r = encode_fn()(&p.tm_pot, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, p.pot_f, dims, strides,
+                           box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
+  return cudaFuncSetAttribute(k_proj_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              p.smem_proj);
+}
+// tile width of the expansion: the split coefficients of bn spheres stay
+// resident, the basis chunks stream through a ring of at least two stages
+cudaError_t cfg_xi(TcPlan& p, int bn) {
+  const int bsz = p.kc_xi * 2 * bn * 128;
+  const int ns = std::min(3, (kSmemCap - kSmemSlack - bsz) / (2 * kChunk));
+  if (ns < 2 || 2 * bn > 512) return cudaErrorInvalidValue;
+  p.bn_xi = bn;
+  p.ns_xi = ns;
+  p.smem_xi = std::max(bsz + ns * 2 * kChunk + kSmemSlack, 120 * 1024);
+  return cudaFuncSetAttribute(k_xi_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, p.smem_xi);
+}
+std::vector<int> bn_candidates(int nsph) {
+  std::vector<int> c;
+  const int top = std::min(256, (nsph + 15) / 16 * 16);
+  for (int bn : {pick_bn(nsph, 256), 32, 64, 96, 128, 160, 192, 256})
+    if (bn >= 16 && bn <= top && std::find(c.begin(), c.end(), bn) == c.end()) c.push_back(bn);
+  return c;
+}
+
+}  // namespace
+
 cudaError_t tc_plan(Launch L, TcPlan& p, const double* basis, const double* bw, int nsph,
                     int nylm, int ngrid, float* pot_f, int ldp) {
   p.on = false;
+  p.tuned = false;
   if (!tc_supported(nylm) || nsph <= 0) return cudaSuccess;
   if (!encode_fn()) return cudaErrorNotSupported;
+  // the per-call grid field: [nsph][ngrid] FP32 rows ldp apart (16-byte multiple)
+  if ((ldp * 4) % 16 != 0 || (reinterpret_cast<uintptr_t>(pot_f) & 15) != 0)
+    return cudaErrorInvalidValue;
   p.nsph = nsph;
   p.nylm = nylm;
   p.ngrid = ngrid;
-  // projection: M = lm (one 128-row tile), K = grid points
-  p.kc_proj = (ngrid + 31) / 32;
-  p.bn_proj = pick_bn(nsph, 256);
-  {
-    const int sb = 2 * kChunk + 2 * p.bn_proj * 128;
-    p.ns_proj = std::min(4, (kSmemCap - kSmemSlack) / sb);
-    while (p.ns_proj < 2 && p.bn_proj > 16) {
-      p.bn_proj -= 16;
-      p.ns_proj = std::min(4, (kSmemCap - kSmemSlack) / (2 * kChunk + 2 * p.bn_proj * 128));
-    }
-    p.smem_proj = p.ns_proj * sb + kSmemSlack;
-    p.smem_proj = std::max(p.smem_proj, 120 * 1024);  // one CTA per SM: no TMEM contention
-  }
-  // expansion: M = grid points (tiles of 128), K = lm
-  p.mt_xi = (ngrid + 127) / 128;
+  p.pot_f = pot_f;
+  p.ldp = ldp;
+  p.kc_proj = (ngrid + 31) / 32;           // projection: M = lm, K = grid points
+  p.mt_xi = (ngrid + 127) / 128;           // expansion: M = grid points, K = lm
   p.kc_xi = (nylm + 31) / 32;
-  p.bn_xi = pick_bn(nsph, 256);
-  for (;;) {
-    const int bsz = p.kc_xi * 2 * p.bn_xi * 128;
-    const int ns = std::min(3, (kSmemCap - kSmemSlack - bsz) / (2 * kChunk));
-    if (ns >= 2 || p.bn_xi <= 16) {
-      p.ns_xi = std::max(ns, 1);
-      p.smem_xi = std::max(bsz + p.ns_xi * 2 * kChunk + kSmemSlack, 120 * 1024);
-      break;
-    }
-    p.bn_xi -= 16;
-  }
-  if (p.ns_xi < 2) return cudaErrorNotSupported;
-  // static operands, split once
   cudaError_t e;
+  // default tile widths: about one tile per SM (narrower where the shared
+  // memory of a wide tile does not fit)
+  int bn = pick_bn(nsph, 256);
+  while ((e = cfg_proj(p, bn)) == cudaErrorInvalidValue && bn > 16) bn -= 16;
+  if (e) return e;
+  bn = pick_bn(nsph, 256);
+  while ((e = cfg_xi(p, bn)) == cudaErrorInvalidValue && bn > 16) bn -= 16;
+  if (e) return e;
+  // static operands, split once
   if ((e = p.img_proj.ensure((size_t)p.kc_proj * 2 * kChunk))) return e;
   if ((e = p.img_xi.ensure((size_t)p.mt_xi * p.kc_xi * 2 * kChunk))) return e;
   {
@@ -602,34 +635,86 @@ cudaError_t tc_plan(Launch L, TcPlan& p, const double* basis, const double* bw, 
     ++*L.launches;
     if ((e = cudaGetLastError())) return e;
   }
-  // the per-call grid field: [nsph][ngrid] FP32 rows ldp apart (16-byte multiple)
-  if ((ldp * 4) % 16 != 0 || (reinterpret_cast<uintptr_t>(pot_f) & 15) != 0)
-    return cudaErrorInvalidValue;
-  {
-    cuuint64_t dims[2] = {(cuuint64_t)ngrid, (cuuint64_t)nsph};
-    cuuint64_t strides[1] = {(cuuint64_t)ldp * 4};
-    cuuint32_t box[2] = {32, (cuuint32_t)p.bn_proj};
-    cuuint32_t es[2] = {1, 1};
-    CUresult r = encode_fn()(&p.tm_pot, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, pot_f, dims, strides,
-                             box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
-                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
-  }
-  if ((e = cudaFuncSetAttribute(k_proj_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                p.smem_proj)))
-    return e;
-  if ((e = cudaFuncSetAttribute(k_xi_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                p.smem_xi)))
-    return e;
   if (!p.err_h) {
     if ((e = cudaHostAlloc(&p.err_h, sizeof(int), cudaHostAllocMapped))) return e;
     if ((e = cudaHostGetDevicePointer(reinterpret_cast<void**>(&p.err_d), p.err_h, 0))) return e;
   }
   *p.err_h = 0;
-  p.pot_f = pot_f;
   p.on = true;
   return cudaSuccess;
+}
+
+// Tile widths picked by measurement: every candidate width of each kernel is
+// launched on the context's own buffers (pot_f and s zeroed first; y and xi
+// are scratch here) and timed with CUDA events on the context's stream; the
+// fastest is kept.  Runs once per problem shape (nsph, nylm, ngrid).
+cudaError_t tc_autotune(Launch L, TcPlan& p, const double* s, double* y, float* xi) {
+  if (!p.on) return cudaSuccess;
+  const long long key = ((long long)p.nsph << 24) ^ ((long long)p.nylm << 12) ^ p.ngrid;
+  if (p.tuned && p.tune_key == key) {
+    cudaError_t e = cfg_proj(p, p.bn_proj);
+    return e ? e : cfg_xi(p, p.bn_xi);
+  }
+  cudaEvent_t e0, e1;
+  cudaError_t e;
+  if ((e = cudaEventCreate(&e0))) return e;
+  if ((e = cudaEventCreate(&e1))) {
+    cudaEventDestroy(e0);
+    return e;
+  }
+  auto timed = [&](auto launch, float* ms) -> cudaError_t {
+    cudaError_t r;
+    if ((r = launch())) return r;  // warm-up
+    if ((r = cudaEventRecord(e0, L.st))) return r;
+    for (int k = 0; k < 3; ++k)
+      if ((r = launch())) return r;
+    if ((r = cudaEventRecord(e1, L.st))) return r;
+    if ((r = cudaEventSynchronize(e1))) return r;
+    if (p.err_h && *p.err_h) return cudaErrorLaunchFailure;
+    return cudaEventElapsedTime(ms, e0, e1);
+  };
+  const std::vector<int> cand = bn_candidates(p.nsph);
+  int best = p.bn_proj;
+  float tbest = 1e30f;
+  e = cudaMemsetAsync(p.pot_f, 0, sizeof(float) * (size_t)p.nsph * p.ldp, L.st);
+  for (size_t k = 0; !e && k < cand.size(); ++k) {
+    if (cfg_proj(p, cand[k]) != cudaSuccess) {
+      cudaGetLastError();
+      continue;
+    }
+    float ms = 0.f;
+    e = timed([&] { return launch_proj_tc(L, p, 1.0, y); }, &ms);
+    if (!e && ms < tbest) {
+      tbest = ms;
+      best = cand[k];
+    }
+  }
+  if (!e) e = cfg_proj(p, best);
+  p.ms_proj = tbest / 3.f;
+  best = p.bn_xi;
+  tbest = 1e30f;
+  if (!e) e = cudaMemsetAsync(const_cast<double*>(s), 0, sizeof(double) * p.nsph * p.nylm, L.st);
+  for (size_t k = 0; !e && k < cand.size(); ++k) {
+    if (cfg_xi(p, cand[k]) != cudaSuccess) {
+      cudaGetLastError();
+      continue;
+    }
+    float ms = 0.f;
+    e = timed([&] { return launch_xi_tc(L, p, s, xi); }, &ms);
+    if (!e && ms < tbest) {
+      tbest = ms;
+      best = cand[k];
+    }
+  }
+  if (!e) e = cfg_xi(p, best);
+  p.ms_xi = tbest / 3.f;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (!e) {
+    p.tuned = true;
+    p.tune_key = key;
+  }
+  return e;
 }
 
 cudaError_t launch_proj_tc(Launch L, const TcPlan& p, double alpha, double* y) {

@@ -25,11 +25,12 @@ DDC_OK = 0
 DDC_ERR_PARAM = 1
 DDC_ERR_NOCONV = 5
 PREC_FP64, PREC_MIXED = 0, 1
-GUESS_REFERENCE, GUESS_ZERO, GUESS_USER = 0, 1, 2
+GUESS_REFERENCE, GUESS_ZERO, GUESS_USER, GUESS_LEARNED = 0, 1, 2, 3
 TOANG = 0.52917721092          # main.f90:99
 TOKCAL = 627.509469            # main.f90:99
 
 _dp = ctypes.POINTER(ctypes.c_double)
+_fp = ctypes.POINTER(ctypes.c_float)
 
 
 class DDCosmoError(RuntimeError):
@@ -118,6 +119,23 @@ _SIGS = {
     "ddc_batch_energy_forces": [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
                                + [_dp] * 5 + [_dp, _dp, ctypes.POINTER(ctypes.c_int),
                                               ctypes.POINTER(RunInfo)],
+    "ddc_guess_create": [ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                         ctypes.POINTER(ctypes.c_void_p)],
+    "ddc_guess_destroy": [ctypes.c_void_p],
+    "ddc_guess_last_error": [ctypes.c_void_p],
+    "ddc_guess_sizes": [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
+                        ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_longlong)],
+    "ddc_guess_get_params": [ctypes.c_void_p, _fp],
+    "ddc_guess_set_params": [ctypes.c_void_p, _fp],
+    "ddc_guess_init_random": [ctypes.c_void_p, ctypes.c_ulonglong],
+    "ddc_guess_fit_scaling": [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                              ctypes.c_longlong],
+    "ddc_guess_train_epoch": [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                              ctypes.c_longlong, ctypes.c_int, ctypes.c_float, _dp],
+    "ddc_guess_predict": [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_longlong],
+    "ddc_guess_features": [ctypes.c_void_p, ctypes.c_void_p],
+    "ddc_guess_targets": [ctypes.c_void_p, ctypes.c_void_p],
+    "ddc_set_guess_model": [ctypes.c_void_p, ctypes.c_void_p],
 }
 
 
@@ -157,6 +175,7 @@ def load_library(path=None):
     L.ddc_last_error.restype = ctypes.c_char_p
     L.ddc_status_string.restype = ctypes.c_char_p
     L.ddc_stage_name.restype = ctypes.c_char_p
+    L.ddc_guess_last_error.restype = ctypes.c_char_p
     _lib = L
     return L
 
@@ -263,6 +282,19 @@ class DDCosmo:
     def set_timed_stages(self, names=None):
         """Time only the named stages (None: every stage)."""
         self._check(self.L.ddc_set_timed_stages(self.h, stage_mask(self.L, names)))
+
+    def set_guess_model(self, model):
+        """Model used by guess=GUESS_LEARNED (a GuessModel, or None)."""
+        self._guess_model = model
+        self._check(self.L.ddc_set_guess_model(self.h, model.h if model else None))
+
+    def guess_rows(self, feat_ptr, target_ptr=None):
+        """Training rows of the last energy+force call into device buffers
+        (raw pointers): features [nsph][nfeat] and, if given, targets
+        [nsph][nout] (needs a model attached for the row widths)."""
+        self._check(self.L.ddc_guess_features(self.h, feat_ptr))
+        if target_ptr is not None:
+            self._check(self.L.ddc_guess_targets(self.h, target_ptr))
 
     # ddinit (ddcosmo.f90:159): coordinates and radii in bohr
     def ddinit(self, x, y, z, rvdw):
@@ -443,3 +475,72 @@ class DDCosmo:
         self._check(self.L.ddc_sizes(self.h, *[ctypes.byref(v) for v in a]))
         self.nsph, self.ncav, self.nylm, self.ngrid = (v.value for v in a)
         return dict(esolv=es.value, sigma=sig, s=s, fx=fx, info=info.as_dict())
+
+
+class GuessModel:
+    """Learned initial guess (ddc_guess_*): a per-sphere network from the
+    sphere's right-hand side, charge, radius and neighbour-distance histogram
+    to the corrections of X0 and S0 over facl * rhs.  BF16 weights, FP32
+    accumulation, trained on device arrays of solver output."""
+
+    def __init__(self, lmax, hidden=256, device=0, params=None):
+        self.L = load_library()
+        h = ctypes.c_void_p()
+        st = self.L.ddc_guess_create(lmax, hidden, device, ctypes.byref(h))
+        if st != DDC_OK:
+            raise DDCosmoError(st, "ddc_guess_create failed")
+        self.h = h
+        self.lmax, self.hidden, self.device = lmax, hidden, device
+        nf, no, npar = ctypes.c_int(), ctypes.c_int(), ctypes.c_longlong()
+        self._check(self.L.ddc_guess_sizes(self.h, ctypes.byref(nf), ctypes.byref(no),
+                                           ctypes.byref(npar)))
+        self.nfeat, self.nout, self.nparams = nf.value, no.value, npar.value
+        if params is not None:
+            self.set_params(params)
+
+    def _check(self, st):
+        if st != DDC_OK:
+            raise DDCosmoError(st, self.L.ddc_guess_last_error(self.h).decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.ddc_guess_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def get_params(self):
+        out = np.zeros(self.nparams, dtype=np.float32)
+        self._check(self.L.ddc_guess_get_params(self.h, out.ctypes.data_as(_fp)))
+        return out
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        if p.size != self.nparams:
+            raise ValueError(f"expected {self.nparams} parameters, got {p.size}")
+        self._check(self.L.ddc_guess_set_params(self.h, p.ctypes.data_as(_fp)))
+
+    def init_random(self, seed=0):
+        self._check(self.L.ddc_guess_init_random(self.h, seed))
+
+    def fit_scaling(self, feat_ptr, target_ptr, n):
+        self._check(self.L.ddc_guess_fit_scaling(self.h, feat_ptr, target_ptr, n))
+
+    def train_epoch(self, feat_ptr, target_ptr, order_ptr, n, batch=4096, lr=1e-3):
+        loss = ctypes.c_double()
+        self._check(self.L.ddc_guess_train_epoch(self.h, feat_ptr, target_ptr, order_ptr, n,
+                                                 batch, lr, ctypes.byref(loss)))
+        return loss.value
+
+    def predict(self, feat_ptr, out_ptr, n):
+        self._check(self.L.ddc_guess_predict(self.h, feat_ptr, out_ptr, n))
+
+    def save(self, path, **meta):
+        np.savez_compressed(path, params=self.get_params(), lmax=self.lmax, hidden=self.hidden,
+                            nfeat=self.nfeat, nout=self.nout, **meta)
+
+    @classmethod
+    def load(cls, path, device=0):
+        d = np.load(path)
+        return cls(int(d["lmax"]), int(d["hidden"]), device, params=d["params"])

@@ -42,10 +42,14 @@ extern "C" {
 #define DDC_GUESS_REFERENCE 0 /* facl * rhs, as cosmo.f90:136-138 / 174-176 */
 #define DDC_GUESS_ZERO 1      /* zero vector */
 #define DDC_GUESS_USER 2      /* the caller's sigma on entry */
+#define DDC_GUESS_LEARNED 3   /* facl * rhs plus the correction predicted by the
+                               * context's guess model (ddc_set_guess_model);
+                               * ddc_energy_forces and ddc_batch_energy_forces */
 
 #define DDC_MAX_LMAX 12
 
 typedef struct ddc_ctx ddc_ctx;
+typedef struct ddc_guess ddc_guess;
 
 /* Control parameters: the reference's Input.txt scalars (main.f90:129-136,
  * ddcosmo.f90:106-107) plus solver knobs that the reference hard-codes
@@ -225,6 +229,42 @@ int ddc_fp64_peak(int device, double* gflops);
 /* The same for FP32 FMA: the denominator of the FP32 operator kernels of the
  * mixed-precision path. */
 int ddc_fp32_peak(int device, double* gflops);
+
+/* Learned initial guess.  No counterpart in the reference, which always
+ * starts from facl * rhs (cosmo.f90:136-138, 174-176); the model only moves
+ * the start, the Jacobi/DIIS solve and its stop test are unchanged.  A model
+ * is a per-sphere network (features -> `hidden` x 3 ReLU layers -> the
+ * corrections of X0 and S0), BF16 weights with FP32 accumulation, on one GPU.
+ * Features and targets are DEVICE arrays of the model's GPU, one row per
+ * sphere: feat[n][nfeat], target[n][nout] (FP32). */
+int ddc_guess_create(int lmax, int hidden, int device, ddc_guess** m);
+int ddc_guess_destroy(ddc_guess* m);
+const char* ddc_guess_last_error(ddc_guess* m);
+/* row widths and the length of the parameter vector of get/set_params */
+int ddc_guess_sizes(ddc_guess* m, int* nfeat, int* nout, long long* nparams);
+/* parameters as one FP32 host vector: weights, biases, then the feature
+ * means, the feature inverse deviations and the output scales */
+int ddc_guess_get_params(ddc_guess* m, float* host);
+int ddc_guess_set_params(ddc_guess* m, const float* host);
+int ddc_guess_init_random(ddc_guess* m, unsigned long long seed);
+/* standardisation statistics from a training set of n rows */
+int ddc_guess_fit_scaling(ddc_guess* m, const float* feat, const float* target, long long n);
+/* one pass over n rows (in the order of the device int array `order`, or
+ * as stored if NULL) in mini-batches of `batch`, Adam with step lr; *loss is
+ * the mean squared error of the scaled outputs over the pass */
+int ddc_guess_train_epoch(ddc_guess* m, const float* feat, const float* target, const int* order,
+                          long long n, int batch, float lr, double* loss);
+/* scaled outputs out[n][nout] (multiply by the output scales for the
+ * corrections) */
+int ddc_guess_predict(ddc_guess* m, const float* feat, float* out, long long n);
+/* training rows from the context's last ddc_energy_forces or
+ * ddc_batch_energy_forces call: features (rhs, psi, radii, distance
+ * histogram) and targets (solution minus facl * rhs, for X then S) of every
+ * sphere, written to device arrays of the context's GPU */
+int ddc_guess_features(ddc_ctx* ctx, float* feat);
+int ddc_guess_targets(ddc_ctx* ctx, float* target);
+/* the model used by DDC_GUESS_LEARNED (same lmax and device; NULL detaches) */
+int ddc_set_guess_model(ddc_ctx* ctx, ddc_guess* m);
 
 /* efld without any device allocation.  No counterpart in the reference: it
  * serves host programs that own all of the GPU's memory (a QM/MM or MD code

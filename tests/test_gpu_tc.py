@@ -4,13 +4,18 @@ the FP64 oracle's lx and lstarx (matvec.f90:94, :161).
 
 A DDC_PREC_MIXED context's ddc_lx / ddc_lstarx / ddc_lx_lstarx apply the
 operators of the inner solves: FP32 triple sums plus the two contractions.
-They must agree with the FP64 operators to FP32 accuracy (bar: 2e-6 of the
-largest entry), which is what the iterative refinement around them needs.
+They must agree with the FP64 operators to FP32 accuracy (bar: 1e-5 of the
+largest entry), which is what the iterative refinement around them needs,
+and the tensor-core contractions must be as accurate as FP32 SIMT ones: the
+same operators with the SIMT contractions (DDC_TC_OFF=1) set the reference
+error, and the tensor-core error may exceed it by at most 25%.
 The cases cover every harmonic count the tensor-core kernels take (lmax 0, 6,
 8, 10: one to four 32-wide k-chunks of the expansion, one to five 128-row
 grid tiles), tile widths from 16 to 64 spheres and the FP32 SIMT fallback
 above 128 harmonics (lmax 11, 12).
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -18,7 +23,7 @@ from conftest import load_golden
 
 pytestmark = pytest.mark.gpu
 
-BAR = 2e-6
+BAR = 1e-5
 
 
 def _globule(n, seed):
@@ -37,13 +42,21 @@ def test_mixed_operators_vs_oracle(oracle, lmax, ngrid, mol):
     x = rng.standard_normal((d.nsph, d.nylm))
     s = rng.standard_normal((d.nsph, d.nylm))
     ref_y, ref_z = d.lx(x), d.lstarx(s)
-    with DDCosmo(lmax=lmax, ngrid=ngrid, iconv=10, eta=0.1, precision=PREC_MIXED) as dd:
-        dd.ddinit(m["x"], m["y"], m["z"], m["r"])
-        y1, z1 = dd.lx(x), dd.lstarx(s)
-        y2, z2 = dd.lx_lstarx(x, s)
-    for a, b in ((y1, ref_y), (y2, ref_y), (z1, ref_z), (z2, ref_z)):
-        err = np.abs(a - b).max() / np.abs(b).max()
-        assert err <= BAR, err
+    errs = {}
+    for mode in ("tc", "simt"):
+        os.environ["DDC_TC_OFF"] = "1" if mode == "simt" else "0"
+        try:
+            with DDCosmo(lmax=lmax, ngrid=ngrid, iconv=10, eta=0.1, precision=PREC_MIXED) as dd:
+                dd.ddinit(m["x"], m["y"], m["z"], m["r"])
+                y1, z1 = dd.lx(x), dd.lstarx(s)
+                y2, z2 = dd.lx_lstarx(x, s)
+        finally:
+            os.environ.pop("DDC_TC_OFF", None)
+        errs[mode] = [np.abs(a - b).max() / np.abs(b).max()
+                      for a, b in ((y1, ref_y), (y2, ref_y), (z1, ref_z), (z2, ref_z))]
+    for et, es in zip(errs["tc"], errs["simt"]):
+        assert et <= BAR, errs
+        assert et <= 1.25 * es + 1e-8, errs
 
 
 @pytest.mark.parametrize("n", [2400, 9472])
