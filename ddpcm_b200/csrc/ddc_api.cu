@@ -635,9 +635,10 @@ int do_init(ddc_ctx* ctx, int n, const std::vector<double4>* hsph, const double4
     if (ctx->prm.precision == DDC_PREC_MIXED)
       for (DBuf* b : {&ctx->rres2, &ctx->dres2, &ctx->eres2})
         CK(b->ensure(sizeof(double) * std::max(nv, (size_t)1)));
-    // FP64 values: the mixed path also takes FP64 pair steps (refinement)
-    CK(ctx->tval.ensure(sizeof(double) * std::max<long long>(ctx->ntri, 1)));
   }
+  // per-triple lx values of the fused passes (FP64 size: the mixed path also
+  // takes FP64 steps in its refinement)
+  CK(ctx->tval.ensure(sizeof(double) * std::max<long long>(ctx->ntri, 1)));
   CKI(sync(ctx));
   ctx->ready = true;
   return DDC_OK;
@@ -684,8 +685,11 @@ int gemm_xi_f32(ddc_ctx* ctx, const double* s, float* xig) {
 int op_lx(ddc_ctx* ctx, const double* x, double* y) {
   DevGeo g = ctx->geo();
   {
+    // the lx part of the fused pass (one value per triple), then the sums
+    // per grid point
     StageScope sc(ctx, ST_LX_POT);
-    CK(launch_lx_pot(ctx->L(), ctx->tb, g, x, ctx->pot.as<double>(), false, ctx->xk.p));
+    CK(launch_lx_vals(ctx->L(), ctx->tb, g, x, ctx->xk.p, ctx->tval.as<double>(), false));
+    CK(launch_lx_gather(ctx->L(), g, ctx->tval.as<double>(), ctx->pot.as<double>()));
   }
   StageScope sc(ctx, ST_PROJ);
   // y = -Bw pot   (intrhs then negate, matvec.f90:131-135)
@@ -707,8 +711,10 @@ int op_lstarx(ddc_ctx* ctx, const double* x, double* y) {
 int op_lx_f32(ddc_ctx* ctx, const double* x, double* y) {
   {
     StageScope sc(ctx, ST_LX_POT);
-    CK(launch_lx_pot_f32(ctx->L(), ctx->tb, ctx->geo(), x, ctx->pot_f.as<float>(), ctx->xk.p,
-                         ctx->ldp_f));
+    DevGeo g = ctx->geo();
+    CK(launch_lx_vals_f32(ctx->L(), ctx->tb, g, x, ctx->xk.p, ctx->tval.as<float>()));
+    CK(launch_lx_gather_f32(ctx->L(), g, ctx->tval.as<float>(), ctx->pot_f.as<float>(),
+                            ctx->ldp_f));
   }
   StageScope sc(ctx, ST_PROJ);
   return gemm_proj_f32(ctx, -1.f, ctx->pot_f.as<float>(), y);
@@ -1224,9 +1230,12 @@ int forces_dev(ddc_ctx* ctx, const double* phi, const double* sigma, const doubl
     return fail(ctx, DDC_ERR_STATE, "forces need igrad=1 at init (zi)");
   if (!xi_ready) CKI(op_xi(ctx, s, ctx->xig.as<double>()));
   {
+    // u_chi(a, n) = sum over the neighbours b of chi(t) * intmlp(X_b): the
+    // chi-weighted lx sum, per triple then per grid point
     StageScope sc(ctx, ST_UCHI);
-    CK(launch_lx_pot(ctx->L(), ctx->tb, ctx->geo(), sigma, ctx->uchi.as<double>(), true,
-                     ctx->xk.p));
+    DevGeo g = ctx->geo();
+    CK(launch_lx_vals(ctx->L(), ctx->tb, g, sigma, ctx->xk.p, ctx->tval.as<double>(), true));
+    CK(launch_lx_gather(ctx->L(), g, ctx->tval.as<double>(), ctx->uchi.as<double>()));
   }
   const double fep = 0.5 * (ctx->prm.eps - 1.0) / ctx->prm.eps;
   CK(ctx->fxa.ensure(sizeof(double) * 3 * std::max(ctx->nsph, 1)));

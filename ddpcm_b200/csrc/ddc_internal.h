@@ -204,16 +204,19 @@ cudaError_t launch_sum_counts(Launch L, const int* cnt, int n, unsigned long lon
 
 // operators
 // xk: scratch of N*(lmax+1)(lmax+2)/2 double2 (K-scaled X in pair layout)
-cudaError_t launch_lx_pot(Launch L, const YlmTables& tb, const DevGeo& g, const double* X,
-                          double* pot, bool chi_only, void* xk);
 cudaError_t launch_lstarx_acc(Launch L, const YlmTables& tb, const DevGeo& g, const double* xi,
                               double* y);
 // FP32 operator variants (mixed precision): pot/xi in FP32, y in FP64
-cudaError_t launch_lx_pot_f32(Launch L, const YlmTables& tb, const DevGeo& g, const double* X,
-                              float* pot, void* xk, int ldp);
 // fused L / L*: val (one lx value per triple, gather-list order) and y = L* rows
 cudaError_t launch_lxs(Launch L, const YlmTables& tb, const DevGeo& g, const double* X,
                        const double* xi, void* xk, double* val, double* y);
+// the lx part of the fused pass alone: one value per triple (gather-list
+// order) for k_lx_gather; chi_only: weight chi(t) instead of chi(t)/f_a(n)
+// (the u_chi sum of the forces)
+cudaError_t launch_lx_vals(Launch L, const YlmTables& tb, const DevGeo& g, const double* X,
+                           void* xk, double* val, bool chi_only);
+cudaError_t launch_lx_vals_f32(Launch L, const YlmTables& tb, const DevGeo& g, const double* X,
+                               void* xk, float* val);
 cudaError_t launch_lxs_geo(Launch L, const YlmTables& tb, const DevGeo& g, float4* tg4,
                            float2* tg2);
 cudaError_t launch_lxs_geo_f64(Launch L, const YlmTables& tb, const DevGeo& g, double4* tg4,

@@ -582,140 +582,6 @@ __device__ __forceinline__ double rsqrt_pos(double x) {
 __device__ __forceinline__ double sqrt_t(double x) { return sqrt(x); }
 __device__ __forceinline__ float sqrt_t(float x) { return sqrtf(x); }
 
-template <int LMAX, class Rl>
-__device__ __forceinline__ Rl ylm_dot2(const YlmTables& tb, Rl sx, Rl sy, Rl sz, Rl t,
-                                       const typename RT<Rl>::V2* __restrict__ xs) {
-  const Rl one = 1;
-  Rl cth = sz, sth = sqrt_t(fmax(Rl(0), one - sz * sz));
-  Rl cp = 1, sp = 0;
-  if (sth != Rl(0)) {
-    Rl r = one / sth;
-    cp = sx * r;
-    sp = sy * r;
-  }
-  const Rl ct = cth * t, st = sth * t, t2 = t * t;
-  Rl accm[LMAX + 1];
-  Rl pmm = 1, cm = 1, sm = 0, cmm1 = 1, smm1 = 0;
-#pragma unroll
-  for (int m = 0; m <= LMAX; ++m) {
-    if (m == 1) {
-      cm = cp;
-      sm = sp;
-    } else if (m >= 2) {
-      Rl cn = Rl(2) * cp * cm - cmm1, sn = Rl(2) * cp * sm - smm1;
-      cmm1 = cm; smm1 = sm; cm = cn; sm = sn;
-    }
-    Rl p0 = pmm, p1 = 0, a = 0;
-#pragma unroll
-    for (int l = m; l <= LMAX; ++l) {
-      Rl P;
-      if (l == m) {
-        P = p0;
-      } else if (l == m + 1) {
-        p1 = Rl(2 * m + 1) * ct * p0;
-        P = p1;
-      } else {
-        P = (cA<Rl>(tb, lmi(l, m)) * ct) * p1 - (cB<Rl>(tb, lmi(l, m)) * t2) * p0;
-        p0 = p1;
-        p1 = P;
-      }
-      const typename RT<Rl>::V2 xv = xs[lmi(l, m)];
-      Rl q = (m == 0) ? xv.x : fma(cm, xv.x, sm * xv.y);
-      a = fma(P, q, a);
-    }
-    accm[m] = a;
-    pmm = -pmm * Rl(2 * m + 1) * st;
-  }
-  Rl s = 0;
-#pragma unroll
-  for (int m = 0; m <= LMAX; ++m) s += accm[m];
-  return s;
-}
-
-template <int LMAX, bool CHI, class Rl>
-__global__ void __launch_bounds__(128) k_lx2(const YlmTables tb, const DevGeo g,
-                                             const typename RT<Rl>::V2* __restrict__ XK,
-                                             Rl* pot, int ldp) {
-  typedef typename RT<Rl>::V2 V2;
-  constexpr int NLM = (LMAX + 1) * (LMAX + 2) / 2;
-  constexpr int NW = 4;
-  extern __shared__ __align__(16) unsigned char smraw[];
-  const int G = g.ngrid;
-  const int maxnb = g.maxnb;
-  Rl* nbd = reinterpret_cast<Rl*>(smraw);  // [maxnb][4]: c_i - c_j, 1/r_j
-  int* nbj = reinterpret_cast<int*>(nbd + 4 * maxnb);  // [maxnb]: j
-  Rl* acc = reinterpret_cast<Rl*>(nbj + ((maxnb + 3) & ~3));  // [NW][G]
-  const int i = blockIdx.x, tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
-  const int k0 = g.inl[i], nn = g.inl[i + 1] - k0;
-  const double4 ci = g.sph[i];
-  for (int b = tid; b < nn; b += 128) {
-    const int j = g.nl[k0 + b];
-    const double4 cj = g.sph[j];
-    nbd[4 * b + 0] = (Rl)(ci.x - cj.x);
-    nbd[4 * b + 1] = (Rl)(ci.y - cj.y);
-    nbd[4 * b + 2] = (Rl)(ci.z - cj.z);
-    nbd[4 * b + 3] = (Rl)(1.0 / cj.w);
-    nbj[b] = j;
-  }
-  for (int q = tid; q < NW * G; q += 128) acc[q] = 0;
-  __syncthreads();
-  const Rl ri = (Rl)ci.w;
-  const Rl eta = (Rl)tb.eta, flow = Rl(1) - eta;
-  const Rl fa = Rl(15) * eta - Rl(12), fb = Rl(10) * eta * eta - Rl(15) * eta + Rl(6);
-  const Rl ie5 = (Rl)(1.0 / (tb.eta * tb.eta * tb.eta * tb.eta * tb.eta));
-  Rl* myacc = acc + w * G;
-  const int q0 = g.pn_ptr[k0], q1 = g.pn_ptr[k0 + nn];
-  for (int base = q0; base < q1; base += 128) {
-    const int q = base + tid;
-    const bool valid = q < q1;
-    Rl val = 0;
-    int n = 0;
-    if (valid) {
-      n = g.pn[q];
-      const int b = g.pn_pair[q];
-      const GP<Rl> gn = grid_pt(g, n, (Rl*)nullptr);
-      const Rl* d = nbd + 4 * b;
-      Rl vx = fma(ri, gn.x, d[0]), vy = fma(ri, gn.y, d[1]), vz = fma(ri, gn.z, d[2]);
-      Rl r2 = vx * vx + vy * vy + vz * vz;
-      Rl rinv = rsqrt_t(r2);
-      Rl t = r2 * rinv * d[3];
-      Rl chi;
-      if (t >= Rl(1)) chi = 0;
-      else if (t <= flow) chi = 1;
-      else {
-        Rl xm = t - Rl(1);
-        chi = (xm * xm * (Rl(1) - t)) * ((Rl(6) * t + fa) * t + fb) * ie5;
-      }
-      Rl W = chi;
-      if (!CHI) {
-        Rl f = (Rl)g.fi[(size_t)i * G + n];
-        if (f > Rl(1)) W = chi / f;
-      }
-      val = W * ylm_dot2<LMAX, Rl>(tb, vx * rinv, vy * rinv, vz * rinv, t,
-                                   XK + (size_t)nbj[b] * NLM);
-    }
-    // same point twice in one warp instruction: sum in lane order first
-    const int key = valid ? n : G + lane;
-    const unsigned grp = __match_any_sync(0xffffffffu, key);
-    Rl s = val;
-    if (__any_sync(0xffffffffu, __popc(grp) > 1)) {
-      s = 0;
-      for (int src = 0; src < 32; ++src) {
-        Rl v = __shfl_sync(0xffffffffu, val, src);
-        if (grp & (1u << src)) s += v;
-      }
-    }
-    if (valid && lane == __ffs(grp) - 1) myacc[n] += s;
-  }
-  __syncthreads();
-  for (int n = tid; n < G; n += 128) {
-    Rl sum = acc[n];
-#pragma unroll
-    for (int ww = 1; ww < NW; ++ww) sum += acc[ww * G + n];
-    pot[(size_t)i * ldp + n] = sum;
-  }
-}
-
 // K-scaled copy of X in (X_{l,m}, X_{l,-m}) pair layout, [N][NLM]
 template <class Rl, bool GAM = false>
 __global__ void k_xk(const YlmTables tb, int nsph, const double* __restrict__ X,
@@ -732,41 +598,8 @@ __global__ void k_xk(const YlmTables tb, int nsph, const double* __restrict__ X,
   XK[e] = mk2<Rl>((Rl)(kk * Xi[ind + m]), m ? (Rl)(kk * Xi[ind - m]) : Rl(0));
 }
 
-template <class Rl>
-size_t lx2_smem(int ngrid, int nbmax) {
-  return sizeof(Rl) * 4 * nbmax + sizeof(int) * ((nbmax + 3) & ~3) + sizeof(Rl) * 4 * ngrid;
-}
-
 #define DDC_LMAX_CASES(X) \
   X(0) X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12)
-
-cudaError_t launch_lx_pot(Launch L, const YlmTables& tb, const DevGeo& g, const double* X,
-                          double* pot, bool chi_only, void* xk) {
-  if (g.nsph == 0) return cudaSuccess;
-  size_t sm = lx2_smem<double>(g.ngrid, g.maxnb);
-  const long long nk = (long long)g.nsph * ((tb.lmax + 1) * (tb.lmax + 2) / 2);
-  double2* XK = static_cast<double2*>(xk);
-  k_xk<double><<<(unsigned)((nk + 255) / 256), 256, 0, L.st>>>(tb, g.nsph, X, XK);
-  ++*L.launches;
-  cudaError_t e = cudaGetLastError();
-  if (e) return e;
-#define CASE(LV)                                                                              \
-  case LV: {                                                                                  \
-    auto kfn = chi_only ? k_lx2<LV, true, double> : k_lx2<LV, false, double>;                 \
-    if ((e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm))) \
-      return e;                                                                               \
-    kfn<<<g.nsph, 128, sm, L.st>>>(tb, g, XK, pot, g.ngrid);                                  \
-    break;                                                                                    \
-  }
-  switch (tb.lmax) {
-    DDC_LMAX_CASES(CASE)
-    default:
-      return cudaErrorInvalidValue;
-  }
-#undef CASE
-  ++*L.launches;
-  return cudaGetLastError();
-}
 
 // ---------------------------------------------------------------------------
 // lstarx (adjrhs ddcosmo.f90:1301-1384, matvec.f90:161-235):
@@ -2714,34 +2547,6 @@ __device__ __forceinline__ float ylm_dot_f(const YlmTables& tb, const AnglesF& a
   return acc;
 }
 
-cudaError_t launch_lx_pot_f32(Launch L, const YlmTables& tb, const DevGeo& g, const double* X,
-                              float* pot, void* xk, int ldp) {
-  if (g.nsph == 0) return cudaSuccess;
-  size_t sm = lx2_smem<float>(g.ngrid, g.maxnb);
-  const long long nk = (long long)g.nsph * ((tb.lmax + 1) * (tb.lmax + 2) / 2);
-  float2* XK = static_cast<float2*>(xk);
-  k_xk<float><<<(unsigned)((nk + 255) / 256), 256, 0, L.st>>>(tb, g.nsph, X, XK);
-  ++*L.launches;
-  cudaError_t e = cudaGetLastError();
-  if (e) return e;
-#define CASE(LV)                                                                              \
-  case LV: {                                                                                  \
-    if ((e = cudaFuncSetAttribute(k_lx2<LV, false, float>,                                    \
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)))     \
-      return e;                                                                               \
-    k_lx2<LV, false, float><<<g.nsph, 128, sm, L.st>>>(tb, g, XK, pot, ldp);                  \
-    break;                                                                                    \
-  }
-  switch (tb.lmax) {
-    DDC_LMAX_CASES(CASE)
-    default:
-      return cudaErrorInvalidValue;
-  }
-#undef CASE
-  ++*L.launches;
-  return cudaGetLastError();
-}
-
 template <int LMAX>
 __global__ void __launch_bounds__(32 * ls_nroles(LMAX)) k_lstarx_f(const YlmTables tb,
                                                                     const DevGeo g,
@@ -2875,12 +2680,13 @@ template <class Rl> __device__ __forceinline__ Rl cBn(const YlmTables& tb, int e
 template <> __device__ __forceinline__ double cBn<double>(const YlmTables& tb, int e) { return tb.Bn[e]; }
 template <> __device__ __forceinline__ float cBn<float>(const YlmTables& tb, int e) { return tb.Bnf[e]; }
 
-template <int LMAX, int M, int OFF, class Rl>
+// LONLY: the lx part only (no L* accumulation)
+template <int LMAX, int M, int OFF, class Rl, bool LONLY = false>
 __device__ __forceinline__ Rl lxs_column(const YlmTables& tb, Rl ct, Rl t2, Rl q0, Rl cm, Rl sm,
                                          Rl c, Rl* acc, const Rl* xr) {
   constexpr int NM = LMAX + 1 - M;
   Rl q1 = 0, dc = 0, ds = 0;
-  const Rl cmc = cm * c, smc = sm * c;
+  const Rl cmc = LONLY ? Rl(0) : cm * c, smc = LONLY ? Rl(0) : sm * c;
 #pragma unroll
   for (int l = M; l <= LMAX; ++l) {
     Rl Q;
@@ -2895,11 +2701,13 @@ __device__ __forceinline__ Rl lxs_column(const YlmTables& tb, Rl ct, Rl t2, Rl q
       q1 = Q;
     }
     if (M == 0) {
-      acc[OFF + l] = fma(Q, c, acc[OFF + l]);
+      if (!LONLY) acc[OFF + l] = fma(Q, c, acc[OFF + l]);
       dc = fma(Q, xr[OFF + l], dc);
     } else {
-      acc[OFF + (l - M)] = fma(Q, cmc, acc[OFF + (l - M)]);
-      acc[OFF + NM + (l - M)] = fma(Q, smc, acc[OFF + NM + (l - M)]);
+      if (!LONLY) {
+        acc[OFF + (l - M)] = fma(Q, cmc, acc[OFF + (l - M)]);
+        acc[OFF + NM + (l - M)] = fma(Q, smc, acc[OFF + NM + (l - M)]);
+      }
       dc = fma(Q, xr[OFF + (l - M)], dc);
       ds = fma(Q, xr[OFF + NM + (l - M)], ds);
     }
@@ -2930,7 +2738,7 @@ __device__ __forceinline__ void lxs_load_role(int role, const typename RT<Rl>::V
 }
 
 // lanes take triples q < count of the chunk's fields sh
-template <int LMAX, int R, class Rl>
+template <int LMAX, int R, class Rl, bool LONLY = false>
 __device__ __forceinline__ void lxs_role(const YlmTables& tb, const Rl* sh, int count, int lane,
                                          Rl* acc, const Rl* xr, Rl* lxp) {
   typedef typename RT<Rl>::V2 V2;
@@ -2945,25 +2753,25 @@ __device__ __forceinline__ void lxs_role(const YlmTables& tb, const Rl* sh, int 
   for (int q = lane; q < count; q += 32) {
     const V4 h = hdr[q];
     const V2 c1 = cs1[q];
-    Rl part = lxs_column<LMAX, M1, 0, Rl>(tb, h.x, h.y, q01[q], c1.x, c1.y, h.z, acc, xr);
+    Rl part = lxs_column<LMAX, M1, 0, Rl, LONLY>(tb, h.x, h.y, q01[q], c1.x, c1.y, h.z, acc, xr);
     if constexpr (ls_has2(LMAX, R)) {
       const V2 c2 = cs2[q];
-      part += lxs_column<LMAX, M2, ls_nvals_m(LMAX, M1), Rl>(tb, h.x, h.y, q02[q], c2.x, c2.y,
-                                                             h.z, acc, xr);
+      part += lxs_column<LMAX, M2, ls_nvals_m(LMAX, M1), Rl, LONLY>(tb, h.x, h.y, q02[q], c2.x,
+                                                                    c2.y, h.z, acc, xr);
     }
     lxp[R * CH + q] = part;
   }
 }
-template <int LMAX, int R, class Rl>
+template <int LMAX, int R, class Rl, bool LONLY = false>
 __device__ __forceinline__ void lxs_run_role(int role, const YlmTables& tb, const Rl* sh,
                                              int count, int lane, Rl* acc, const Rl* xr,
                                              Rl* lxp) {
   if (role == R) {
-    lxs_role<LMAX, R, Rl>(tb, sh, count, lane, acc, xr, lxp);
+    lxs_role<LMAX, R, Rl, LONLY>(tb, sh, count, lane, acc, xr, lxp);
     return;
   }
   if constexpr (R + 1 < ls_nroles(LMAX))
-    lxs_run_role<LMAX, R + 1, Rl>(role, tb, sh, count, lane, acc, xr, lxp);
+    lxs_run_role<LMAX, R + 1, Rl, LONLY>(role, tb, sh, count, lane, acc, xr, lxp);
 }
 
 // the inputs of one triple's shared fields, loaded one chunk ahead
@@ -2982,7 +2790,7 @@ __device__ __forceinline__ LxsIn<Rl> lxs_load(const DevGeo& g, const Rl* __restr
   in.ca = g.sph[an.x];
   in.gn = grid_pt(g, an.y, (Rl*)nullptr);
   in.f = g.fi[pa];
-  in.xv = xi[pa];
+  in.xv = xi ? xi[pa] : Rl(0);
   return in;
 }
 // the shared fields of one triple from its inputs (column col of the buffer)
@@ -3103,7 +2911,7 @@ __device__ __forceinline__ LxsInP<Rl> lxs_load_pre(const DevGeo& g, const Rl* __
   in.g4 = tgeo4_of(g, q, (Rl*)nullptr);
   in.g2 = tgeo2_of(g, q, (Rl*)nullptr);
   in.w = grid_pt(g, an.y, (Rl*)nullptr).w;
-  in.xv = xi[(size_t)an.x * g.ngrid + an.y];
+  in.xv = xi ? xi[(size_t)an.x * g.ngrid + an.y] : Rl(0);
   return in;
 }
 template <int LMAX, class Rl>
@@ -3156,10 +2964,15 @@ cudaError_t launch_lxs_geo_f64(Launch L, const YlmTables& tb, const DevGeo& g, d
 template <class Rl> __host__ __device__ constexpr bool lxs_piped() { return sizeof(Rl) == 4; }
 // Up to lmax 10: three blocks per SM in FP32 (at most 112 registers), two in
 // FP64 (at most 168)
-template <int LMAX, class Rl, bool PRE = false>
+// MODE 0: L x (val) and L* xi (y) together; 1: L x only (xi, y unused);
+// 2: L x only with the weight chi(t) in place of chi(t)/f_a(n) (the u_chi sum
+// of the forces, on-the-fly geometry only)
+template <int LMAX, class Rl, bool PRE = false, int MODE = 0>
 __global__ void __launch_bounds__(32 * ls_nroles(LMAX), LMAX > 10 ? 1 : (sizeof(Rl) == 4 ? 3 : 2))
     k_lxs(const YlmTables tb, const DevGeo g, const typename RT<Rl>::V2* __restrict__ XK,
           const Rl* __restrict__ xi, Rl* __restrict__ val, double* __restrict__ y) {
+  static_assert(!(PRE && MODE == 2), "chi-only weights need the on-the-fly geometry");
+  constexpr bool LONLY = MODE != 0;
   constexpr int NR = ls_nroles(LMAX);
   constexpr int CH = 32 * NR;  // triples per chunk = threads per block
   constexpr int NF = lxs_nfields(LMAX);
@@ -3185,8 +2998,13 @@ __global__ void __launch_bounds__(32 * ls_nroles(LMAX), LMAX > 10 ? 1 : (sizeof(
   // an: the triple's gather-list entry (a, n), loaded a chunk earlier than
   // the inputs that depend on it
   auto load = [&](int q, int2 an) -> In {
-    if constexpr (PRE) return lxs_load_pre<Rl>(g, xi, q, an);
-    else return lxs_load<Rl>(g, xi, q, an);
+    if constexpr (PRE) {
+      return lxs_load_pre<Rl>(g, LONLY ? nullptr : xi, q, an);
+    } else {
+      In in = lxs_load<Rl>(g, LONLY ? nullptr : xi, q, an);
+      if constexpr (MODE == 2) in.f = 1.0;  // W = chi(t)
+      return in;
+    }
   };
   auto fields = [&](const In& in, Rl* buf) {
     if constexpr (PRE) lxs_fields_pre<LMAX, Rl>(in, buf, tid);
@@ -3207,7 +3025,7 @@ __global__ void __launch_bounds__(32 * ls_nroles(LMAX), LMAX > 10 ? 1 : (sizeof(
       const int n2 = k + 2 < nch ? min(CH, q1 - c0 - 2 * CH) : 0;
       if (tid < n1) cur = load(c0 + CH + tid, an1);
       if (tid < n2) an1 = g.ls[c0 + 2 * CH + tid];
-      lxs_run_role<LMAX, 0, Rl>(role, tb, fld, cnt, lane, acc, xr, lxp);
+      lxs_run_role<LMAX, 0, Rl, LONLY>(role, tb, fld, cnt, lane, acc, xr, lxp);
       __syncthreads();
       if (tid < cnt) {
         Rl sv = lxp[tid];
@@ -3216,7 +3034,8 @@ __global__ void __launch_bounds__(32 * ls_nroles(LMAX), LMAX > 10 ? 1 : (sizeof(
         val[c0 + tid] = sv;
       }
     }
-    ls_finish_role<LMAX, 0, Rl, true>(role, tb, acc, y + (size_t)b * tb.nylm, lane);
+    if constexpr (!LONLY)
+      ls_finish_role<LMAX, 0, Rl, true>(role, tb, acc, y + (size_t)b * tb.nylm, lane);
     return;
   }
   if (nch > 0 && tid < min(CH, q1 - q0)) fields(load(q0 + tid, g.ls[q0 + tid]), fld);
@@ -3234,8 +3053,8 @@ __global__ void __launch_bounds__(32 * ls_nroles(LMAX), LMAX > 10 ? 1 : (sizeof(
     if (tid < n1) nxt = load(c0 + CH + tid, an1);
     int2 an2 = make_int2(0, 0);
     if (tid < n2) an2 = g.ls[c0 + 2 * CH + tid];
-    lxs_run_role<LMAX, 0, Rl>(role, tb, fld + (k & 1) * NF * CH, cnt, lane, acc, xr,
-                              lxp + (k & 1) * NR * CH);
+    lxs_run_role<LMAX, 0, Rl, LONLY>(role, tb, fld + (k & 1) * NF * CH, cnt, lane, acc, xr,
+                                     lxp + (k & 1) * NR * CH);
     if (tid < n1) fields(nxt, fld + ((k + 1) & 1) * NF * CH);
     __syncthreads();
     // lx values of chunk k: the roles' shares in role order (buffer k&1 of
@@ -3249,7 +3068,8 @@ __global__ void __launch_bounds__(32 * ls_nroles(LMAX), LMAX > 10 ? 1 : (sizeof(
     }
     an1 = an2;
   }
-  ls_finish_role<LMAX, 0, Rl, true>(role, tb, acc, y + (size_t)b * tb.nylm, lane);
+  if constexpr (!LONLY)
+    ls_finish_role<LMAX, 0, Rl, true>(role, tb, acc, y + (size_t)b * tb.nylm, lane);
 }
 
 // pot_a(n) = sum over a's CSR pairs (a, b) of the lx values of the triples
@@ -3326,7 +3146,7 @@ __global__ void __launch_bounds__(32 * kGatherWarps)
   }
 }
 
-template <class Rl>
+template <class Rl, int MODE>
 static cudaError_t lxs_launch(Launch L, const YlmTables& tb, const DevGeo& g, const double* X,
                               const Rl* xi, void* xk, Rl* val, double* y) {
   if (g.nsph == 0) return cudaSuccess;
@@ -3341,8 +3161,8 @@ static cudaError_t lxs_launch(Launch L, const YlmTables& tb, const DevGeo& g, co
   case LV: {                                                                                  \
     constexpr int NR = ls_nroles(LV);                                                         \
     const size_t sm = sizeof(Rl) * (lxs_piped<Rl>() ? 2 : 1) * (lxs_nfields(LV) + NR) * 32 * NR; \
-    const bool pre = sizeof(Rl) == 4 ? g.tgeo4 != nullptr : g.tgeo4d != nullptr;              \
-    auto kfn = pre ? k_lxs<LV, Rl, true> : k_lxs<LV, Rl, false>;                              \
+    const bool pre = MODE != 2 && (sizeof(Rl) == 4 ? g.tgeo4 != nullptr : g.tgeo4d != nullptr); \
+    auto kfn = pre ? k_lxs<LV, Rl, MODE != 2, MODE> : k_lxs<LV, Rl, false, MODE>;             \
     if (sm > 48 * 1024) {                                                                     \
       if ((e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize,         \
                                     (int)sm)))                                                \
@@ -3382,11 +3202,20 @@ static cudaError_t gather_launch(Launch L, const DevGeo& g, const Rl* val, Rl* p
 }
 cudaError_t launch_lxs(Launch L, const YlmTables& tb, const DevGeo& g, const double* X,
                        const double* xi, void* xk, double* val, double* y) {
-  return lxs_launch<double>(L, tb, g, X, xi, xk, val, y);
+  return lxs_launch<double, 0>(L, tb, g, X, xi, xk, val, y);
 }
 cudaError_t launch_lxs_f32(Launch L, const YlmTables& tb, const DevGeo& g, const double* X,
                            const float* xi, void* xk, float* val, double* y) {
-  return lxs_launch<float>(L, tb, g, X, xi, xk, val, y);
+  return lxs_launch<float, 0>(L, tb, g, X, xi, xk, val, y);
+}
+cudaError_t launch_lx_vals(Launch L, const YlmTables& tb, const DevGeo& g, const double* X,
+                           void* xk, double* val, bool chi_only) {
+  return chi_only ? lxs_launch<double, 2>(L, tb, g, X, nullptr, xk, val, nullptr)
+                  : lxs_launch<double, 1>(L, tb, g, X, nullptr, xk, val, nullptr);
+}
+cudaError_t launch_lx_vals_f32(Launch L, const YlmTables& tb, const DevGeo& g, const double* X,
+                               void* xk, float* val) {
+  return lxs_launch<float, 1>(L, tb, g, X, nullptr, xk, val, nullptr);
 }
 cudaError_t launch_lx_gather(Launch L, const DevGeo& g, const double* val, double* pot) {
   return gather_launch<double>(L, g, val, pot, g.ngrid);
