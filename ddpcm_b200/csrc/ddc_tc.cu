@@ -233,6 +233,39 @@ __global__ void k_pack_static(const double* __restrict__ src, int ld, bool trans
   *reinterpret_cast<float*>(base + kChunk + sw128_off(r, k32)) = lo;
 }
 
+// Accumulation.  The tensor cores round a sum toward zero each time an MMA
+// adds into its accumulator, so a long K loop in one accumulator drifts (a
+// bias of up to 2^-23 of the partial per step: 4-5e-6 of the result over the
+// 590-point projection).  Both kernels therefore keep two accumulators per
+// tile (after Ootomo and Yokota, "Recovering single precision accuracy from
+// Tensor Cores while surpassing the FP32 theoretical peak performance", 2022):
+//   * the main term A_hi*B_hi of one 32-wide K chunk (four MMAs) goes into a
+//     fresh accumulator, which the epilogue warps add into FP32 registers
+//     (round to nearest) before the MMAs of chunk + 2 reuse it (ping-pong);
+//   * the correction terms A_hi*B_lo + A_lo*B_hi, 2^-11 of the main term,
+//     stay in one accumulator over the whole K loop (their rounding is
+//     negligible) and are added at the end.
+// Tensor memory: columns [0, bn) and [bn, 2 bn) hold the two main buffers,
+// [2 bn, 3 bn) the correction.  The epilogue thread (lane quarter q of the
+// 128 rows, column half h) owns columns 16 h + 32 j, j < kMaxJ.
+constexpr int kMaxJ = 5;             // bn <= 32 * kMaxJ = 160
+constexpr int kMaxBn = 32 * kMaxJ;
+
+// acc[16 j + k] += tensor memory (rows 32 q.., columns col0 + 16 h + 32 j + k)
+__device__ __forceinline__ void tmem_add(uint32_t tmem, int q, int half, uint32_t col0, int bn,
+                                         float (&acc)[16 * kMaxJ]) {
+#pragma unroll
+  for (int j = 0; j < kMaxJ; ++j) {
+    const int c = 16 * half + 32 * j;
+    if (c < bn) {
+      float v[16];
+      tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + col0 + (uint32_t)c, v);
+#pragma unroll
+      for (int k = 0; k < 16; ++k) acc[16 * j + k] += v[k];
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // projection: y(lm, i) = alpha sum_n bw(lm, n) pot(n, i), FP64 out
 // ---------------------------------------------------------------------------
@@ -246,7 +279,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   const uint32_t bbytes = (uint32_t)bn * 128;
   const uint32_t sbytes = 2 * kChunk + 2 * bbytes;  // A hi | A lo | B hi | B lo
   uint64_t* bars = reinterpret_cast<uint64_t*>(sm + (size_t)nstage * sbytes);
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 3 * nstage + 1);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 3 * nstage + 5);
   volatile int* abort = reinterpret_cast<volatile int*>(tslot + 1);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int i0 = blockIdx.x * bn;
@@ -255,23 +288,30 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   auto FULL = [&](int s) { return bar0 + 8u * s; };
   auto READY = [&](int s) { return bar0 + 8u * (nstage + s); };
   auto EMPTY = [&](int s) { return bar0 + 8u * (2 * nstage + s); };
-  const uint32_t ACCF = bar0 + 8u * (3 * nstage);
+  auto MFULL = [&](int b) { return bar0 + 8u * (3 * nstage + b); };
+  auto MEMPTY = [&](int b) { return bar0 + 8u * (3 * nstage + 2 + b); };
+  const uint32_t DONE = bar0 + 8u * (3 * nstage + 4);
   if (threadIdx.x == 0) {
     for (int s = 0; s < nstage; ++s) {
       mbar_init(FULL(s), 1);
       mbar_init(READY(s), kSplitWarps);
       mbar_init(EMPTY(s), 1);
     }
-    mbar_init(ACCF, 1);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(MFULL(b), 1);
+      mbar_init(MEMPTY(b), kSplitWarps);
+    }
+    mbar_init(DONE, 1);
     *abort = 0;
     fence_barrier_init();
   }
-  const uint32_t ncols = tmem_cols(bn);
+  const uint32_t ncols = tmem_cols(3 * bn);
   if (warp == 1) tmem_alloc(su32(tslot), ncols);
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tslot;
+  const uint32_t corr = tmem + (uint32_t)(2 * bn);
 
   if (warp == 0) {
     if (lane == 0) {
@@ -294,67 +334,94 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     if (lane == 0) {
       const uint32_t idesc = idesc_tf32(128, bn);
       for (int kc = 0; kc < kcn; ++kc) {
-        const int s = kc % nstage;
+        const int s = kc % nstage, b = kc & 1;
         const uint32_t ph = (uint32_t)(kc / nstage) & 1u;
         if (!mbar_wait(READY(s), ph, abort, err, 2)) break;
+        if (kc >= 2 && !mbar_wait(MEMPTY(b), (uint32_t)((kc >> 1) - 1) & 1u, abort, err, 5))
+          break;
         tc_fence_after();
         const uint32_t st = sbase + s * sbytes;
         const uint64_t ah = sw128_desc(st), al = sw128_desc(st + kChunk);
         const uint64_t bh = sw128_desc(st + 2 * kChunk), bl = sw128_desc(st + 2 * kChunk + bbytes);
+        const uint32_t mainb = tmem + (uint32_t)(b * bn);
 #pragma unroll
         for (int ks = 0; ks < 4; ++ks) {
           const uint64_t o = (uint64_t)(ks * 2);  // 32 bytes along K, in 16-byte units
-          mma_tf32(tmem, ah + o, bh + o, idesc, (kc | ks) != 0);
-          mma_tf32(tmem, ah + o, bl + o, idesc, 1);
-          mma_tf32(tmem, al + o, bh + o, idesc, 1);
+          mma_tf32(mainb, ah + o, bh + o, idesc, ks != 0);
+          mma_tf32(corr, ah + o, bl + o, idesc, (kc | ks) != 0);
+          mma_tf32(corr, al + o, bh + o, idesc, 1);
         }
         mma_commit(EMPTY(s));
+        mma_commit(MFULL(b));
       }
-      mma_commit(ACCF);
+      mma_commit(DONE);
     }
   } else {
     const int t = threadIdx.x - 64;
-    for (int kc = 0; kc < kcn; ++kc) {
-      const int s = kc % nstage;
-      const uint32_t ph = (uint32_t)(kc / nstage) & 1u;
-      if (!mbar_wait(FULL(s), ph, abort, err, 3)) break;
-      float4* bh = reinterpret_cast<float4*>(sm + (size_t)s * sbytes + 2 * kChunk);
-      float4* bl = reinterpret_cast<float4*>(sm + (size_t)s * sbytes + 2 * kChunk + bbytes);
-      for (int e = t; e < (int)(bbytes / 16); e += 32 * kSplitWarps) {
-        const float4 v = bh[e];
-        float4 h, l;
-        split_f32(v.x, h.x, l.x);
-        split_f32(v.y, h.y, l.y);
-        split_f32(v.z, h.z, l.z);
-        split_f32(v.w, h.w, l.w);
-        bh[e] = h;
-        bl[e] = l;
-      }
-      fence_proxy_async();
-      __syncwarp();
-      if (lane == 0) mbar_arrive(READY(s));
-    }
-    if (mbar_wait(ACCF, 0, abort, err, 4)) {
-      tc_fence_after();
-      const int q = warp & 3, half = (warp - 2) >> 2;
-      const int lm = 32 * q + lane;
-      for (int c0 = 16 * half; c0 < bn; c0 += 32) {
-        float v[16];
-        tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)c0, v);
-        if (lm < nylm) {
+    const int q = warp & 3, half = (warp - 2) >> 2;
+    float acc[16 * kMaxJ];
 #pragma unroll
-          for (int j = 0; j < 16; ++j) {
-            const int i = i0 + c0 + j;
-            if (i < nsph) y[(size_t)i * nylm + lm] = alpha * (double)v[j];
-          }
+    for (int k = 0; k < 16 * kMaxJ; ++k) acc[k] = 0.f;
+    bool ok = true;
+    // split chunk kc, then add the main term of chunk kc - 1 (the MMAs of kc
+    // run meanwhile)
+    for (int kc = 0; ok && kc <= kcn; ++kc) {
+      if (kc < kcn) {
+        const int s = kc % nstage;
+        const uint32_t ph = (uint32_t)(kc / nstage) & 1u;
+        if (!mbar_wait(FULL(s), ph, abort, err, 3)) {
+          ok = false;
+          break;
         }
+        float4* bh = reinterpret_cast<float4*>(sm + (size_t)s * sbytes + 2 * kChunk);
+        float4* bl = reinterpret_cast<float4*>(sm + (size_t)s * sbytes + 2 * kChunk + bbytes);
+        for (int e = t; e < (int)(bbytes / 16); e += 32 * kSplitWarps) {
+          const float4 v = bh[e];
+          float4 h, l;
+          split_f32(v.x, h.x, l.x);
+          split_f32(v.y, h.y, l.y);
+          split_f32(v.z, h.z, l.z);
+          split_f32(v.w, h.w, l.w);
+          bh[e] = h;
+          bl[e] = l;
+        }
+        fence_proxy_async();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(READY(s));
+      }
+      if (kc >= 1) {
+        const int c = kc - 1, b = c & 1;
+        if (!mbar_wait(MFULL(b), (uint32_t)(c >> 1) & 1u, abort, err, 4)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        tmem_add(tmem, q, half, (uint32_t)(b * bn), bn, acc);
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(MEMPTY(b));
+      }
+    }
+    if (ok && mbar_wait(DONE, 0, abort, err, 6)) {
+      tc_fence_after();
+      tmem_add(tmem, q, half, (uint32_t)(2 * bn), bn, acc);
+      const int lm = 32 * q + lane;
+      if (lm < nylm) {
+#pragma unroll
+        for (int j = 0; j < kMaxJ; ++j)
+#pragma unroll
+          for (int k = 0; k < 16; ++k) {
+            const int i = i0 + 16 * half + 32 * j + k;
+            if (16 * half + 32 * j < bn && i < nsph)
+              y[(size_t)i * nylm + lm] = alpha * (double)acc[16 * j + k];
+          }
       }
     }
   }
   tc_fence_before();
   __syncthreads();
   if (warp == 1) {
-    if (*abort && lane == 0) mbar_drain(ACCF, 0);  // MMAs issued before giving up
+    if (*abort && lane == 0) mbar_drain(DONE, 0);  // MMAs issued before giving up
     __syncwarp();
     tc_fence_after();
     tmem_dealloc(tmem, ncols);
@@ -374,7 +441,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   unsigned char* bsm = sm;                                   // kcn x (B hi | B lo)
   unsigned char* asm_ = sm + (size_t)kcn * 2 * bbytes;       // nstage x (A hi | A lo)
   uint64_t* bars = reinterpret_cast<uint64_t*>(asm_ + (size_t)nstage * 2 * kChunk);
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 2 * nstage + 6);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 2 * nstage + 8);
   volatile int* abort = reinterpret_cast<volatile int*>(tslot + 1);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int i0 = blockIdx.x * bn;
@@ -382,29 +449,34 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   auto FULL = [&](int st) { return bar0 + 8u * st; };
   auto EMPTY = [&](int st) { return bar0 + 8u * (nstage + st); };
   const uint32_t BREADY = bar0 + 8u * (2 * nstage);
-  auto ACCF = [&](int a) { return bar0 + 8u * (2 * nstage + 1 + a); };
-  auto ACCE = [&](int a) { return bar0 + 8u * (2 * nstage + 3 + a); };
-  const uint32_t DONE = bar0 + 8u * (2 * nstage + 5);
+  auto MFULL = [&](int b) { return bar0 + 8u * (2 * nstage + 1 + b); };
+  auto MEMPTY = [&](int b) { return bar0 + 8u * (2 * nstage + 3 + b); };
+  const uint32_t CFULL = bar0 + 8u * (2 * nstage + 5);
+  const uint32_t CEMPTY = bar0 + 8u * (2 * nstage + 6);
+  const uint32_t DONE = bar0 + 8u * (2 * nstage + 7);
   if (threadIdx.x == 0) {
     for (int st = 0; st < nstage; ++st) {
       mbar_init(FULL(st), 1);
       mbar_init(EMPTY(st), 1);
     }
     mbar_init(BREADY, kSplitWarps);
-    for (int a = 0; a < 2; ++a) {
-      mbar_init(ACCF(a), 1);
-      mbar_init(ACCE(a), kSplitWarps);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(MFULL(b), 1);
+      mbar_init(MEMPTY(b), kSplitWarps);
     }
+    mbar_init(CFULL, 1);
+    mbar_init(CEMPTY, kSplitWarps);
     mbar_init(DONE, 1);
     *abort = 0;
     fence_barrier_init();
   }
-  const uint32_t ncols = tmem_cols(2 * bn);
+  const uint32_t ncols = tmem_cols(3 * bn);
   if (warp == 1) tmem_alloc(su32(tslot), ncols);
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tslot;
+  const uint32_t corr = tmem + (uint32_t)(2 * bn);
   const int nit = mtn * kcn;
 
   if (warp == 0) {
@@ -428,32 +500,30 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       const uint32_t idesc = idesc_tf32(128, bn);
       const uint32_t abase = su32(asm_), bbase = su32(bsm);
       bool ok = mbar_wait(BREADY, 0, abort, err, 12);
-      for (int mt = 0; ok && mt < mtn; ++mt) {
-        const int a = mt & 1;
-        if (mt >= 2 && !mbar_wait(ACCE(a), (uint32_t)((mt >> 1) - 1) & 1u, abort, err, 13)) break;
+      for (int it = 0; ok && it < nit; ++it) {
+        const int mt = it / kcn, kc = it - mt * kcn, st = it % nstage, b = it & 1;
+        if (!mbar_wait(FULL(st), (uint32_t)(it / nstage) & 1u, abort, err, 14)) break;
+        if (it >= 2 && !mbar_wait(MEMPTY(b), (uint32_t)((it >> 1) - 1) & 1u, abort, err, 13))
+          break;
+        // the correction accumulator of the previous grid tile has been read
+        if (kc == 0 && mt >= 1 && !mbar_wait(CEMPTY, (uint32_t)(mt - 1) & 1u, abort, err, 16))
+          break;
         tc_fence_after();
-        const uint32_t d = tmem + (uint32_t)(a * bn);
-        for (int kc = 0; kc < kcn; ++kc) {
-          const int it = mt * kcn + kc, st = it % nstage;
-          if (!mbar_wait(FULL(st), (uint32_t)(it / nstage) & 1u, abort, err, 14)) {
-            ok = false;
-            break;
-          }
-          tc_fence_after();
-          const uint64_t ah = sw128_desc(abase + st * 2 * kChunk);
-          const uint64_t al = sw128_desc(abase + st * 2 * kChunk + kChunk);
-          const uint64_t bh = sw128_desc(bbase + kc * 2 * bbytes);
-          const uint64_t bl = sw128_desc(bbase + kc * 2 * bbytes + bbytes);
+        const uint64_t ah = sw128_desc(abase + st * 2 * kChunk);
+        const uint64_t al = sw128_desc(abase + st * 2 * kChunk + kChunk);
+        const uint64_t bh = sw128_desc(bbase + kc * 2 * bbytes);
+        const uint64_t bl = sw128_desc(bbase + kc * 2 * bbytes + bbytes);
+        const uint32_t mainb = tmem + (uint32_t)(b * bn);
 #pragma unroll
-          for (int ks = 0; ks < 4; ++ks) {
-            const uint64_t o = (uint64_t)(ks * 2);
-            mma_tf32(d, ah + o, bh + o, idesc, (kc | ks) != 0);
-            mma_tf32(d, ah + o, bl + o, idesc, 1);
-            mma_tf32(d, al + o, bh + o, idesc, 1);
-          }
-          mma_commit(EMPTY(st));
+        for (int ks = 0; ks < 4; ++ks) {
+          const uint64_t o = (uint64_t)(ks * 2);
+          mma_tf32(mainb, ah + o, bh + o, idesc, ks != 0);
+          mma_tf32(corr, ah + o, bl + o, idesc, (kc | ks) != 0);
+          mma_tf32(corr, al + o, bh + o, idesc, 1);
         }
-        if (ok) mma_commit(ACCF(a));
+        mma_commit(EMPTY(st));
+        mma_commit(MFULL(b));
+        if (kc == kcn - 1) mma_commit(CFULL);
       }
       mma_commit(DONE);  // completes once every MMA issued above has
     }
@@ -489,25 +559,35 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     __syncwarp();
     if (lane == 0) mbar_arrive(BREADY);
     const int q = warp & 3, half = (warp - 2) >> 2;
-    for (int mt = 0; mt < mtn; ++mt) {
-      const int a = mt & 1;
-      if (!mbar_wait(ACCF(a), (uint32_t)(mt >> 1) & 1u, abort, err, 15)) break;
-      tc_fence_after();
-      const int m = mt * 128 + 32 * q + lane;
-      for (int c0 = 16 * half; c0 < bn; c0 += 32) {
-        float v[16];
-        tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(a * bn + c0), v);
-        if (m < ngrid) {
+    float acc[16 * kMaxJ];
 #pragma unroll
-          for (int j = 0; j < 16; ++j) {
-            const int i = i0 + c0 + j;
-            if (i < nsph) xi[(size_t)i * ngrid + m] = v[j];
-          }
-        }
-      }
+    for (int k = 0; k < 16 * kMaxJ; ++k) acc[k] = 0.f;
+    for (int it = 0; it < nit; ++it) {
+      const int mt = it / kcn, kc = it - mt * kcn, b = it & 1;
+      if (!mbar_wait(MFULL(b), (uint32_t)(it >> 1) & 1u, abort, err, 15)) break;
+      tc_fence_after();
+      tmem_add(tmem, q, half, (uint32_t)(b * bn), bn, acc);
       tc_fence_before();
       __syncwarp();
-      if (lane == 0) mbar_arrive(ACCE(a));
+      if (lane == 0) mbar_arrive(MEMPTY(b));
+      if (kc == kcn - 1) {
+        if (!mbar_wait(CFULL, (uint32_t)mt & 1u, abort, err, 17)) break;
+        tc_fence_after();
+        tmem_add(tmem, q, half, (uint32_t)(2 * bn), bn, acc);
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(CEMPTY);
+        const int m = mt * 128 + 32 * q + lane;
+#pragma unroll
+        for (int j = 0; j < kMaxJ; ++j)
+#pragma unroll
+          for (int k = 0; k < 16; ++k) {
+            const int i = i0 + 16 * half + 32 * j + k;
+            if (m < ngrid && 16 * half + 32 * j < bn && i < nsph)
+              xi[(size_t)i * ngrid + m] = acc[16 * j + k];
+            acc[16 * j + k] = 0.f;
+          }
+      }
     }
   }
   tc_fence_before();
@@ -544,8 +624,8 @@ EncodeTiledFn encode_fn() {
 // (the MMA's N step), at most `cap`
 int pick_bn(int nsph, int cap) {
   int want = (nsph + 147) / 148;
-  want = ((want + 15) / 16) * 16;
-  return std::max(16, std::min(cap, want));
+  want = ((want + 31) / 32) * 32;
+  return std::max(32, std::min(cap, want));
 }
 
 }  // namespace
@@ -557,6 +637,7 @@ namespace {
 // tile width bn of the projection: pipeline depth, shared memory and the TMA
 // box of the grid field (bn rows of 32 values)
 cudaError_t cfg_proj(TcPlan& p, int bn) {
+  if (bn % 32 != 0 || bn > kMaxBn) return cudaErrorInvalidValue;
   const int sb = 2 * kChunk + 2 * bn * 128;
   p.bn_proj = bn;
   p.ns_proj = std::min(4, (kSmemCap - kSmemSlack) / sb);
@@ -577,9 +658,10 @@ cudaError_t cfg_proj(TcPlan& p, int bn) {
 // tile width of the expansion: the split coefficients of bn spheres stay
 // resident, the basis chunks stream through a ring of at least two stages
 cudaError_t cfg_xi(TcPlan& p, int bn) {
+  if (bn % 32 != 0 || bn > kMaxBn) return cudaErrorInvalidValue;
   const int bsz = p.kc_xi * 2 * bn * 128;
   const int ns = std::min(3, (kSmemCap - kSmemSlack - bsz) / (2 * kChunk));
-  if (ns < 2 || 2 * bn > 512) return cudaErrorInvalidValue;
+  if (ns < 2) return cudaErrorInvalidValue;
   p.bn_xi = bn;
   p.ns_xi = ns;
   p.smem_xi = std::max(bsz + ns * 2 * kChunk + kSmemSlack, 120 * 1024);
@@ -587,9 +669,9 @@ cudaError_t cfg_xi(TcPlan& p, int bn) {
 }
 std::vector<int> bn_candidates(int nsph) {
   std::vector<int> c;
-  const int top = std::min(256, (nsph + 15) / 16 * 16);
-  for (int bn : {pick_bn(nsph, 256), 32, 64, 96, 128, 160, 192, 256})
-    if (bn >= 16 && bn <= top && std::find(c.begin(), c.end(), bn) == c.end()) c.push_back(bn);
+  const int top = std::min(kMaxBn, std::max(32, (nsph + 31) / 32 * 32));
+  for (int bn : {pick_bn(nsph, kMaxBn), 32, 64, 96, 128, 160})
+    if (bn <= top && std::find(c.begin(), c.end(), bn) == c.end()) c.push_back(bn);
   return c;
 }
 
@@ -615,11 +697,11 @@ cudaError_t tc_plan(Launch L, TcPlan& p, const double* basis, const double* bw, 
   cudaError_t e;
   // default tile widths: about one tile per SM (narrower where the shared
   // memory of a wide tile does not fit)
-  int bn = pick_bn(nsph, 256);
-  while ((e = cfg_proj(p, bn)) == cudaErrorInvalidValue && bn > 16) bn -= 16;
+  int bn = pick_bn(nsph, kMaxBn);
+  while ((e = cfg_proj(p, bn)) == cudaErrorInvalidValue && bn > 32) bn -= 32;
   if (e) return e;
-  bn = pick_bn(nsph, 256);
-  while ((e = cfg_xi(p, bn)) == cudaErrorInvalidValue && bn > 16) bn -= 16;
+  bn = pick_bn(nsph, kMaxBn);
+  while ((e = cfg_xi(p, bn)) == cudaErrorInvalidValue && bn > 32) bn -= 32;
   if (e) return e;
   // static operands, split once
   if ((e = p.img_proj.ensure((size_t)p.kc_proj * 2 * kChunk))) return e;

@@ -88,7 +88,8 @@ def test_training_lowers_the_loss():
     model.fit_scaling(f.data_ptr(), t.data_ptr(), n)
     model.init_random(5)
     losses = [model.train_epoch(f.data_ptr(), t.data_ptr(), 0, n, 128, 2e-3) for _ in range(12)]
-    assert losses[-1] < 0.7 * losses[0], losses
+    assert losses[-1] < 0.8 * losses[0], losses
+    assert all(b < a for a, b in zip(losses[:4], losses[1:5])), losses
 
 
 def _solve(mol, guess, model=None, precision=0):

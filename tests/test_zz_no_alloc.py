@@ -71,7 +71,11 @@ def test_efld_noalloc_matches_efld_on_consecutive_calls():
                        handle)
                 assert st == 0
                 torch.cuda.synchronize(dev)
-                np.testing.assert_allclose(d_ef.cpu().numpy(), ref, rtol=1e-13, atol=1e-18)
+                # the chunk count (and with it the summation order) may differ
+                # from ddc_efld's: agreement to 1e-13 of the field's scale
+                got = d_ef.cpu().numpy()
+                assert np.isfinite(got).all()
+                assert np.abs(got - ref).max() <= 1e-13 * np.abs(ref).max()
 
 
 def test_efld_noalloc_rejects_sizes_beyond_its_scratch():
