@@ -680,7 +680,6 @@ std::vector<int> bn_candidates(int nsph) {
 cudaError_t tc_plan(Launch L, TcPlan& p, const double* basis, const double* bw, int nsph,
                     int nylm, int ngrid, float* pot_f, int ldp) {
   p.on = false;
-  p.tuned = false;
   if (!tc_supported(nylm) || nsph <= 0) return cudaSuccess;
   if (!encode_fn()) return cudaErrorNotSupported;
   // the per-call grid field: [nsph][ngrid] FP32 rows ldp apart (16-byte multiple)
@@ -733,9 +732,9 @@ cudaError_t tc_plan(Launch L, TcPlan& p, const double* basis, const double* bw, 
 cudaError_t tc_autotune(Launch L, TcPlan& p, const double* s, double* y, float* xi) {
   if (!p.on) return cudaSuccess;
   const long long key = ((long long)p.nsph << 24) ^ ((long long)p.nylm << 12) ^ p.ngrid;
-  if (p.tuned && p.tune_key == key) {
-    cudaError_t e = cfg_proj(p, p.bn_proj);
-    return e ? e : cfg_xi(p, p.bn_xi);
+  if (p.tuned && p.tune_key == key) {  // same shape as the last measurement
+    cudaError_t e = cfg_proj(p, p.tuned_bn_proj);
+    return e ? e : cfg_xi(p, p.tuned_bn_xi);
   }
   cudaEvent_t e0, e1;
   cudaError_t e;
@@ -795,6 +794,8 @@ cudaError_t tc_autotune(Launch L, TcPlan& p, const double* s, double* y, float* 
   if (!e) {
     p.tuned = true;
     p.tune_key = key;
+    p.tuned_bn_proj = p.bn_proj;
+    p.tuned_bn_xi = p.bn_xi;
   }
   return e;
 }
