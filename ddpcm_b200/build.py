@@ -9,7 +9,6 @@ Host code is compiled with ``-ffp-contract=off`` so that the Lebedev grid and
 the normalisation tables follow the written operation order.
 """
 import os
-import shutil
 import subprocess
 import sys
 
@@ -27,12 +26,6 @@ def nvcc():
         if p and (os.path.sep not in p or os.path.exists(p)):
             return p
     return "nvcc"
-
-
-def cuda_libdir():
-    """The toolkit's library directory beside nvcc (cuBLAS is linked from it)."""
-    root = os.path.dirname(os.path.dirname(os.path.realpath(shutil.which(nvcc()) or nvcc())))
-    return os.path.join(root, "lib64")
 
 
 def _stale():

@@ -1085,12 +1085,8 @@ int task_after(ddc_ctx* ctx, SolveTask& t) {
   }
   // correction: (D + O32) e = r from e = D^-1 r
   CK(cudaMemcpyAsync(t.b.e, t.b.d, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx->st));
-  // the inner stop test bounds the inner increment, and the error of an
-  // iterate is about increment / (1 - rate) with a rate near 0.8: the floor
-  // at 0.1 tol leaves the next FP64 check below tol instead of just above it
-  // (which would cost a whole extra refinement)
   const double rho = 1e-5;
-  const double itol = std::max(rho * t.last, 0.1 * t.tol);
+  const double itol = std::max(rho * t.last, 0.3 * t.tol);
   // the correction is wanted to ~1e-5 relative: FP32 history vectors suffice
   jd_begin(ctx, t.jd, t.b.r, t.b.e, itol, t.budget, t.b, t.inf, &t.logpos, true);
   t.phase = 1;

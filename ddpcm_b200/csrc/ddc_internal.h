@@ -232,16 +232,11 @@ cudaError_t launch_lx_gather_f32(Launch L, const DevGeo& g, const float* val, fl
 cudaError_t launch_lstarx_acc_f32(Launch L, const YlmTables& tb, const DevGeo& g,
                                   const float* xi, double* y);
 cudaError_t launch_to_float(Launch L, long long n, const double* x, float* y);
-cudaError_t launch_to_double(Launch L, long long n, const float* x, double* y);
 // r = rhs - y - x/facl ; d = facl*r (Jacobi increment at x), partial H-norm of d
 cudaError_t launch_residual(Launch L, const YlmTables& tb, long long n, const double* rhs,
                             const double* y, const double* x, double* r, double* d,
                             double* partials, int nblk);
 cudaError_t launch_axpy(Launch L, long long n, double a, const double* x, double* y);
-// C[M x N] = alpha * op(A) * B (+ beta*C), column-major FP64
-cudaError_t launch_dgemm(Launch L, bool transA, int M, int N, int K, double alpha,
-                         const double* A, int lda, const double* B, int ldb, double beta,
-                         double* C, int ldc);
 // dst[c*rows + r] = src[r*cols + c] (FP64)
 cudaError_t launch_transpose(Launch L, int rows, int cols, const double* src, double* dst);
 // C[n*ldc + m] = alpha * sum_k A[k*lda + m] B[n*ldb + k] (FP64, pipelined)

@@ -825,72 +825,13 @@ cudaError_t launch_lstarx_acc(Launch L, const YlmTables& tb, const DevGeo& g, co
 }
 
 // ---------------------------------------------------------------------------
-// FP64 GEMM, column-major: C = alpha op(A) B + beta C.  Used for the
-// projection (intrhs, ddcosmo.f90:789-821) C(nylm,N) = -Bw(nylm,G) pot(G,N)
-// and for xi(G,N) = basis^T(G,nylm) S(nylm,N) (matvec.f90:189-204).
-// 64x64 tile, 256 threads, 4x4 outputs per thread.
+// Register-tiled SIMT GEMM, column-major C[M x N] = alpha * op(A) * B: the
+// FP32 projection and expansion of the mixed path when the harmonics do not
+// fit one 128-row tensor-core tile (lmax 11, 12).  BM x BN tile per block,
+// BK deep, TM x TN outputs per thread, shared tiles double buffered with the
+// next tile prefetched into registers.  Acc is the arithmetic/accumulation
+// type; inputs are converted when staged.
 // ---------------------------------------------------------------------------
-constexpr int GBM = 64, GBN = 64, GBK = 16;
-template <bool TA>
-__global__ void __launch_bounds__(256) k_dgemm(int M, int N, int K, double alpha,
-                                               const double* __restrict__ A, int lda,
-                                               const double* __restrict__ B, int ldb, double beta,
-                                               double* C, int ldc) {
-  __shared__ double As[GBK][GBM + 1];
-  __shared__ double Bs[GBK][GBN + 1];
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  const int m0 = blockIdx.x * GBM, n0 = blockIdx.y * GBN;
-  double acc[4][4];
-#pragma unroll
-  for (int a = 0; a < 4; ++a)
-#pragma unroll
-    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
-  for (int k0 = 0; k0 < K; k0 += GBK) {
-    for (int e = threadIdx.x; e < GBM * GBK; e += 256) {
-      int mm, kk;
-      if (TA) { kk = e % GBK; mm = e / GBK; } else { mm = e % GBM; kk = e / GBM; }
-      int m = m0 + mm, k = k0 + kk;
-      double v = 0.0;
-      if (m < M && k < K) v = TA ? A[(size_t)m * lda + k] : A[(size_t)k * lda + m];
-      As[kk][mm] = v;
-    }
-    for (int e = threadIdx.x; e < GBK * GBN; e += 256) {
-      int kk = e % GBK, nn = e / GBK;
-      int n = n0 + nn, k = k0 + kk;
-      Bs[kk][nn] = (n < N && k < K) ? B[(size_t)n * ldb + k] : 0.0;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int kk = 0; kk < GBK; ++kk) {
-      double a[4], b[4];
-#pragma unroll
-      for (int r = 0; r < 4; ++r) a[r] = As[kk][ty + 16 * r];
-#pragma unroll
-      for (int c = 0; c < 4; ++c) b[c] = Bs[kk][tx + 16 * c];
-#pragma unroll
-      for (int r = 0; r < 4; ++r)
-#pragma unroll
-        for (int c = 0; c < 4; ++c) acc[r][c] = fma(a[r], b[c], acc[r][c]);
-    }
-    __syncthreads();
-  }
-#pragma unroll
-  for (int r = 0; r < 4; ++r)
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      int m = m0 + ty + 16 * r, n = n0 + tx + 16 * c;
-      if (m < M && n < N) {
-        double* p = C + (size_t)n * ldc + m;
-        *p = beta == 0.0 ? alpha * acc[r][c] : alpha * acc[r][c] + beta * *p;
-      }
-    }
-}
-// Register-tiled GEMM, column-major C[M x N] = alpha * op(A) * B, used for
-// the one-off right-hand-side projections (M = nylm <= 128 rows in one
-// tile); the operators' per-iteration GEMMs go through cuBLAS.  BM x BN
-// tile per block, BK deep, TM x TN outputs per thread, shared tiles double
-// buffered with the next tile prefetched into registers.  Acc is the
-// arithmetic/accumulation type; inputs are converted when staged.
 template <bool TA, class TAin, class TBin, class TC, class Acc, int BM, int BN, int BK, int TM,
           int TN>
 __global__ void __launch_bounds__((BM / TM) * (BN / TN)) k_gemm2(int M, int N, int K, Acc alpha,
@@ -998,6 +939,11 @@ cudaError_t gemm2(Launch L, int M, int N, int K, Acc alpha, const TAin* A, int l
 // accumulating an 8 x 4 block from vector shared-memory reads.
 namespace dgp {
 constexpr int BM = 128, BN = 64, BK = 16;
+// B rows padded by two doubles: the copies write 16 consecutive k of one
+// column, which would otherwise fall into one bank group (row stride 512 B);
+// with 528 B they spread over 16 banks (two-way), and rows stay 16-byte aligned
+constexpr int BNP = BN + 2;
+constexpr int SMEM = (2 * BK * BM + 2 * BK * BNP) * 8;
 }
 __device__ __forceinline__ void cp_async8(void* sdst, const void* gsrc, bool valid) {
   const uint32_t d = (uint32_t)__cvta_generic_to_shared(sdst);
@@ -1010,8 +956,9 @@ __global__ void __launch_bounds__(256) k_dgemm_cp(int M, int N, int K, double al
                                                   const double* __restrict__ B, int ldb,
                                                   double* __restrict__ C, int ldc) {
   using namespace dgp;
-  __shared__ __align__(16) double As[2][BK][BM];
-  __shared__ __align__(16) double Bs[2][BK][BN];
+  extern __shared__ __align__(16) double dg_smem[];
+  double(*As)[BK][BM] = reinterpret_cast<double(*)[BK][BM]>(dg_smem);
+  double(*Bs)[BK][BNP] = reinterpret_cast<double(*)[BK][BNP]>(dg_smem + 2 * BK * BM);
   const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
   const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
   auto load = [&](int buf, int k0) {
@@ -1102,7 +1049,10 @@ cudaError_t launch_dgemm_nn(Launch L, int M, int N, int K, double alpha, const d
                             int lda, const double* B, int ldb, double* C, int ldc) {
   if (M == 0 || N == 0) return cudaSuccess;
   dim3 grid((M + dgp::BM - 1) / dgp::BM, (N + dgp::BN - 1) / dgp::BN);
-  k_dgemm_cp<<<grid, 256, 0, L.st>>>(M, N, K, alpha, A, lda, B, ldb, C, ldc);
+  cudaError_t e = cudaFuncSetAttribute(k_dgemm_cp, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       dgp::SMEM);
+  if (e) return e;
+  k_dgemm_cp<<<grid, 256, dgp::SMEM, L.st>>>(M, N, K, alpha, A, lda, B, ldb, C, ldc);
   ++*L.launches;
   return cudaGetLastError();
 }
@@ -1120,23 +1070,6 @@ cudaError_t launch_xi_f32_simt(Launch L, int nylm, int nsph, int ngrid, const fl
                                                   nylm, xi, ngrid);
 }
 
-cudaError_t launch_dgemm(Launch L, bool transA, int M, int N, int K, double alpha,
-                         const double* A, int lda, const double* B, int ldb, double beta,
-                         double* C, int ldc) {
-  if (M == 0 || N == 0) return cudaSuccess;
-  if (beta == 0.0)
-    return transA ? gemm2<true, double, double, double, double>(L, M, N, K, alpha, A, lda, B, ldb,
-                                                                C, ldc)
-                  : gemm2<false, double, double, double, double>(L, M, N, K, alpha, A, lda, B,
-                                                                 ldb, C, ldc);
-  dim3 grid((M + GBM - 1) / GBM, (N + GBN - 1) / GBN);
-  if (transA)
-    k_dgemm<true><<<grid, 256, 0, L.st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
-  else
-    k_dgemm<false><<<grid, 256, 0, L.st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
-  ++*L.launches;
-  return cudaGetLastError();
-}
 
 // wghpot (ddcosmo.f90:1187-1224): g(n,i) = -ui * phi(cavity index)
 __global__ void k_wghpot(long long np, const double* __restrict__ ui, const int* __restrict__ cavidx,
@@ -3232,16 +3165,6 @@ __global__ void k_to_float(long long n, const double* __restrict__ x, float* y) 
 cudaError_t launch_to_float(Launch L, long long n, const double* x, float* y) {
   if (n == 0) return cudaSuccess;
   k_to_float<<<(unsigned)((n + 255) / 256), 256, 0, L.st>>>(n, x, y);
-  ++*L.launches;
-  return cudaGetLastError();
-}
-__global__ void k_to_double(long long n, const float* __restrict__ x, double* y) {
-  long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (e < n) y[e] = (double)x[e];
-}
-cudaError_t launch_to_double(Launch L, long long n, const float* x, double* y) {
-  if (n == 0) return cudaSuccess;
-  k_to_double<<<(unsigned)((n + 255) / 256), 256, 0, L.st>>>(n, x, y);
   ++*L.launches;
   return cudaGetLastError();
 }
