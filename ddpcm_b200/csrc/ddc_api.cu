@@ -164,6 +164,11 @@ struct ddc_ctx {
   ddc_guess* gmodel = nullptr;
   DBuf gfeat;
   bool have_flow = false, guess_preset = false;
+  // near / far split of the solute potential and field at the cavity:
+  // tables of degree kFarDegree on the grid, the per-sphere expansions
+  YlmTables tbP{};
+  DBuf farBT, farDT, farA;
+  bool far_on = false;
   // pinned landing buffer of the small device-to-host reads (reduced sums)
   double* hred = nullptr;
   // second stream of the force tail: the field of zeta at the nuclei runs
@@ -329,10 +334,8 @@ struct StageScope {
   }
 };
 
-void build_tables(ddc_ctx* c) {
-  YlmTables& tb = c->tb;
+void build_tables_for(YlmTables& tb, int lmax, double eta, int ngrid) {
   memset(&tb, 0, sizeof(tb));
-  const int lmax = c->prm.lmax;
   const double pi = 4.0 * std::atan(1.0), sq2 = std::sqrt(2.0);
   std::vector<double> fact(std::max(2 * lmax + 1, 2));
   fact[0] = 1.0;
@@ -381,10 +384,15 @@ void build_tables(ddc_ctx* c) {
     tb.Bf[e] = (float)tb.B[e];
     tb.Bnf[e] = (float)tb.Bn[e];
   }
-  tb.eta = c->prm.eta;
+  tb.eta = eta;
   tb.lmax = lmax;
   tb.nylm = (lmax + 1) * (lmax + 1);
-  tb.ngrid = c->ngrid;
+  tb.ngrid = ngrid;
+}
+void build_tables(ddc_ctx* c) {
+  build_tables_for(c->tb, c->prm.lmax, c->prm.eta, c->ngrid);
+  // the degree of the far-field expansions of the solute potential
+  build_tables_for(c->tbP, kFarDegree, c->prm.eta, c->ngrid);
 }
 
 // deterministic reduction of `nvals` partial columns into red[0..nvals-1], copied to host.
@@ -639,6 +647,21 @@ int do_init(ddc_ctx* ctx, int n, const std::vector<double4>* hsph, const double4
   // per-triple lx values of the fused passes (FP64 size: the mixed path also
   // takes FP64 steps in its refinement)
   CK(ctx->tval.ensure(sizeof(double) * std::max<long long>(ctx->ntri, 1)));
+  // near / far split of the solute potential at the cavity for large systems
+  // (DDC_FAR_OFF=1 in the environment keeps the direct sums: a diagnostic
+  // switch for the tests)
+  {
+    const char* off = std::getenv("DDC_FAR_OFF");
+    ctx->far_on = N >= kFarMinSpheres && G <= 640 && !(off && off[0] == '1');
+    if (ctx->far_on) {
+      const int YP = ctx->tbP.nylm;
+      CK(ctx->farBT.ensure(sizeof(double) * YP * G));
+      CK(ctx->farDT.ensure(sizeof(double) * 3 * YP * G));
+      CK(ctx->farA.ensure(sizeof(double) * (size_t)YP * N));
+      CK(launch_far_tables(L, ctx->tbP, ctx->grid.as<double4>(), G, ctx->farBT.as<double>(),
+                           ctx->farDT.as<double>()));
+    }
+  }
   CKI(sync(ctx));
   ctx->ready = true;
   return DDC_OK;
@@ -1164,6 +1187,29 @@ int need_ready(ddc_ctx* ctx) {
 int dot_dev(ddc_ctx* ctx, long long n, const double* a, const double* b, double* out) {
   CK(launch_dot_partial(ctx->L(), n, a, b, ctx->partials.as<double>(), reduce_blocks()));
   return reduce_to_host(ctx, 1, out);
+}
+
+// Solute potential (and, with ef, field) at the context's cavity points from
+// charges q at its sphere centres (mkrhs.f90:102-114, main.f90:241): near /
+// far split for large systems, direct sums otherwise.  trange: per-target
+// source ranges of a batch (direct path); the split uses the molecule ranges.
+int solute_pot_field(ddc_ctx* ctx, const double* q, double* phi, double* ef, const int2* trange) {
+  const int N = ctx->nsph, NC = ctx->ncav;
+  StageScope sc(ctx, ST_COULOMB);
+  if (ctx->far_on) {
+    CK(launch_far_pot_field(ctx->L(), ctx->tbP, N, ctx->ngrid, ctx->sph.as<double4>(), q,
+                            ctx->mrange_ptr(), kFarRho, ctx->cavoff.as<int>(),
+                            ctx->cavpt.as<int>(), ctx->ccav.as<double>(), ctx->farBT.as<double>(),
+                            ctx->farDT.as<double>(), ctx->farA.as<double>(), phi, ef));
+  } else if (ef) {
+    CK(launch_coulomb_pot_field(ctx->L(), N, q, ctx->cx.as<double>(), ctx->cy.as<double>(),
+                                ctx->cz.as<double>(), NC, ctx->ccav.as<double>(), phi, ef,
+                                trange));
+  } else {
+    CK(launch_coulomb_pot(ctx->L(), N, q, ctx->cx.as<double>(), ctx->cy.as<double>(),
+                          ctx->cz.as<double>(), NC, ctx->ccav.as<double>(), phi, trange));
+  }
+  return DDC_OK;
 }
 
 // right-hand side of the direct solve from the cavity potential: wghpot and
@@ -1918,17 +1964,9 @@ int ddc_energy_forces(ddc_ctx* ctx, int n, const double* charge, const double* x
   // forces, the solute field at the cavity (main.f90:241-253) comes from the
   // same pass over the pairs
   if (ctx->prm.igrad) CK(ctx->ef1.ensure(sizeof(double) * 3 * std::max(NC, 1)));
-  {
-  StageScope sc(ctx, ST_COULOMB);
-  if (ctx->prm.igrad)
-    CK(launch_coulomb_pot_field(ctx->L(), N, dq, ctx->cx.as<double>(), ctx->cy.as<double>(),
-                                ctx->cz.as<double>(), NC, ctx->ccav.as<double>(), dphi,
-                                ctx->ef1.as<double>(), nullptr));
-  else
-    CK(launch_coulomb_pot(ctx->L(), N, dq, ctx->cx.as<double>(), ctx->cy.as<double>(),
-                          ctx->cz.as<double>(), NC, ctx->ccav.as<double>(), dphi, nullptr));
+  CKI(solute_pot_field(ctx, dq, dphi, ctx->prm.igrad ? ctx->ef1.as<double>() : nullptr,
+                       nullptr));
   CK(launch_psi(ctx->L(), N, ctx->nylm, dq, dpsi));
-  }
   CKI(sync(ctx));
   double t2 = now_s();
   inf->t_mkrhs = t2 - t1;
@@ -2118,18 +2156,9 @@ int ddc_batch_energy_forces(ddc_ctx* ctx, int nmol, const int* off, const double
   // the potential and (with forces) the solute field at the cavity, each
   // molecule's points from its own nuclei
   if (ctx->prm.igrad) CK(ctx->ef1.ensure(sizeof(double) * 3 * std::max(NC, 1)));
-  {
-    StageScope sc(ctx, ST_COULOMB);
-    if (ctx->prm.igrad)
-      CK(launch_coulomb_pot_field(ctx->L(), N, dq, ctx->cx.as<double>(), ctx->cy.as<double>(),
-                                  ctx->cz.as<double>(), NC, ctx->ccav.as<double>(), dphi,
-                                  ctx->ef1.as<double>(), ctx->tr_cav.as<int2>()));
-    else
-      CK(launch_coulomb_pot(ctx->L(), N, dq, ctx->cx.as<double>(), ctx->cy.as<double>(),
-                            ctx->cz.as<double>(), NC, ctx->ccav.as<double>(), dphi,
-                            ctx->tr_cav.as<int2>()));
-    CK(launch_psi(ctx->L(), N, ctx->nylm, dq, dpsi));
-  }
+  CKI(solute_pot_field(ctx, dq, dphi, ctx->prm.igrad ? ctx->ef1.as<double>() : nullptr,
+                       ctx->tr_cav.as<int2>()));
+  CK(launch_psi(ctx->L(), N, ctx->nylm, dq, dpsi));
   CKI(sync(ctx));
   double t2 = now_s();
   inf->t_mkrhs = t2 - t1;

@@ -305,6 +305,22 @@ cudaError_t launch_reduce_partials(Launch L, const double* partials, int nblk, i
 int reduce_blocks();
 
 // electrostatics
+// near / far split of the solute potential (and field) at the cavity points:
+// charges farther than kFarRho * r_i from a sphere enter through a local
+// expansion of degree kFarDegree about its centre, the others directly; used
+// from kFarMinSpheres spheres on (below, the direct sums are cheaper)
+constexpr int kFarDegree = 10;
+constexpr double kFarRho = 8.0;
+constexpr int kFarMinSpheres = 4096;
+// BT[lm][n] = Y_lm(s_n), DT[k][lm][n] = grad_k R_lm(s_n) for the degree of tbP
+cudaError_t launch_far_tables(Launch L, const YlmTables& tbP, const double4* grid, int ngrid,
+                              double* BT, double* DT);
+// phi (and ef, if not null) at the cavity points; A: scratch [nsph][nylm(tbP)]
+cudaError_t launch_far_pot_field(Launch L, const YlmTables& tbP, int nsph, int ngrid,
+                                 const double4* sph, const double* q, const int2* mrange,
+                                 double rho, const int* cavoff, const int* cavpt,
+                                 const double* ccav, const double* BT, const double* DT,
+                                 double* A, double* phi, double* ef);
 // trange: per target, the source index range it sums over (nullptr: all)
 // launch_coulomb_pot plus the field of the same sources at the targets, ef (3, ntrg)
 cudaError_t launch_coulomb_pot_field(Launch L, int nsrc, const double* q, const double* sx,

@@ -3527,3 +3527,291 @@ cudaError_t launch_fp32_probe(Launch L, int blocks, int iters, float* out) {
 }
 
 }  // namespace ddc
+
+namespace ddc {
+// ---------------------------------------------------------------------------
+// Solute potential and field at the cavity points with a near / far split
+// (mkrhs.f90:102-114 and the field of efld.f90:97-114 at the cavity,
+// main.f90:241).  Every cavity point lies on its sphere's surface,
+// p = c_i + r_i s_n.  A charge q_j farther than rho * r_i from c_i contributes,
+// by the addition theorem (|p - c_j| > r_i = |p - c_i|),
+//   q_j / |p - c_j| = sum_lm [q_j / d (4 pi / (2l+1)) t^l Y_lm(d^)] Y_lm(s_n),
+//   t = r_i / d <= 1 / rho,  d = c_j - c_i,
+// so the far charges of sphere i are summed once into its local expansion
+//   A_lm(i) = sum_{far j} q_j / d (4 pi / (2l+1)) t^l Y_lm(d^)   (degree P)
+// and evaluated at its cavity points: phi_far = sum_lm A_lm Y_lm(s_n) and
+// E_far = -(1 / r_i) sum_lm A_lm grad R_lm(s_n), with R_lm(u) = |u|^l Y_lm(u^)
+// the regular solid harmonic.  The accumulation of A is the L* machinery
+// (the adjrhs sum "weight * 4 pi/(2l+1) t^l Y_lm(s)" over (point, source)
+// pairs) with the weight -q_j / d.  The near charges (and the sphere's own)
+// are summed directly.  Truncation: at most t^(P+1) / (1 - t) of each far
+// term, 1e-10 for P = 10, rho = 8.
+// ---------------------------------------------------------------------------
+// A(i, lm) for every sphere: block per sphere, role warps over chunks of
+// sources of its molecule
+template <int LMAX>
+__global__ void __launch_bounds__(32 * ls_nroles(LMAX)) k_far_acc(const YlmTables tb, int nsph,
+                                                                   const double4* __restrict__ sph,
+                                                                   const double* __restrict__ q,
+                                                                   const int2* __restrict__ mrange,
+                                                                   double rho, double* A) {
+  constexpr int NR = ls_nroles(LMAX);
+  constexpr int CH = 32 * NR;
+  constexpr int NVM = ls_max_nvals(LMAX);
+  extern __shared__ double sh[];  // [ls_nfields][CH]
+  const int i = blockIdx.x;
+  const int role = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const double4 ci = sph[i];
+  const double cut2 = (rho * ci.w) * (rho * ci.w);
+  const int lo = mrange ? mrange[i].x : 0, hi = mrange ? mrange[i].y : nsph;
+  double acc[NVM];
+#pragma unroll
+  for (int v = 0; v < NVM; ++v) acc[v] = 0.0;
+  for (int j0 = lo; j0 < hi; j0 += CH) {
+    const int chunk = min(CH, hi - j0);
+    {
+      const int tt = threadIdx.x;
+      double* col = sh + tt;
+      double ct = 0.0, t2 = 0.0, st = 0.0, w = 0.0;
+      Angles a{1.0, 0.0, 1.0, 0.0};
+      if (tt < chunk) {
+        const int j = j0 + tt;
+        const double4 cj = sph[j];
+        const double vx = cj.x - ci.x, vy = cj.y - ci.y, vz = cj.z - ci.z;
+        const double d2 = vx * vx + vy * vy + vz * vz;
+        if (j != i && d2 > cut2) {
+          const double di = 1.0 / sqrt(d2);
+          const double t = ci.w * di;
+          a = angles_of(vx * di, vy * di, vz * di);
+          ct = a.c * t;
+          t2 = t * t;
+          st = a.s * t;
+          w = -q[j] * di;
+        }
+      }
+      col[0] = ct;
+      col[CH] = t2;
+      double pmm = w, cm = 1.0, sm = 0.0, cmm1 = 1.0, smm1 = 0.0;
+#pragma unroll
+      for (int m = 0; m <= LMAX; ++m) {
+        if (m == 1) {
+          cm = a.cp;
+          sm = a.sp;
+        } else if (m >= 2) {
+          const double cn = 2.0 * a.cp * cm - cmm1, sn = 2.0 * a.cp * sm - smm1;
+          cmm1 = cm; smm1 = sm; cm = cn; sm = sn;
+        }
+        col[(2 + 3 * m) * CH] = pmm;
+        col[(3 + 3 * m) * CH] = cm;
+        col[(4 + 3 * m) * CH] = sm;
+        pmm = -pmm * (2.0 * m + 1.0) * st;
+      }
+    }
+    __syncthreads();
+    ls_run_role<LMAX, 0, double>(role, tb, sh, CH, chunk, lane, acc);
+    __syncthreads();
+  }
+  ls_finish_role<LMAX, 0, double>(role, tb, acc, A + (size_t)i * tb.nylm, lane);
+}
+
+// Tables on the grid, once per context: BT[lm][n] = Y_lm(s_n) and
+// DT[k][lm][n] = d R_lm / d u_k at u = s_n (k = x, y, z), by fourth-order
+// central differences of R_lm(u) = |u|^l Y_lm(u / |u|) with step 1e-4
+// (truncation ~h^4 l^5 / 30 and rounding ~1e-16 / h: about 1e-12 relative)
+__global__ void k_far_tables(const YlmTables tb, const double4* __restrict__ grid, int ngrid,
+                             double* BT, double* DT) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= 4 * ngrid) return;
+  const int n = e % ngrid, k = e / ngrid;  // k = 0: values; 1..3: d/du_{k-1}
+  const double4 g = grid[n];
+  const int ny = tb.nylm;
+  double y[(DDC_MAX_LMAX + 1) * (DDC_MAX_LMAX + 1)];
+  if (k == 0) {
+    ylmbas_ref(tb, g.x, g.y, g.z, y);
+    for (int lm = 0; lm < ny; ++lm) BT[(size_t)lm * ngrid + n] = y[lm];
+    return;
+  }
+  double acc[(DDC_MAX_LMAX + 1) * (DDC_MAX_LMAX + 1)];
+  for (int lm = 0; lm < ny; ++lm) acc[lm] = 0.0;
+  const double h = 1e-4;
+  const double cst[4] = {1.0, -8.0, 8.0, -1.0};   // f(-2h), f(-h), f(h), f(2h)
+  const double off[4] = {-2.0, -1.0, 1.0, 2.0};
+  for (int s = 0; s < 4; ++s) {
+    double u[3] = {g.x, g.y, g.z};
+    u[k - 1] += off[s] * h;
+    const double r = sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+    ylmbas_ref(tb, u[0] / r, u[1] / r, u[2] / r, y);
+    double rl = 1.0;
+    for (int l = 0; l <= tb.lmax; ++l) {
+      for (int m = -l; m <= l; ++m) acc[l * l + l + m] += cst[s] * rl * y[l * l + l + m];
+      rl *= r;
+    }
+  }
+  for (int lm = 0; lm < ny; ++lm)
+    DT[((size_t)(k - 1) * ny + lm) * ngrid + n] = acc[lm] / (12.0 * h);
+}
+
+// Potential and field at the cavity points of sphere i (block per sphere):
+// the near charges directly (compacted into shared memory in passes of at
+// most kNearCap), the far ones from A(i).  With ef == nullptr only phi.
+constexpr int kNearCap = 1024;
+__global__ void __launch_bounds__(128) k_far_cav(int nsph, int ngrid, int ny,
+                                                 const double4* __restrict__ sph,
+                                                 const double* __restrict__ q,
+                                                 const int2* __restrict__ mrange, double rho,
+                                                 const int* __restrict__ cavoff,
+                                                 const int* __restrict__ cavpt,
+                                                 const double* __restrict__ ccav,
+                                                 const double* __restrict__ A,
+                                                 const double* __restrict__ BT,
+                                                 const double* __restrict__ DT, double* phi,
+                                                 double* ef) {
+  __shared__ double4 near[kNearCap];
+  __shared__ double sA[(DDC_MAX_LMAX + 1) * (DDC_MAX_LMAX + 1)];
+  __shared__ int s_cnt, s_scan;
+  const int i = blockIdx.x, tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const double4 ci = sph[i];
+  const double cut2 = (rho * ci.w) * (rho * ci.w);
+  const int lo = mrange ? mrange[i].x : 0, hi = mrange ? mrange[i].y : nsph;
+  const int c0 = cavoff[i], c1 = cavoff[i + 1];
+  for (int lm = tid; lm < ny; lm += blockDim.x) sA[lm] = A[(size_t)i * ny + lm];
+  // every thread owns cavity points c0 + tid, c0 + tid + 128, ... (at most
+  // ngrid per sphere): accumulators for up to kPts of them
+  constexpr int kPts = 5;  // 5 * 128 = 640 >= ngrid up to 590 points
+  double v[kPts], ex[kPts], ey[kPts], ez[kPts], px[kPts], py[kPts], pz[kPts];
+#pragma unroll
+  for (int u = 0; u < kPts; ++u) {
+    v[u] = ex[u] = ey[u] = ez[u] = 0.0;
+    const int c = c0 + tid + 128 * u;
+    px[u] = py[u] = pz[u] = 0.0;
+    if (c < c1) {
+      px[u] = ccav[3 * (size_t)c];
+      py[u] = ccav[3 * (size_t)c + 1];
+      pz[u] = ccav[3 * (size_t)c + 2];
+    }
+  }
+  if (tid == 0) s_scan = lo;
+  __syncthreads();
+  // passes over the molecule: compact near charges, then sum them
+  while (true) {
+    if (tid == 0) s_cnt = 0;
+    __syncthreads();
+    const int start = s_scan;
+    if (start >= hi) break;
+    int j = start;
+    // scan in steps of 128 candidates while the buffer has room for a step
+    for (; j < hi; j += 128) {
+      __syncthreads();
+      if (s_cnt + 128 > kNearCap) break;
+      const int jj = j + tid;
+      bool nb = false;
+      double4 cj = make_double4(0, 0, 0, 0);
+      if (jj < hi) {
+        cj = sph[jj];
+        const double dx = cj.x - ci.x, dy = cj.y - ci.y, dz = cj.z - ci.z;
+        nb = jj == i || dx * dx + dy * dy + dz * dz <= cut2;
+      }
+      const unsigned bal = __ballot_sync(0xffffffffu, nb);
+      __shared__ int wbase[4];
+      if (lane == 0) wbase[w] = __popc(bal);
+      __syncthreads();
+      if (tid == 0) {
+        int b = s_cnt;
+        for (int k = 0; k < 4; ++k) {
+          const int c = wbase[k];
+          wbase[k] = b;
+          b += c;
+        }
+        s_cnt = b;
+      }
+      __syncthreads();
+      if (nb) near[wbase[w] + __popc(bal & ((1u << lane) - 1u))] = make_double4(cj.x, cj.y, cj.z, q[jj]);
+    }
+    __syncthreads();
+    if (tid == 0) s_scan = j;
+    const int cnt = s_cnt;
+    for (int k = 0; k < cnt; ++k) {
+      const double4 s = near[k];
+#pragma unroll
+      for (int u = 0; u < kPts; ++u) {
+        if (c0 + tid + 128 * u < c1) {
+          const double dx = px[u] - s.x, dy = py[u] - s.y, dz = pz[u] - s.z;
+          const double ri = rsqrt_pos(dx * dx + dy * dy + dz * dz);
+          v[u] = fma(s.w, ri, v[u]);
+          const double f = s.w * (ri * ri * ri);
+          ex[u] = fma(f, dx, ex[u]);
+          ey[u] = fma(f, dy, ey[u]);
+          ez[u] = fma(f, dz, ez[u]);
+        }
+      }
+    }
+    __syncthreads();
+  }
+  // far part from the local expansion
+  const double iri = 1.0 / ci.w;
+#pragma unroll
+  for (int u = 0; u < kPts; ++u) {
+    const int c = c0 + tid + 128 * u;
+    if (c >= c1) continue;
+    const int n = cavpt[c] - i * ngrid;
+    double fp = 0.0, fx = 0.0, fy = 0.0, fz = 0.0;
+    for (int lm = 0; lm < ny; ++lm) {
+      const double a = sA[lm];
+      fp = fma(a, BT[(size_t)lm * ngrid + n], fp);
+      if (ef) {
+        fx = fma(a, DT[(size_t)lm * ngrid + n], fx);
+        fy = fma(a, DT[((size_t)ny + lm) * ngrid + n], fy);
+        fz = fma(a, DT[((size_t)2 * ny + lm) * ngrid + n], fz);
+      }
+    }
+    phi[c] = v[u] + fp;
+    if (ef) {
+      ef[3 * (size_t)c] = ex[u] - iri * fx;
+      ef[3 * (size_t)c + 1] = ey[u] - iri * fy;
+      ef[3 * (size_t)c + 2] = ez[u] - iri * fz;
+    }
+  }
+}
+
+cudaError_t launch_far_tables(Launch L, const YlmTables& tbP, const double4* grid, int ngrid,
+                              double* BT, double* DT) {
+  const int n = 4 * ngrid;
+  k_far_tables<<<(n + 63) / 64, 64, 0, L.st>>>(tbP, grid, ngrid, BT, DT);
+  ++*L.launches;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_far_pot_field(Launch L, const YlmTables& tbP, int nsph, int ngrid,
+                                 const double4* sph, const double* q, const int2* mrange,
+                                 double rho, const int* cavoff, const int* cavpt,
+                                 const double* ccav, const double* BT, const double* DT,
+                                 double* A, double* phi, double* ef) {
+  if (nsph == 0) return cudaSuccess;
+  if (ngrid > 640) return cudaErrorInvalidValue;  // k_far_cav holds 5 x 128 points per thread set
+  cudaError_t e;
+#define CASE(LV)                                                                              \
+  case LV: {                                                                                  \
+    constexpr int NR = ls_nroles(LV);                                                         \
+    const size_t sm = sizeof(double) * ls_nfields(LV) * 32 * NR;                              \
+    if (sm > 48 * 1024)                                                                       \
+      if ((e = cudaFuncSetAttribute(k_far_acc<LV>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                    (int)sm)))                                                \
+        return e;                                                                             \
+    k_far_acc<LV><<<nsph, 32 * NR, sm, L.st>>>(tbP, nsph, sph, q, mrange, rho, A);            \
+    break;                                                                                    \
+  }
+  switch (tbP.lmax) {
+    DDC_LMAX_CASES(CASE)
+    default:
+      return cudaErrorInvalidValue;
+  }
+#undef CASE
+  ++*L.launches;
+  if ((e = cudaGetLastError())) return e;
+  k_far_cav<<<nsph, 128, 0, L.st>>>(nsph, ngrid, tbP.nylm, sph, q, mrange, rho, cavoff, cavpt,
+                                    ccav, A, BT, DT, phi, ef);
+  ++*L.launches;
+  return cudaGetLastError();
+}
+
+}  // namespace ddc
