@@ -45,6 +45,7 @@ def build(force=False, verbose=False):
     cmd = [nvcc(), "-O3", "-std=c++17", *ARCH, "-lineinfo", "-shared",
            "-Xcompiler", "-fPIC,-ffp-contract=off", "-Xptxas", "-warn-spills" if verbose else "-O3",
            "-I", os.path.join(HERE, "..", "include"),
+           "-Xlinker", "--no-undefined",  # a missing definition fails the build, not the load
            "-o", LIB + ".tmp", *[os.path.join(CSRC, s) for s in SOURCES]]
     if verbose:
         print(" ".join(cmd), file=sys.stderr)

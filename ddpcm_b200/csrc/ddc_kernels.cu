@@ -932,18 +932,20 @@ cudaError_t gemm2(Launch L, int M, int N, int K, Acc alpha, const TAin* A, int l
   return cudaGetLastError();
 }
 
-// Pipelined FP64 GEMM of the operators' projection and expansion (FP64
-// path): C[n*ldc + m] = alpha * sum_k A[k*lda + m] B[n*ldb + k].  128 x 64
-// tiles, 16-deep k slabs copied to shared memory with cp.async (the next
-// slab in flight while the current one is used), 256 threads each
-// accumulating an 8 x 4 block from vector shared-memory reads.
+// FP64 GEMM of the operators' projection and expansion (FP64 path, the
+// refinement steps and the one-off RHS projections) on the FP64 tensor
+// cores (DMMA, mma.sync m8n8k4; tcgen05 has no FP64 kind):
+//   C[n*ldc + m] = alpha * sum_k A[k*lda + m] B[n*ldb + k].
+// 128 x 64 tiles, 8 warps of 32 x 32 (4 x 4 MMA tiles of 8 x 8), 16-deep k
+// slabs copied to shared memory with cp.async (the next slab in flight).
+// Shared rows are padded so that each warp's fragment loads take the
+// minimum two wavefronts: A rows of 136 doubles (a row stride of 16 banks
+// mod 32 separates k and k + 1), B rows of 20 (8 banks mod 32 separates
+// four columns).  Each output is one FMA chain in k order.
 namespace dgp {
 constexpr int BM = 128, BN = 64, BK = 16;
-// B rows padded by two doubles: the copies write 16 consecutive k of one
-// column, which would otherwise fall into one bank group (row stride 512 B);
-// with 528 B they spread over 16 banks (two-way), and rows stay 16-byte aligned
-constexpr int BNP = BN + 2;
-constexpr int SMEM = (2 * BK * BM + 2 * BK * BNP) * 8;
+constexpr int AS = BM + 8, BS = BK + 4;
+constexpr int SMEM = (2 * BK * AS + 2 * BN * BS) * 8;
 }
 __device__ __forceinline__ void cp_async8(void* sdst, const void* gsrc, bool valid) {
   const uint32_t d = (uint32_t)__cvta_generic_to_shared(sdst);
@@ -951,41 +953,43 @@ __device__ __forceinline__ void cp_async8(void* sdst, const void* gsrc, bool val
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(gsrc), "r"(n)
                : "memory");
 }
-__global__ void __launch_bounds__(256) k_dgemm_cp(int M, int N, int K, double alpha,
-                                                  const double* __restrict__ A, int lda,
-                                                  const double* __restrict__ B, int ldb,
-                                                  double* __restrict__ C, int ldc) {
+__global__ void __launch_bounds__(256, 3) k_dgemm_dmma(int M, int N, int K, double alpha,
+                                                       const double* __restrict__ A, int lda,
+                                                       const double* __restrict__ B, int ldb,
+                                                       double* __restrict__ C, int ldc) {
   using namespace dgp;
   extern __shared__ __align__(16) double dg_smem[];
-  double(*As)[BK][BM] = reinterpret_cast<double(*)[BK][BM]>(dg_smem);
-  double(*Bs)[BK][BNP] = reinterpret_cast<double(*)[BK][BNP]>(dg_smem + 2 * BK * BM);
-  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  double* As = dg_smem;                // [2][BK][AS]
+  double* Bs = dg_smem + 2 * BK * AS;  // [2][BN][BS]
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int wm = warp & 3, wn = warp >> 2;
   const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
   auto load = [&](int buf, int k0) {
 #pragma unroll
     for (int u = 0; u < BM * BK / 256; ++u) {
       const int e = tid + u * 256;
-      const int mm = e & (BM - 1), kk = e / BM;
+      const int mm = e % BM, kk = e / BM;
       const int m = m0 + mm, k = k0 + kk;
       const bool ok = m < M && k < K;
-      cp_async8(&As[buf][kk][mm], ok ? A + (size_t)k * lda + m : A, ok);
+      cp_async8(As + (buf * BK + kk) * AS + mm, ok ? A + (size_t)k * lda + m : A, ok);
     }
 #pragma unroll
     for (int u = 0; u < BN * BK / 256; ++u) {
       const int e = tid + u * 256;
-      const int kk = e & (BK - 1), nn = e / BK;
+      const int kk = e % BK, nn = e / BK;
       const int n = n0 + nn, k = k0 + kk;
       const bool ok = n < N && k < K;
-      cp_async8(&Bs[buf][kk][nn], ok ? B + (size_t)n * ldb + k : B, ok);
+      cp_async8(Bs + (buf * BN + nn) * BS + kk, ok ? B + (size_t)n * ldb + k : B, ok);
     }
     asm volatile("cp.async.commit_group;" ::: "memory");
   };
-  double acc[8][4];
+  double acc[4][4][2];
 #pragma unroll
-  for (int r = 0; r < 8; ++r)
+  for (int i = 0; i < 4; ++i)
 #pragma unroll
-    for (int c = 0; c < 4; ++c) acc[r][c] = 0.0;
+    for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
   const int nk = (K + BK - 1) / BK;
+  const int fr = lane >> 2, fk = lane & 3;  // fragment row / k of this lane
   load(0, 0);
   for (int t = 0; t < nk; ++t) {
     const int buf = t & 1;
@@ -996,40 +1000,36 @@ __global__ void __launch_bounds__(256) k_dgemm_cp(int M, int N, int K, double al
       asm volatile("cp.async.wait_group 0;" ::: "memory");
     }
     __syncthreads();
+    const double* as = As + buf * BK * AS;
+    const double* bs = Bs + buf * BN * BS;
 #pragma unroll
-    for (int kk = 0; kk < BK; ++kk) {
-      const double2* ap = reinterpret_cast<const double2*>(&As[buf][kk][ty * 8]);
-      const double2* bp = reinterpret_cast<const double2*>(&Bs[buf][kk][tx * 4]);
-      double a[8], b[4];
+    for (int ks = 0; ks < BK; ks += 4) {
+      double a[4], b[4];
 #pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        const double2 v = ap[r];
-        a[2 * r] = v.x;
-        a[2 * r + 1] = v.y;
-      }
+      for (int i = 0; i < 4; ++i) a[i] = as[(ks + fk) * AS + wm * 32 + i * 8 + fr];
 #pragma unroll
-      for (int c = 0; c < 2; ++c) {
-        const double2 v = bp[c];
-        b[2 * c] = v.x;
-        b[2 * c + 1] = v.y;
-      }
+      for (int j = 0; j < 4; ++j) b[j] = bs[(wn * 32 + j * 8 + fr) * BS + ks + fk];
 #pragma unroll
-      for (int r = 0; r < 8; ++r)
+      for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int c = 0; c < 4; ++c) acc[r][c] = fma(a[r], b[c], acc[r][c]);
+        for (int j = 0; j < 4; ++j)
+          asm volatile(
+              "mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+              : "+d"(acc[i][j][0]), "+d"(acc[i][j][1])
+              : "d"(a[i]), "d"(b[j]));
     }
     __syncthreads();
   }
 #pragma unroll
-  for (int c = 0; c < 4; ++c) {
-    const int n = n0 + tx * 4 + c;
-    if (n >= N) continue;
+  for (int i = 0; i < 4; ++i)
 #pragma unroll
-    for (int r = 0; r < 8; ++r) {
-      const int m = m0 + ty * 8 + r;
-      if (m < M) C[(size_t)n * ldc + m] = alpha * acc[r][c];
-    }
-  }
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int m = m0 + wm * 32 + i * 8 + fr;
+        const int n = n0 + wn * 32 + j * 8 + 2 * fk + h;
+        if (m < M && n < N) C[(size_t)n * ldc + m] = alpha * acc[i][j][h];
+      }
 }
 // dst[c*rows + r] = src[r*cols + c]
 __global__ void k_transpose(int rows, int cols, const double* __restrict__ src, double* dst) {
@@ -1049,10 +1049,10 @@ cudaError_t launch_dgemm_nn(Launch L, int M, int N, int K, double alpha, const d
                             int lda, const double* B, int ldb, double* C, int ldc) {
   if (M == 0 || N == 0) return cudaSuccess;
   dim3 grid((M + dgp::BM - 1) / dgp::BM, (N + dgp::BN - 1) / dgp::BN);
-  cudaError_t e = cudaFuncSetAttribute(k_dgemm_cp, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaError_t e = cudaFuncSetAttribute(k_dgemm_dmma, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        dgp::SMEM);
   if (e) return e;
-  k_dgemm_cp<<<grid, 256, dgp::SMEM, L.st>>>(M, N, K, alpha, A, lda, B, ldb, C, ldc);
+  k_dgemm_dmma<<<grid, 256, dgp::SMEM, L.st>>>(M, N, K, alpha, A, lda, B, ldb, C, ldc);
   ++*L.launches;
   return cudaGetLastError();
 }

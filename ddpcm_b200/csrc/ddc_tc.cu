@@ -21,7 +21,8 @@
 // projection to FP64 with alpha applied (no separate conversion pass) and
 // writes xi as FP32 in the layout of the fused L / L* kernel.
 //
-// Roles (one CTA per output tile, 10 warps):
+// Roles (one CTA per output tile -- for the expansion, one 128-point grid
+// tile of one group of spheres -- 10 warps):
 //   warp 0      one lane issues the bulk / TMA copies into a ring of stages
 //   warp 1      allocates tensor memory; one lane issues the MMAs
 //   warps 2..9  split the per-call operand, then drain the accumulator
@@ -271,7 +272,7 @@ __device__ __forceinline__ void tmem_add(uint32_t tmem, int q, int half, uint32_
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kTcThreads, 1)
     k_proj_tc(const __grid_constant__ CUtensorMap tm_pot, const float* __restrict__ aimg,
-              int nsph, int nylm, int kcn, int bn, int nstage, double alpha,
+              int nsph, int nylm, int kcn, int bn, int nstage, int nbuf, double alpha,
               double* __restrict__ y, int* err) {
   extern __shared__ unsigned char sm_raw[];
   unsigned char* sm = reinterpret_cast<unsigned char*>(
@@ -279,7 +280,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   const uint32_t bbytes = (uint32_t)bn * 128;
   const uint32_t sbytes = 2 * kChunk + 2 * bbytes;  // A hi | A lo | B hi | B lo
   uint64_t* bars = reinterpret_cast<uint64_t*>(sm + (size_t)nstage * sbytes);
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 3 * nstage + 5);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 3 * nstage + 9);
   volatile int* abort = reinterpret_cast<volatile int*>(tslot + 1);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int i0 = blockIdx.x * bn;
@@ -289,15 +290,15 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   auto READY = [&](int s) { return bar0 + 8u * (nstage + s); };
   auto EMPTY = [&](int s) { return bar0 + 8u * (2 * nstage + s); };
   auto MFULL = [&](int b) { return bar0 + 8u * (3 * nstage + b); };
-  auto MEMPTY = [&](int b) { return bar0 + 8u * (3 * nstage + 2 + b); };
-  const uint32_t DONE = bar0 + 8u * (3 * nstage + 4);
+  auto MEMPTY = [&](int b) { return bar0 + 8u * (3 * nstage + 4 + b); };
+  const uint32_t DONE = bar0 + 8u * (3 * nstage + 8);
   if (threadIdx.x == 0) {
     for (int s = 0; s < nstage; ++s) {
       mbar_init(FULL(s), 1);
       mbar_init(READY(s), kSplitWarps);
       mbar_init(EMPTY(s), 1);
     }
-    for (int b = 0; b < 2; ++b) {
+    for (int b = 0; b < nbuf; ++b) {
       mbar_init(MFULL(b), 1);
       mbar_init(MEMPTY(b), kSplitWarps);
     }
@@ -305,13 +306,13 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     *abort = 0;
     fence_barrier_init();
   }
-  const uint32_t ncols = tmem_cols(3 * bn);
+  const uint32_t ncols = tmem_cols((nbuf + 1) * bn);
   if (warp == 1) tmem_alloc(su32(tslot), ncols);
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tslot;
-  const uint32_t corr = tmem + (uint32_t)(2 * bn);
+  const uint32_t corr = tmem + (uint32_t)(nbuf * bn);
 
   if (warp == 0) {
     if (lane == 0) {
@@ -334,10 +335,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     if (lane == 0) {
       const uint32_t idesc = idesc_tf32(128, bn);
       for (int kc = 0; kc < kcn; ++kc) {
-        const int s = kc % nstage, b = kc & 1;
+        const int s = kc % nstage, b = kc % nbuf;
         const uint32_t ph = (uint32_t)(kc / nstage) & 1u;
         if (!mbar_wait(READY(s), ph, abort, err, 2)) break;
-        if (kc >= 2 && !mbar_wait(MEMPTY(b), (uint32_t)((kc >> 1) - 1) & 1u, abort, err, 5))
+        if (kc >= nbuf && !mbar_wait(MEMPTY(b), (uint32_t)(kc / nbuf - 1) & 1u, abort, err, 5))
           break;
         tc_fence_after();
         const uint32_t st = sbase + s * sbytes;
@@ -363,9 +364,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 #pragma unroll
     for (int k = 0; k < 16 * kMaxJ; ++k) acc[k] = 0.f;
     bool ok = true;
-    // split chunk kc, then add the main term of chunk kc - 1 (the MMAs of kc
-    // run meanwhile)
-    for (int kc = 0; ok && kc <= kcn; ++kc) {
+    // split chunk kc, then add the main term of chunk kc - lag: up to nbuf
+    // chunks' MMAs run while the epilogue works
+    const int lag = nbuf - 1;
+    for (int kc = 0; ok && kc < kcn + lag; ++kc) {
       if (kc < kcn) {
         const int s = kc % nstage;
         const uint32_t ph = (uint32_t)(kc / nstage) & 1u;
@@ -389,9 +391,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         __syncwarp();
         if (lane == 0) mbar_arrive(READY(s));
       }
-      if (kc >= 1) {
-        const int c = kc - 1, b = c & 1;
-        if (!mbar_wait(MFULL(b), (uint32_t)(c >> 1) & 1u, abort, err, 4)) {
+      if (kc >= lag) {
+        const int c = kc - lag, b = c % nbuf;
+        if (!mbar_wait(MFULL(b), (uint32_t)(c / nbuf) & 1u, abort, err, 4)) {
           ok = false;
           break;
         }
@@ -404,7 +406,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     }
     if (ok && mbar_wait(DONE, 0, abort, err, 6)) {
       tc_fence_after();
-      tmem_add(tmem, q, half, (uint32_t)(2 * bn), bn, acc);
+      tmem_add(tmem, q, half, (uint32_t)(nbuf * bn), bn, acc);
       const int lm = 32 * q + lane;
       if (lm < nylm) {
 #pragma unroll
@@ -434,6 +436,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 __global__ void __launch_bounds__(kTcThreads, 1)
     k_xi_tc(const double* __restrict__ s, const float* __restrict__ aimg, int nsph, int nylm,
             int ngrid, int mtn, int kcn, int bn, int nstage, float* __restrict__ xi, int* err) {
+  // this CTA: grid-point tile blockIdx.y (of mtn) for spheres i0 .. i0 + bn
+  const int mt0 = blockIdx.y;
   extern __shared__ unsigned char sm_raw[];
   unsigned char* sm = reinterpret_cast<unsigned char*>(
       (reinterpret_cast<uintptr_t>(sm_raw) + 1023) & ~uintptr_t(1023));
@@ -477,7 +481,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   tc_fence_after();
   const uint32_t tmem = *tslot;
   const uint32_t corr = tmem + (uint32_t)(2 * bn);
-  const int nit = mtn * kcn;
+  const int nit = kcn;  // one grid-point tile per CTA
+  (void)mtn;
 
   if (warp == 0) {
     if (lane == 0) {
@@ -488,8 +493,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         const uint32_t ph = (uint32_t)(it / nstage) & 1u;
         if (it >= nstage && !mbar_wait(EMPTY(st), ph ^ 1u, abort, err, 11)) break;
         mbar_expect_tx(FULL(st), 2 * kChunk);
-        bulk_load(abase + st * 2 * kChunk, aimg + (size_t)it * (2 * kChunk / 4), 2 * kChunk,
-                  FULL(st));
+        bulk_load(abase + st * 2 * kChunk, aimg + (size_t)(mt0 * kcn + it) * (2 * kChunk / 4),
+                  2 * kChunk, FULL(st));
         issued = it + 1;
       }
       for (int it = max(0, issued - nstage); it < issued; ++it)
@@ -577,7 +582,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         tc_fence_before();
         __syncwarp();
         if (lane == 0) mbar_arrive(CEMPTY);
-        const int m = mt * 128 + 32 * q + lane;
+        const int m = (mt0 + mt) * 128 + 32 * q + lane;
 #pragma unroll
         for (int j = 0; j < kMaxJ; ++j)
 #pragma unroll
@@ -802,15 +807,17 @@ cudaError_t tc_autotune(Launch L, TcPlan& p, const double* s, double* y, float* 
 
 cudaError_t launch_proj_tc(Launch L, const TcPlan& p, double alpha, double* y) {
   const int grid = (p.nsph + p.bn_proj - 1) / p.bn_proj;
+  // main-term buffers in tensor memory: as many as fit beside the correction
+  const int nbuf = std::min(4, 512 / p.bn_proj - 1);
   k_proj_tc<<<grid, kTcThreads, p.smem_proj, L.st>>>(p.tm_pot, p.img_proj.as<float>(), p.nsph,
                                                      p.nylm, p.kc_proj, p.bn_proj, p.ns_proj,
-                                                     alpha, y, p.err_d);
+                                                     nbuf, alpha, y, p.err_d);
   ++*L.launches;
   return cudaGetLastError();
 }
 
 cudaError_t launch_xi_tc(Launch L, const TcPlan& p, const double* s, float* xi) {
-  const int grid = (p.nsph + p.bn_xi - 1) / p.bn_xi;
+  const dim3 grid((p.nsph + p.bn_xi - 1) / p.bn_xi, p.mt_xi);
   k_xi_tc<<<grid, kTcThreads, p.smem_xi, L.st>>>(s, p.img_xi.as<float>(), p.nsph, p.nylm,
                                                  p.ngrid, p.mt_xi, p.kc_xi, p.bn_xi, p.ns_xi, xi,
                                                  p.err_d);

@@ -15,6 +15,9 @@ def test_library_exports_every_header_symbol():
     L = ctypes.CDLL(lib)
     missing = [n for n in names if not hasattr(L, n)]
     assert not missing, missing
+    # every symbol the library needs resolves at load time (no missing
+    # definition waiting for its first call)
+    ctypes.CDLL(lib, mode=os.RTLD_NOW)
 
 
 def test_status_strings_and_defaults_without_gpu():
