@@ -63,6 +63,7 @@ struct TcPlan {
   bool tuned = false;        // tile widths measured for tune_key's shape
   long long tune_key = 0;
   int tuned_bn_proj = 0, tuned_bn_xi = 0;
+  bool xi_split = false, tuned_xi_split = false;  // expansion: one grid tile per CTA
   float ms_proj = 0.f, ms_xi = 0.f;  // measured launch times of the chosen widths
   int nsph = 0, nylm = 0, ngrid = 0, ldp = 0;
   int kc_proj = 0, bn_proj = 0, ns_proj = 0, smem_proj = 0;

@@ -435,9 +435,12 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kTcThreads, 1)
     k_xi_tc(const double* __restrict__ s, const float* __restrict__ aimg, int nsph, int nylm,
-            int ngrid, int mtn, int kcn, int bn, int nstage, float* __restrict__ xi, int* err) {
-  // this CTA: grid-point tile blockIdx.y (of mtn) for spheres i0 .. i0 + bn
-  const int mt0 = blockIdx.y;
+            int ngrid, int mtn, int mtper, int kcn, int bn, int nstage, float* __restrict__ xi,
+            int* err) {
+  // this CTA: grid-point tiles mt0 .. mt0 + mtc - 1 (of mtn) for spheres
+  // i0 .. i0 + bn (all tiles in one CTA, or one tile per CTA)
+  const int mt0 = blockIdx.y * mtper;
+  const int mtc = min(mtper, mtn - mt0);
   extern __shared__ unsigned char sm_raw[];
   unsigned char* sm = reinterpret_cast<unsigned char*>(
       (reinterpret_cast<uintptr_t>(sm_raw) + 1023) & ~uintptr_t(1023));
@@ -481,8 +484,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   tc_fence_after();
   const uint32_t tmem = *tslot;
   const uint32_t corr = tmem + (uint32_t)(2 * bn);
-  const int nit = kcn;  // one grid-point tile per CTA
-  (void)mtn;
+  const int nit = mtc * kcn;
 
   if (warp == 0) {
     if (lane == 0) {
@@ -738,6 +740,7 @@ cudaError_t tc_autotune(Launch L, TcPlan& p, const double* s, double* y, float* 
   if (!p.on) return cudaSuccess;
   const long long key = ((long long)p.nsph << 24) ^ ((long long)p.nylm << 12) ^ p.ngrid;
   if (p.tuned && p.tune_key == key) {  // same shape as the last measurement
+    p.xi_split = p.tuned_xi_split;
     cudaError_t e = cfg_proj(p, p.tuned_bn_proj);
     return e ? e : cfg_xi(p, p.tuned_bn_xi);
   }
@@ -778,6 +781,7 @@ cudaError_t tc_autotune(Launch L, TcPlan& p, const double* s, double* y, float* 
   if (!e) e = cfg_proj(p, best);
   p.ms_proj = tbest / 3.f;
   best = p.bn_xi;
+  bool best_split = false;
   tbest = 1e30f;
   if (!e) e = cudaMemsetAsync(const_cast<double*>(s), 0, sizeof(double) * p.nsph * p.nylm, L.st);
   for (size_t k = 0; !e && k < cand.size(); ++k) {
@@ -785,13 +789,18 @@ cudaError_t tc_autotune(Launch L, TcPlan& p, const double* s, double* y, float* 
       cudaGetLastError();
       continue;
     }
-    float ms = 0.f;
-    e = timed([&] { return launch_xi_tc(L, p, s, xi); }, &ms);
-    if (!e && ms < tbest) {
-      tbest = ms;
-      best = cand[k];
+    for (int split = 0; !e && split < 2; ++split) {  // all grid tiles per CTA, or one
+      p.xi_split = split == 1;
+      float ms = 0.f;
+      e = timed([&] { return launch_xi_tc(L, p, s, xi); }, &ms);
+      if (!e && ms < tbest) {
+        tbest = ms;
+        best = cand[k];
+        best_split = p.xi_split;
+      }
     }
   }
+  p.xi_split = best_split;
   if (!e) e = cfg_xi(p, best);
   p.ms_xi = tbest / 3.f;
   cudaEventDestroy(e0);
@@ -801,6 +810,7 @@ cudaError_t tc_autotune(Launch L, TcPlan& p, const double* s, double* y, float* 
     p.tune_key = key;
     p.tuned_bn_proj = p.bn_proj;
     p.tuned_bn_xi = p.bn_xi;
+    p.tuned_xi_split = p.xi_split;
   }
   return e;
 }
@@ -817,10 +827,11 @@ cudaError_t launch_proj_tc(Launch L, const TcPlan& p, double alpha, double* y) {
 }
 
 cudaError_t launch_xi_tc(Launch L, const TcPlan& p, const double* s, float* xi) {
-  const dim3 grid((p.nsph + p.bn_xi - 1) / p.bn_xi, p.mt_xi);
+  const int mtper = p.xi_split ? 1 : p.mt_xi;
+  const dim3 grid((p.nsph + p.bn_xi - 1) / p.bn_xi, (p.mt_xi + mtper - 1) / mtper);
   k_xi_tc<<<grid, kTcThreads, p.smem_xi, L.st>>>(s, p.img_xi.as<float>(), p.nsph, p.nylm,
-                                                 p.ngrid, p.mt_xi, p.kc_xi, p.bn_xi, p.ns_xi, xi,
-                                                 p.err_d);
+                                                 p.ngrid, p.mt_xi, mtper, p.kc_xi, p.bn_xi,
+                                                 p.ns_xi, xi, p.err_d);
   ++*L.launches;
   return cudaGetLastError();
 }
