@@ -3654,7 +3654,7 @@ __global__ void k_far_tables(const YlmTables tb, const double4* __restrict__ gri
 // Potential and field at the cavity points of sphere i (block per sphere):
 // the near charges directly (compacted into shared memory in passes of at
 // most kNearCap), the far ones from A(i).  With ef == nullptr only phi.
-constexpr int kNearCap = 1024;
+constexpr int kNearCap = 2048;
 __global__ void __launch_bounds__(128) k_far_cav(int nsph, int ngrid, int ny,
                                                  const double4* __restrict__ sph,
                                                  const double* __restrict__ q,
@@ -3666,7 +3666,7 @@ __global__ void __launch_bounds__(128) k_far_cav(int nsph, int ngrid, int ny,
                                                  const double* __restrict__ BT,
                                                  const double* __restrict__ DT, double* phi,
                                                  double* ef) {
-  __shared__ double4 near[kNearCap];
+  extern __shared__ double4 near[];  // [kNearCap], dynamic (64 KB)
   __shared__ double sA[(DDC_MAX_LMAX + 1) * (DDC_MAX_LMAX + 1)];
   __shared__ int s_cnt, s_scan;
   const int i = blockIdx.x, tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
@@ -3699,33 +3699,46 @@ __global__ void __launch_bounds__(128) k_far_cav(int nsph, int ngrid, int ny,
     const int start = s_scan;
     if (start >= hi) break;
     int j = start;
-    // scan in steps of 128 candidates while the buffer has room for a step
-    for (; j < hi; j += 128) {
+    // scan in steps of 512 candidates (four per thread) while the buffer has
+    // room for a step; list order: sub-step, warp, lane (deterministic)
+    for (; j < hi; j += 512) {
       __syncthreads();
-      if (s_cnt + 128 > kNearCap) break;
-      const int jj = j + tid;
-      bool nb = false;
-      double4 cj = make_double4(0, 0, 0, 0);
-      if (jj < hi) {
-        cj = sph[jj];
-        const double dx = cj.x - ci.x, dy = cj.y - ci.y, dz = cj.z - ci.z;
-        nb = jj == i || dx * dx + dy * dy + dz * dz <= cut2;
+      if (s_cnt + 512 > kNearCap) break;
+      bool nb[4];
+      double4 cj[4];
+      unsigned bal[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int jj = j + 128 * u + tid;
+        nb[u] = false;
+        cj[u] = make_double4(0, 0, 0, 0);
+        if (jj < hi) {
+          cj[u] = sph[jj];
+          cj[u].w = q[jj];
+          const double dx = cj[u].x - ci.x, dy = cj[u].y - ci.y, dz = cj[u].z - ci.z;
+          nb[u] = jj == i || dx * dx + dy * dy + dz * dz <= cut2;
+        }
+        bal[u] = __ballot_sync(0xffffffffu, nb[u]);
       }
-      const unsigned bal = __ballot_sync(0xffffffffu, nb);
-      __shared__ int wbase[4];
-      if (lane == 0) wbase[w] = __popc(bal);
+      __shared__ int wbase[4][4];
+      if (lane == 0)
+#pragma unroll
+        for (int u = 0; u < 4; ++u) wbase[u][w] = __popc(bal[u]);
       __syncthreads();
       if (tid == 0) {
         int b = s_cnt;
-        for (int k = 0; k < 4; ++k) {
-          const int c = wbase[k];
-          wbase[k] = b;
-          b += c;
-        }
+        for (int u = 0; u < 4; ++u)
+          for (int k = 0; k < 4; ++k) {
+            const int c = wbase[u][k];
+            wbase[u][k] = b;
+            b += c;
+          }
         s_cnt = b;
       }
       __syncthreads();
-      if (nb) near[wbase[w] + __popc(bal & ((1u << lane) - 1u))] = make_double4(cj.x, cj.y, cj.z, q[jj]);
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (nb[u]) near[wbase[u][w] + __popc(bal[u] & ((1u << lane) - 1u))] = cj[u];
     }
     __syncthreads();
     if (tid == 0) s_scan = j;
@@ -3808,8 +3821,11 @@ cudaError_t launch_far_pot_field(Launch L, const YlmTables& tbP, int nsph, int n
 #undef CASE
   ++*L.launches;
   if ((e = cudaGetLastError())) return e;
-  k_far_cav<<<nsph, 128, 0, L.st>>>(nsph, ngrid, tbP.nylm, sph, q, mrange, rho, cavoff, cavpt,
-                                    ccav, A, BT, DT, phi, ef);
+  const int smn = (int)sizeof(double4) * kNearCap;
+  if ((e = cudaFuncSetAttribute(k_far_cav, cudaFuncAttributeMaxDynamicSharedMemorySize, smn)))
+    return e;
+  k_far_cav<<<nsph, 128, smn, L.st>>>(nsph, ngrid, tbP.nylm, sph, q, mrange, rho, cavoff, cavpt,
+                                      ccav, A, BT, DT, phi, ef);
   ++*L.launches;
   return cudaGetLastError();
 }
