@@ -2586,8 +2586,8 @@ cudaError_t launch_lstarx_acc_f32(Launch L, const YlmTables& tb, const DevGeo& g
 // Block per sphere b over its gather list (the lstarx layout), in chunks
 // of one triple per thread, software pipelined over two shared buffers:
 // every thread issues the global loads of its triple of chunk k+1, then the
-// role warps (as in k_lstarx: a role owns the Legendre columns m and
-// lmax-m) run the normalised recurrence over chunk k and feed each value to
+// role warps (a role owns a set of Legendre columns, below) run the
+// normalised recurrence over chunk k and feed each value to
 // both contractions (registers accumulate the L* rows, the role's share of
 // each triple's lx value goes to shared memory), then the thread turns its
 // loaded inputs into chunk k+1's fields (prefix Q_m^m with W folded in,
@@ -2599,15 +2599,86 @@ cudaError_t launch_lstarx_acc_f32(Launch L, const YlmTables& tb, const DevGeo& g
 // bit-reproducible.
 // ---------------------------------------------------------------------------
 // Shared fields of a chunk, in units of Rl with CH triples: a 4-vector
-// (ct, t2, c = w_n xi_a(n), 0) per triple, then per column m the prefix
-// q0[m] (W and t^m folded in) and the pair (cos m phi, sin m phi).  A role
-// reads a triple with one 4-vector load plus two loads per column.
-__host__ __device__ constexpr int lxs_nfields(int L) { return 4 + 3 * (L + 1); }
-__host__ __device__ constexpr int lxs_q0(int CH, int m) { return 4 * CH + 3 * CH * m; }
-__host__ __device__ constexpr int lxs_cs(int CH, int m) { return 4 * CH + 3 * CH * m + CH; }
+// (ct, t2, c = w_n xi_a(n), q0[0]) per triple, then per column m >= 1 the
+// prefix q0[m] (W and t^m folded in) and the pair (cos m phi, sin m phi).
+// A role reads a triple with one 4-vector load plus two loads per column
+// m >= 1 (column 0 has cos = 1, sin = 0 and its prefix in the 4-vector).
+__host__ __device__ constexpr int lxs_nfields(int L) { return 4 + 3 * L; }
+__host__ __device__ constexpr int lxs_q0(int CH, int m) { return 4 * CH + 3 * CH * (m - 1); }
+__host__ __device__ constexpr int lxs_cs(int CH, int m) { return 4 * CH + 3 * CH * (m - 1) + CH; }
 template <class Rl> struct V4T;
 template <> struct V4T<float> { typedef float4 T; };
 template <> struct V4T<double> { typedef double4 T; };
+
+// Roles of the fused pass: NR warps share the lmax+1 Legendre columns.  Per
+// triple a column m costs about 5 (m = 0) or 7 (m > 0) operations for each
+// of its lmax+1-m values (recurrence, L* and L contractions) plus a fixed
+// part.  FP64 passes keep the pairing m / lmax-m of k_lstarx (lmax/2+1
+// roles; their summation order, pinned to the oracle's results at 1e-13,
+// stays that of the pairing).  FP32 passes give the columns to the roles
+// greedily, the most expensive first, each to the least-loaded role (lowest
+// index on ties); a role runs its columns in increasing m and holds them in
+// that order in its register arrays.  At lmax 10 the FP32 pass runs four
+// roles of about three columns each (128 registers, four blocks of 128
+// threads per SM): per triple, each role's fixed cost (header load, loop,
+// lx share to shared memory) is paid four times instead of six, 1.25 ms
+// per launch at the 20,000-sphere workload against 1.35 ms for six roles
+// (paired or greedy alike: the SM is issue-bound, and other blocks fill the
+// barrier waits of an uneven role split).
+template <class Rl>
+__host__ __device__ constexpr int lxs_nroles(int L) {
+  return sizeof(Rl) == 4 && L == 10 ? 4 : L / 2 + 1;
+}
+// blocks per SM the pass is compiled for
+template <class Rl>
+__host__ __device__ constexpr int lxs_min_blocks(int L) {
+  return L > 10 ? 1 : sizeof(Rl) == 8 ? 2 : L == 10 ? 4 : 3;
+}
+__host__ __device__ constexpr int lxs_cost(int L, int m) {
+  return m == 0 ? 5 * (L + 1) + 4 : 7 * (L + 1 - m) + 4;
+}
+__host__ __device__ constexpr int lxs_role_of(int L, int NR, int m, bool greedy) {
+  if (!greedy) return m <= L - m ? m : L - m;
+  int load[DDC_MAX_LMAX + 1] = {};
+  int role[DDC_MAX_LMAX + 1] = {};
+  bool done[DDC_MAX_LMAX + 1] = {};
+  for (int k = 0; k <= L; ++k) {
+    int best = -1;
+    for (int c = 0; c <= L; ++c)
+      if (!done[c] && (best < 0 || lxs_cost(L, c) > lxs_cost(L, best))) best = c;
+    int r = 0;
+    for (int s = 1; s < NR; ++s)
+      if (load[s] < load[r]) r = s;
+    done[best] = true;
+    load[r] += lxs_cost(L, best);
+    role[best] = r;
+  }
+  return role[m];
+}
+// offset of column m in its role's register arrays
+__host__ __device__ constexpr int lxs_off_of(int L, int NR, int m, bool g) {
+  int off = 0;
+  for (int c = 0; c < m; ++c)
+    if (lxs_role_of(L, NR, c, g) == lxs_role_of(L, NR, m, g)) off += ls_nvals_m(L, c);
+  return off;
+}
+__host__ __device__ constexpr int lxs_role_nvals(int L, int NR, int r, bool g) {
+  int n = 0;
+  for (int c = 0; c <= L; ++c)
+    if (lxs_role_of(L, NR, c, g) == r) n += ls_nvals_m(L, c);
+  return n;
+}
+__host__ __device__ constexpr int lxs_max_nvals(int L, int NR, bool g) {
+  int mx = 0;
+  for (int r = 0; r < NR; ++r)
+    mx = lxs_role_nvals(L, NR, r, g) > mx ? lxs_role_nvals(L, NR, r, g) : mx;
+  return mx;
+}
+__host__ __device__ constexpr int lxs_first_col(int L, int NR, int r, bool g) {
+  for (int c = 0; c <= L; ++c)
+    if (lxs_role_of(L, NR, c, g) == r) return c;
+  return -1;
+}
 
 template <class Rl> __device__ __forceinline__ Rl cBn(const YlmTables& tb, int e);
 template <> __device__ __forceinline__ double cBn<double>(const YlmTables& tb, int e) { return tb.Bn[e]; }
@@ -2660,51 +2731,94 @@ __device__ __forceinline__ void lxs_load_col(const typename RT<Rl>::V2* __restri
   }
 }
 
-template <int LMAX, int R, class Rl>
+// X_b of role R's columns into its registers
+template <int LMAX, int NR, int R, int M, class Rl>
+__device__ __forceinline__ void lxs_load_cols(const typename RT<Rl>::V2* xb, Rl* xr) {
+  if constexpr (lxs_role_of(LMAX, NR, M, sizeof(Rl) == 4) == R)
+    lxs_load_col<LMAX, M, lxs_off_of(LMAX, NR, M, sizeof(Rl) == 4), Rl>(xb, xr);
+  if constexpr (M < LMAX) lxs_load_cols<LMAX, NR, R, M + 1, Rl>(xb, xr);
+}
+template <int LMAX, int NR, int R, class Rl>
 __device__ __forceinline__ void lxs_load_role(int role, const typename RT<Rl>::V2* xb, Rl* xr) {
   if (role == R) {
-    lxs_load_col<LMAX, R, 0, Rl>(xb, xr);
-    if constexpr (ls_has2(LMAX, R)) lxs_load_col<LMAX, LMAX - R, ls_nvals_m(LMAX, R), Rl>(xb, xr);
+    lxs_load_cols<LMAX, NR, R, 0, Rl>(xb, xr);
     return;
   }
-  if constexpr (R + 1 < ls_nroles(LMAX)) lxs_load_role<LMAX, R + 1, Rl>(role, xb, xr);
+  if constexpr (R + 1 < NR) lxs_load_role<LMAX, NR, R + 1, Rl>(role, xb, xr);
+}
+
+// role R's share of triple q: its columns in increasing m, the lx parts
+// summed in that order
+template <int LMAX, int NR, int R, int M, class Rl, bool LONLY>
+__device__ __forceinline__ void lxs_cols(const YlmTables& tb, const Rl* sh, int q,
+                                         const typename V4T<Rl>::T& h, Rl* acc, const Rl* xr,
+                                         Rl& part) {
+  typedef typename RT<Rl>::V2 V2;
+  constexpr int CH = 32 * NR;
+  if constexpr (lxs_role_of(LMAX, NR, M, sizeof(Rl) == 4) == R) {
+    constexpr int OFF = lxs_off_of(LMAX, NR, M, sizeof(Rl) == 4);
+    Rl v;
+    if constexpr (M == 0) {
+      v = lxs_column<LMAX, 0, OFF, Rl, LONLY>(tb, h.x, h.y, h.w, Rl(1), Rl(0), h.z, acc, xr);
+    } else {
+      const V2 c2 = reinterpret_cast<const V2*>(sh + lxs_cs(CH, M))[q];
+      v = lxs_column<LMAX, M, OFF, Rl, LONLY>(tb, h.x, h.y, sh[lxs_q0(CH, M) + q], c2.x, c2.y,
+                                              h.z, acc, xr);
+    }
+    if constexpr (M == lxs_first_col(LMAX, NR, R, sizeof(Rl) == 4)) part = v;
+    else part += v;
+  }
+  if constexpr (M < LMAX) lxs_cols<LMAX, NR, R, M + 1, Rl, LONLY>(tb, sh, q, h, acc, xr, part);
 }
 
 // lanes take triples q < count of the chunk's fields sh
-template <int LMAX, int R, class Rl, bool LONLY = false>
+template <int LMAX, int NR, int R, class Rl, bool LONLY = false>
 __device__ __forceinline__ void lxs_role(const YlmTables& tb, const Rl* sh, int count, int lane,
                                          Rl* acc, const Rl* xr, Rl* lxp) {
-  typedef typename RT<Rl>::V2 V2;
   typedef typename V4T<Rl>::T V4;
-  constexpr int CH = 32 * ls_nroles(LMAX);
-  constexpr int M1 = R, M2 = LMAX - R;
+  constexpr int CH = 32 * NR;
   const V4* hdr = reinterpret_cast<const V4*>(sh);
-  const Rl* q01 = sh + lxs_q0(CH, M1);
-  const V2* cs1 = reinterpret_cast<const V2*>(sh + lxs_cs(CH, M1));
-  const Rl* q02 = sh + lxs_q0(CH, M2);
-  const V2* cs2 = reinterpret_cast<const V2*>(sh + lxs_cs(CH, M2));
   for (int q = lane; q < count; q += 32) {
     const V4 h = hdr[q];
-    const V2 c1 = cs1[q];
-    Rl part = lxs_column<LMAX, M1, 0, Rl, LONLY>(tb, h.x, h.y, q01[q], c1.x, c1.y, h.z, acc, xr);
-    if constexpr (ls_has2(LMAX, R)) {
-      const V2 c2 = cs2[q];
-      part += lxs_column<LMAX, M2, ls_nvals_m(LMAX, M1), Rl, LONLY>(tb, h.x, h.y, q02[q], c2.x,
-                                                                    c2.y, h.z, acc, xr);
-    }
+    Rl part;
+    lxs_cols<LMAX, NR, R, 0, Rl, LONLY>(tb, sh, q, h, acc, xr, part);
     lxp[R * CH + q] = part;
   }
 }
-template <int LMAX, int R, class Rl, bool LONLY = false>
+template <int LMAX, int NR, int R, class Rl, bool LONLY = false>
 __device__ __forceinline__ void lxs_run_role(int role, const YlmTables& tb, const Rl* sh,
                                              int count, int lane, Rl* acc, const Rl* xr,
                                              Rl* lxp) {
   if (role == R) {
-    lxs_role<LMAX, R, Rl, LONLY>(tb, sh, count, lane, acc, xr, lxp);
+    lxs_role<LMAX, NR, R, Rl, LONLY>(tb, sh, count, lane, acc, xr, lxp);
     return;
   }
-  if constexpr (R + 1 < ls_nroles(LMAX))
-    lxs_run_role<LMAX, R + 1, Rl, LONLY>(role, tb, sh, count, lane, acc, xr, lxp);
+  if constexpr (R + 1 < NR)
+    lxs_run_role<LMAX, NR, R + 1, Rl, LONLY>(role, tb, sh, count, lane, acc, xr, lxp);
+}
+
+// the L* rows of role R: lane sums by a fixed shuffle tree, then its columns
+template <int LMAX, int NR, int R, int M, class Rl, bool GAM>
+__device__ __forceinline__ void lxs_store_cols(const YlmTables& tb, const Rl* acc, double* yi,
+                                               int lane) {
+  if constexpr (lxs_role_of(LMAX, NR, M, sizeof(Rl) == 4) == R)
+    ls_store<LMAX, M, lxs_off_of(LMAX, NR, M, sizeof(Rl) == 4), Rl, GAM>(tb, acc, yi, lane);
+  if constexpr (M < LMAX) lxs_store_cols<LMAX, NR, R, M + 1, Rl, GAM>(tb, acc, yi, lane);
+}
+template <int LMAX, int NR, int R, class Rl, bool GAM>
+__device__ __forceinline__ void lxs_finish_role(int role, const YlmTables& tb, Rl* acc,
+                                                double* yi, int lane) {
+  if (role == R) {
+    constexpr int NV = lxs_role_nvals(LMAX, NR, R, sizeof(Rl) == 4);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+#pragma unroll
+      for (int o = 16; o >= 1; o >>= 1) acc[v] += __shfl_xor_sync(0xffffffffu, acc[v], o);
+    }
+    lxs_store_cols<LMAX, NR, R, 0, Rl, GAM>(tb, acc, yi, lane);
+    return;
+  }
+  if constexpr (R + 1 < NR) lxs_finish_role<LMAX, NR, R + 1, Rl, GAM>(role, tb, acc, yi, lane);
 }
 
 // the inputs of one triple's shared fields, loaded one chunk ahead
@@ -2790,25 +2904,22 @@ __device__ __forceinline__ LxsGeo<Rl> lxs_geom(const YlmTables& tb, double4 ca, 
 }
 // the shared fields of one triple (column tt of the chunk's buffer) from its
 // geometry, grid weight and xi_a(n)
-template <int LMAX, class Rl>
+template <int LMAX, int NR, class Rl>
 __device__ __forceinline__ void lxs_fields(const LxsGeo<Rl>& gm, Rl w, Rl xv, Rl* sh, int tt) {
-  constexpr int CH = 32 * ls_nroles(LMAX);
+  constexpr int CH = 32 * NR;
   typedef typename RT<Rl>::V2 V2;
   typedef typename V4T<Rl>::T V4;
   V4 h;
   h.x = gm.ct;
   h.y = gm.t2;
   h.z = w * xv;
-  h.w = 0;
+  h.w = gm.W;  // q0[0]
   reinterpret_cast<V4*>(sh)[tt] = h;
-  Rl pmm = gm.W, cm = 1, sm = 0, cmm1 = 1, smm1 = 0;
   const Rl cp = gm.cp, sp = gm.sp, st = gm.st;
+  Rl pmm = -gm.W * Rl(1) * st, cm = cp, sm = sp, cmm1 = 1, smm1 = 0;
 #pragma unroll
-  for (int m = 0; m <= LMAX; ++m) {
-    if (m == 1) {
-      cm = cp;
-      sm = sp;
-    } else if (m >= 2) {
+  for (int m = 1; m <= LMAX; ++m) {
+    if (m >= 2) {
       const Rl cn = Rl(2) * cp * cm - cmm1, sn = Rl(2) * cp * sm - smm1;
       cmm1 = cm; smm1 = sm; cm = cn; sm = sn;
     }
@@ -2820,10 +2931,10 @@ __device__ __forceinline__ void lxs_fields(const LxsGeo<Rl>& gm, Rl w, Rl xv, Rl
     pmm = -pmm * Rl(2 * m + 1) * st;
   }
 }
-template <int LMAX, class Rl>
+template <int LMAX, int NR, class Rl>
 __device__ __forceinline__ void lxs_fields(const YlmTables& tb, const LxsIn<Rl>& in, double4 cb,
                                            Rl irb, Rl* sh, int tt) {
-  lxs_fields<LMAX, Rl>(lxs_geom<Rl>(tb, in.ca, in.gn, in.f, cb, irb), in.gn.w, in.xv, sh, tt);
+  lxs_fields<LMAX, NR, Rl>(lxs_geom<Rl>(tb, in.ca, in.gn, in.f, cb, irb), in.gn.w, in.xv, sh, tt);
 }
 // the geometry precomputed at ddinit (DevGeo::tgeo4/tgeo2 in FP32,
 // tgeo4d/tgeo2d in FP64)
@@ -2847,7 +2958,7 @@ __device__ __forceinline__ LxsInP<Rl> lxs_load_pre(const DevGeo& g, const Rl* __
   in.xv = xi ? xi[(size_t)an.x * g.ngrid + an.y] : Rl(0);
   return in;
 }
-template <int LMAX, class Rl>
+template <int LMAX, int NR, class Rl>
 __device__ __forceinline__ void lxs_fields_pre(const LxsInP<Rl>& in, Rl* sh, int tt) {
   LxsGeo<Rl> gm;
   gm.ct = in.g4.x;
@@ -2856,7 +2967,7 @@ __device__ __forceinline__ void lxs_fields_pre(const LxsInP<Rl>& in, Rl* sh, int
   gm.W = in.g4.w;
   gm.cp = in.g2.x;
   gm.sp = in.g2.y;
-  lxs_fields<LMAX, Rl>(gm, in.w, in.xv, sh, tt);
+  lxs_fields<LMAX, NR, Rl>(gm, in.w, in.xv, sh, tt);
 }
 // the geometry of every triple, block per sphere b over its gather list
 template <class Rl>
@@ -2895,21 +3006,21 @@ cudaError_t launch_lxs_geo_f64(Launch L, const YlmTables& tb, const DevGeo& g, d
 // FP32 chunks are double-buffered (software pipeline); FP64 chunks use one
 // buffer so that two blocks fit in shared memory
 template <class Rl> __host__ __device__ constexpr bool lxs_piped() { return sizeof(Rl) == 4; }
-// Up to lmax 10: three blocks per SM in FP32 (at most 112 registers), two in
-// FP64 (at most 168)
+// Blocks per SM: lxs_min_blocks (FP32 at lmax 10: four of 128 threads, at
+// most 128 registers; other FP32 cases three; FP64 two, at most 168)
 // MODE 0: L x (val) and L* xi (y) together; 1: L x only (xi, y unused);
 // 2: L x only with the weight chi(t) in place of chi(t)/f_a(n) (the u_chi sum
 // of the forces, on-the-fly geometry only)
 template <int LMAX, class Rl, bool PRE = false, int MODE = 0>
-__global__ void __launch_bounds__(32 * ls_nroles(LMAX), LMAX > 10 ? 1 : (sizeof(Rl) == 4 ? 3 : 2))
+__global__ void __launch_bounds__(32 * lxs_nroles<Rl>(LMAX), lxs_min_blocks<Rl>(LMAX))
     k_lxs(const YlmTables tb, const DevGeo g, const typename RT<Rl>::V2* __restrict__ XK,
           const Rl* __restrict__ xi, Rl* __restrict__ val, double* __restrict__ y) {
   static_assert(!(PRE && MODE == 2), "chi-only weights need the on-the-fly geometry");
   constexpr bool LONLY = MODE != 0;
-  constexpr int NR = ls_nroles(LMAX);
+  constexpr int NR = lxs_nroles<Rl>(LMAX);
   constexpr int CH = 32 * NR;  // triples per chunk = threads per block
   constexpr int NF = lxs_nfields(LMAX);
-  constexpr int NVM = ls_max_nvals(LMAX);
+  constexpr int NVM = lxs_max_nvals(LMAX, NR, sizeof(Rl) == 4);
   constexpr int NLM = (LMAX + 1) * (LMAX + 2) / 2;
   extern __shared__ __align__(16) unsigned char smraw[];
   constexpr int NBUF = lxs_piped<Rl>() ? 2 : 1;
@@ -2924,7 +3035,7 @@ __global__ void __launch_bounds__(32 * ls_nroles(LMAX), LMAX > 10 ? 1 : (sizeof(
   Rl acc[NVM], xr[NVM];
 #pragma unroll
   for (int v = 0; v < NVM; ++v) acc[v] = xr[v] = 0;
-  lxs_load_role<LMAX, 0, Rl>(role, XK + (size_t)b * NLM, xr);
+  lxs_load_role<LMAX, NR, 0, Rl>(role, XK + (size_t)b * NLM, xr);
   // with the geometry precomputed at ddinit only xi_a(n) and the grid weight
   // are read per triple besides the two geometry vectors
   typedef typename std::conditional<PRE, LxsInP<Rl>, LxsIn<Rl>>::type In;
@@ -2940,8 +3051,8 @@ __global__ void __launch_bounds__(32 * ls_nroles(LMAX), LMAX > 10 ? 1 : (sizeof(
     }
   };
   auto fields = [&](const In& in, Rl* buf) {
-    if constexpr (PRE) lxs_fields_pre<LMAX, Rl>(in, buf, tid);
-    else lxs_fields<LMAX, Rl>(tb, in, cb, irb, buf, tid);
+    if constexpr (PRE) lxs_fields_pre<LMAX, NR, Rl>(in, buf, tid);
+    else lxs_fields<LMAX, NR, Rl>(tb, in, cb, irb, buf, tid);
   };
   if constexpr (!lxs_piped<Rl>()) {
     // FP64: one buffer (two blocks per SM fit), two barriers per chunk; the
@@ -2958,7 +3069,7 @@ __global__ void __launch_bounds__(32 * ls_nroles(LMAX), LMAX > 10 ? 1 : (sizeof(
       const int n2 = k + 2 < nch ? min(CH, q1 - c0 - 2 * CH) : 0;
       if (tid < n1) cur = load(c0 + CH + tid, an1);
       if (tid < n2) an1 = g.ls[c0 + 2 * CH + tid];
-      lxs_run_role<LMAX, 0, Rl, LONLY>(role, tb, fld, cnt, lane, acc, xr, lxp);
+      lxs_run_role<LMAX, NR, 0, Rl, LONLY>(role, tb, fld, cnt, lane, acc, xr, lxp);
       __syncthreads();
       if (tid < cnt) {
         Rl sv = lxp[tid];
@@ -2968,7 +3079,7 @@ __global__ void __launch_bounds__(32 * ls_nroles(LMAX), LMAX > 10 ? 1 : (sizeof(
       }
     }
     if constexpr (!LONLY)
-      ls_finish_role<LMAX, 0, Rl, true>(role, tb, acc, y + (size_t)b * tb.nylm, lane);
+      lxs_finish_role<LMAX, NR, 0, Rl, true>(role, tb, acc, y + (size_t)b * tb.nylm, lane);
     return;
   }
   if (nch > 0 && tid < min(CH, q1 - q0)) fields(load(q0 + tid, g.ls[q0 + tid]), fld);
@@ -2986,7 +3097,7 @@ __global__ void __launch_bounds__(32 * ls_nroles(LMAX), LMAX > 10 ? 1 : (sizeof(
     if (tid < n1) nxt = load(c0 + CH + tid, an1);
     int2 an2 = make_int2(0, 0);
     if (tid < n2) an2 = g.ls[c0 + 2 * CH + tid];
-    lxs_run_role<LMAX, 0, Rl, LONLY>(role, tb, fld + (k & 1) * NF * CH, cnt, lane, acc, xr,
+    lxs_run_role<LMAX, NR, 0, Rl, LONLY>(role, tb, fld + (k & 1) * NF * CH, cnt, lane, acc, xr,
                                      lxp + (k & 1) * NR * CH);
     if (tid < n1) fields(nxt, fld + ((k + 1) & 1) * NF * CH);
     __syncthreads();
@@ -3002,7 +3113,7 @@ __global__ void __launch_bounds__(32 * ls_nroles(LMAX), LMAX > 10 ? 1 : (sizeof(
     an1 = an2;
   }
   if constexpr (!LONLY)
-    ls_finish_role<LMAX, 0, Rl, true>(role, tb, acc, y + (size_t)b * tb.nylm, lane);
+    lxs_finish_role<LMAX, NR, 0, Rl, true>(role, tb, acc, y + (size_t)b * tb.nylm, lane);
 }
 
 // pot_a(n) = sum over a's CSR pairs (a, b) of the lx values of the triples
@@ -3092,7 +3203,7 @@ static cudaError_t lxs_launch(Launch L, const YlmTables& tb, const DevGeo& g, co
   if (e) return e;
 #define CASE(LV)                                                                              \
   case LV: {                                                                                  \
-    constexpr int NR = ls_nroles(LV);                                                         \
+    constexpr int NR = lxs_nroles<Rl>(LV);                                                    \
     const size_t sm = sizeof(Rl) * (lxs_piped<Rl>() ? 2 : 1) * (lxs_nfields(LV) + NR) * 32 * NR; \
     const bool pre = MODE != 2 && (sizeof(Rl) == 4 ? g.tgeo4 != nullptr : g.tgeo4d != nullptr); \
     auto kfn = pre ? k_lxs<LV, Rl, MODE != 2, MODE> : k_lxs<LV, Rl, false, MODE>;             \
@@ -3654,7 +3765,7 @@ __global__ void k_far_tables(const YlmTables tb, const double4* __restrict__ gri
 // Potential and field at the cavity points of sphere i (block per sphere):
 // the near charges directly (compacted into shared memory in passes of at
 // most kNearCap), the far ones from A(i).  With ef == nullptr only phi.
-constexpr int kNearCap = 2048;
+constexpr int kNearCap = 1024;
 __global__ void __launch_bounds__(128) k_far_cav(int nsph, int ngrid, int ny,
                                                  const double4* __restrict__ sph,
                                                  const double* __restrict__ q,
@@ -3666,7 +3777,7 @@ __global__ void __launch_bounds__(128) k_far_cav(int nsph, int ngrid, int ny,
                                                  const double* __restrict__ BT,
                                                  const double* __restrict__ DT, double* phi,
                                                  double* ef) {
-  extern __shared__ double4 near[];  // [kNearCap], dynamic (64 KB)
+  __shared__ double4 near[kNearCap];
   __shared__ double sA[(DDC_MAX_LMAX + 1) * (DDC_MAX_LMAX + 1)];
   __shared__ int s_cnt, s_scan;
   const int i = blockIdx.x, tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
@@ -3699,46 +3810,33 @@ __global__ void __launch_bounds__(128) k_far_cav(int nsph, int ngrid, int ny,
     const int start = s_scan;
     if (start >= hi) break;
     int j = start;
-    // scan in steps of 512 candidates (four per thread) while the buffer has
-    // room for a step; list order: sub-step, warp, lane (deterministic)
-    for (; j < hi; j += 512) {
+    // scan in steps of 128 candidates while the buffer has room for a step
+    for (; j < hi; j += 128) {
       __syncthreads();
-      if (s_cnt + 512 > kNearCap) break;
-      bool nb[4];
-      double4 cj[4];
-      unsigned bal[4];
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int jj = j + 128 * u + tid;
-        nb[u] = false;
-        cj[u] = make_double4(0, 0, 0, 0);
-        if (jj < hi) {
-          cj[u] = sph[jj];
-          cj[u].w = q[jj];
-          const double dx = cj[u].x - ci.x, dy = cj[u].y - ci.y, dz = cj[u].z - ci.z;
-          nb[u] = jj == i || dx * dx + dy * dy + dz * dz <= cut2;
-        }
-        bal[u] = __ballot_sync(0xffffffffu, nb[u]);
+      if (s_cnt + 128 > kNearCap) break;
+      const int jj = j + tid;
+      bool nb = false;
+      double4 cj = make_double4(0, 0, 0, 0);
+      if (jj < hi) {
+        cj = sph[jj];
+        const double dx = cj.x - ci.x, dy = cj.y - ci.y, dz = cj.z - ci.z;
+        nb = jj == i || dx * dx + dy * dy + dz * dz <= cut2;
       }
-      __shared__ int wbase[4][4];
-      if (lane == 0)
-#pragma unroll
-        for (int u = 0; u < 4; ++u) wbase[u][w] = __popc(bal[u]);
+      const unsigned bal = __ballot_sync(0xffffffffu, nb);
+      __shared__ int wbase[4];
+      if (lane == 0) wbase[w] = __popc(bal);
       __syncthreads();
       if (tid == 0) {
         int b = s_cnt;
-        for (int u = 0; u < 4; ++u)
-          for (int k = 0; k < 4; ++k) {
-            const int c = wbase[u][k];
-            wbase[u][k] = b;
-            b += c;
-          }
+        for (int k = 0; k < 4; ++k) {
+          const int c = wbase[k];
+          wbase[k] = b;
+          b += c;
+        }
         s_cnt = b;
       }
       __syncthreads();
-#pragma unroll
-      for (int u = 0; u < 4; ++u)
-        if (nb[u]) near[wbase[u][w] + __popc(bal[u] & ((1u << lane) - 1u))] = cj[u];
+      if (nb) near[wbase[w] + __popc(bal & ((1u << lane) - 1u))] = make_double4(cj.x, cj.y, cj.z, q[jj]);
     }
     __syncthreads();
     if (tid == 0) s_scan = j;
@@ -3821,11 +3919,8 @@ cudaError_t launch_far_pot_field(Launch L, const YlmTables& tbP, int nsph, int n
 #undef CASE
   ++*L.launches;
   if ((e = cudaGetLastError())) return e;
-  const int smn = (int)sizeof(double4) * kNearCap;
-  if ((e = cudaFuncSetAttribute(k_far_cav, cudaFuncAttributeMaxDynamicSharedMemorySize, smn)))
-    return e;
-  k_far_cav<<<nsph, 128, smn, L.st>>>(nsph, ngrid, tbP.nylm, sph, q, mrange, rho, cavoff, cavpt,
-                                      ccav, A, BT, DT, phi, ef);
+  k_far_cav<<<nsph, 128, 0, L.st>>>(nsph, ngrid, tbP.nylm, sph, q, mrange, rho, cavoff, cavpt,
+                                    ccav, A, BT, DT, phi, ef);
   ++*L.launches;
   return cudaGetLastError();
 }
