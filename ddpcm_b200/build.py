@@ -16,7 +16,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libddcosmo_gpu.so")
-SOURCES = ["ddc_api.cu", "ddc_kernels.cu", "ddc_tc.cu", "ddc_guess.cu", "ddc_noalloc.cu"]
+SOURCES = ["ddc_api.cu", "ddc_kernels.cu", "ddc_tc.cu", "ddc_guess.cu", "ddc_noalloc.cu",
+           "ddc_zfar.cu"]
 HEADERS = ["ddc_internal.h", "lebedev_orbits.inc"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

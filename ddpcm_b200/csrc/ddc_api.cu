@@ -169,6 +169,10 @@ struct ddc_ctx {
   YlmTables tbP{};
   DBuf farBT, farDT, farA;
   bool far_on = false;
+  // grouped multipole field of zeta at the nuclei (mixed energy+force flow)
+  DBuf zg_cell, zg_sph, zg_start, zg_cen, zg_npt, zg_ptr, zg_cnt, zg_tmp, zg_M, zg_pk, zg_scr;
+  ZGroups zg;
+  bool zfar_on = false;
   // pinned landing buffer of the small device-to-host reads (reduced sums)
   double* hred = nullptr;
   // second stream of the force tail: the field of zeta at the nuclei runs
@@ -660,6 +664,36 @@ int do_init(ddc_ctx* ctx, int n, const std::vector<double4>* hsph, const double4
       CK(ctx->farA.ensure(sizeof(double) * (size_t)YP * N));
       CK(launch_far_tables(L, ctx->tbP, ctx->grid.as<double4>(), G, ctx->farBT.as<double>(),
                            ctx->farDT.as<double>()));
+    }
+    // the field of zeta at the nuclei of one large molecule in the mixed
+    // flow: spheres grouped for the multipole far field (DDC_ZFAR_OFF=1, or
+    // DDC_FAR_OFF=1, keeps the direct FP32 pair sums)
+    const char* zoff = std::getenv("DDC_ZFAR_OFF");
+    ctx->zfar_on = ctx->prm.precision == DDC_PREC_MIXED && ctx->prm.igrad && ctx->nmol <= 1 &&
+                   N >= kZetaMinSpheres && !(off && off[0] == '1') && !(zoff && zoff[0] == '1');
+    if (ctx->zfar_on) {
+      CK(ctx->zg_cell.ensure(sizeof(int) * N));
+      CK(ctx->zg_sph.ensure(sizeof(int) * N));
+      CK(ctx->zg_start.ensure(sizeof(int) * (N + 1)));
+      CK(ctx->zg_cen.ensure(sizeof(double4) * N));
+      CK(ctx->zg_npt.ensure(sizeof(int) * (N + 1)));
+      CK(ctx->zg_ptr.ensure(sizeof(int) * (N + 1)));
+      CK(ctx->zg_cnt.ensure(sizeof(int)));
+      const size_t tb = zgroups_scan_bytes(N);
+      CK(ctx->zg_tmp.ensure(tb));
+      ZGroups& z = ctx->zg;
+      z.cellid = ctx->zg_cell.as<int>();
+      z.gsph = ctx->zg_sph.as<int>();
+      z.gstart = ctx->zg_start.as<int>();
+      z.gcen = ctx->zg_cen.as<double4>();
+      z.gnpt = ctx->zg_npt.as<int>();
+      z.gptr = ctx->zg_ptr.as<int>();
+      CK(launch_zgroups_build(L, N, ctx->sph.as<double4>(), ctx->cavoff.as<int>(), z,
+                              ctx->zg_cnt.as<int>(), reinterpret_cast<int*>(ctx->hred),
+                              ctx->zg_tmp.p, tb));
+      CK(ctx->zg_M.ensure(sizeof(float2) * zgroups_moment_count(z)));
+      CK(ctx->zg_pk.ensure(sizeof(float4) * std::max(ctx->ncav, 1)));
+      CK(ctx->zg_scr.ensure(sizeof(double) * 3 * (size_t)zgroups_nchunk(z) * N));
     }
   }
   CKI(sync(ctx));
@@ -2042,16 +2076,24 @@ int ddc_energy_forces(ddc_ctx* ctx, int n, const double* charge, const double* x
     CK(ctx->ef2.ensure(sizeof(double) * 3 * std::max(N, 1)));
     const bool mixed = ctx->prm.precision == DDC_PREC_MIXED;
     const int ch2 = mixed ? efield_chunks_f32(NC, N) : efield_chunks(NC, N);
-    CK(ctx->ef_scratch.ensure(sizeof(double) * 3 * ((size_t)ch2 * N + 1)));
-    // in mixed precision the force-only field of zeta uses FP32 pair arithmetic
+    if (!ctx->zfar_on) CK(ctx->ef_scratch.ensure(sizeof(double) * 3 * ((size_t)ch2 * N + 1)));
+    // in mixed precision the force-only field of zeta uses FP32 pair
+    // arithmetic, with the grouped multipole far field for large molecules
     auto efield = mixed ? launch_efield_f32 : launch_efield;
     CK(cudaEventRecord(ctx->ev_fork, ctx->st));
     CK(cudaStreamWaitEvent(ctx->st2, ctx->ev_fork, 0));
     {
       StageScope sc(ctx, ST_EFIELD, ctx->st2);
-      CK(efield(Launch{ctx->st2, &ctx->launches}, NC, ctx->zeta.as<double>(),
-                ctx->ccav.as<double>(), N, ctx->csph.as<double>(), ctx->ef2.as<double>(),
-                ctx->ef_scratch.as<double>(), ch2, nullptr));
+      if (ctx->zfar_on)
+        CK(launch_zeta_field_far(Launch{ctx->st2, &ctx->launches}, N, ctx->sph.as<double4>(),
+                                 ctx->cavoff.as<int>(), ctx->ccav.as<double>(),
+                                 ctx->zeta.as<double>(), ctx->zg, ctx->zg_pk.as<float4>(),
+                                 ctx->zg_M.as<float2>(), ctx->zg_scr.as<double>(),
+                                 ctx->ef2.as<double>()));
+      else
+        CK(efield(Launch{ctx->st2, &ctx->launches}, NC, ctx->zeta.as<double>(),
+                  ctx->ccav.as<double>(), N, ctx->csph.as<double>(), ctx->ef2.as<double>(),
+                  ctx->ef_scratch.as<double>(), ch2, nullptr));
     }
     CK(cudaEventRecord(ctx->ev_join, ctx->st2));
     // forces and the zeta contraction on the main stream; whatever happens

@@ -322,6 +322,37 @@ cudaError_t launch_far_pot_field(Launch L, const YlmTables& tbP, int nsph, int n
                                  double rho, const int* cavoff, const int* cavpt,
                                  const double* ccav, const double* BT, const double* DT,
                                  double* A, double* phi, double* ef);
+// Field of the cavity charges zeta at the nuclei in the mixed-precision
+// energy+force flow (force-only, FP32 pair arithmetic): from
+// kZetaMinSpheres spheres on, the spheres are grouped by the cells of a
+// uniform grid (side >= kZetaCell bohr, Morton order), and a group farther
+// than kZetaRho group radii from a nucleus acts through its multipole
+// expansion of degree kZetaDegree; nearer groups are summed directly
+constexpr int kZetaDegree = 16;
+constexpr double kZetaRho = 3.0;
+constexpr double kZetaCell = 12.0;
+constexpr int kZetaMinSpheres = 4096;
+struct ZGroups {
+  int ngroup = 0;
+  int* cellid = nullptr;   // [nsph] scratch
+  int* gsph = nullptr;     // [nsph] spheres in group order
+  int* gstart = nullptr;   // [nsph+1] group g owns gsph[gstart[g] .. gstart[g+1])
+  double4* gcen = nullptr; // [nsph] centroid and radius of each group
+  int* gnpt = nullptr;     // [nsph+1] cavity points per group
+  int* gptr = nullptr;     // [nsph+1] their exclusive scan
+};
+size_t zgroups_scan_bytes(int nsph);
+// builds the groups (one host read of the group count)
+cudaError_t launch_zgroups_build(Launch L, int nsph, const double4* sph, const int* cavoff,
+                                 ZGroups& zg, int* dcount, int* hcount, void* scan_tmp,
+                                 size_t scan_bytes);
+int zgroups_nchunk(const ZGroups& zg);
+size_t zgroups_moment_count(const ZGroups& zg);
+// ef(3, nsph) from zeta(ncav); zpk[ncav], M[moment count], scratch
+// [nchunk][nsph][3]
+cudaError_t launch_zeta_field_far(Launch L, int nsph, const double4* sph, const int* cavoff,
+                                  const double* ccav, const double* zeta, const ZGroups& zg,
+                                  float4* zpk, float2* M, double* scratch, double* ef);
 // trange: per target, the source index range it sums over (nullptr: all)
 // launch_coulomb_pot plus the field of the same sources at the targets, ef (3, ntrg)
 cudaError_t launch_coulomb_pot_field(Launch L, int nsrc, const double* q, const double* sx,
