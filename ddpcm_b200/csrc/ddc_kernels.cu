@@ -953,6 +953,17 @@ __device__ __forceinline__ void cp_async8(void* sdst, const void* gsrc, bool val
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(gsrc), "r"(n)
                : "memory");
 }
+__device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
 __global__ void __launch_bounds__(256, 3) k_dgemm_dmma(int M, int N, int K, double alpha,
                                                        const double* __restrict__ A, int lda,
                                                        const double* __restrict__ B, int ldb,
@@ -3082,6 +3093,73 @@ __global__ void __launch_bounds__(32 * lxs_nroles<Rl>(LMAX), lxs_min_blocks<Rl>(
       lxs_finish_role<LMAX, NR, 0, Rl, true>(role, tb, acc, y + (size_t)b * tb.nylm, lane);
     return;
   }
+  if constexpr (PRE && lxs_piped<Rl>()) {
+    // FP32 with the geometry precomputed at ddinit: each thread copies its
+    // triple's two geometry vectors (24 bytes) to its own shared slot with
+    // cp.async two chunks ahead of their use (two chunks of role work cover
+    // the latency, and no registers hold them meanwhile; a thread reads only
+    // the slot it wrote, after its own wait_group).  The grid weight and
+    // xi_a(n) come through registers one chunk ahead, the gather-list entry
+    // that addresses them two chunks ahead.  (xi_a(n) by cp.async as well
+    // was slower: the copy's issue waits for its gather-list entry.)
+    typename V4T<Rl>::T* gs4 = reinterpret_cast<typename V4T<Rl>::T*>(lxp + NBUF * NR * CH);
+    typename RT<Rl>::V2* gs2 = reinterpret_cast<typename RT<Rl>::V2*>(gs4 + 2 * CH);
+    auto geo_copy = [&](int k) {  // chunk k's geometry into stage k & 1
+      const int q = q0 + k * CH + tid;
+      if (k < nch && q < q1) {
+        cp_async16(gs4 + (k & 1) * CH + tid, g.tgeo4 + q);
+        cp_async8(gs2 + (k & 1) * CH + tid, g.tgeo2 + q, true);
+      }
+      cp_async_commit();
+    };
+    auto wx = [&](int2 an, Rl& w, Rl& xv) {
+      w = grid_pt(g, an.y, (Rl*)nullptr).w;
+      xv = LONLY ? Rl(0) : xi[(size_t)an.x * g.ngrid + an.y];
+    };
+    auto fields_at = [&](int k, Rl w, Rl xv) {
+      LxsInP<Rl> in;
+      in.g4 = gs4[(k & 1) * CH + tid];
+      in.g2 = gs2[(k & 1) * CH + tid];
+      in.w = w;
+      in.xv = xv;
+      lxs_fields_pre<LMAX, NR, Rl>(in, fld + (k & 1) * NF * CH, tid);
+    };
+    geo_copy(0);
+    geo_copy(1);
+    Rl w1 = 0, xv1 = 0;
+    int2 an1 = make_int2(0, 0);
+    if (nch > 0 && tid < min(CH, q1 - q0)) wx(g.ls[q0 + tid], w1, xv1);
+    if (nch > 1 && tid < min(CH, q1 - q0 - CH)) an1 = g.ls[q0 + CH + tid];
+    cp_async_wait<1>();
+    if (nch > 0 && tid < min(CH, q1 - q0)) fields_at(0, w1, xv1);
+    __syncthreads();
+    for (int k = 0; k < nch; ++k) {
+      const int c0 = q0 + k * CH, cnt = min(CH, q1 - c0);
+      const int n1 = k + 1 < nch ? min(CH, q1 - c0 - CH) : 0;
+      const int n2 = k + 2 < nch ? min(CH, q1 - c0 - 2 * CH) : 0;
+      geo_copy(k + 2);
+      if (tid < n1) wx(an1, w1, xv1);
+      int2 an2 = make_int2(0, 0);
+      if (tid < n2) an2 = g.ls[c0 + 2 * CH + tid];
+      lxs_run_role<LMAX, NR, 0, Rl, LONLY>(role, tb, fld + (k & 1) * NF * CH, cnt, lane, acc,
+                                           xr, lxp + (k & 1) * NR * CH);
+      cp_async_wait<1>();  // chunk k+1's copies done (chunk k+2's may be in flight)
+      if (tid < n1) fields_at(k + 1, w1, xv1);
+      __syncthreads();
+      if (tid < cnt) {
+        const Rl* lp = lxp + (k & 1) * NR * CH;
+        Rl sv = lp[tid];
+#pragma unroll
+        for (int r = 1; r < NR; ++r) sv += lp[r * CH + tid];
+        val[c0 + tid] = sv;
+      }
+      an1 = an2;
+    }
+    cp_async_wait<0>();
+    if constexpr (!LONLY)
+      lxs_finish_role<LMAX, NR, 0, Rl, true>(role, tb, acc, y + (size_t)b * tb.nylm, lane);
+    return;
+  }
   if (nch > 0 && tid < min(CH, q1 - q0)) fields(load(q0 + tid, g.ls[q0 + tid]), fld);
   int2 an1 = make_int2(0, 0);
   if (nch > 1 && tid < min(CH, q1 - q0 - CH)) an1 = g.ls[q0 + CH + tid];
@@ -3204,8 +3282,9 @@ static cudaError_t lxs_launch(Launch L, const YlmTables& tb, const DevGeo& g, co
 #define CASE(LV)                                                                              \
   case LV: {                                                                                  \
     constexpr int NR = lxs_nroles<Rl>(LV);                                                    \
-    const size_t sm = sizeof(Rl) * (lxs_piped<Rl>() ? 2 : 1) * (lxs_nfields(LV) + NR) * 32 * NR; \
     const bool pre = MODE != 2 && (sizeof(Rl) == 4 ? g.tgeo4 != nullptr : g.tgeo4d != nullptr); \
+    const size_t sm = sizeof(Rl) * (lxs_piped<Rl>() ? 2 : 1) * (lxs_nfields(LV) + NR) * 32 * NR + \
+                      (pre && lxs_piped<Rl>() ? 2 * 32 * NR * 6 * sizeof(Rl) : 0);             \
     auto kfn = pre ? k_lxs<LV, Rl, MODE != 2, MODE> : k_lxs<LV, Rl, false, MODE>;             \
     if (sm > 48 * 1024) {                                                                     \
       if ((e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize,         \

@@ -24,7 +24,8 @@
 // group's expansion (truncation below (1/3)^17 / (1 - 1/3) = 1.2e-8 of the
 // group's charge scale, under the FP32 rounding of the pair sums); a warp
 // whose 32 nuclei are not all far sums the group's points directly (FP32
-// pairs as in k_efield_f2, flushed to FP64 every 256 points).  The moments
+// pairs as in k_efield_f2, in warp tiles of 32 points staged in shared
+// memory, flushed to FP64 every 256 points).  The moments
 // are accumulated in FP64 and stored in FP32 (scaled coordinates keep every
 // term of order one); the evaluation runs in FP32 and each group's
 // contribution is added in FP64.  Every sum has a fixed order: per target,
@@ -418,6 +419,7 @@ __global__ void __launch_bounds__(kZTile) k_zg_field(int nsph, int ngroup,
   __shared__ float2 sM[kZChunk][kZNM];
   __shared__ double4 sC[kZChunk];
   __shared__ int sP[kZChunk + 1];
+  __shared__ float4 sT[kZTile / 32][32];  // per-warp point tiles of the direct sums
   const int tid = threadIdx.x, ch = blockIdx.y;
   const int g0 = ch * kZChunk, ng = min(ngroup - g0, kZChunk);
   for (int e = tid; e < ng * kZNM; e += kZTile) sM[e / kZNM][e % kZNM] = M[(size_t)g0 * kZNM + e];
@@ -442,14 +444,26 @@ __global__ void __launch_bounds__(kZTile) k_zg_field(int nsph, int ngroup,
       ey += (double)fy * s;
       ez += (double)fz * s;
     } else {
+      // the warp's own tiles of 32 points: one coalesced load per lane (the
+      // next tile's in flight while this one is summed), broadcast reads
+      // from shared memory; the padding of a last partial tile has charge
+      // zero and sits far away
+      const int w = tid >> 5, lane = tid & 31;
       const float vx = (float)dx, vy = (float)dy, vz = (float)dz;
-      const int k1 = sP[gi + 1];
-      for (int k0 = sP[gi]; k0 < k1; k0 += 256) {
-        const int ke = min(k1, k0 + 256);
-        float fx = 0.f, fy = 0.f, fz = 0.f;
-#pragma unroll 4
-        for (int k = k0; k < ke; ++k) {
-          const float4 p = zpk[k];
+      const int kb = sP[gi], k1 = sP[gi + 1];
+      const float4 pad = make_float4(1e4f, 1e4f, 1e4f, 0.f);
+      float4 nxt = kb + lane < k1 ? zpk[kb + lane] : pad;
+      float fx = 0.f, fy = 0.f, fz = 0.f;
+      int t = 0;
+      for (int k0 = kb; k0 < k1; k0 += 32, ++t) {
+        __syncwarp();
+        sT[w][lane] = nxt;
+        __syncwarp();
+        const int kn = k0 + 32 + lane;
+        nxt = kn < k1 ? zpk[kn] : pad;
+#pragma unroll 8
+        for (int j = 0; j < 32; ++j) {
+          const float4 p = sT[w][j];
           const float qx = vx - p.x, qy = vy - p.y, qz = vz - p.z;
           const float r2 = fmaf(qx, qx, fmaf(qy, qy, qz * qz));
           const float ri = rsqrtf(r2);
@@ -458,10 +472,16 @@ __global__ void __launch_bounds__(kZTile) k_zg_field(int nsph, int ngroup,
           fy = fmaf(wv, qy, fy);
           fz = fmaf(wv, qz, fz);
         }
-        ex += fx;
-        ey += fy;
-        ez += fz;
+        if ((t & 7) == 7) {  // FP32 partial sums of 256 points into FP64
+          ex += fx;
+          ey += fy;
+          ez += fz;
+          fx = fy = fz = 0.f;
+        }
       }
+      ex += fx;
+      ey += fy;
+      ez += fz;
     }
   }
   if (act) {
