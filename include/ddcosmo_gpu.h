@@ -63,7 +63,8 @@ typedef struct {
   double eta;          /* switch-function regularisation */
   int iprint;          /* >0: print the iteration log like jacobi_diis */
   int max_iter;        /* 200 in the reference */
-  int ndiis;           /* 25 in the reference; 0 disables DIIS */
+  int ndiis;           /* 25 in the reference; 0 disables DIIS (the FP32 inner
+                        * solves of DDC_PREC_MIXED keep at most 15) */
   int precision;       /* DDC_PREC_* */
   int guess;           /* DDC_GUESS_* */
   int device;          /* CUDA device ordinal */
