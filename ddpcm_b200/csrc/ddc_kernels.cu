@@ -3744,12 +3744,14 @@ __global__ void __launch_bounds__(32 * ls_nroles(LMAX)) k_far_acc(const YlmTable
                                                                    const double4* __restrict__ sph,
                                                                    const double* __restrict__ q,
                                                                    const int2* __restrict__ mrange,
+                                                                   const int* __restrict__ cavoff,
                                                                    double rho, double* A) {
   constexpr int NR = ls_nroles(LMAX);
   constexpr int CH = 32 * NR;
   constexpr int NVM = ls_max_nvals(LMAX);
   extern __shared__ double sh[];  // [ls_nfields][CH]
   const int i = blockIdx.x;
+  if (cavoff[i + 1] == cavoff[i]) return;  // buried: A(i) is never read
   const int role = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const double4 ci = sph[i];
   const double cut2 = (rho * ci.w) * (rho * ci.w);
@@ -3843,34 +3845,28 @@ __global__ void k_far_tables(const YlmTables tb, const double4* __restrict__ gri
 
 // Potential and field at the cavity points of sphere i (block per sphere):
 // the near charges directly (compacted into shared memory in passes of at
-// most kNearCap), the far ones from A(i).  With ef == nullptr only phi.
+// most kNearCap), the far ones from A(i).  With ef == nullptr only phi.  A
+// sphere without cavity points (buried) has nothing to do; the others run
+// with NU = ceil(points / 128) point slots per thread (a sphere has 90
+// points on average at the 20k workload, up to 590), so no thread steps
+// through empty slots in the pair loop.
 constexpr int kNearCap = 1024;
-__global__ void __launch_bounds__(128) k_far_cav(int nsph, int ngrid, int ny,
-                                                 const double4* __restrict__ sph,
-                                                 const double* __restrict__ q,
-                                                 const int2* __restrict__ mrange, double rho,
-                                                 const int* __restrict__ cavoff,
-                                                 const int* __restrict__ cavpt,
-                                                 const double* __restrict__ ccav,
-                                                 const double* __restrict__ A,
-                                                 const double* __restrict__ BT,
-                                                 const double* __restrict__ DT, double* phi,
-                                                 double* ef) {
-  __shared__ double4 near[kNearCap];
-  __shared__ double sA[(DDC_MAX_LMAX + 1) * (DDC_MAX_LMAX + 1)];
-  __shared__ int s_cnt, s_scan;
-  const int i = blockIdx.x, tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-  const double4 ci = sph[i];
-  const double cut2 = (rho * ci.w) * (rho * ci.w);
-  const int lo = mrange ? mrange[i].x : 0, hi = mrange ? mrange[i].y : nsph;
-  const int c0 = cavoff[i], c1 = cavoff[i + 1];
-  for (int lm = tid; lm < ny; lm += blockDim.x) sA[lm] = A[(size_t)i * ny + lm];
-  // every thread owns cavity points c0 + tid, c0 + tid + 128, ... (at most
-  // ngrid per sphere): accumulators for up to kPts of them
-  constexpr int kPts = 5;  // 5 * 128 = 640 >= ngrid up to 590 points
-  double v[kPts], ex[kPts], ey[kPts], ez[kPts], px[kPts], py[kPts], pz[kPts];
+template <int NU>
+__device__ __forceinline__ void far_cav_body(int i, int ngrid, int ny, double4 ci, double cut2,
+                                             int lo, int hi, int c0, int c1,
+                                             const double4* __restrict__ sph,
+                                             const double* __restrict__ q,
+                                             const int* __restrict__ cavpt,
+                                             const double* __restrict__ ccav,
+                                             const double* __restrict__ BT,
+                                             const double* __restrict__ DT, double* phi,
+                                             double* ef, double4* near, const double* sA,
+                                             int& s_cnt, int& s_scan, int* wbase) {
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  // thread tid owns cavity points c0 + tid + 128 u, u < NU
+  double v[NU], ex[NU], ey[NU], ez[NU], px[NU], py[NU], pz[NU];
 #pragma unroll
-  for (int u = 0; u < kPts; ++u) {
+  for (int u = 0; u < NU; ++u) {
     v[u] = ex[u] = ey[u] = ez[u] = 0.0;
     const int c = c0 + tid + 128 * u;
     px[u] = py[u] = pz[u] = 0.0;
@@ -3902,7 +3898,6 @@ __global__ void __launch_bounds__(128) k_far_cav(int nsph, int ngrid, int ny,
         nb = jj == i || dx * dx + dy * dy + dz * dz <= cut2;
       }
       const unsigned bal = __ballot_sync(0xffffffffu, nb);
-      __shared__ int wbase[4];
       if (lane == 0) wbase[w] = __popc(bal);
       __syncthreads();
       if (tid == 0) {
@@ -3923,7 +3918,7 @@ __global__ void __launch_bounds__(128) k_far_cav(int nsph, int ngrid, int ny,
     for (int k = 0; k < cnt; ++k) {
       const double4 s = near[k];
 #pragma unroll
-      for (int u = 0; u < kPts; ++u) {
+      for (int u = 0; u < NU; ++u) {
         if (c0 + tid + 128 * u < c1) {
           const double dx = px[u] - s.x, dy = py[u] - s.y, dz = pz[u] - s.z;
           const double ri = rsqrt_pos(dx * dx + dy * dy + dz * dz);
@@ -3940,7 +3935,7 @@ __global__ void __launch_bounds__(128) k_far_cav(int nsph, int ngrid, int ny,
   // far part from the local expansion
   const double iri = 1.0 / ci.w;
 #pragma unroll
-  for (int u = 0; u < kPts; ++u) {
+  for (int u = 0; u < NU; ++u) {
     const int c = c0 + tid + 128 * u;
     if (c >= c1) continue;
     const int n = cavpt[c] - i * ngrid;
@@ -3960,6 +3955,45 @@ __global__ void __launch_bounds__(128) k_far_cav(int nsph, int ngrid, int ny,
       ef[3 * (size_t)c + 1] = ey[u] - iri * fy;
       ef[3 * (size_t)c + 2] = ez[u] - iri * fz;
     }
+  }
+}
+
+__global__ void __launch_bounds__(128) k_far_cav(int nsph, int ngrid, int ny,
+                                                 const double4* __restrict__ sph,
+                                                 const double* __restrict__ q,
+                                                 const int2* __restrict__ mrange, double rho,
+                                                 const int* __restrict__ cavoff,
+                                                 const int* __restrict__ cavpt,
+                                                 const double* __restrict__ ccav,
+                                                 const double* __restrict__ A,
+                                                 const double* __restrict__ BT,
+                                                 const double* __restrict__ DT, double* phi,
+                                                 double* ef) {
+  __shared__ double4 near[kNearCap];
+  __shared__ double sA[(DDC_MAX_LMAX + 1) * (DDC_MAX_LMAX + 1)];
+  __shared__ int s_cnt, s_scan, wbase[4];
+  const int i = blockIdx.x;
+  const int c0 = cavoff[i], c1 = cavoff[i + 1];
+  if (c1 == c0) return;  // buried: no cavity points
+  const double4 ci = sph[i];
+  const double cut2 = (rho * ci.w) * (rho * ci.w);
+  const int lo = mrange ? mrange[i].x : 0, hi = mrange ? mrange[i].y : nsph;
+  for (int lm = threadIdx.x; lm < ny; lm += blockDim.x) sA[lm] = A[(size_t)i * ny + lm];
+  // 5 * 128 = 640 >= ngrid up to 590 points
+  switch ((c1 - c0 + 127) / 128) {
+#define FAR_CAV_CASE(NU)                                                                        \
+  case NU:                                                                                      \
+    far_cav_body<NU>(i, ngrid, ny, ci, cut2, lo, hi, c0, c1, sph, q, cavpt, ccav, BT, DT, phi, \
+                     ef, near, sA, s_cnt, s_scan, wbase);                                       \
+    break;
+    FAR_CAV_CASE(1)
+    FAR_CAV_CASE(2)
+    FAR_CAV_CASE(3)
+    FAR_CAV_CASE(4)
+    FAR_CAV_CASE(5)
+#undef FAR_CAV_CASE
+    default:
+      break;
   }
 }
 
@@ -3987,7 +4021,7 @@ cudaError_t launch_far_pot_field(Launch L, const YlmTables& tbP, int nsph, int n
       if ((e = cudaFuncSetAttribute(k_far_acc<LV>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
                                     (int)sm)))                                                \
         return e;                                                                             \
-    k_far_acc<LV><<<nsph, 32 * NR, sm, L.st>>>(tbP, nsph, sph, q, mrange, rho, A);            \
+    k_far_acc<LV><<<nsph, 32 * NR, sm, L.st>>>(tbP, nsph, sph, q, mrange, cavoff, rho, A);    \
     break;                                                                                    \
   }
   switch (tbP.lmax) {
