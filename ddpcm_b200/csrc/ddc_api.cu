@@ -138,6 +138,7 @@ struct ddc_ctx {
   DBuf csph, cx, cy, cz;  // csph(3,n) and SoA centres
   // work
   DBuf pot, xig, gbuf, rhs, x, y, xn, partials, red, hist_x, hist_e;
+  DBuf rcount;  // arrival counter of the solver kernels' last-block sums (kept zero)
   DBuf phi, psi, sigma, s, q, fx, zeta, ef1, ef2, ef_scratch, uchi;
   DBuf in1, in2, in3, in4, out1;  // staging for host-pointer calls
   // mixed precision: FP32 grid/basis copies, FP32 grid fields, refinement vectors
@@ -419,6 +420,17 @@ int reduce_to_host(ddc_ctx* ctx, int nvals, double* host, int stride = 1, int nb
   return DDC_OK;
 }
 
+// values the last block of a solver kernel already summed into red
+int read_reduced(ddc_ctx* ctx, int nvals, double* host) {
+  if (nvals > kMaxHist + 1 || !ctx->hred)
+    return fail(ctx, DDC_ERR_STATE, "reduction read beyond the pinned buffer");
+  CK(cudaMemcpyAsync(ctx->hred, ctx->red.p, sizeof(double) * nvals, cudaMemcpyDeviceToHost,
+                     ctx->st));
+  CKI(sync(ctx));
+  memcpy(host, ctx->hred, sizeof(double) * nvals);
+  return DDC_OK;
+}
+
 // The per-item counts that are about to be scanned into 32-bit offsets must
 // total less than 2^31: summed in 64 bits on the device first.
 int check_count_total(ddc_ctx* ctx, const int* cnt, int n, const char* what) {
@@ -583,6 +595,10 @@ int do_init(ddc_ctx* ctx, int n, const std::vector<double4>* hsph, const double4
   CK(ctx->hist_e.ensure(sizeof(double) * std::max(nv, (size_t)1) * nd));
   CK(ctx->partials.ensure(sizeof(double) * reduce_blocks() * (kMaxHist + 1)));
   CK(ctx->red.ensure(sizeof(double) * (kMaxHist + 1)));
+  if (!ctx->rcount.p) {
+    CK(ctx->rcount.ensure(sizeof(unsigned)));
+    CK(cudaMemsetAsync(ctx->rcount.p, 0, sizeof(unsigned), ctx->st));
+  }
   // the basis transposed to [Y][G] for the FP64 expansion xi = basis^T s
   CK(ctx->basisT.ensure(sizeof(double) * G * NY));
   CK(launch_transpose(L, G, NY, ctx->basis.as<double>(), ctx->basisT.as<double>()));
@@ -975,9 +991,10 @@ int jd_step(ddc_ctx* ctx, JDState& s) {
     {
       StageScope sc(ctx, ST_JACOBI);
       CK(launch_jacobi_step(ctx->L(), ctx->tb, n, s.rhs, s.y, s.x, xnew, enew, hist,
-                            ctx->partials.as<double>(), nblk, s.f32, &jblk));
+                            ctx->partials.as<double>(), nblk, s.f32, &jblk,
+                            ctx->rcount.as<unsigned>(), ctx->red.as<double>()));
     }
-    CKI(reduce_to_host(ctx, nm, row.data(), kMaxHist + 1, jblk));
+    CKI(read_reduced(ctx, nm, row.data()));
     if (shift) {
       for (int j = 2; j <= s.nmat - 10; j++)
         for (int k = 2; k <= s.nmat - 10; k++) Bm(j, k) = Bm(j + 10, k + 10);
@@ -1021,17 +1038,18 @@ int jd_step(ddc_ctx* ctx, JDState& s) {
     hist.n = 0;
     StageScope sc(ctx, ST_JACOBI);
     CK(launch_jacobi_step(ctx->L(), ctx->tb, n, s.rhs, s.y, s.x, s.hx, s.he, hist,
-                          ctx->partials.as<double>(), nblk, s.f32, nullptr));
+                          ctx->partials.as<double>(), nblk, s.f32, nullptr,
+                          ctx->rcount.as<unsigned>(), ctx->red.as<double>()));
     comb.n = 0;
     xj = s.hx;
   }
   {
     StageScope sc(ctx, ST_COMBINE);
     CK(launch_diis_combine(ctx->L(), ctx->tb, n, comb, xj, s.x, ctx->partials.as<double>(),
-                           nblk, s.f32));
+                           nblk, s.f32, ctx->rcount.as<unsigned>(), ctx->red.as<double>()));
   }
   double ss = 0.0;
-  CKI(reduce_to_host(ctx, 1, &ss));
+  CKI(read_reduced(ctx, 1, &ss));
   s.rms = std::sqrt(ss / (double)std::max(ctx->nsph, 1));
   if (*s.logpos < 256) s.inf->norms[*s.logpos] = s.rms;
   ++*s.logpos;
@@ -1066,6 +1084,10 @@ struct SolveTask {
   JDState jd;
   int logpos = 0, its = 0, restarts = 0, budget = 0, outer = 0;
   bool done = false, ok = false;
+  // mixed, from the reference or the zero start: the first residual (at a
+  // start that is never converged) comes from the FP32 operator, like the
+  // inner iterations; the convergence test runs from the second refinement on
+  bool f32_first = false;
 };
 
 void task_begin(ddc_ctx* ctx, SolveTask& t, bool adjoint, const double* rhs, double* x,
@@ -1084,6 +1106,8 @@ void task_begin(ddc_ctx* ctx, SolveTask& t, bool adjoint, const double* rhs, dou
   t.budget = ctx->prm.max_iter;
   t.last = 0.0;
   t.done = t.ok = false;
+  t.f32_first = t.mixed && !ctx->guess_preset &&
+                (ctx->prm.guess == DDC_GUESS_REFERENCE || ctx->prm.guess == DDC_GUESS_ZERO);
   if (!t.mixed) jd_begin(ctx, t.jd, rhs, x, t.tol, ctx->prm.max_iter, t.b, inf, &t.logpos);
   if (!t.mixed && t.jd.done) t.done = true;
 }
@@ -1098,7 +1122,7 @@ OpKind task_next(const SolveTask& t, const double** in, double** out) {
   }
   *in = t.x;
   *out = t.b.y;
-  return OP_F64;
+  return t.f32_first && t.outer == 0 ? OP_F32 : OP_F64;
 }
 
 int task_after(ddc_ctx* ctx, SolveTask& t) {
@@ -1137,12 +1161,15 @@ int task_after(ddc_ctx* ctx, SolveTask& t) {
   double ss = 0.0;
   CKI(reduce_to_host(ctx, 1, &ss));
   t.last = std::sqrt(ss / (double)std::max(ctx->nsph, 1));
-  if (ctx->prm.iprint > 0) printf("  refinement %d: FP64 increment norm %14.4E\n", t.outer, t.last);
+  const bool f32_res = t.f32_first && t.outer == 1;
+  if (ctx->prm.iprint > 0)
+    printf("  refinement %d: %s increment norm %14.4E\n", t.outer, f32_res ? "FP32" : "FP64",
+           t.last);
   if (!std::isfinite(t.last)) {
     t.done = true;
     return fail(ctx, DDC_ERR_NUMERIC, "non-finite increment norm");
   }
-  if (t.last < t.tol) {
+  if (t.last < t.tol && !f32_res) {
     t.done = t.ok = true;
     return DDC_OK;
   }

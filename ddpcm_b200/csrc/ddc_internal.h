@@ -285,16 +285,20 @@ cudaError_t guess_infer(Launch L, ddc_guess* m, const YlmTables& tb, int nsph, c
                         const double* g, const double* psi, double* x, double* s);
 
 // solver
-// xnew = facl*(rhs - y); e = xnew - x; partial dots e.h_k (k < hist.n) and e.e.
+// xnew = facl*(rhs - y); e = xnew - x; dots e.h_k (k < hist.n) and e.e.
 // xnew, e and the history are FP32 when f32 (mixed-path inner solves), else FP64.
+// The block partials go to partials; the last block sums them into out[0..hist.n]
+// (counter: a zeroed device word, left zeroed).
 cudaError_t launch_jacobi_step(Launch L, const YlmTables& tb, long long n, const double* rhs,
                                const double* y, const double* x, void* xnew, void* e,
                                const HistPtrs& hist, double* partials, int nblk, bool f32,
-                               int* nblk_used);  // blocks launched (<= nblk): partial rows
-// xout = sum c_k p_k (or xjac if hist.n == 0); partial of sum_l 1/(l+1) (xout-x)^2; x = xout
+                               int* nblk_used,  // blocks launched (<= nblk): partial rows
+                               unsigned* counter, double* out);
+// xout = sum c_k p_k (or xjac if hist.n == 0); sum_l 1/(l+1) (xout-x)^2 into
+// out[0] (through partials and counter as above); x = xout
 cudaError_t launch_diis_combine(Launch L, const YlmTables& tb, long long n, const HistPtrs& hist,
                                 const void* xjac, double* x, double* partials, int nblk,
-                                bool f32);
+                                bool f32, unsigned* counter, double* out);
 cudaError_t launch_hnorm_partial(Launch L, const YlmTables& tb, long long n, const double* x,
                                  double* partials, int nblk);
 cudaError_t launch_dot_partial(Launch L, long long n, const double* a, const double* b,

@@ -1188,6 +1188,30 @@ __device__ __forceinline__ void block_sum_store(double (&v)[NV], int nv, double*
   }
 }
 
+// The last block of a grid to finish (an arrival counter) sums the per-block
+// partials of all blocks, in block order, into out[k] for k < nv and resets
+// the counter: the solver kernels hand their final sums to the host without
+// a separate reduction launch.  A fixed order: reproducible.
+__device__ __forceinline__ void last_block_reduce(const double* partials, int stride, int nv,
+                                                  unsigned* counter, double* out) {
+  __shared__ unsigned s_last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) s_last = atomicAdd(counter, 1u) == gridDim.x - 1 ? 1u : 0u;
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int k = w; k < nv; k += nw) {
+    double v = 0.0;
+    for (int b = lane; b < (int)gridDim.x; b += 32) v += __ldcg(partials + (size_t)b * stride + k);
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) out[k] = v;
+  }
+  if (threadIdx.x == 0) *counter = 0u;
+}
+
 // Element tiles of the solver kernels: a block takes 4 x 256 consecutive
 // elements per step, thread t the elements t, t+256, t+512, t+768, so that
 // each thread has four independent loads of every vector in flight.
@@ -1214,7 +1238,7 @@ __global__ void __launch_bounds__(kSolT, 4) k_jacobi_step(const YlmTables tb, lo
                                                        const double* __restrict__ y,
                                                        const double* __restrict__ x, H* xnew,
                                                        H* e, const HistPtrs hist,
-                                                       double* partials) {
+                                                       double* partials, unsigned* counter, double* out) {
   constexpr int U = 2 * kSolU;  // eight elements per thread and tile
   constexpr int TILE = U * kSolT;
   constexpr int NW = kSolT / 32;
@@ -1299,6 +1323,7 @@ __global__ void __launch_bounds__(kSolT, 4) k_jacobi_step(const YlmTables tb, lo
     for (int ww = 0; ww < NW; ++ww) t += red[kMaxHist + 1 + ww];
     partials[(size_t)blockIdx.x * (kMaxHist + 1) + nh] = t;
   }
+  last_block_reduce(partials, kMaxHist + 1, nh + 1, counter, out);
 }
 // One wave: as many blocks as fit on the device at once (at most nblk, the
 // partial-row capacity).
@@ -1322,23 +1347,24 @@ static int one_wave_blocks(KFN kfn, int nblk) {
 template <class H>
 static int jacobi_launch(Launch L, const YlmTables& tb, long long n, const double* rhs,
                          const double* y, const double* x, H* xnew, H* e, const HistPtrs& hist,
-                         double* partials, int nblk) {
+                         double* partials, int nblk, unsigned* counter, double* out) {
   const int used = one_wave_blocks(k_jacobi_step<H>, nblk);
-  k_jacobi_step<H><<<used, kSolT, 0, L.st>>>(tb, n, rhs, y, x, xnew, e, hist, partials);
+  k_jacobi_step<H><<<used, kSolT, 0, L.st>>>(tb, n, rhs, y, x, xnew, e, hist, partials, counter,
+                                             out);
   return used;
 }
 cudaError_t launch_jacobi_step(Launch L, const YlmTables& tb, long long n, const double* rhs,
                                const double* y, const double* x, void* xnew, void* e,
                                const HistPtrs& hist, double* partials, int nblk, bool f32,
-                               int* nblk_used) {
+                               int* nblk_used, unsigned* counter, double* out) {
   if (hist.n > kMaxHist - 1 || n >= (1LL << 31)) return cudaErrorInvalidValue;
   int used;
   if (f32)
     used = jacobi_launch<float>(L, tb, n, rhs, y, x, static_cast<float*>(xnew),
-                                static_cast<float*>(e), hist, partials, nblk);
+                                static_cast<float*>(e), hist, partials, nblk, counter, out);
   else
     used = jacobi_launch<double>(L, tb, n, rhs, y, x, static_cast<double*>(xnew),
-                                 static_cast<double*>(e), hist, partials, nblk);
+                                 static_cast<double*>(e), hist, partials, nblk, counter, out);
   if (nblk_used) *nblk_used = used;
   ++*L.launches;
   return cudaGetLastError();
@@ -1350,7 +1376,7 @@ template <class H>
 __global__ void __launch_bounds__(kSolT) k_diis_combine(const YlmTables tb, long long n,
                                                         const HistPtrs hist,
                                                         const H* __restrict__ xjac, double* x,
-                                                        double* partials) {
+                                                        double* partials, unsigned* counter, double* out) {
   double acc = 0.0;
   const int nh = hist.n, nylm = tb.nylm;
   const int dt = kSolT % nylm;
@@ -1394,17 +1420,18 @@ __global__ void __launch_bounds__(kSolT) k_diis_combine(const YlmTables tb, long
   }
   double v[1] = {acc};
   block_sum_store<1>(v, 1, partials);
+  last_block_reduce(partials, 1, 1, counter, out);
 }
 cudaError_t launch_diis_combine(Launch L, const YlmTables& tb, long long n, const HistPtrs& hist,
                                 const void* xjac, double* x, double* partials, int nblk,
-                                bool f32) {
+                                bool f32, unsigned* counter, double* out) {
   if (f32)
     k_diis_combine<float><<<nblk, kSolT, 0, L.st>>>(tb, n, hist, static_cast<const float*>(xjac),
-                                                    x, partials);
+                                                    x, partials, counter, out);
   else
     k_diis_combine<double><<<nblk, kSolT, 0, L.st>>>(tb, n, hist,
                                                      static_cast<const double*>(xjac), x,
-                                                     partials);
+                                                     partials, counter, out);
   ++*L.launches;
   return cudaGetLastError();
 }
@@ -3194,35 +3221,37 @@ __global__ void __launch_bounds__(32 * lxs_nroles<Rl>(LMAX), lxs_min_blocks<Rl>(
     lxs_finish_role<LMAX, NR, 0, Rl, true>(role, tb, acc, y + (size_t)b * tb.nylm, lane);
 }
 
-// pot_a(n) = sum over a's CSR pairs (a, b) of the lx values of the triples
-// (a, n, b), read from b's gather list (pair slot lsstart).  Block per
-// sphere a; warp w takes the pairs p = w, w + NW, ... in order and adds into
-// its own shared row, lanes over the pair's points (distinct within a pair,
-// so no two lanes of a warp touch one entry).  Four strided loads per lane
-// are issued before their adds, and the next pair's first loads before the
-// current pair's adds (two pairs in flight per warp).  The rows are summed
-// in row order at the end: a fixed summation order, no atomics.
-constexpr int kGatherWarps = 4;  // at most; fewer when NW rows of ngrid do not fit
+// pot_a(n) = sum over a's CSR pairs (a, b), in CSR order, of the lx values
+// of the triples (a, n, b), read from b's gather list at the pair's block
+// (lsstart).  Warp per sphere a, with a private shared row of ngrid values
+// and the pairs' bounds staged in shared memory: lanes take the pair's
+// points (distinct within a pair, so no two lanes touch one entry), four
+// strided loads per lane, and the next pair's first loads are issued before
+// the current pair's adds; a __syncwarp between pairs orders the updates of
+// a point by its pairs.  No block barriers (each warp runs its sphere from
+// start to end) and no atomics: a fixed summation order.
+constexpr int kGatherWarps = 4;  // spheres per block
 template <class Rl>
 __global__ void __launch_bounds__(32 * kGatherWarps)
     k_lx_gather(const DevGeo g, const Rl* __restrict__ val, Rl* pot, int ldp) {
   constexpr int U = 4;
-  const int NW = blockDim.x >> 5;
   extern __shared__ __align__(16) unsigned char smraw[];
   const int G = g.ngrid;
   const int mb = (g.maxnb + 3) & ~3;
-  int* pst = reinterpret_cast<int*>(smraw);  // [maxnb+1]: pn_ptr of the pairs
-  int* dl = pst + mb + 4;                    // [maxnb]: lsstart - pn_ptr
-  Rl* acc = reinterpret_cast<Rl*>(dl + mb);  // [NW][G]
-  const int a = blockIdx.x, tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int a = blockIdx.x * kGatherWarps + w;
+  if (a >= g.nsph) return;  // warp-uniform; the kernel has no block barriers
+  // per warp: pst[mb + 4] (pn_ptr of the pairs), dl[mb] (lsstart - pn_ptr),
+  // then the row (16-byte aligned: mb is a multiple of four)
+  int* pst = reinterpret_cast<int*>(smraw) + (size_t)w * (2 * mb + 4);
+  int* dl = pst + mb + 4;
+  Rl* row = reinterpret_cast<Rl*>(reinterpret_cast<int*>(smraw) + kGatherWarps * (2 * mb + 4)) +
+            (size_t)w * G;
   const int k0 = g.inl[a], nn = g.inl[a + 1] - k0;
-  for (int k = tid; k <= nn; k += 32 * NW) pst[k] = g.pn_ptr[k0 + k];
-  for (int k = tid; k < nn; k += 32 * NW) dl[k] = g.lsstart[k0 + k] - g.pn_ptr[k0 + k];
-  for (int q = tid; q < NW * G; q += 32 * NW) acc[q] = 0;
-  __syncthreads();
-  Rl* myacc = acc + w * G;
-  // the first 32*U points of the warp's next pair are loaded before the
-  // current pair's values are added, so two pairs' loads are in flight
+  for (int k = lane; k <= nn; k += 32) pst[k] = g.pn_ptr[k0 + k];
+  for (int k = lane; k < nn; k += 32) dl[k] = g.lsstart[k0 + k] - g.pn_ptr[k0 + k];
+  for (int n = lane; n < G; n += 32) row[n] = Rl(0);
+  __syncwarp();
   auto load = [&](int base, int q1, int d, int* n, Rl* v) {
 #pragma unroll
     for (int u = 0; u < U; ++u) {
@@ -3234,17 +3263,17 @@ __global__ void __launch_bounds__(32 * kGatherWarps)
   auto add = [&](const int* n, const Rl* v) {
 #pragma unroll
     for (int u = 0; u < U; ++u)
-      if (n[u] >= 0) myacc[n[u]] += v[u];
+      if (n[u] >= 0) row[n[u]] += v[u];
   };
   int cn[U];
   Rl cv[U];
-  if (w < nn) load(pst[w] + lane, pst[w + 1], dl[w], cn, cv);
-  for (int p = w; p < nn; p += NW) {
+  if (nn > 0) load(pst[0] + lane, pst[1], dl[0], cn, cv);
+  for (int p = 0; p < nn; ++p) {
     const int q0 = pst[p], q1 = pst[p + 1], d = dl[p];
     int nn1[U];
     Rl nv1[U];
-    const bool more = p + NW < nn;
-    if (more) load(pst[p + NW] + lane, pst[p + NW + 1], dl[p + NW], nn1, nv1);
+    const bool more = p + 1 < nn;
+    if (more) load(pst[p + 1] + lane, pst[p + 2], dl[p + 1], nn1, nv1);
     add(cn, cv);
     for (int base = q0 + lane + 32 * U; base < q1; base += 32 * U) {
       int n2[U];
@@ -3252,6 +3281,7 @@ __global__ void __launch_bounds__(32 * kGatherWarps)
       load(base, q1, d, n2, v2);
       add(n2, v2);
     }
+    __syncwarp();
     if (more) {
 #pragma unroll
       for (int u = 0; u < U; ++u) {
@@ -3260,12 +3290,7 @@ __global__ void __launch_bounds__(32 * kGatherWarps)
       }
     }
   }
-  __syncthreads();
-  for (int n = tid; n < G; n += 32 * NW) {
-    Rl sum = acc[n];
-    for (int ww = 1; ww < NW; ++ww) sum += acc[ww * G + n];
-    pot[(size_t)a * ldp + n] = sum;
-  }
+  for (int n = lane; n < G; n += 32) pot[(size_t)a * ldp + n] = row[n];
 }
 
 template <class Rl, int MODE>
@@ -3310,16 +3335,14 @@ template <class Rl>
 static cudaError_t gather_launch(Launch L, const DevGeo& g, const Rl* val, Rl* pot, int ldp) {
   if (g.nsph == 0) return cudaSuccess;
   const int mb = (g.maxnb + 3) & ~3;
-  const size_t idx = sizeof(int) * (2 * mb + 4), row = sizeof(Rl) * g.ngrid;
-  const size_t cap = 200 * 1024;  // within the 227 KB opt-in limit
-  const int nw = (int)std::max<size_t>(1, std::min<size_t>(kGatherWarps, (cap - idx) / row));
-  const size_t sm = idx + row * nw;
+  const size_t sm = kGatherWarps * (sizeof(int) * (2 * mb + 4) + sizeof(Rl) * g.ngrid);
   cudaError_t e;
   if (sm > 48 * 1024)
     if ((e = cudaFuncSetAttribute(k_lx_gather<Rl>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)sm)))
       return e;
-  k_lx_gather<Rl><<<g.nsph, 32 * nw, sm, L.st>>>(g, val, pot, ldp);
+  k_lx_gather<Rl><<<(g.nsph + kGatherWarps - 1) / kGatherWarps, 32 * kGatherWarps, sm, L.st>>>(
+      g, val, pot, ldp);
   ++*L.launches;
   return cudaGetLastError();
 }
