@@ -173,6 +173,7 @@ struct ddc_ctx {
   // grouped multipole field of zeta at the nuclei (mixed energy+force flow)
   DBuf zg_cell, zg_sph, zg_start, zg_cen, zg_npt, zg_ptr, zg_cnt, zg_tmp, zg_M, zg_pk, zg_scr;
   ZGroups zg;
+  bool zg_on = false;  // cell groups built for this molecule (single molecule, >= 4,096 spheres)
   bool zfar_on = false;
   // pinned landing buffer of the small device-to-host reads (reduced sums)
   double* hred = nullptr;
@@ -478,13 +479,41 @@ int do_init(ddc_ctx* ctx, int n, const std::vector<double4>* hsph, const double4
   CK(ctx->bw.ensure(sizeof(double) * G * NY));
   CK(launch_basis(L, ctx->tb, ctx->grid.as<double4>(), ctx->basis.as<double>(),
                   ctx->bw.as<double>()));
+  // cell groups of one large molecule: candidates for the neighbour list,
+  // the near lists of the cavity far field and the groups of the field of
+  // zeta (DDC_CELLS_OFF=1 keeps the all-pairs scans: a diagnostic switch)
+  {
+    const char* coff = std::getenv("DDC_CELLS_OFF");
+    ctx->zg_on = ctx->nmol <= 1 && N >= kZetaMinSpheres && !(coff && coff[0] == '1');
+    if (ctx->zg_on) {
+      CK(ctx->zg_cell.ensure(sizeof(int) * N));
+      CK(ctx->zg_sph.ensure(sizeof(int) * N));
+      CK(ctx->zg_start.ensure(sizeof(int) * (N + 1)));
+      CK(ctx->zg_cen.ensure(sizeof(double4) * N));
+      CK(ctx->zg_cnt.ensure(sizeof(int)));
+      ZGroups& z = ctx->zg;
+      z.cellid = ctx->zg_cell.as<int>();
+      z.gsph = ctx->zg_sph.as<int>();
+      z.gstart = ctx->zg_start.as<int>();
+      z.gcen = ctx->zg_cen.as<double4>();
+      z.gnpt = nullptr;
+      z.gptr = nullptr;
+      if (!ctx->hred) CK(cudaMallocHost(&ctx->hred, sizeof(double) * (kMaxHist + 1)));
+      CK(launch_zgroups_cells(L, N, ctx->sph.as<double4>(), z, ctx->zg_cnt.as<int>(),
+                              reinterpret_cast<int*>(ctx->hred)));
+    }
+  }
   // neighbour list
   size_t scan_n = (size_t)std::max<long long>(N, 1);
   CK(ctx->cnt.ensure(sizeof(int) * (scan_n + 1)));
   CK(ctx->inl.ensure(sizeof(int) * (N + 1)));
   CK(cudaMemsetAsync(ctx->cnt.p, 0, sizeof(int) * (N + 1), ctx->st));
-  if (N > 0)
-    CK(launch_csr_count(L, N, ctx->sph.as<double4>(), ctx->cnt.as<int>(), ctx->mrange_ptr()));
+  if (N > 0) {
+    if (ctx->zg_on)
+      CK(launch_csr_count_cells(L, N, ctx->sph.as<double4>(), ctx->zg, ctx->cnt.as<int>()));
+    else
+      CK(launch_csr_count(L, N, ctx->sph.as<double4>(), ctx->cnt.as<int>(), ctx->mrange_ptr()));
+  }
   size_t tb_bytes = scan_temp_bytes(N);
   CK(ctx->scan_tmp.ensure(tb_bytes));
   CKI(check_count_total(ctx, ctx->cnt.as<int>(), N, "neighbour pairs"));
@@ -512,8 +541,12 @@ int do_init(ddc_ctx* ctx, int n, const std::vector<double4>* hsph, const double4
                                                 std::to_string(mx) + ")");
   }
   if (N > 0) {
-    CK(launch_csr_fill(L, N, ctx->sph.as<double4>(), ctx->inl.as<int>(), ctx->nl.as<int>(),
-                       ctx->mrange_ptr()));
+    if (ctx->zg_on)
+      CK(launch_csr_fill_cells(L, N, ctx->sph.as<double4>(), ctx->zg, ctx->inl.as<int>(),
+                               ctx->nl.as<int>()));
+    else
+      CK(launch_csr_fill(L, N, ctx->sph.as<double4>(), ctx->inl.as<int>(), ctx->nl.as<int>(),
+                         ctx->mrange_ptr()));
     CK(launch_csr_rev(L, N, ctx->inl.as<int>(), ctx->nl.as<int>(), ctx->rev.as<int>()));
   }
   // fi, ui, zi
@@ -685,28 +718,17 @@ int do_init(ddc_ctx* ctx, int n, const std::vector<double4>* hsph, const double4
     // flow: spheres grouped for the multipole far field (DDC_ZFAR_OFF=1, or
     // DDC_FAR_OFF=1, keeps the direct FP32 pair sums)
     const char* zoff = std::getenv("DDC_ZFAR_OFF");
-    ctx->zfar_on = ctx->prm.precision == DDC_PREC_MIXED && ctx->prm.igrad && ctx->nmol <= 1 &&
-                   N >= kZetaMinSpheres && !(off && off[0] == '1') && !(zoff && zoff[0] == '1');
+    ctx->zfar_on = ctx->zg_on && ctx->prm.precision == DDC_PREC_MIXED && ctx->prm.igrad &&
+                   !(off && off[0] == '1') && !(zoff && zoff[0] == '1');
     if (ctx->zfar_on) {
-      CK(ctx->zg_cell.ensure(sizeof(int) * N));
-      CK(ctx->zg_sph.ensure(sizeof(int) * N));
-      CK(ctx->zg_start.ensure(sizeof(int) * (N + 1)));
-      CK(ctx->zg_cen.ensure(sizeof(double4) * N));
       CK(ctx->zg_npt.ensure(sizeof(int) * (N + 1)));
       CK(ctx->zg_ptr.ensure(sizeof(int) * (N + 1)));
-      CK(ctx->zg_cnt.ensure(sizeof(int)));
       const size_t tb = zgroups_scan_bytes(N);
       CK(ctx->zg_tmp.ensure(tb));
       ZGroups& z = ctx->zg;
-      z.cellid = ctx->zg_cell.as<int>();
-      z.gsph = ctx->zg_sph.as<int>();
-      z.gstart = ctx->zg_start.as<int>();
-      z.gcen = ctx->zg_cen.as<double4>();
       z.gnpt = ctx->zg_npt.as<int>();
       z.gptr = ctx->zg_ptr.as<int>();
-      CK(launch_zgroups_build(L, N, ctx->sph.as<double4>(), ctx->cavoff.as<int>(), z,
-                              ctx->zg_cnt.as<int>(), reinterpret_cast<int*>(ctx->hred),
-                              ctx->zg_tmp.p, tb));
+      CK(launch_zgroups_points(L, ctx->cavoff.as<int>(), z, ctx->zg_tmp.p, tb));
       CK(ctx->zg_M.ensure(sizeof(float2) * zgroups_moment_count(z)));
       CK(ctx->zg_pk.ensure(sizeof(float4) * std::max(ctx->ncav, 1)));
       CK(ctx->zg_scr.ensure(sizeof(double) * 3 * (size_t)zgroups_nchunk(z) * N));
@@ -1271,7 +1293,8 @@ int solute_pot_field(ddc_ctx* ctx, const double* q, double* phi, double* ef, con
     CK(launch_far_pot_field(ctx->L(), ctx->tbP, N, ctx->ngrid, ctx->sph.as<double4>(), q,
                             ctx->mrange_ptr(), kFarRho, ctx->cavoff.as<int>(),
                             ctx->cavpt.as<int>(), ctx->ccav.as<double>(), ctx->farBT.as<double>(),
-                            ctx->farDT.as<double>(), ctx->farA.as<double>(), phi, ef));
+                            ctx->farDT.as<double>(), ctx->farA.as<double>(), phi, ef,
+                            ctx->zg_on ? &ctx->zg : nullptr));
   } else if (ef) {
     CK(launch_coulomb_pot_field(ctx->L(), N, q, ctx->cx.as<double>(), ctx->cy.as<double>(),
                                 ctx->cz.as<double>(), NC, ctx->ccav.as<double>(), phi, ef,

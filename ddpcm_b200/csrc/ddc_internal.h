@@ -320,12 +320,14 @@ constexpr int kFarMinSpheres = 4096;
 // BT[lm][n] = Y_lm(s_n), DT[k][lm][n] = grad_k R_lm(s_n) for the degree of tbP
 cudaError_t launch_far_tables(Launch L, const YlmTables& tbP, const double4* grid, int ngrid,
                               double* BT, double* DT);
-// phi (and ef, if not null) at the cavity points; A: scratch [nsph][nylm(tbP)]
+struct ZGroups;  // cell groups of one molecule (below)
+// phi (and ef, if not null) at the cavity points; A: scratch [nsph][nylm(tbP)];
+// zg (null for a batch): the near charges are searched in the candidate groups
 cudaError_t launch_far_pot_field(Launch L, const YlmTables& tbP, int nsph, int ngrid,
                                  const double4* sph, const double* q, const int2* mrange,
                                  double rho, const int* cavoff, const int* cavpt,
                                  const double* ccav, const double* BT, const double* DT,
-                                 double* A, double* phi, double* ef);
+                                 double* A, double* phi, double* ef, const ZGroups* zg);
 // Field of the cavity charges zeta at the nuclei in the mixed-precision
 // energy+force flow (force-only, FP32 pair arithmetic): from
 // kZetaMinSpheres spheres on, the spheres are grouped by the cells of a
@@ -336,6 +338,9 @@ constexpr int kZetaDegree = 16;
 constexpr double kZetaRho = 3.0;
 constexpr double kZetaCell = 12.0;
 constexpr int kZetaMinSpheres = 4096;
+// Cell groups of one molecule of kZetaMinSpheres spheres or more: the
+// candidates of the neighbour list, of the near lists of the cavity far
+// field and the source groups of the field of zeta
 struct ZGroups {
   int ngroup = 0;
   int* cellid = nullptr;   // [nsph] scratch
@@ -346,10 +351,20 @@ struct ZGroups {
   int* gptr = nullptr;     // [nsph+1] their exclusive scan
 };
 size_t zgroups_scan_bytes(int nsph);
-// builds the groups (one host read of the group count)
-cudaError_t launch_zgroups_build(Launch L, int nsph, const double4* sph, const int* cavoff,
-                                 ZGroups& zg, int* dcount, int* hcount, void* scan_tmp,
-                                 size_t scan_bytes);
+// the cell groups of one molecule: members, centroids and radii (one host
+// read of the group count); used by the neighbour list, the near lists of
+// the cavity far field and the field of zeta
+cudaError_t launch_zgroups_cells(Launch L, int nsph, const double4* sph, ZGroups& zg,
+                                 int* dcount, int* hcount);
+// per-group cavity-point counts and offsets (gnpt, gptr) for the field of zeta
+cudaError_t launch_zgroups_points(Launch L, const int* cavoff, ZGroups& zg, void* scan_tmp,
+                                  size_t scan_bytes);
+// neighbour list of one molecule from its cell groups (same lists as
+// launch_csr_count / launch_csr_fill)
+cudaError_t launch_csr_count_cells(Launch L, int nsph, const double4* sph, const ZGroups& zg,
+                                   int* cnt);
+cudaError_t launch_csr_fill_cells(Launch L, int nsph, const double4* sph, const ZGroups& zg,
+                                  const int* inl, int* nl);
 int zgroups_nchunk(const ZGroups& zg);
 size_t zgroups_moment_count(const ZGroups& zg);
 // ef(3, nsph) from zeta(ncav); zpk[ncav], M[moment count], scratch

@@ -195,6 +195,80 @@ cudaError_t launch_csr_fill(Launch L, int nsph, const double4* sph, const int* i
   return cudaGetLastError();
 }
 
+// The same lists for one molecule from its cell groups (ddc_zfar.cu): a warp
+// per sphere tests the groups' bounding spheres (a neighbour j of i lies in
+// a group g with |c_i - c_g| <= r_i + R_g, since R_g >= |c_j - c_g| + r_j;
+// a 1e-6 bohr margin covers rounding), then the candidate groups' members
+// with the same overlap test as k_csr.  The fill pass ranks the sphere's
+// neighbours (all distinct) into ascending order, so the list is the one
+// k_csr writes.  Neighbour counts are at most 255 (checked before the fill).
+template <bool FILL>
+__global__ void __launch_bounds__(256) k_csr_cells(int nsph, const double4* __restrict__ sph,
+                                                   const ZGroups zg, int* cnt, const int* inl,
+                                                   int* nl) {
+  __shared__ int buf[8][256];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int i = blockIdx.x * 8 + w;
+  if (i >= nsph) return;  // warp-uniform; no block barriers
+  const double4 ci = sph[i];
+  int found = 0;
+  for (int g0 = 0; g0 < zg.ngroup; g0 += 32) {
+    const int g = g0 + lane;
+    bool cand = false;
+    if (g < zg.ngroup) {
+      const double4 cg = zg.gcen[g];
+      const double dx = ci.x - cg.x, dy = ci.y - cg.y, dz = ci.z - cg.z;
+      const double lim = ci.w + cg.w + 1e-6;
+      cand = dx * dx + dy * dy + dz * dz <= lim * lim;
+    }
+    unsigned m = __ballot_sync(0xffffffffu, cand);
+    while (m) {
+      const int gg = g0 + __ffs(m) - 1;
+      m &= m - 1;
+      const int s0 = zg.gstart[gg], s1 = zg.gstart[gg + 1];
+      for (int k0 = s0; k0 < s1; k0 += 32) {
+        const int k = k0 + lane;
+        int j = -1;
+        bool nb = false;
+        if (k < s1) {
+          j = zg.gsph[k];
+          nb = j != i && is_nb(ci, sph[j]);
+        }
+        const unsigned bm = __ballot_sync(0xffffffffu, nb);
+        if (FILL && nb) {
+          const int pos = found + __popc(bm & ((1u << lane) - 1u));
+          if (pos < 256) buf[w][pos] = j;
+        }
+        found += __popc(bm);
+      }
+    }
+  }
+  if constexpr (!FILL) {
+    if (lane == 0) cnt[i] = found;
+  } else {
+    __syncwarp();
+    const int base = inl[i], nf = min(found, 256);
+    for (int e = lane; e < nf; e += 32) {
+      const int v = buf[w][e];
+      int r = 0;
+      for (int f = 0; f < nf; ++f) r += buf[w][f] < v;
+      nl[base + r] = v;
+    }
+  }
+}
+cudaError_t launch_csr_count_cells(Launch L, int nsph, const double4* sph, const ZGroups& zg,
+                                   int* cnt) {
+  k_csr_cells<false><<<(nsph + 7) / 8, 256, 0, L.st>>>(nsph, sph, zg, cnt, nullptr, nullptr);
+  ++*L.launches;
+  return cudaGetLastError();
+}
+cudaError_t launch_csr_fill_cells(Launch L, int nsph, const double4* sph, const ZGroups& zg,
+                                  const int* inl, int* nl) {
+  k_csr_cells<true><<<(nsph + 7) / 8, 256, 0, L.st>>>(nsph, sph, zg, nullptr, inl, nl);
+  ++*L.launches;
+  return cudaGetLastError();
+}
+
 // rev[k] for k = (i, j): position of i in the neighbour list of j
 __global__ void k_csr_rev(int nsph, const int* __restrict__ inl, const int* __restrict__ nl,
                           int* rev) {
@@ -3874,6 +3948,7 @@ __global__ void k_far_tables(const YlmTables tb, const double4* __restrict__ gri
 // points on average at the 20k workload, up to 590), so no thread steps
 // through empty slots in the pair loop.
 constexpr int kNearCap = 1024;
+constexpr int kCandGroups = 512;
 template <int NU>
 __device__ __forceinline__ void far_cav_body(int i, int ngrid, int ny, double4 ci, double cut2,
                                              int lo, int hi, int c0, int c1,
@@ -3884,8 +3959,23 @@ __device__ __forceinline__ void far_cav_body(int i, int ngrid, int ny, double4 c
                                              const double* __restrict__ BT,
                                              const double* __restrict__ DT, double* phi,
                                              double* ef, double4* near, const double* sA,
-                                             int& s_cnt, int& s_scan, int* wbase) {
+                                             int& s_cnt, int& s_scan, int* wbase,
+                                             const int* cgl, const int* cpre, int ncg,
+                                             const int* __restrict__ gsph,
+                                             const int* __restrict__ gstart) {
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  // candidate f of the scan: sphere f of the molecule's range, or with cell
+  // groups (ncg > 0) the member f - cpre[k] of candidate group cgl[k]
+  auto cand = [&](int f) -> int {
+    if (ncg == 0) return f;
+    int a = 0, b = ncg;  // cpre[a] <= f < cpre[b]
+    while (b - a > 1) {
+      const int mid = (a + b) >> 1;
+      if (cpre[mid] <= f) a = mid;
+      else b = mid;
+    }
+    return gsph[gstart[cgl[a]] + (f - cpre[a])];
+  };
   // thread tid owns cavity points c0 + tid + 128 u, u < NU
   double v[NU], ex[NU], ey[NU], ez[NU], px[NU], py[NU], pz[NU];
 #pragma unroll
@@ -3915,10 +4005,12 @@ __device__ __forceinline__ void far_cav_body(int i, int ngrid, int ny, double4 c
       const int jj = j + tid;
       bool nb = false;
       double4 cj = make_double4(0, 0, 0, 0);
+      int js = 0;
       if (jj < hi) {
-        cj = sph[jj];
+        js = cand(jj);
+        cj = sph[js];
         const double dx = cj.x - ci.x, dy = cj.y - ci.y, dz = cj.z - ci.z;
-        nb = jj == i || dx * dx + dy * dy + dz * dz <= cut2;
+        nb = js == i || dx * dx + dy * dy + dz * dz <= cut2;
       }
       const unsigned bal = __ballot_sync(0xffffffffu, nb);
       if (lane == 0) wbase[w] = __popc(bal);
@@ -3933,7 +4025,7 @@ __device__ __forceinline__ void far_cav_body(int i, int ngrid, int ny, double4 c
         s_cnt = b;
       }
       __syncthreads();
-      if (nb) near[wbase[w] + __popc(bal & ((1u << lane) - 1u))] = make_double4(cj.x, cj.y, cj.z, q[jj]);
+      if (nb) near[wbase[w] + __popc(bal & ((1u << lane) - 1u))] = make_double4(cj.x, cj.y, cj.z, q[js]);
     }
     __syncthreads();
     if (tid == 0) s_scan = j;
@@ -3991,23 +4083,85 @@ __global__ void __launch_bounds__(128) k_far_cav(int nsph, int ngrid, int ny,
                                                  const double* __restrict__ A,
                                                  const double* __restrict__ BT,
                                                  const double* __restrict__ DT, double* phi,
-                                                 double* ef) {
+                                                 double* ef, const ZGroups zg) {
   __shared__ double4 near[kNearCap];
   __shared__ double sA[(DDC_MAX_LMAX + 1) * (DDC_MAX_LMAX + 1)];
   __shared__ int s_cnt, s_scan, wbase[4];
-  const int i = blockIdx.x;
+  __shared__ int cgl[kCandGroups], cpre[kCandGroups + 1];
+  __shared__ int s_ncg;
+  const int i = blockIdx.x, tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
   const int c0 = cavoff[i], c1 = cavoff[i + 1];
   if (c1 == c0) return;  // buried: no cavity points
   const double4 ci = sph[i];
   const double cut2 = (rho * ci.w) * (rho * ci.w);
-  const int lo = mrange ? mrange[i].x : 0, hi = mrange ? mrange[i].y : nsph;
-  for (int lm = threadIdx.x; lm < ny; lm += blockDim.x) sA[lm] = A[(size_t)i * ny + lm];
+  int lo = mrange ? mrange[i].x : 0, hi = mrange ? mrange[i].y : nsph;
+  for (int lm = tid; lm < ny; lm += blockDim.x) sA[lm] = A[(size_t)i * ny + lm];
+  // with cell groups (one molecule): the groups that can hold a near charge
+  // (|c_i - c_g| <= rho r_i + R_g, R_g bounding the members' centres; 1e-6
+  // bohr of margin for rounding), compacted in group order, and the prefix
+  // sums of their sizes; more than kCandGroups keeps the full scan
+  int ncg = 0;
+  if (zg.ngroup > 0) {
+    if (tid == 0) s_ncg = 0;
+    __syncthreads();
+    const double reach = rho * ci.w;
+    for (int g0 = 0; g0 < zg.ngroup; g0 += 128) {
+      const int g = g0 + tid;
+      bool c = false;
+      if (g < zg.ngroup) {
+        const double4 cg = zg.gcen[g];
+        const double dx = ci.x - cg.x, dy = ci.y - cg.y, dz = ci.z - cg.z;
+        const double lim = reach + cg.w + 1e-6;
+        c = dx * dx + dy * dy + dz * dz <= lim * lim;
+      }
+      const unsigned bal = __ballot_sync(0xffffffffu, c);
+      if (lane == 0) wbase[w] = __popc(bal);
+      __syncthreads();
+      if (tid == 0) {
+        int b = s_ncg;
+        for (int k = 0; k < 4; ++k) {
+          const int n = wbase[k];
+          wbase[k] = b;
+          b += n;
+        }
+        s_ncg = b;
+      }
+      __syncthreads();
+      const int pos = wbase[w] + __popc(bal & ((1u << lane) - 1u));
+      if (c && pos < kCandGroups) cgl[pos] = g;
+      __syncthreads();
+    }
+    ncg = s_ncg;
+    if (ncg <= kCandGroups) {
+      // prefix sums of the candidate groups' sizes (warp 0, in order)
+      if (w == 0) {
+        int run = 0;
+        for (int k0 = 0; k0 < ncg; k0 += 32) {
+          const int k = k0 + lane;
+          int v = k < ncg ? zg.gstart[cgl[k] + 1] - zg.gstart[cgl[k]] : 0;
+#pragma unroll
+          for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, v, o);
+            if (lane >= o) v += t;
+          }
+          if (k < ncg) cpre[k + 1] = run + v;
+          run += __shfl_sync(0xffffffffu, v, 31);
+        }
+        if (lane == 0) cpre[0] = 0;
+      }
+      __syncthreads();
+      lo = 0;
+      hi = ncg > 0 ? cpre[ncg] : 0;
+    } else {
+      ncg = 0;  // too many candidates: scan the molecule
+    }
+  }
   // 5 * 128 = 640 >= ngrid up to 590 points
   switch ((c1 - c0 + 127) / 128) {
 #define FAR_CAV_CASE(NU)                                                                        \
   case NU:                                                                                      \
     far_cav_body<NU>(i, ngrid, ny, ci, cut2, lo, hi, c0, c1, sph, q, cavpt, ccav, BT, DT, phi, \
-                     ef, near, sA, s_cnt, s_scan, wbase);                                       \
+                     ef, near, sA, s_cnt, s_scan, wbase, cgl, cpre, ncg, zg.gsph, zg.gstart);  \
     break;
     FAR_CAV_CASE(1)
     FAR_CAV_CASE(2)
@@ -4032,7 +4186,7 @@ cudaError_t launch_far_pot_field(Launch L, const YlmTables& tbP, int nsph, int n
                                  const double4* sph, const double* q, const int2* mrange,
                                  double rho, const int* cavoff, const int* cavpt,
                                  const double* ccav, const double* BT, const double* DT,
-                                 double* A, double* phi, double* ef) {
+                                 double* A, double* phi, double* ef, const ZGroups* zg) {
   if (nsph == 0) return cudaSuccess;
   if (ngrid > 640) return cudaErrorInvalidValue;  // k_far_cav holds 5 x 128 points per thread set
   cudaError_t e;
@@ -4055,8 +4209,9 @@ cudaError_t launch_far_pot_field(Launch L, const YlmTables& tbP, int nsph, int n
 #undef CASE
   ++*L.launches;
   if ((e = cudaGetLastError())) return e;
+  ZGroups none;
   k_far_cav<<<nsph, 128, 0, L.st>>>(nsph, ngrid, tbP.nylm, sph, q, mrange, rho, cavoff, cavpt,
-                                    ccav, A, BT, DT, phi, ef);
+                                    ccav, A, BT, DT, phi, ef, zg && !mrange ? *zg : none);
   ++*L.launches;
   return cudaGetLastError();
 }

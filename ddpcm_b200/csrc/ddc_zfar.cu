@@ -183,35 +183,29 @@ __global__ void __launch_bounds__(1024) k_zg_build(int nsph, const double4* __re
   }
 }
 
-// Centroid and radius (max |c_j - c_g| + r_j: every cavity point of sphere
-// j lies on its surface) of each group, and its cavity-point count; warp per
-// group, fixed shuffle trees.  gnpt[G] = 0 (the scan reads one past).
+// Centroid c_g and radius R_g = max |c_j - c_g| + r_j of each group; warp
+// per group, fixed shuffle trees.  R_g bounds the group's cavity points (on
+// the members' surfaces) and its members' overlaps: a sphere i overlapping
+// a member j has |c_i - c_g| <= r_i + r_j + |c_j - c_g| <= r_i + R_g.
 __global__ void __launch_bounds__(128) k_zg_geom(int ngroup, const int* __restrict__ gstart,
                                                  const int* __restrict__ gsph,
                                                  const double4* __restrict__ sph,
-                                                 const int* __restrict__ cavoff,
-                                                 double4* __restrict__ gcen,
-                                                 int* __restrict__ gnpt) {
+                                                 double4* __restrict__ gcen) {
   const int g = blockIdx.x * 4 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
-  if (g == ngroup && lane == 0) gnpt[ngroup] = 0;
   if (g >= ngroup) return;
   const int s0 = gstart[g], s1 = gstart[g + 1];
   double sx = 0.0, sy = 0.0, sz = 0.0;
-  int np = 0;
   for (int k = s0 + lane; k < s1; k += 32) {
-    const int j = gsph[k];
-    const double4 c = sph[j];
+    const double4 c = sph[gsph[k]];
     sx += c.x;
     sy += c.y;
     sz += c.z;
-    np += cavoff[j + 1] - cavoff[j];
   }
 #pragma unroll
   for (int o = 16; o >= 1; o >>= 1) {
     sx += __shfl_xor_sync(kFull, sx, o);
     sy += __shfl_xor_sync(kFull, sy, o);
     sz += __shfl_xor_sync(kFull, sz, o);
-    np += __shfl_xor_sync(kFull, np, o);
   }
   const double inv = 1.0 / (double)(s1 - s0);
   const double cx = sx * inv, cy = sy * inv, cz = sz * inv;
@@ -223,10 +217,25 @@ __global__ void __launch_bounds__(128) k_zg_geom(int ngroup, const int* __restri
   }
 #pragma unroll
   for (int o = 16; o >= 1; o >>= 1) R = fmax(R, __shfl_xor_sync(kFull, R, o));
-  if (lane == 0) {
-    gcen[g] = make_double4(cx, cy, cz, R);
-    gnpt[g] = np;
+  if (lane == 0) gcen[g] = make_double4(cx, cy, cz, R);
+}
+
+// cavity points per group (gnpt[G] = 0: the scan reads one past)
+__global__ void __launch_bounds__(128) k_zg_npt(int ngroup, const int* __restrict__ gstart,
+                                                const int* __restrict__ gsph,
+                                                const int* __restrict__ cavoff,
+                                                int* __restrict__ gnpt) {
+  const int g = blockIdx.x * 4 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  if (g == ngroup && lane == 0) gnpt[ngroup] = 0;
+  if (g >= ngroup) return;
+  int np = 0;
+  for (int k = gstart[g] + lane; k < gstart[g + 1]; k += 32) {
+    const int j = gsph[k];
+    np += cavoff[j + 1] - cavoff[j];
   }
+#pragma unroll
+  for (int o = 16; o >= 1; o >>= 1) np += __shfl_xor_sync(kFull, np, o);
+  if (lane == 0) gnpt[g] = np;
 }
 
 // one column m of the moments for the points a thread owns: acc[n] +=
@@ -507,9 +516,8 @@ __global__ void k_zg_reduce(int nsph, int nchunk, const int* __restrict__ gsph,
 
 size_t zgroups_scan_bytes(int nsph) { return scan_temp_bytes(nsph); }
 
-cudaError_t launch_zgroups_build(Launch L, int nsph, const double4* sph, const int* cavoff,
-                                 ZGroups& zg, int* dcount, int* hcount, void* scan_tmp,
-                                 size_t scan_bytes) {
+cudaError_t launch_zgroups_cells(Launch L, int nsph, const double4* sph, ZGroups& zg,
+                                 int* dcount, int* hcount) {
   if (nsph <= 0) return cudaErrorInvalidValue;
   k_zg_build<<<1, 1024, 0, L.st>>>(nsph, sph, kZetaCell, zg.cellid, zg.gsph, zg.gstart, dcount);
   ++*L.launches;
@@ -519,9 +527,16 @@ cudaError_t launch_zgroups_build(Launch L, int nsph, const double4* sph, const i
   if ((e = cudaStreamSynchronize(L.st))) return e;
   zg.ngroup = *hcount;
   if (zg.ngroup <= 0 || zg.ngroup > nsph) return cudaErrorUnknown;
-  k_zg_geom<<<(zg.ngroup + 4) / 4, 128, 0, L.st>>>(zg.ngroup, zg.gstart, zg.gsph, sph, cavoff,
-                                                    zg.gcen, zg.gnpt);
+  k_zg_geom<<<(zg.ngroup + 3) / 4, 128, 0, L.st>>>(zg.ngroup, zg.gstart, zg.gsph, sph, zg.gcen);
   ++*L.launches;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_zgroups_points(Launch L, const int* cavoff, ZGroups& zg, void* scan_tmp,
+                                  size_t scan_bytes) {
+  k_zg_npt<<<(zg.ngroup + 4) / 4, 128, 0, L.st>>>(zg.ngroup, zg.gstart, zg.gsph, cavoff, zg.gnpt);
+  ++*L.launches;
+  cudaError_t e;
   if ((e = cudaGetLastError())) return e;
   return scan_exclusive(L, zg.gnpt, zg.gptr, zg.ngroup, scan_tmp, scan_bytes);
 }
