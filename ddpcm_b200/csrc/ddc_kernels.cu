@@ -3834,8 +3834,65 @@ namespace ddc {
 // are summed directly.  Truncation: at most t^(P+1) / (1 - t) of each far
 // term, 1e-10 for P = 10, rho = 8.
 // ---------------------------------------------------------------------------
-// A(i, lm) for every sphere: block per sphere, role warps over chunks of
-// sources of its molecule
+// The L* half of the normalised recurrence of the fused pass, FP64:
+// Q_l = ct Q_{l-1} - Bn t^2 Q_{l-2} (three operations per value; the scale
+// gam_lm sits in Kg, applied when the rows are stored), accumulated into the
+// column's register rows (layout of ls_column)
+template <int LMAX, int M, int OFF>
+__device__ __forceinline__ void fa_column(const YlmTables& tb, double ct, double t2, double q0,
+                                          double cm, double sm, double* acc) {
+  constexpr int NM = LMAX + 1 - M;
+  double q1 = 0.0;
+#pragma unroll
+  for (int l = M; l <= LMAX; ++l) {
+    double Q;
+    if (l == M) {
+      Q = q0;
+    } else if (l == M + 1) {
+      q1 = ct * q0;
+      Q = q1;
+    } else {
+      Q = fma(ct, q1, -(tb.Bn[lmi(l, M)] * t2) * q0);
+      q0 = q1;
+      q1 = Q;
+    }
+    if (M == 0) {
+      acc[OFF + l] += Q;
+    } else {
+      acc[OFF + (l - M)] = fma(Q, cm, acc[OFF + (l - M)]);
+      acc[OFF + NM + (l - M)] = fma(Q, sm, acc[OFF + NM + (l - M)]);
+    }
+  }
+}
+template <int LMAX, int R>
+__device__ __forceinline__ void fa_role(const YlmTables& tb, const double* sh, int stride,
+                                        int count, int lane, double* acc) {
+  constexpr int M1 = R, M2 = LMAX - R;
+  for (int q = lane; q < count; q += 32) {
+    const double ct = sh[q], t2 = sh[stride + q];
+    fa_column<LMAX, M1, 0>(tb, ct, t2, sh[(2 + 3 * M1) * stride + q],
+                           sh[(3 + 3 * M1) * stride + q], sh[(4 + 3 * M1) * stride + q], acc);
+    if constexpr (ls_has2(LMAX, R))
+      fa_column<LMAX, M2, ls_nvals_m(LMAX, M1)>(tb, ct, t2, sh[(2 + 3 * M2) * stride + q],
+                                                sh[(3 + 3 * M2) * stride + q],
+                                                sh[(4 + 3 * M2) * stride + q], acc);
+  }
+}
+template <int LMAX, int R>
+__device__ __forceinline__ void fa_run_role(int role, const YlmTables& tb, const double* sh,
+                                            int stride, int count, int lane, double* acc) {
+  if (role == R) {
+    fa_role<LMAX, R>(tb, sh, stride, count, lane, acc);
+    return;
+  }
+  if constexpr (R + 1 < ls_nroles(LMAX)) fa_run_role<LMAX, R + 1>(role, tb, sh, stride, count, lane, acc);
+}
+
+// A(i, lm) for every sphere with cavity points: block per sphere, role warps
+// over chunks of the sources of its molecule.  Per source the thread forms
+// 1/d and 1/sin(theta) with the refined hardware reciprocal square root
+// (rsqrt_pos), the prefix and cos/sin(m phi) (the fields of k_lstarx); the
+// roles run the normalised recurrence (fa_column) and store with Kg.
 template <int LMAX>
 __global__ void __launch_bounds__(32 * ls_nroles(LMAX)) k_far_acc(const YlmTables tb, int nsph,
                                                                    const double4* __restrict__ sph,
@@ -3861,20 +3918,26 @@ __global__ void __launch_bounds__(32 * ls_nroles(LMAX)) k_far_acc(const YlmTable
     {
       const int tt = threadIdx.x;
       double* col = sh + tt;
-      double ct = 0.0, t2 = 0.0, st = 0.0, w = 0.0;
-      Angles a{1.0, 0.0, 1.0, 0.0};
+      double ct = 0.0, t2 = 0.0, st = 0.0, w = 0.0, cp = 1.0, sp = 0.0;
       if (tt < chunk) {
         const int j = j0 + tt;
         const double4 cj = sph[j];
         const double vx = cj.x - ci.x, vy = cj.y - ci.y, vz = cj.z - ci.z;
         const double d2 = vx * vx + vy * vy + vz * vz;
         if (j != i && d2 > cut2) {
-          const double di = 1.0 / sqrt(d2);
-          const double t = ci.w * di;
-          a = angles_of(vx * di, vy * di, vz * di);
-          ct = a.c * t;
+          const double di = rsqrt_pos(d2);
+          const double t = ci.w * di, c = vz * di;
+          const double s2 = fma(-c, c, 1.0);
+          double sn = 0.0;
+          if (s2 > 1e-280) {  // off the pole (at a pole only m = 0 survives)
+            const double rs = rsqrt_pos(s2);
+            sn = s2 * rs;
+            cp = vx * di * rs;
+            sp = vy * di * rs;
+          }
+          ct = c * t;
           t2 = t * t;
-          st = a.s * t;
+          st = sn * t;
           w = -q[j] * di;
         }
       }
@@ -3884,10 +3947,10 @@ __global__ void __launch_bounds__(32 * ls_nroles(LMAX)) k_far_acc(const YlmTable
 #pragma unroll
       for (int m = 0; m <= LMAX; ++m) {
         if (m == 1) {
-          cm = a.cp;
-          sm = a.sp;
+          cm = cp;
+          sm = sp;
         } else if (m >= 2) {
-          const double cn = 2.0 * a.cp * cm - cmm1, sn = 2.0 * a.cp * sm - smm1;
+          const double cn = 2.0 * cp * cm - cmm1, sn = 2.0 * cp * sm - smm1;
           cmm1 = cm; smm1 = sm; cm = cn; sm = sn;
         }
         col[(2 + 3 * m) * CH] = pmm;
@@ -3897,10 +3960,10 @@ __global__ void __launch_bounds__(32 * ls_nroles(LMAX)) k_far_acc(const YlmTable
       }
     }
     __syncthreads();
-    ls_run_role<LMAX, 0, double>(role, tb, sh, CH, chunk, lane, acc);
+    fa_run_role<LMAX, 0>(role, tb, sh, CH, chunk, lane, acc);
     __syncthreads();
   }
-  ls_finish_role<LMAX, 0, double>(role, tb, acc, A + (size_t)i * tb.nylm, lane);
+  ls_finish_role<LMAX, 0, double, true>(role, tb, acc, A + (size_t)i * tb.nylm, lane);
 }
 
 // Tables on the grid, once per context: BT[lm][n] = Y_lm(s_n) and
