@@ -421,17 +421,6 @@ int reduce_to_host(ddc_ctx* ctx, int nvals, double* host, int stride = 1, int nb
   return DDC_OK;
 }
 
-// values the last block of a solver kernel already summed into red
-int read_reduced(ddc_ctx* ctx, int nvals, double* host) {
-  if (nvals > kMaxHist + 1 || !ctx->hred)
-    return fail(ctx, DDC_ERR_STATE, "reduction read beyond the pinned buffer");
-  CK(cudaMemcpyAsync(ctx->hred, ctx->red.p, sizeof(double) * nvals, cudaMemcpyDeviceToHost,
-                     ctx->st));
-  CKI(sync(ctx));
-  memcpy(host, ctx->hred, sizeof(double) * nvals);
-  return DDC_OK;
-}
-
 // The per-item counts that are about to be scanned into 32-bit offsets must
 // total less than 2^31: summed in 64 bits on the device first.
 int check_count_total(ddc_ctx* ctx, const int* cnt, int n, const char* what) {
@@ -464,7 +453,8 @@ int do_init(ddc_ctx* ctx, int n, const std::vector<double4>* hsph, const double4
   // grid fields, cavity and triple lists are indexed with 32-bit integers
   if (NP >= (long long)INT_MAX)
     return fail(ctx, DDC_ERR_UNSUPPORTED, "nsph * ngrid exceeds 2^31 - 1 grid points");
-  CK(ctx->red.ensure(sizeof(double) * (kMaxHist + 1)));  // also the count checks' scratch
+  // two rows (the direct and adjoint solves' reductions); also the count checks' scratch
+  CK(ctx->red.ensure(sizeof(double) * 2 * (kMaxHist + 1)));
   auto L = ctx->L();
   CK(ctx->sph.ensure(sizeof(double4) * std::max(N, 1)));
   if (hsph)
@@ -498,7 +488,7 @@ int do_init(ddc_ctx* ctx, int n, const std::vector<double4>* hsph, const double4
       z.gcen = ctx->zg_cen.as<double4>();
       z.gnpt = nullptr;
       z.gptr = nullptr;
-      if (!ctx->hred) CK(cudaMallocHost(&ctx->hred, sizeof(double) * (kMaxHist + 1)));
+      if (!ctx->hred) CK(cudaMallocHost(&ctx->hred, sizeof(double) * 2 * (kMaxHist + 1)));
       CK(launch_zgroups_cells(L, N, ctx->sph.as<double4>(), z, ctx->zg_cnt.as<int>(),
                               reinterpret_cast<int*>(ctx->hred)));
     }
@@ -627,7 +617,7 @@ int do_init(ddc_ctx* ctx, int n, const std::vector<double4>* hsph, const double4
   CK(ctx->hist_x.ensure(sizeof(double) * std::max(nv, (size_t)1) * nd));
   CK(ctx->hist_e.ensure(sizeof(double) * std::max(nv, (size_t)1) * nd));
   CK(ctx->partials.ensure(sizeof(double) * reduce_blocks() * (kMaxHist + 1)));
-  CK(ctx->red.ensure(sizeof(double) * (kMaxHist + 1)));
+  CK(ctx->red.ensure(sizeof(double) * 2 * (kMaxHist + 1)));
   if (!ctx->rcount.p) {
     CK(ctx->rcount.ensure(sizeof(unsigned)));
     CK(cudaMemsetAsync(ctx->rcount.p, 0, sizeof(unsigned), ctx->st));
@@ -635,7 +625,7 @@ int do_init(ddc_ctx* ctx, int n, const std::vector<double4>* hsph, const double4
   // the basis transposed to [Y][G] for the FP64 expansion xi = basis^T s
   CK(ctx->basisT.ensure(sizeof(double) * G * NY));
   CK(launch_transpose(L, G, NY, ctx->basis.as<double>(), ctx->basisT.as<double>()));
-  if (!ctx->hred) CK(cudaMallocHost(&ctx->hred, sizeof(double) * (kMaxHist + 1)));
+  if (!ctx->hred) CK(cudaMallocHost(&ctx->hred, sizeof(double) * 2 * (kMaxHist + 1)));
   if (ctx->prm.igrad && !ctx->st2) {
     CK(cudaStreamCreateWithFlags(&ctx->st2, cudaStreamNonBlocking));
     CK(cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
@@ -940,6 +930,12 @@ struct JDState {
   bool f32 = false;  // history vectors in FP32 (inner solves of the mixed path)
   ddc_solve_info* inf = nullptr;
   int* logpos = nullptr;
+  int set = 0;  // which device row / pinned row of the reductions (0 direct, 1 adjoint)
+  // between the three host steps of an iteration (jd_a, jd_b, jd_c)
+  int p_nm = 0;
+  bool p_shift = false;
+  std::vector<int> p_map;
+  void* p_xnew = nullptr;
   // history slot k of hx / he in the history precision
   void* slot(double* base, int k, long long n) const {
     return reinterpret_cast<char*>(base) + (size_t)k * n * (f32 ? sizeof(float) : sizeof(double));
@@ -957,7 +953,9 @@ int jd_ndiis(const ddc_ctx* ctx, bool f32) {
 }
 
 void jd_begin(ddc_ctx* ctx, JDState& s, const double* rhs, double* x, double tol, int max_iter,
-              const SolveBufs& b, ddc_solve_info* inf, int* logpos, bool f32 = false) {
+              const SolveBufs& b, ddc_solve_info* inf, int* logpos, bool f32 = false,
+              int set = 0) {
+  s.set = set;
   const int ndiis = jd_ndiis(ctx, f32);
   s.rhs = rhs;
   s.x = x;
@@ -982,20 +980,24 @@ void jd_begin(ddc_ctx* ctx, JDState& s, const double* rhs, double* x, double tol
   s.logpos = logpos;
 }
 
-// one iteration after y = op(x) (jacobi_diis.f90:120-160 with diis :183-230)
-int jd_step(ddc_ctx* ctx, JDState& s) {
+// One iteration after y = op(x) (jacobi_diis.f90:120-160 with diis
+// :183-230), in three host steps so that two systems solved together share
+// their synchronisations: jd_a launches the Jacobi step with the Gram row
+// and queues the row's copy to pinned memory; jd_b (after a synchronisation)
+// updates the bordered system (makeb), solves it (gjinv) and launches the
+// extrapolation with the increment norm, its copy queued; jd_c (after a
+// synchronisation) reads the norm and applies the stop test.
+double* red_row(ddc_ctx* ctx, int set) { return ctx->red.as<double>() + set * (kMaxHist + 1); }
+double* hred_row(ddc_ctx* ctx, int set) { return ctx->hred + set * (kMaxHist + 1); }
+
+int jd_a(ddc_ctx* ctx, JDState& s) {
   const long long n = (long long)ctx->nsph * ctx->nylm;
   const int ndiis = jd_ndiis(ctx, s.f32);
   const int nblk = reduce_blocks();
-  const int lenb = s.lenb;
-  auto Bm = [&](int j, int k) -> double& { return s.B[(size_t)(k - 1) * lenb + (j - 1)]; };
   ++s.it;
   HistPtrs hist{};
-  HistPtrs comb{};
-  const void* xj = s.xjac;
-  int jblk = nblk;
+  double* out = red_row(ctx, s.set);
   if (ndiis != 0) {
-    std::vector<double> row(kMaxHist + 2);
     const int phys_new = s.map[s.nmat - 1];
     int nm = s.nmat;
     std::vector<int> pmap = s.map;
@@ -1012,17 +1014,43 @@ int jd_step(ddc_ctx* ctx, JDState& s) {
     void* enew = s.slot(s.he, phys_new, n);
     {
       StageScope sc(ctx, ST_JACOBI);
+      int jblk = nblk;
       CK(launch_jacobi_step(ctx->L(), ctx->tb, n, s.rhs, s.y, s.x, xnew, enew, hist,
                             ctx->partials.as<double>(), nblk, s.f32, &jblk,
-                            ctx->rcount.as<unsigned>(), ctx->red.as<double>()));
+                            ctx->rcount.as<unsigned>(), out));
     }
-    CKI(read_reduced(ctx, nm, row.data()));
-    if (shift) {
+    CK(cudaMemcpyAsync(hred_row(ctx, s.set), out, sizeof(double) * nm, cudaMemcpyDeviceToHost,
+                       ctx->st));
+    s.p_nm = nm;
+    s.p_shift = shift;
+    s.p_map = pmap;
+    s.p_xnew = xnew;
+  } else {
+    hist.n = 0;
+    StageScope sc(ctx, ST_JACOBI);
+    CK(launch_jacobi_step(ctx->L(), ctx->tb, n, s.rhs, s.y, s.x, s.hx, s.he, hist,
+                          ctx->partials.as<double>(), nblk, s.f32, nullptr,
+                          ctx->rcount.as<unsigned>(), out));
+  }
+  return DDC_OK;
+}
+
+int jd_b(ddc_ctx* ctx, JDState& s) {
+  const long long n = (long long)ctx->nsph * ctx->nylm;
+  const int ndiis = jd_ndiis(ctx, s.f32);
+  const int lenb = s.lenb;
+  auto Bm = [&](int j, int k) -> double& { return s.B[(size_t)(k - 1) * lenb + (j - 1)]; };
+  HistPtrs comb{};
+  const void* xj = s.hx;
+  double* out = red_row(ctx, s.set);
+  if (ndiis != 0) {
+    const double* row = hred_row(ctx, s.set);
+    if (s.p_shift) {
       for (int j = 2; j <= s.nmat - 10; j++)
         for (int k = 2; k <= s.nmat - 10; k++) Bm(j, k) = Bm(j + 10, k + 10);
-      s.map = pmap;
+      s.map = s.p_map;
     }
-    s.nmat = nm;
+    s.nmat = s.p_nm;
     // makeb (jacobi_diis.f90:232-270)
     if (s.nmat == 1) {
       Bm(1, 1) = 0.0;
@@ -1055,23 +1083,20 @@ int jd_step(ddc_ctx* ctx, JDState& s) {
       s.restarts++;
       comb.n = 0;
     }
-    xj = xnew;
-  } else {
-    hist.n = 0;
-    StageScope sc(ctx, ST_JACOBI);
-    CK(launch_jacobi_step(ctx->L(), ctx->tb, n, s.rhs, s.y, s.x, s.hx, s.he, hist,
-                          ctx->partials.as<double>(), nblk, s.f32, nullptr,
-                          ctx->rcount.as<unsigned>(), ctx->red.as<double>()));
-    comb.n = 0;
-    xj = s.hx;
+    xj = s.p_xnew;
   }
   {
     StageScope sc(ctx, ST_COMBINE);
     CK(launch_diis_combine(ctx->L(), ctx->tb, n, comb, xj, s.x, ctx->partials.as<double>(),
-                           nblk, s.f32, ctx->rcount.as<unsigned>(), ctx->red.as<double>()));
+                           reduce_blocks(), s.f32, ctx->rcount.as<unsigned>(), out));
   }
-  double ss = 0.0;
-  CKI(read_reduced(ctx, 1, &ss));
+  CK(cudaMemcpyAsync(hred_row(ctx, s.set), out, sizeof(double), cudaMemcpyDeviceToHost,
+                     ctx->st));
+  return DDC_OK;
+}
+
+int jd_c(ddc_ctx* ctx, JDState& s) {
+  const double ss = hred_row(ctx, s.set)[0];
   s.rms = std::sqrt(ss / (double)std::max(ctx->nsph, 1));
   if (*s.logpos < 256) s.inf->norms[*s.logpos] = s.rms;
   ++*s.logpos;
@@ -1083,6 +1108,14 @@ int jd_step(ddc_ctx* ctx, JDState& s) {
   s.ok = s.rms < s.tol;
   s.done = s.ok || s.it >= s.max_iter;
   return DDC_OK;
+}
+
+int jd_step(ddc_ctx* ctx, JDState& s) {
+  CKI(jd_a(ctx, s));
+  CKI(sync(ctx));
+  CKI(jd_b(ctx, s));
+  CKI(sync(ctx));
+  return jd_c(ctx, s);
 }
 
 // FP64 solve: the reference's Jacobi/DIIS on the FP64 operator.
@@ -1110,6 +1143,7 @@ struct SolveTask {
   // start that is never converged) comes from the FP32 operator, like the
   // inner iterations; the convergence test runs from the second refinement on
   bool f32_first = false;
+  int set = 0;  // work-vector set and reduction row (0 direct, 1 adjoint)
 };
 
 void task_begin(ddc_ctx* ctx, SolveTask& t, bool adjoint, const double* rhs, double* x,
@@ -1121,6 +1155,7 @@ void task_begin(ddc_ctx* ctx, SolveTask& t, bool adjoint, const double* rhs, dou
   t.inf = inf;
   memset(inf, 0, sizeof(*inf));
   t.b = solve_bufs(ctx, set);
+  t.set = set;
   t.tol = std::pow(10.0, -(double)ctx->prm.iconv);
   t.t0 = now_s();
   t.phase = 0;
@@ -1130,7 +1165,8 @@ void task_begin(ddc_ctx* ctx, SolveTask& t, bool adjoint, const double* rhs, dou
   t.done = t.ok = false;
   t.f32_first = t.mixed && !ctx->guess_preset &&
                 (ctx->prm.guess == DDC_GUESS_REFERENCE || ctx->prm.guess == DDC_GUESS_ZERO);
-  if (!t.mixed) jd_begin(ctx, t.jd, rhs, x, t.tol, ctx->prm.max_iter, t.b, inf, &t.logpos);
+  if (!t.mixed)
+    jd_begin(ctx, t.jd, rhs, x, t.tol, ctx->prm.max_iter, t.b, inf, &t.logpos, false, set);
   if (!t.mixed && t.jd.done) t.done = true;
 }
 
@@ -1147,32 +1183,38 @@ OpKind task_next(const SolveTask& t, const double** in, double** out) {
   return t.f32_first && t.outer == 0 ? OP_F32 : OP_F64;
 }
 
-int task_after(ddc_ctx* ctx, SolveTask& t) {
+// the task's next step is a Jacobi/DIIS iteration (FP64 solve, or an inner
+// solve of the mixed refinement)
+bool task_in_jd(const SolveTask& t) { return !t.mixed || t.phase == 1; }
+
+// the task's bookkeeping after a Jacobi/DIIS iteration
+int task_after_jd(ddc_ctx* ctx, SolveTask& t) {
+  if (!t.jd.done) return DDC_OK;
   if (!t.mixed) {
-    CKI(jd_step(ctx, t.jd));
-    if (t.jd.done) {
-      t.done = true;
-      t.ok = t.jd.ok;
-      t.its = t.jd.ok ? t.jd.it : ctx->prm.max_iter;
-      t.restarts += t.jd.restarts;
-      t.last = t.jd.rms;
-    }
+    t.done = true;
+    t.ok = t.jd.ok;
+    t.its = t.jd.ok ? t.jd.it : ctx->prm.max_iter;
+    t.restarts += t.jd.restarts;
+    t.last = t.jd.rms;
     return DDC_OK;
   }
   const long long n = (long long)ctx->nsph * ctx->nylm;
-  if (t.phase == 1) {
+  const int done = t.jd.ok ? t.jd.it : t.jd.max_iter;
+  t.its += done;
+  t.budget -= done;
+  t.restarts += t.jd.restarts;
+  CK(launch_axpy(ctx->L(), n, 1.0, t.b.e, t.x));
+  t.phase = 0;
+  if (t.outer >= 64) t.done = true;
+  return DDC_OK;
+}
+
+int task_after(ddc_ctx* ctx, SolveTask& t) {
+  if (task_in_jd(t)) {
     CKI(jd_step(ctx, t.jd));
-    if (t.jd.done) {
-      const int done = t.jd.ok ? t.jd.it : t.jd.max_iter;
-      t.its += done;
-      t.budget -= done;
-      t.restarts += t.jd.restarts;
-      CK(launch_axpy(ctx->L(), n, 1.0, t.b.e, t.x));
-      t.phase = 0;
-      if (t.outer >= 64) t.done = true;
-    }
-    return DDC_OK;
+    return task_after_jd(ctx, t);
   }
+  const long long n = (long long)ctx->nsph * ctx->nylm;
   // phase 0: y = L x in FP64 is ready
   ++t.outer;
   {
@@ -1204,7 +1246,7 @@ int task_after(ddc_ctx* ctx, SolveTask& t) {
   const double rho = 1e-5;
   const double itol = std::max(rho * t.last, 0.3 * t.tol);
   // the correction is wanted to ~1e-5 relative: FP32 history vectors suffice
-  jd_begin(ctx, t.jd, t.b.r, t.b.e, itol, t.budget, t.b, t.inf, &t.logpos, true);
+  jd_begin(ctx, t.jd, t.b.r, t.b.e, itol, t.budget, t.b, t.inf, &t.logpos, true, t.set);
   t.phase = 1;
   return DDC_OK;
 }
@@ -1244,8 +1286,24 @@ int solve_tasks(ddc_ctx* ctx, SolveTask* t, int nt) {
       for (int q = 0; q < nt; q++)
         if (k[q] != OP_NONE) CKI(op_single(ctx, k[q], t[q].adjoint, in[q], out[q]));
     }
-    for (int q = 0; q < nt; q++)
-      if (k[q] != OP_NONE) CKI(task_after(ctx, t[q]));
+    if (nt == 2 && k[0] != OP_NONE && k[1] != OP_NONE && task_in_jd(t[0]) && task_in_jd(t[1])) {
+      // both systems take a Jacobi/DIIS iteration: one synchronisation for
+      // both Gram rows and one for both increment norms (each system keeps
+      // its own state, history and reduction row)
+      CKI(jd_a(ctx, t[0].jd));
+      CKI(jd_a(ctx, t[1].jd));
+      CKI(sync(ctx));
+      CKI(jd_b(ctx, t[0].jd));
+      CKI(jd_b(ctx, t[1].jd));
+      CKI(sync(ctx));
+      CKI(jd_c(ctx, t[0].jd));
+      CKI(jd_c(ctx, t[1].jd));
+      CKI(task_after_jd(ctx, t[0]));
+      CKI(task_after_jd(ctx, t[1]));
+    } else {
+      for (int q = 0; q < nt; q++)
+        if (k[q] != OP_NONE) CKI(task_after(ctx, t[q]));
+    }
   }
   int rc = DDC_OK;
   for (int q = 0; q < nt; q++) {
