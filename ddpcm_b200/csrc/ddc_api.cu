@@ -125,6 +125,7 @@ struct ddc_ctx {
   // geometry
   DBuf sph, grid, basis, bw, fi, ui, zi, inl, nl, rev, pn_ptr, pn, pn_pair, ls_ptr, ls, ntri_pt;
   DBuf lsstart, fxa, fda, fvec, xk;
+  DBuf pn_bits;  // per pair, which grid points lie inside the neighbour (ddinit scratch)
   // batched molecules: partition, per-target N-body ranges, per-molecule DIIS state
   int nmol = 1;
   bool batch_init = false;  // set while ddc_batch_energy_forces initialises
@@ -569,8 +570,10 @@ int do_init(ddc_ctx* ctx, int n, const std::vector<double4>* hsph, const double4
   CK(ctx->cnt.ensure(sizeof(int) * (std::max(scan_n, pscan) + 1)));
   CK(ctx->pn_ptr.ensure(sizeof(int) * (npair + 1)));
   CK(cudaMemsetAsync(ctx->cnt.p, 0, sizeof(int) * (npair + 1), ctx->st));
-  CK(launch_pair_count(L, N, G, ctx->sph.as<double4>(), ctx->grid.as<double4>(),
-                       ctx->inl.as<int>(), ctx->nl.as<int>(), ctx->cnt.as<int>()));
+  CK(ctx->pn_bits.ensure(sizeof(unsigned) * std::max(npair, 1) * (size_t)((G + 31) / 32)));
+  CK(launch_pair_count(L, N, npair, G, ctx->sph.as<double4>(), ctx->grid.as<double4>(),
+                       ctx->inl.as<int>(), ctx->nl.as<int>(), ctx->cnt.as<int>(),
+                       ctx->pn_bits.as<unsigned>()));
   CKI(check_count_total(ctx, ctx->cnt.as<int>(), npair, "(sphere, point, neighbour) triples"));
   size_t tb2 = scan_temp_bytes(npair);
   CK(ctx->scan_tmp.ensure(std::max(tb_bytes, tb2)));
@@ -583,9 +586,9 @@ int do_init(ddc_ctx* ctx, int n, const std::vector<double4>* hsph, const double4
   ctx->ntri = ntri;
   CK(ctx->pn.ensure(sizeof(uint16_t) * std::max(ntri, 1)));
   CK(ctx->pn_pair.ensure(std::max(ntri, 1)));
-  CK(launch_pair_fill(L, N, G, ctx->sph.as<double4>(), ctx->grid.as<double4>(), ctx->inl.as<int>(),
-                      ctx->nl.as<int>(), ctx->pn_ptr.as<int>(), ctx->pn.as<uint16_t>(),
-                      ctx->pn_pair.as<uint8_t>()));
+  CK(launch_pair_fill(L, N, npair, G, ctx->sph.as<double4>(), ctx->grid.as<double4>(),
+                      ctx->inl.as<int>(), ctx->nl.as<int>(), ctx->pn_bits.as<unsigned>(),
+                      ctx->pn_ptr.as<int>(), ctx->pn.as<uint16_t>(), ctx->pn_pair.as<uint8_t>()));
   CK(ctx->ls_ptr.ensure(sizeof(int) * (N + 1)));
   CK(cudaMemsetAsync(ctx->cnt.p, 0, sizeof(int) * (N + 1), ctx->st));
   CK(launch_ls_count(L, N, ctx->inl.as<int>(), ctx->rev.as<int>(), ctx->pn_ptr.as<int>(),
@@ -1124,7 +1127,7 @@ int jd_step(ddc_ctx* ctx, JDState& s) {
 // H-norm is the reference's convergence test (jacobi_diis.f90:143-150), so
 // the solve stops exactly when the FP64 Jacobi increment is below
 // 10^-iconv.  Otherwise the correction equation L e = r is solved with
-// Jacobi/DIIS on the FP32 operator (from e = d, to 1e-5 relative) and x += e.
+// Jacobi/DIIS on the FP32 operator (from e = d, to 1e-4 relative) and x += e.
 // A SolveTask is one such solve as a resumable state; solve_tasks advances
 // one or two of them, one operator application each per round.
 enum OpKind { OP_NONE = 0, OP_F64 = 1, OP_F32 = 2 };
@@ -1243,9 +1246,16 @@ int task_after(ddc_ctx* ctx, SolveTask& t) {
   }
   // correction: (D + O32) e = r from e = D^-1 r
   CK(cudaMemcpyAsync(t.b.e, t.b.d, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx->st));
-  const double rho = 1e-5;
+  // Each inner solve reduces its increment by rho (floor 0.3 tol).  Every
+  // restart of the inner DIIS costs about ten iterations before the
+  // extrapolation has a subspace again, so the split between the two inner
+  // solves matters: at the 20,000-sphere workload rho = 1e-5 takes 88 / 86
+  // iterations, 3e-5 86 / 80, 1e-4 80 / 79 (Esolv 2e-10 from the FP64
+  // oracle; at most 3.9e-10 over eight smaller molecules, as with 1e-5), and
+  // 3e-4 84 / 71 but 1.7e-9 on the 600-sphere configuration.
+  // The correction is wanted to 1e-4 relative: FP32 history vectors suffice.
+  const double rho = 1e-4;
   const double itol = std::max(rho * t.last, 0.3 * t.tol);
-  // the correction is wanted to ~1e-5 relative: FP32 history vectors suffice
   jd_begin(ctx, t.jd, t.b.r, t.b.e, itol, t.budget, t.b, t.inf, &t.logpos, true, t.set);
   t.phase = 1;
   return DDC_OK;

@@ -187,11 +187,13 @@ cudaError_t launch_cav_count(Launch L, int nsph, int ngrid, const double* ui, in
 cudaError_t launch_cav_fill(Launch L, int nsph, int ngrid, const double* ui, const double4* sph,
                             const double4* grid, const int* cavoff, int* cavidx, int* cavpt,
                             double* ccav);
-cudaError_t launch_pair_count(Launch L, int nsph, int ngrid, const double4* sph,
-                              const double4* grid, const int* inl, const int* nl, int* cnt);
-cudaError_t launch_pair_fill(Launch L, int nsph, int ngrid, const double4* sph,
+cudaError_t launch_pair_count(Launch L, int nsph, int npair, int ngrid, const double4* sph,
+                              const double4* grid, const int* inl, const int* nl, int* cnt,
+                              unsigned* bits);  // bits: [npair][ceil(ngrid / 32)] words
+cudaError_t launch_pair_fill(Launch L, int nsph, int npair, int ngrid, const double4* sph,
                              const double4* grid, const int* inl, const int* nl,
-                             const int* pn_ptr, uint16_t* pn, uint8_t* pn_pair);
+                             const unsigned* bits, const int* pn_ptr, uint16_t* pn,
+                             uint8_t* pn_pair);
 cudaError_t launch_ls_count(Launch L, int nsph, const int* inl, const int* rev, const int* pn_ptr,
                             int* cnt);
 cudaError_t launch_ls_fill(Launch L, int nsph, const int* inl, const int* nl, const int* rev,

@@ -409,59 +409,73 @@ cudaError_t launch_cav_fill(Launch L, int nsph, int ngrid, const double* ui, con
 // sphere i with t_n^ij < 1 (calcv's test, ddcosmo.f90:1707-1716).  Warp per
 // pair, ballot over points in ascending order.
 // ---------------------------------------------------------------------------
+// The count pass stores each pair's membership bits (one 32-bit word per 32
+// grid points), and the fill pass expands them: the exact geometry of every
+// (pair, point) is evaluated once
 template <bool FILL>
-__global__ void k_pairs(int nsph, int ngrid, const double4* __restrict__ sph,
+__global__ void k_pairs(int nsph, int npair, int ngrid, const double4* __restrict__ sph,
                         const double4* __restrict__ grid, const int* __restrict__ inl,
-                        const int* __restrict__ nl, int* cnt, const int* pn_ptr, uint16_t* pn,
-                        uint8_t* pn_pair) {
+                        const int* __restrict__ nl, int* cnt, unsigned* __restrict__ bits,
+                        const int* pn_ptr, uint16_t* pn, uint8_t* pn_pair) {
   int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-  int npair = inl[nsph];
   if (warp >= npair) return;
   const int k = warp;
-  // sphere owning entry k: binary search in inl
-  int lo = 0, hi = nsph - 1;
-  while (lo < hi) {
-    int mid = (lo + hi + 1) >> 1;
-    if (inl[mid] <= k) lo = mid; else hi = mid - 1;
-  }
-  const int i = lo, j = nl[k];
-  const double4 ci = sph[i], cj = sph[j];
-  int base = FILL ? pn_ptr[k] : 0;
-  for (int n0 = 0; n0 < ngrid; n0 += 32) {
-    int n = n0 + lane;
-    bool in = false;
-    if (n < ngrid) in = rel_exact(ci, grid[n], cj).t < 1.0;
-    unsigned mask = __ballot_sync(0xffffffffu, in);
-    if (FILL && in) {
-      const int pos = base + __popc(mask & ((1u << lane) - 1u));
-      pn[pos] = (uint16_t)n;
-      pn_pair[pos] = (uint8_t)(k - inl[i]);
+  const int nw = (ngrid + 31) >> 5;
+  unsigned* kb = bits + (size_t)k * nw;
+  if constexpr (!FILL) {
+    // sphere owning entry k: binary search in inl
+    int lo = 0, hi = nsph - 1;
+    while (lo < hi) {
+      int mid = (lo + hi + 1) >> 1;
+      if (inl[mid] <= k) lo = mid; else hi = mid - 1;
     }
-    base += __popc(mask);
+    const int i = lo, j = nl[k];
+    const double4 ci = sph[i], cj = sph[j];
+    int total = 0;
+    for (int w = 0; w < nw; ++w) {
+      const int n = 32 * w + lane;
+      bool in = false;
+      if (n < ngrid) in = rel_exact(ci, grid[n], cj).t < 1.0;
+      const unsigned mask = __ballot_sync(0xffffffffu, in);
+      if (lane == 0) kb[w] = mask;
+      total += __popc(mask);
+    }
+    if (lane == 0) cnt[k] = total;
+  } else {
+    int lo = 0, hi = nsph - 1;
+    while (lo < hi) {
+      int mid = (lo + hi + 1) >> 1;
+      if (inl[mid] <= k) lo = mid; else hi = mid - 1;
+    }
+    const int i = lo;
+    int base = pn_ptr[k];
+    for (int w = 0; w < nw; ++w) {
+      const unsigned mask = kb[w];
+      if ((mask >> lane) & 1u) {
+        const int pos = base + __popc(mask & ((1u << lane) - 1u));
+        pn[pos] = (uint16_t)(32 * w + lane);
+        pn_pair[pos] = (uint8_t)(k - inl[i]);
+      }
+      base += __popc(mask);
+    }
   }
-  if (!FILL && lane == 0) cnt[k] = base;
 }
-cudaError_t launch_pair_count(Launch L, int nsph, int ngrid, const double4* sph,
-                              const double4* grid, const int* inl, const int* nl, int* cnt) {
-  int npair;
-  cudaError_t e = cudaMemcpyAsync(&npair, inl + nsph, sizeof(int), cudaMemcpyDeviceToHost, L.st);
-  if (e) return e;
-  if ((e = cudaStreamSynchronize(L.st))) return e;
+cudaError_t launch_pair_count(Launch L, int nsph, int npair, int ngrid, const double4* sph,
+                              const double4* grid, const int* inl, const int* nl, int* cnt,
+                              unsigned* bits) {
   if (npair == 0) return cudaSuccess;
-  k_pairs<false><<<(npair + 7) / 8, 256, 0, L.st>>>(nsph, ngrid, sph, grid, inl, nl, cnt, nullptr,
-                                                    nullptr, nullptr);
+  k_pairs<false><<<(npair + 7) / 8, 256, 0, L.st>>>(nsph, npair, ngrid, sph, grid, inl, nl, cnt,
+                                                    bits, nullptr, nullptr, nullptr);
   ++*L.launches;
   return cudaGetLastError();
 }
-cudaError_t launch_pair_fill(Launch L, int nsph, int ngrid, const double4* sph,
+cudaError_t launch_pair_fill(Launch L, int nsph, int npair, int ngrid, const double4* sph,
                              const double4* grid, const int* inl, const int* nl,
-                             const int* pn_ptr, uint16_t* pn, uint8_t* pn_pair) {
-  int npair;
-  cudaError_t e = cudaMemcpyAsync(&npair, inl + nsph, sizeof(int), cudaMemcpyDeviceToHost, L.st);
-  if (e) return e;
-  if ((e = cudaStreamSynchronize(L.st))) return e;
+                             const unsigned* bits, const int* pn_ptr, uint16_t* pn,
+                             uint8_t* pn_pair) {
   if (npair == 0) return cudaSuccess;
-  k_pairs<true><<<(npair + 7) / 8, 256, 0, L.st>>>(nsph, ngrid, sph, grid, inl, nl, nullptr, pn_ptr,
+  k_pairs<true><<<(npair + 7) / 8, 256, 0, L.st>>>(nsph, npair, ngrid, sph, grid, inl, nl,
+                                                   nullptr, const_cast<unsigned*>(bits), pn_ptr,
                                                    pn, pn_pair);
   ++*L.launches;
   return cudaGetLastError();
@@ -2910,27 +2924,30 @@ __device__ __forceinline__ void lxs_run_role(int role, const YlmTables& tb, cons
 }
 
 // the L* rows of role R: lane sums by a fixed shuffle tree, then its columns
-template <int LMAX, int NR, int R, int M, class Rl, bool GAM>
+// G: the greedy column map (else the pairing); the fused pass's choice by
+// default
+template <int LMAX, int NR, int R, int M, class Rl, bool GAM, bool G = sizeof(Rl) == 4>
 __device__ __forceinline__ void lxs_store_cols(const YlmTables& tb, const Rl* acc, double* yi,
                                                int lane) {
-  if constexpr (lxs_role_of(LMAX, NR, M, sizeof(Rl) == 4) == R)
-    ls_store<LMAX, M, lxs_off_of(LMAX, NR, M, sizeof(Rl) == 4), Rl, GAM>(tb, acc, yi, lane);
-  if constexpr (M < LMAX) lxs_store_cols<LMAX, NR, R, M + 1, Rl, GAM>(tb, acc, yi, lane);
+  if constexpr (lxs_role_of(LMAX, NR, M, G) == R)
+    ls_store<LMAX, M, lxs_off_of(LMAX, NR, M, G), Rl, GAM>(tb, acc, yi, lane);
+  if constexpr (M < LMAX) lxs_store_cols<LMAX, NR, R, M + 1, Rl, GAM, G>(tb, acc, yi, lane);
 }
-template <int LMAX, int NR, int R, class Rl, bool GAM>
+template <int LMAX, int NR, int R, class Rl, bool GAM, bool G = sizeof(Rl) == 4>
 __device__ __forceinline__ void lxs_finish_role(int role, const YlmTables& tb, Rl* acc,
                                                 double* yi, int lane) {
   if (role == R) {
-    constexpr int NV = lxs_role_nvals(LMAX, NR, R, sizeof(Rl) == 4);
+    constexpr int NV = lxs_role_nvals(LMAX, NR, R, G);
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
 #pragma unroll
       for (int o = 16; o >= 1; o >>= 1) acc[v] += __shfl_xor_sync(0xffffffffu, acc[v], o);
     }
-    lxs_store_cols<LMAX, NR, R, 0, Rl, GAM>(tb, acc, yi, lane);
+    lxs_store_cols<LMAX, NR, R, 0, Rl, GAM, G>(tb, acc, yi, lane);
     return;
   }
-  if constexpr (R + 1 < NR) lxs_finish_role<LMAX, NR, R + 1, Rl, GAM>(role, tb, acc, yi, lane);
+  if constexpr (R + 1 < NR)
+    lxs_finish_role<LMAX, NR, R + 1, Rl, GAM, G>(role, tb, acc, yi, lane);
 }
 
 // the inputs of one triple's shared fields, loaded one chunk ahead
@@ -3864,18 +3881,28 @@ __device__ __forceinline__ void fa_column(const YlmTables& tb, double ct, double
     }
   }
 }
+// Roles of k_far_acc: at lmax 10 four roles of about three columns each
+// (the greedy map of the FP32 fused pass: each role's per-source fixed cost
+// paid four times instead of six), else the pairing m / lmax-m
+__host__ __device__ constexpr bool fa_greedy(int L) { return L == 10; }
+__host__ __device__ constexpr int fa_nroles(int L) { return fa_greedy(L) ? 4 : L / 2 + 1; }
+template <int LMAX, int R, int M>
+__device__ __forceinline__ void fa_cols(const YlmTables& tb, const double* sh, int stride, int q,
+                                        double ct, double t2, double* acc) {
+  constexpr int NR = fa_nroles(LMAX);
+  constexpr bool G = fa_greedy(LMAX);
+  if constexpr (lxs_role_of(LMAX, NR, M, G) == R)
+    fa_column<LMAX, M, lxs_off_of(LMAX, NR, M, G)>(tb, ct, t2, sh[(2 + 3 * M) * stride + q],
+                                                   sh[(3 + 3 * M) * stride + q],
+                                                   sh[(4 + 3 * M) * stride + q], acc);
+  if constexpr (M < LMAX) fa_cols<LMAX, R, M + 1>(tb, sh, stride, q, ct, t2, acc);
+}
 template <int LMAX, int R>
 __device__ __forceinline__ void fa_role(const YlmTables& tb, const double* sh, int stride,
                                         int count, int lane, double* acc) {
-  constexpr int M1 = R, M2 = LMAX - R;
   for (int q = lane; q < count; q += 32) {
     const double ct = sh[q], t2 = sh[stride + q];
-    fa_column<LMAX, M1, 0>(tb, ct, t2, sh[(2 + 3 * M1) * stride + q],
-                           sh[(3 + 3 * M1) * stride + q], sh[(4 + 3 * M1) * stride + q], acc);
-    if constexpr (ls_has2(LMAX, R))
-      fa_column<LMAX, M2, ls_nvals_m(LMAX, M1)>(tb, ct, t2, sh[(2 + 3 * M2) * stride + q],
-                                                sh[(3 + 3 * M2) * stride + q],
-                                                sh[(4 + 3 * M2) * stride + q], acc);
+    fa_cols<LMAX, R, 0>(tb, sh, stride, q, ct, t2, acc);
   }
 }
 template <int LMAX, int R>
@@ -3885,7 +3912,8 @@ __device__ __forceinline__ void fa_run_role(int role, const YlmTables& tb, const
     fa_role<LMAX, R>(tb, sh, stride, count, lane, acc);
     return;
   }
-  if constexpr (R + 1 < ls_nroles(LMAX)) fa_run_role<LMAX, R + 1>(role, tb, sh, stride, count, lane, acc);
+  if constexpr (R + 1 < fa_nroles(LMAX))
+    fa_run_role<LMAX, R + 1>(role, tb, sh, stride, count, lane, acc);
 }
 
 // A(i, lm) for every sphere with cavity points: block per sphere, role warps
@@ -3894,15 +3922,16 @@ __device__ __forceinline__ void fa_run_role(int role, const YlmTables& tb, const
 // (rsqrt_pos), the prefix and cos/sin(m phi) (the fields of k_lstarx); the
 // roles run the normalised recurrence (fa_column) and store with Kg.
 template <int LMAX>
-__global__ void __launch_bounds__(32 * ls_nroles(LMAX)) k_far_acc(const YlmTables tb, int nsph,
+__global__ void __launch_bounds__(32 * fa_nroles(LMAX), fa_greedy(LMAX) ? 4 : 1)
+    k_far_acc(const YlmTables tb, int nsph,
                                                                    const double4* __restrict__ sph,
                                                                    const double* __restrict__ q,
                                                                    const int2* __restrict__ mrange,
                                                                    const int* __restrict__ cavoff,
                                                                    double rho, double* A) {
-  constexpr int NR = ls_nroles(LMAX);
+  constexpr int NR = fa_nroles(LMAX);
   constexpr int CH = 32 * NR;
-  constexpr int NVM = ls_max_nvals(LMAX);
+  constexpr int NVM = lxs_max_nvals(LMAX, NR, fa_greedy(LMAX));
   extern __shared__ double sh[];  // [ls_nfields][CH]
   const int i = blockIdx.x;
   if (cavoff[i + 1] == cavoff[i]) return;  // buried: A(i) is never read
@@ -3963,7 +3992,8 @@ __global__ void __launch_bounds__(32 * ls_nroles(LMAX)) k_far_acc(const YlmTable
     fa_run_role<LMAX, 0>(role, tb, sh, CH, chunk, lane, acc);
     __syncthreads();
   }
-  ls_finish_role<LMAX, 0, double, true>(role, tb, acc, A + (size_t)i * tb.nylm, lane);
+  lxs_finish_role<LMAX, NR, 0, double, true, fa_greedy(LMAX)>(role, tb, acc,
+                                                              A + (size_t)i * tb.nylm, lane);
 }
 
 // Tables on the grid, once per context: BT[lm][n] = Y_lm(s_n) and
@@ -4255,7 +4285,7 @@ cudaError_t launch_far_pot_field(Launch L, const YlmTables& tbP, int nsph, int n
   cudaError_t e;
 #define CASE(LV)                                                                              \
   case LV: {                                                                                  \
-    constexpr int NR = ls_nroles(LV);                                                         \
+    constexpr int NR = fa_nroles(LV);                                                         \
     const size_t sm = sizeof(double) * ls_nfields(LV) * 32 * NR;                              \
     if (sm > 48 * 1024)                                                                       \
       if ((e = cudaFuncSetAttribute(k_far_acc<LV>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
