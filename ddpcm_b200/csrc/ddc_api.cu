@@ -131,6 +131,7 @@ struct ddc_ctx {
   bool batch_init = false;  // set while ddc_batch_energy_forces initialises
   bool capturing = false;   // stream capture in progress: no stage events
   std::vector<int> h_off;
+  DBuf b_cmol, b_cfirst, b_part, b_cnt, b_coef, b_ext;  // chunked batched Jacobi/DIIS
   DBuf d_off, mrange, tr_cav, tr_nuc, b_nmat, b_slot, b_B, b_status, b_iters, b_restarts, b_norm,
       b_out;
   const int2* mrange_ptr() const { return nmol > 1 ? mrange.as<int2>() : nullptr; }
@@ -1498,7 +1499,35 @@ int batch_setup(ddc_ctx* ctx, BatchSys& b, bool adjoint, const double* rhs, doub
   CK(ctx->b_iters.ensure(sizeof(int) * 2 * nmol));
   CK(ctx->b_restarts.ensure(sizeof(int) * 2 * nmol));
   CK(ctx->b_norm.ensure(sizeof(double) * 2 * nmol));
+  // element chunks of each molecule (the same for both sets)
+  std::vector<int> cfirst(nmol + 1, 0), cmol;
+  for (int k = 0; k < nmol; k++) {
+    const long long len = (long long)(ctx->h_off[k + 1] - ctx->h_off[k]) * ctx->nylm;
+    const int nc = (int)((len + kBatchChunk - 1) / kBatchChunk);
+    for (int c = 0; c < nc; c++) cmol.push_back(k);
+    cfirst[k + 1] = cfirst[k] + nc;
+  }
+  const int nchunk = cfirst[nmol];
+  CK(ctx->b_cmol.ensure(sizeof(int) * std::max(nchunk, 1)));
+  CK(ctx->b_cfirst.ensure(sizeof(int) * (nmol + 1)));
+  CK(ctx->b_part.ensure(sizeof(double) * 2 * (size_t)std::max(nchunk, 1) * (kMaxHist + 1)));
+  CK(ctx->b_cnt.ensure(sizeof(unsigned) * 2 * nmol));
+  CK(ctx->b_coef.ensure(sizeof(double) * 2 * (size_t)nmol * kMaxHist));
+  CK(ctx->b_ext.ensure(sizeof(int) * 2 * nmol));
   BatchState& bs = b.bs;
+  bs.nchunk = nchunk;
+  bs.cmol = ctx->b_cmol.as<int>();
+  bs.cfirst = ctx->b_cfirst.as<int>();
+  bs.part = ctx->b_part.as<double>() + (size_t)set * std::max(nchunk, 1) * (kMaxHist + 1);
+  bs.cnt = ctx->b_cnt.as<unsigned>() + (size_t)set * nmol;
+  bs.coef = ctx->b_coef.as<double>() + (size_t)set * nmol * kMaxHist;
+  bs.ext = ctx->b_ext.as<int>() + (size_t)set * nmol;
+  if (nchunk)
+    CK(cudaMemcpyAsync(ctx->b_cmol.p, cmol.data(), sizeof(int) * nchunk, cudaMemcpyHostToDevice,
+                       ctx->st));
+  CK(cudaMemcpyAsync(ctx->b_cfirst.p, cfirst.data(), sizeof(int) * (nmol + 1),
+                     cudaMemcpyHostToDevice, ctx->st));
+  CK(cudaMemsetAsync(bs.cnt, 0, sizeof(unsigned) * nmol, ctx->st));
   bs.nmol = nmol;
   bs.ndiis = nd;
   bs.max_iter = ctx->prm.max_iter;

@@ -138,6 +138,8 @@ enum Stage {
 
 // History of DIIS vectors for the fused Jacobi step / extrapolation.
 constexpr int kMaxHist = 32;
+// elements per chunk of the batched Jacobi/DIIS kernels
+constexpr int kBatchChunk = 2048;
 // The vectors are FP64, or FP32 for the inner solves of the mixed path.
 struct HistPtrs {
   const void* p[kMaxHist];
@@ -160,6 +162,15 @@ struct BatchState {
   double* norm;       // [nmol] last increment norm
   double* hx;         // [ndiis][n_total]
   double* he;         // [ndiis][n_total]
+  // element chunks of the per-molecule kernels: chunk c holds up to
+  // kBatchChunk consecutive elements of molecule cmol[c]
+  int nchunk;
+  const int* cmol;    // [nchunk]
+  const int* cfirst;  // [nmol+1] first chunk of each molecule
+  double* part;       // [nchunk][kMaxHist+1] per-chunk partial sums
+  unsigned* cnt;      // [nmol] arrival counters, zero between kernels
+  double* coef;       // [nmol][kMaxHist] extrapolation coefficients
+  int* ext;           // [nmol] terms of the extrapolation; negative after a singular solve
 };
 
 // ---------------------------------------------------------------------------

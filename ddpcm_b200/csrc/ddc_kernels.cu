@@ -3515,8 +3515,7 @@ cudaError_t launch_axpy(Launch L, long long n, double a, const double* x, double
 // ---------------------------------------------------------------------------
 // Batched solves: many molecules concatenated into one system.  The
 // operators act per sphere and need no change; the Jacobi/DIIS driver
-// (jacobi_diis.f90) runs per molecule, fused into one kernel per iteration
-// with one block per molecule.
+// (jacobi_diis.f90) runs per molecule over element chunks (below).
 // ---------------------------------------------------------------------------
 // Gauss-Jordan with full pivoting (gjinv, jacobi_diis.f90:272-360), one warp,
 // lane j owns row j.  a is n x n column-major in shared memory, b the rhs.
@@ -3592,164 +3591,278 @@ __device__ bool gjinv_warp(int n, double* a, double* b, int* piv) {
   return true;
 }
 
-__global__ void __launch_bounds__(256) k_batch_diis(const YlmTables tb, BatchState bs,
-                                                    const double* __restrict__ rhs,
-                                                    const double* __restrict__ y, double* x) {
-  const int k = blockIdx.x;
-  const int lenb = bs.ndiis + 1;
-  __shared__ int s_status, s_nm, s_new, s_shift, s_ok, s_nmold;
+// The per-molecule Jacobi/DIIS step runs over element chunks of kBChunk
+// consecutive elements (a molecule owns one or more chunks), so that a
+// large molecule's vectors are read by many blocks at once.  Two kernels:
+// k_batch_gram forms the Jacobi iterate, the increment and the chunk's Gram
+// partials, and the molecule's last chunk to finish sums the partials in
+// chunk order, updates the bordered matrix and solves it (one warp);
+// k_batch_extrap forms the extrapolated iterate and the chunk's part of the
+// increment norm, and the molecule's last chunk sets its norm, iteration
+// count and status.  The history reads are spread over the whole device.
+constexpr int kBChunk = kBatchChunk;
+static_assert(kBChunk % (kSolU * kSolT) == 0 && kBChunk % (32 * 16) == 0, "chunk tiling");
+
+// Logical-to-physical history slots of molecule k for this step: after
+// `nmat` reaches ndiis the ten oldest are dropped (jacobi_diis.f90:196-205).
+__device__ __forceinline__ int batch_hist_perm(const BatchState& bs, int k, int* pm) {
+  const int nd = bs.ndiis, nm_old = bs.nmat[k];
+  const bool shift = nm_old >= nd;
+  const int* sl = bs.slot + (size_t)k * nd;
+  for (int j = threadIdx.x; j < nd; j += blockDim.x) pm[j] = shift ? sl[(j + 10) % nd] : sl[j];
+  return shift ? nm_old - 10 : nm_old;
+}
+
+// Last arriving chunk of molecule k (the counter is reset for the next
+// kernel).  Every block of the molecule calls it after writing its partials.
+__device__ __forceinline__ bool batch_last_chunk(const BatchState& bs, int k) {
+  __shared__ unsigned s_last;
+  __threadfence();
+  __syncthreads();
+  const unsigned nc = (unsigned)(bs.cfirst[k + 1] - bs.cfirst[k]);
+  if (threadIdx.x == 0) {
+    s_last = atomicAdd(bs.cnt + k, 1u) == nc - 1 ? 1u : 0u;
+    if (s_last) bs.cnt[k] = 0u;
+  }
+  __syncthreads();
+  if (s_last) __threadfence();
+  return s_last != 0;
+}
+
+// Sums entries [0, nv) of molecule k's chunk partials in chunk order.
+__device__ __forceinline__ void batch_sum_parts(const BatchState& bs, int k, int nv,
+                                                double* out) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int c0 = bs.cfirst[k], c1 = bs.cfirst[k + 1];
+  for (int h = w; h < nv; h += nw) {
+    double v = 0.0;
+    for (int c = c0 + lane; c < c1; c += 32) v += __ldcg(bs.part + (size_t)c * (kMaxHist + 1) + h);
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) out[h] = v;
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(kSolT) k_batch_gram(const YlmTables tb, BatchState bs,
+                                                      const double* __restrict__ rhs,
+                                                      const double* __restrict__ y,
+                                                      const double* __restrict__ x) {
+  constexpr int U = kBChunk / kSolT;
+  constexpr int NW = kSolT / 32;
+  constexpr int KS = (kMaxHist + NW - 1) / NW;
+  constexpr int HL = 16;
+  const int c = blockIdx.x, k = bs.cmol[c];
+  if (bs.status[k] != 0) return;
   __shared__ int pm[kMaxHist];
-  __shared__ double row[kMaxHist + 1], coef[kMaxHist];
+  __shared__ double es[kBChunk];
+  __shared__ double red[kMaxHist + 1 + NW];
+  __shared__ double row[kMaxHist + 1];
+  const int nm = batch_hist_perm(bs, k, pm), nh = nm - 1;
+  __syncthreads();
+  const int nylm = tb.nylm, lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const long long N = bs.n_total;
+  const long long b0 = (long long)bs.off[k] * nylm + (long long)(c - bs.cfirst[k]) * kBChunk;
+  const int cnt = (int)min((long long)kBChunk, (long long)bs.off[k + 1] * nylm - b0);
+  double* xnew = bs.hx + (size_t)pm[nm - 1] * N;
+  double* enew = bs.he + (size_t)pm[nm - 1] * N;
+  double ee = 0.0;
+  {
+    const int dt = kSolT % nylm;
+    int lm = (int)((b0 + threadIdx.x) % nylm);
+    double rv[U], yv[U], xv[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int j = threadIdx.x + u * kSolT;
+      rv[u] = j < cnt ? rhs[b0 + j] : 0.0;
+      yv[u] = j < cnt ? y[b0 + j] : 0.0;
+      xv[u] = j < cnt ? x[b0 + j] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int j = threadIdx.x + u * kSolT;
+      double ev = 0.0;
+      if (j < cnt) {
+        const double xn = tb.facl[l_of(lm)] * (rv[u] - yv[u]);
+        ev = xn - xv[u];
+        xnew[b0 + j] = xn;
+        enew[b0 + j] = ev;
+      }
+      es[j] = ev;
+      ee = fma(ev, ev, ee);
+      lm = lm_add(lm, dt, nylm);
+    }
+  }
+  __syncthreads();
+  double d[KS];
+#pragma unroll
+  for (int s = 0; s < KS; ++s) {
+    d[s] = 0.0;
+    const int kk = w + NW * s;
+    if (kk < nh) {
+      const double* hk = bs.he + (size_t)pm[kk] * N + b0;
+      for (int j0 = 0; j0 < kBChunk; j0 += 32 * HL) {
+        double hv[HL];
+#pragma unroll
+        for (int u = 0; u < HL; ++u) {
+          const int j = j0 + u * 32 + lane;
+          hv[u] = j < cnt ? hk[j] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < HL; ++u) d[s] = fma(es[j0 + u * 32 + lane], hv[u], d[s]);
+      }
+    }
+  }
+#pragma unroll
+  for (int s = 0; s < KS; ++s) {
+    double v = d[s];
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int kk = w + NW * s;
+    if (lane == 0 && kk < nh) red[kk] = v;
+  }
+#pragma unroll
+  for (int o = 16; o >= 1; o >>= 1) ee += __shfl_xor_sync(0xffffffffu, ee, o);
+  if (lane == 0) red[kMaxHist + 1 + w] = ee;
+  __syncthreads();
+  double* part = bs.part + (size_t)c * (kMaxHist + 1);
+  if (threadIdx.x < nh) {
+    part[threadIdx.x] = red[threadIdx.x];
+  } else if (threadIdx.x == nh) {
+    double t = 0.0;
+    for (int ww = 0; ww < NW; ++ww) t += red[kMaxHist + 1 + ww];
+    part[nh] = t;
+  }
+  if (!batch_last_chunk(bs, k)) return;
+  batch_sum_parts(bs, k, nh + 1, row);
+  if (threadIdx.x >= 32) return;
+  // bordered Gram matrix (makeb, jacobi_diis.f90:232-270) and its solve
   __shared__ double ga[(kMaxHist + 1) * (kMaxHist + 1)], gb[kMaxHist + 1];
   __shared__ int gpiv[kMaxHist + 1];
-  if (threadIdx.x == 0) s_status = bs.status[k];
-  __syncthreads();
-  if (s_status != 0) return;
-  const int nd = bs.ndiis;
+  const int nd = bs.ndiis, lenb = nd + 1, nm_old = bs.nmat[k];
+  double* B = bs.B + (size_t)k * lenb * lenb;
+  auto Bm = [&](int j, int kk) -> double& { return B[(size_t)(kk - 1) * lenb + (j - 1)]; };
   if (threadIdx.x == 0) {
-    const int nm = bs.nmat[k];
-    const int* sl = bs.slot + (size_t)k * nd;
-    s_new = sl[nm - 1];
-    s_nmold = nm;
-    if (nm >= nd) {  // drop the 10 oldest (jacobi_diis.f90:196-205)
-      for (int j = 0; j < nd; ++j) pm[j] = sl[(j + 10) % nd];
-      s_nm = nm - 10;
-      s_shift = 1;
+    if (nm_old >= nd) {
+      for (int j = 2; j <= nm_old - 10; ++j)
+        for (int kk = 2; kk <= nm_old - 10; ++kk) Bm(j, kk) = Bm(j + 10, kk + 10);
+    }
+    if (nm == 1) {
+      Bm(1, 1) = 0.0;
+      Bm(1, 2) = 1.0;
+      Bm(2, 1) = 1.0;
+      Bm(2, 2) = row[0];
     } else {
-      for (int j = 0; j < nd; ++j) pm[j] = sl[j];
-      s_nm = nm;
-      s_shift = 0;
-    }
-  }
-  __syncthreads();
-  const int nm = s_nm, nh = nm - 1;
-  const long long N = bs.n_total;
-  const long long e0 = (long long)bs.off[k] * tb.nylm, e1 = (long long)bs.off[k + 1] * tb.nylm;
-  double* xnew = bs.hx + (size_t)s_new * N;
-  double* enew = bs.he + (size_t)s_new * N;
-  double d[kMaxHist + 1];
-#pragma unroll
-  for (int h = 0; h <= kMaxHist; ++h) d[h] = 0.0;
-  for (long long e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
-    const int lm = (int)(e % tb.nylm);
-    const double xn = tb.facl[l_of(lm)] * (rhs[e] - y[e]);
-    const double ev = xn - x[e];
-    xnew[e] = xn;
-    enew[e] = ev;
-#pragma unroll
-    for (int h = 0; h < kMaxHist; ++h)
-      if (h < nh) d[h] = fma(ev, bs.he[(size_t)pm[h] * N + e], d[h]);
-    d[kMaxHist] = fma(ev, ev, d[kMaxHist]);
-  }
-  double v[kMaxHist + 1];
-#pragma unroll
-  for (int h = 0; h <= kMaxHist; ++h) v[h] = (h < nh) ? d[h] : (h == nh ? d[kMaxHist] : 0.0);
-  {  // block sums of v[0..nh] into row[]
-    __shared__ double sh[kMaxHist + 1][8];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-#pragma unroll
-    for (int h = 0; h <= kMaxHist; ++h) {
-      if (h <= nh) {
-        double t = v[h];
-#pragma unroll
-        for (int o = 16; o >= 1; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
-        if (lane == 0) sh[h][w] = t;
+      Bm(nm + 1, 1) = 1.0;
+      Bm(1, nm + 1) = 1.0;
+      for (int i = 1; i <= nm - 1; ++i) {
+        Bm(nm + 1, i + 1) = row[i - 1];
+        Bm(i + 1, nm + 1) = row[i - 1];
       }
+      Bm(nm + 1, nm + 1) = row[nm - 1];
     }
-    __syncthreads();
-    if (threadIdx.x <= nh) {
-      double t = 0.0;
-      for (int ww = 0; ww < (int)(blockDim.x >> 5); ++ww) t += sh[threadIdx.x][ww];
-      row[threadIdx.x] = t;
-    }
-    __syncthreads();
+    const int n1 = nm + 1;
+    for (int kk = 1; kk <= n1; ++kk)
+      for (int j = 1; j <= n1; ++j) ga[(kk - 1) * n1 + (j - 1)] = Bm(j, kk);
+    for (int j = 0; j < n1; ++j) gb[j] = 0.0;
+    gb[0] = 1.0;
   }
-  if (threadIdx.x < 32) {
-    double* B = bs.B + (size_t)k * lenb * lenb;
-    auto Bm = [&](int j, int kk) -> double& { return B[(size_t)(kk - 1) * lenb + (j - 1)]; };
-    if (threadIdx.x == 0) {
-      if (s_shift) {
-        const int old = s_nmold;
-        for (int j = 2; j <= old - 10; ++j)
-          for (int kk = 2; kk <= old - 10; ++kk) Bm(j, kk) = Bm(j + 10, kk + 10);
-      }
-      if (nm == 1) {  // makeb (jacobi_diis.f90:232-270)
-        Bm(1, 1) = 0.0;
-        Bm(1, 2) = 1.0;
-        Bm(2, 1) = 1.0;
-        Bm(2, 2) = row[0];
-      } else {
-        Bm(nm + 1, 1) = 1.0;
-        Bm(1, nm + 1) = 1.0;
-        for (int i = 1; i <= nm - 1; ++i) {
-          Bm(nm + 1, i + 1) = row[i - 1];
-          Bm(i + 1, nm + 1) = row[i - 1];
-        }
-        Bm(nm + 1, nm + 1) = row[nm - 1];
-      }
-      const int n1 = nm + 1;
-      for (int kk = 1; kk <= n1; ++kk)
-        for (int j = 1; j <= n1; ++j) ga[(kk - 1) * n1 + (j - 1)] = Bm(j, kk);
-      for (int j = 0; j < n1; ++j) gb[j] = 0.0;
-      gb[0] = 1.0;
-    }
-    __syncwarp();
-    const bool ok = gjinv_warp(nm + 1, ga, gb, gpiv);
-    if (threadIdx.x == 0) {
-      int* sl = bs.slot + (size_t)k * nd;
-      if (s_shift)
-        for (int j = 0; j < nd; ++j) sl[j] = pm[j];
-      if (ok) {
-        for (int h = 0; h < nm; ++h) coef[h] = gb[h + 1];
-        bs.nmat[k] = nm + 1;
-      } else {  // singular: restart the history (jacobi_diis.f90:214-217)
-        bs.nmat[k] = 1;
-        bs.restarts[k] += 1;
-      }
-      s_ok = ok ? 1 : 0;
-    }
-  }
-  __syncthreads();
-  // extrapolation, increment H-norm and update (diis :222-226, hnorm)
-  double acc = 0.0;
-  const bool ok = s_ok != 0;
-  for (long long e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
-    double xo;
+  __syncwarp();
+  const bool ok = gjinv_warp(nm + 1, ga, gb, gpiv);
+  if (threadIdx.x == 0) {
+    int* sl = bs.slot + (size_t)k * nd;
+    if (nm_old >= nd)
+      for (int j = 0; j < nd; ++j) sl[j] = pm[j];
+    double* cf = bs.coef + (size_t)k * kMaxHist;
     if (ok) {
-      xo = 0.0;
-      for (int h = 0; h < nm; ++h) xo = fma(coef[h], bs.hx[(size_t)pm[h] * N + e], xo);
-    } else {
-      xo = xnew[e];
+      for (int h = 0; h < nm; ++h) cf[h] = gb[h + 1];
+      bs.nmat[k] = nm + 1;
+    } else {  // singular: restart the history (jacobi_diis.f90:214-217)
+      bs.nmat[k] = 1;
+      bs.restarts[k] += 1;
     }
-    const double dd = xo - x[e];
-    const int l = l_of((int)(e % tb.nylm));
-    acc = fma(dd * dd, 1.0 / (1.0 + l), acc);
-    x[e] = xo;
+    bs.ext[k] = ok ? nm : -nm;
   }
-  {
-    __shared__ double sh2[8];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+}
+
+// DIIS extrapolation (jacobi_diis.f90:222-226) or, after a singular Gram
+// system, the Jacobi iterate; increment H-norm (hnorm) and update.
+__global__ void __launch_bounds__(kSolT) k_batch_extrap(const YlmTables tb, BatchState bs,
+                                                        double* x) {
+  const int c = blockIdx.x, k = bs.cmol[c];
+  if (bs.status[k] != 0) return;
+  __shared__ int pm[kMaxHist];
+  __shared__ double cf[kMaxHist];
+  __shared__ double tot[1];
+  const int ext = bs.ext[k], nm = ext > 0 ? ext : -ext;
+  const bool ok = ext > 0;
+  if (threadIdx.x < nm) {
+    pm[threadIdx.x] = bs.slot[(size_t)k * bs.ndiis + threadIdx.x];
+    cf[threadIdx.x] = ok ? bs.coef[(size_t)k * kMaxHist + threadIdx.x] : 0.0;
+  }
+  __syncthreads();
+  const int nylm = tb.nylm;
+  const long long N = bs.n_total;
+  const long long b0 = (long long)bs.off[k] * nylm + (long long)(c - bs.cfirst[k]) * kBChunk;
+  const int cnt = (int)min((long long)kBChunk, (long long)bs.off[k + 1] * nylm - b0);
+  const double* xjac = bs.hx + (size_t)pm[nm - 1] * N + b0;
+  const int dt = kSolT % nylm;
+  double acc = 0.0;
 #pragma unroll
-    for (int o = 16; o >= 1; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if (lane == 0) sh2[w] = acc;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double t = 0.0;
-      for (int ww = 0; ww < (int)(blockDim.x >> 5); ++ww) t += sh2[ww];
-      const int nsph = bs.off[k + 1] - bs.off[k];
-      const double nrm = sqrt(t / (double)max(nsph, 1));
-      bs.norm[k] = nrm;
-      const int it = bs.iters[k] + 1;
-      bs.iters[k] = it;
-      bs.status[k] = (nrm < bs.tol) ? 1 : (it >= bs.max_iter ? 2 : (isfinite(nrm) ? 0 : 3));
+  for (int u0 = 0; u0 < kBChunk / kSolT; u0 += kSolU) {
+    double xo[kSolU];
+    bool in[kSolU];
+#pragma unroll
+    for (int u = 0; u < kSolU; ++u) {
+      in[u] = threadIdx.x + (u0 + u) * kSolT < cnt;
+      xo[u] = 0.0;
     }
+    if (ok) {
+#pragma unroll 4
+      for (int h = 0; h < nm; ++h) {
+        const double* hk = bs.hx + (size_t)pm[h] * N + b0;
+        double hv[kSolU];
+#pragma unroll
+        for (int u = 0; u < kSolU; ++u)
+          hv[u] = in[u] ? hk[threadIdx.x + (u0 + u) * kSolT] : 0.0;
+#pragma unroll
+        for (int u = 0; u < kSolU; ++u) xo[u] = fma(cf[h], hv[u], xo[u]);
+      }
+    } else {
+#pragma unroll
+      for (int u = 0; u < kSolU; ++u) xo[u] = in[u] ? xjac[threadIdx.x + (u0 + u) * kSolT] : 0.0;
+    }
+    int lm = (int)((b0 + threadIdx.x + u0 * kSolT) % nylm);
+#pragma unroll
+    for (int u = 0; u < kSolU; ++u) {
+      if (in[u]) {
+        const long long q = b0 + threadIdx.x + (u0 + u) * kSolT;
+        const double dd = xo[u] - x[q];
+        acc = fma(dd * dd, 1.0 / (1.0 + l_of(lm)), acc);
+        x[q] = xo[u];
+      }
+      lm = lm_add(lm, dt, nylm);
+    }
+  }
+  double v[1] = {acc};
+  block_sum_store<1, kMaxHist + 1>(v, 1, bs.part);  // chunk c is block c
+  if (!batch_last_chunk(bs, k)) return;
+  batch_sum_parts(bs, k, 1, tot);
+  if (threadIdx.x == 0) {
+    const int nsph = bs.off[k + 1] - bs.off[k];
+    const double nrm = sqrt(tot[0] / (double)max(nsph, 1));
+    bs.norm[k] = nrm;
+    const int it = bs.iters[k] + 1;
+    bs.iters[k] = it;
+    bs.status[k] = (nrm < bs.tol) ? 1 : (it >= bs.max_iter ? 2 : (isfinite(nrm) ? 0 : 3));
   }
 }
 cudaError_t launch_batch_diis(Launch L, const YlmTables& tb, const BatchState& bs,
                               const double* rhs, const double* y, double* x) {
-  if (bs.nmol == 0) return cudaSuccess;
-  k_batch_diis<<<bs.nmol, 256, 0, L.st>>>(tb, bs, rhs, y, x);
-  ++*L.launches;
+  if (bs.nchunk == 0) return cudaSuccess;
+  k_batch_gram<<<bs.nchunk, kSolT, 0, L.st>>>(tb, bs, rhs, y, x);
+  k_batch_extrap<<<bs.nchunk, kSolT, 0, L.st>>>(tb, bs, x);
+  *L.launches += 2;
   return cudaGetLastError();
 }
 

