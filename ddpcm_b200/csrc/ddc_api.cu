@@ -132,6 +132,8 @@ struct ddc_ctx {
   bool capturing = false;   // stream capture in progress: no stage events
   std::vector<int> h_off;
   DBuf b_cmol, b_cfirst, b_part, b_cnt, b_coef, b_ext;  // chunked batched Jacobi/DIIS
+  DBuf b_sphmol;        // molecule of each sphere (batched solves)
+  SweepMask sweep{};    // set while the batched sweeps are captured
   DBuf d_off, mrange, tr_cav, tr_nuc, b_nmat, b_slot, b_B, b_status, b_iters, b_restarts, b_norm,
       b_out;
   const int2* mrange_ptr() const { return nmol > 1 ? mrange.as<int2>() : nullptr; }
@@ -221,6 +223,7 @@ struct ddc_ctx {
     g.cavidx = cavidx.as<int>();
     g.cavpt = cavpt.as<int>();
     g.ccav = ccav.as<double>();
+    g.act = sweep;
     return g;
   }
 };
@@ -1528,6 +1531,14 @@ int batch_setup(ddc_ctx* ctx, BatchSys& b, bool adjoint, const double* rhs, doub
   CK(cudaMemcpyAsync(ctx->b_cfirst.p, cfirst.data(), sizeof(int) * (nmol + 1),
                      cudaMemcpyHostToDevice, ctx->st));
   CK(cudaMemsetAsync(bs.cnt, 0, sizeof(unsigned) * nmol, ctx->st));
+  {
+    std::vector<int> sphmol(ctx->nsph);
+    for (int k = 0; k < nmol; k++)
+      for (int i = ctx->h_off[k]; i < ctx->h_off[k + 1]; i++) sphmol[i] = k;
+    CK(ctx->b_sphmol.ensure(sizeof(int) * std::max(ctx->nsph, 1)));
+    CK(cudaMemcpyAsync(ctx->b_sphmol.p, sphmol.data(), sizeof(int) * ctx->nsph,
+                       cudaMemcpyHostToDevice, ctx->st));
+  }
   bs.nmol = nmol;
   bs.ndiis = nd;
   bs.max_iter = ctx->prm.max_iter;
@@ -1614,6 +1625,9 @@ int batch_run(ddc_ctx* ctx, BatchSys* sys, int ns) {
   cudaGraphExec_t exec = nullptr;
   CK(cudaStreamSynchronize(ctx->st));
   ctx->capturing = true;
+  // the sweeps skip the spheres of molecules whose systems have all stopped
+  ctx->sweep = SweepMask{ctx->b_sphmol.as<int>(), sys[0].bs.status,
+                         ns == 2 ? sys[1].bs.status : nullptr};
   cudaError_t ce = cudaStreamBeginCapture(ctx->st, cudaStreamCaptureModeThreadLocal);
   int orc = DDC_OK;
   if (ce == cudaSuccess) {
@@ -1633,6 +1647,7 @@ int batch_run(ddc_ctx* ctx, BatchSys* sys, int ns) {
     if (ce == cudaSuccess) ce = ee;
   }
   ctx->capturing = false;
+  ctx->sweep = SweepMask{};
   if (orc != DDC_OK) {
     if (graph) cudaGraphDestroy(graph);
     cudaGetLastError();

@@ -95,6 +95,15 @@ struct YlmTables {
 };
 
 // Device geometry handed to every kernel.
+// Spheres a batched sweep may skip: those of molecules whose systems have
+// all stopped (their operator outputs are not read again).  mol == null:
+// every sphere is computed.
+struct SweepMask {
+  const int* mol;  // [nsph] molecule of each sphere
+  const int* st0;  // [nmol] Jacobi/DIIS status of the first system (0: running)
+  const int* st1;  // [nmol] status of the second system, or null
+};
+
 struct DevGeo {
   int nsph, ngrid, nylm, ncav, npair;
   int maxnb;  // largest neighbour count of a sphere
@@ -127,6 +136,7 @@ struct DevGeo {
   const int* cavidx;
   const int* cavpt;
   const double* ccav;
+  SweepMask act;
 };
 
 // Stages timed with CUDA events when ddc_params.timing = 1.

@@ -14,6 +14,13 @@
 
 namespace ddc {
 
+// True for a sphere of a batched molecule whose systems have all stopped.
+__device__ __forceinline__ bool sweep_skip(const SweepMask& m, int sph) {
+  if (!m.mol) return false;
+  const int k = m.mol[sph];
+  return m.st0[k] != 0 && (!m.st1 || m.st1[k] != 0);
+}
+
 #define DADD __dadd_rn
 #define DSUB __dsub_rn
 #define DMUL __dmul_rn
@@ -828,6 +835,7 @@ __global__ void __launch_bounds__(32 * ls_nroles(LMAX)) k_lstarx(const YlmTables
   constexpr int NVM = ls_max_nvals(LMAX);
   extern __shared__ double sh[];  // [NF][CH]
   const int i = blockIdx.x;
+  if (sweep_skip(g.act, i)) return;
   const int role = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const double4 ci = g.sph[i];
   const int G = g.ngrid;
@@ -2617,6 +2625,7 @@ __global__ void __launch_bounds__(32 * ls_nroles(LMAX)) k_lstarx_f(const YlmTabl
   constexpr int NVM = ls_max_nvals(LMAX);
   extern __shared__ float shf[];  // [NF][CH]
   const int i = blockIdx.x;
+  if (sweep_skip(g.act, i)) return;
   const int role = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const double4 ci = g.sph[i];
   const int G = g.ngrid;
@@ -3156,6 +3165,7 @@ __global__ void __launch_bounds__(32 * lxs_nroles<Rl>(LMAX), lxs_min_blocks<Rl>(
   Rl* fld = reinterpret_cast<Rl*>(smraw);  // [NBUF][NF][CH]
   Rl* lxp = fld + NBUF * NF * CH;          // [NBUF][NR][CH]
   const int b = blockIdx.x, tid = threadIdx.x;
+  if (sweep_skip(g.act, b)) return;
   const int role = tid >> 5, lane = tid & 31;
   const int q0 = g.ls_ptr[b], q1 = g.ls_ptr[b + 1];
   const int nch = (q1 - q0 + CH - 1) / CH;
@@ -3331,7 +3341,8 @@ __global__ void __launch_bounds__(32 * kGatherWarps)
   const int mb = (g.maxnb + 3) & ~3;
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int a = blockIdx.x * kGatherWarps + w;
-  if (a >= g.nsph) return;  // warp-uniform; the kernel has no block barriers
+  // warp-uniform; the kernel has no block barriers
+  if (a >= g.nsph || sweep_skip(g.act, a)) return;
   // per warp: pst[mb + 4] (pn_ptr of the pairs), dl[mb] (lsstart - pn_ptr),
   // then the row (16-byte aligned: mb is a multiple of four)
   int* pst = reinterpret_cast<int*>(smraw) + (size_t)w * (2 * mb + 4);
