@@ -2767,7 +2767,7 @@ __host__ __device__ constexpr int lxs_nroles(int L) {
 // blocks per SM the pass is compiled for
 template <class Rl>
 __host__ __device__ constexpr int lxs_min_blocks(int L) {
-  return L > 10 ? 1 : sizeof(Rl) == 8 ? 2 : L == 10 ? 4 : 3;
+  return L > 10 ? 1 : sizeof(Rl) == 8 ? (L <= 8 ? 4 : 2) : L == 10 ? 4 : 3;
 }
 __host__ __device__ constexpr int lxs_cost(int L, int m) {
   return m == 0 ? 5 * (L + 1) + 4 : 7 * (L + 1 - m) + 4;
@@ -3145,7 +3145,9 @@ cudaError_t launch_lxs_geo_f64(Launch L, const YlmTables& tb, const DevGeo& g, d
 // buffer so that two blocks fit in shared memory
 template <class Rl> __host__ __device__ constexpr bool lxs_piped() { return sizeof(Rl) == 4; }
 // Blocks per SM: lxs_min_blocks (FP32 at lmax 10: four of 128 threads, at
-// most 128 registers; other FP32 cases three; FP64 two, at most 168)
+// most 128 registers; other FP32 cases three; FP64 up to lmax 8 four, at
+// most 128 registers: 253 against 282 ms for the 256-globule batch solve at
+// lmax 6 with two; FP64 at lmax 9-10 two, at most 168)
 // MODE 0: L x (val) and L* xi (y) together; 1: L x only (xi, y unused);
 // 2: L x only with the weight chi(t) in place of chi(t)/f_a(n) (the u_chi sum
 // of the forces, on-the-fly geometry only)
