@@ -743,7 +743,7 @@ int do_init(ddc_ctx* ctx, int n, const std::vector<double4>* hsph, const double4
 // (matvec.f90:131-135, bw = w_n Y_lm(s_n))
 int gemm_proj(ddc_ctx* ctx, double alpha, const double* pot, double* y) {
   CK(launch_dgemm_nn(ctx->L(), ctx->nylm, ctx->nsph, ctx->ngrid, alpha, ctx->bw.as<double>(),
-                     ctx->nylm, pot, ctx->ngrid, y, ctx->nylm));
+                     ctx->nylm, pot, ctx->ngrid, y, ctx->nylm, ctx->sweep));
   return DDC_OK;
 }
 // projection of the FP32 field (rows ldp_f apart) into the FP64 vector y
@@ -758,7 +758,7 @@ int gemm_proj_f32(ddc_ctx* ctx, float alpha, const float* pot, double* y) {
 // xi(n,i) = sum_lm basis(lm,n) s(lm,i)   (matvec.f90:189-204)
 int gemm_xi(ddc_ctx* ctx, const double* s, double* xig) {
   CK(launch_dgemm_nn(ctx->L(), ctx->ngrid, ctx->nsph, ctx->nylm, 1.0, ctx->basisT.as<double>(),
-                     ctx->ngrid, s, ctx->nylm, xig, ctx->ngrid));
+                     ctx->ngrid, s, ctx->nylm, xig, ctx->ngrid, ctx->sweep));
   return DDC_OK;
 }
 // FP32 xi of the FP64 vector s

@@ -263,9 +263,12 @@ cudaError_t launch_residual(Launch L, const YlmTables& tb, long long n, const do
 cudaError_t launch_axpy(Launch L, long long n, double a, const double* x, double* y);
 // dst[c*rows + r] = src[r*cols + c] (FP64)
 cudaError_t launch_transpose(Launch L, int rows, int cols, const double* src, double* dst);
-// C[n*ldc + m] = alpha * sum_k A[k*lda + m] B[n*ldb + k] (FP64, pipelined)
+// C[n*ldc + m] = alpha * sum_k A[k*lda + m] B[n*ldb + k] (FP64, pipelined);
+// with act.mol set the N columns are spheres and tiles of skipped spheres
+// are left alone
 cudaError_t launch_dgemm_nn(Launch L, int M, int N, int K, double alpha, const double* A,
-                            int lda, const double* B, int ldb, double* C, int ldc);
+                            int lda, const double* B, int ldb, double* C, int ldc,
+                            const SweepMask& act = SweepMask{});
 // FP32 SIMT projection / expansion (mixed path, more than 128 harmonics)
 cudaError_t launch_proj_f32_simt(Launch L, int nylm, int nsph, int ngrid, float alpha,
                                  const float* bw_f, const float* pot, int ldp, double* y);

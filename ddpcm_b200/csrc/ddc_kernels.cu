@@ -1063,7 +1063,8 @@ __device__ __forceinline__ void cp_async_wait() {
 __global__ void __launch_bounds__(256, 3) k_dgemm_dmma(int M, int N, int K, double alpha,
                                                        const double* __restrict__ A, int lda,
                                                        const double* __restrict__ B, int ldb,
-                                                       double* __restrict__ C, int ldc) {
+                                                       double* __restrict__ C, int ldc,
+                                                       const SweepMask act) {
   using namespace dgp;
   extern __shared__ __align__(16) double dg_smem[];
   double* As = dg_smem;                // [2][BK][AS]
@@ -1071,6 +1072,10 @@ __global__ void __launch_bounds__(256, 3) k_dgemm_dmma(int M, int N, int K, doub
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int wm = warp & 3, wn = warp >> 2;
   const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+  // columns are spheres: a batched sweep skips a tile whose spheres all belong
+  // to stopped molecules
+  if (act.mol && __syncthreads_and(tid >= BN || n0 + tid >= N || sweep_skip(act, n0 + tid)))
+    return;
   auto load = [&](int buf, int k0) {
 #pragma unroll
     for (int u = 0; u < BM * BK / 256; ++u) {
@@ -1153,13 +1158,14 @@ cudaError_t launch_transpose(Launch L, int rows, int cols, const double* src, do
   return cudaGetLastError();
 }
 cudaError_t launch_dgemm_nn(Launch L, int M, int N, int K, double alpha, const double* A,
-                            int lda, const double* B, int ldb, double* C, int ldc) {
+                            int lda, const double* B, int ldb, double* C, int ldc,
+                            const SweepMask& act) {
   if (M == 0 || N == 0) return cudaSuccess;
   dim3 grid((M + dgp::BM - 1) / dgp::BM, (N + dgp::BN - 1) / dgp::BN);
   cudaError_t e = cudaFuncSetAttribute(k_dgemm_dmma, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        dgp::SMEM);
   if (e) return e;
-  k_dgemm_dmma<<<grid, 256, dgp::SMEM, L.st>>>(M, N, K, alpha, A, lda, B, ldb, C, ldc);
+  k_dgemm_dmma<<<grid, 256, dgp::SMEM, L.st>>>(M, N, K, alpha, A, lda, B, ldb, C, ldc, act);
   ++*L.launches;
   return cudaGetLastError();
 }
