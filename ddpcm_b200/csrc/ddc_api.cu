@@ -133,6 +133,8 @@ struct ddc_ctx {
   std::vector<int> h_off;
   DBuf b_cmol, b_cfirst, b_part, b_cnt, b_coef, b_ext;  // chunked batched Jacobi/DIIS
   DBuf b_sphmol;        // molecule of each sphere (batched solves)
+  DBuf b_tolk, b_maxk;  // per-molecule tolerance and budget of the inner solves
+  DBuf b_run, b_upd, b_onorm;  // mixed refinement of a batch: outer status, update mask, norms
   SweepMask sweep{};    // set while the batched sweeps are captured
   DBuf d_off, mrange, tr_cav, tr_nuc, b_nmat, b_slot, b_B, b_status, b_iters, b_restarts, b_norm,
       b_out;
@@ -1483,9 +1485,16 @@ struct BatchSys {
   ddc_solve_info* inf = nullptr;
 };
 
+// f32: an inner solve of the mixed refinement (FP32 history of at most
+// kInnerDiis vectors); status0 (host, or null: every non-empty molecule
+// runs), tolk and maxk (host, or null: the parameters' tolerance and budget)
+// give the molecules' starting status, tolerance and iteration budget.
 int batch_setup(ddc_ctx* ctx, BatchSys& b, bool adjoint, const double* rhs, double* x,
-                int* iters, ddc_solve_info* inf, int set) {
-  const int nmol = ctx->nmol, nd = std::max(ctx->prm.ndiis, 11);
+                int* iters, ddc_solve_info* inf, int set, bool f32 = false,
+                const int* status0 = nullptr, const double* tolk = nullptr,
+                const int* maxk = nullptr) {
+  const int nmol = ctx->nmol;
+  const int nd = std::max(f32 ? std::min(ctx->prm.ndiis, kInnerDiis) : ctx->prm.ndiis, 11);
   if (ctx->prm.ndiis == 0) return fail(ctx, DDC_ERR_UNSUPPORTED, "batched solves need DIIS");
   std::vector<int> nmat(nmol, 1), slot((size_t)nmol * nd);
   for (int k = 0; k < nmol; k++)
@@ -1493,6 +1502,7 @@ int batch_setup(ddc_ctx* ctx, BatchSys& b, bool adjoint, const double* rhs, doub
   std::vector<int> status(nmol, 0);
   for (int k = 0; k < nmol; k++)
     if (ctx->h_off[k + 1] == ctx->h_off[k]) status[k] = 1;  // empty molecule
+    else if (status0) status[k] = status0[k];
   const size_t lenb = nd + 1, lb2 = lenb * lenb;
   // room for both sets
   CK(ctx->b_nmat.ensure(sizeof(int) * 2 * nmol));
@@ -1555,6 +1565,21 @@ int batch_setup(ddc_ctx* ctx, BatchSys& b, bool adjoint, const double* rhs, doub
   const SolveBufs sb = solve_bufs(ctx, set);
   bs.hx = sb.hx;
   bs.he = sb.he;
+  bs.f32 = f32 ? 1 : 0;
+  bs.tolk = nullptr;
+  bs.maxk = nullptr;
+  if (tolk) {
+    CK(ctx->b_tolk.ensure(sizeof(double) * 2 * nmol));
+    double* dt = ctx->b_tolk.as<double>() + (size_t)set * nmol;
+    CK(cudaMemcpyAsync(dt, tolk, sizeof(double) * nmol, cudaMemcpyHostToDevice, ctx->st));
+    bs.tolk = dt;
+  }
+  if (maxk) {
+    CK(ctx->b_maxk.ensure(sizeof(int) * 2 * nmol));
+    int* dm = ctx->b_maxk.as<int>() + (size_t)set * nmol;
+    CK(cudaMemcpyAsync(dm, maxk, sizeof(int) * nmol, cudaMemcpyHostToDevice, ctx->st));
+    bs.maxk = dm;
+  }
   CK(cudaMemcpyAsync(bs.nmat, nmat.data(), sizeof(int) * nmol, cudaMemcpyHostToDevice, ctx->st));
   CK(cudaMemcpyAsync(bs.slot, slot.data(), sizeof(int) * nmol * nd, cudaMemcpyHostToDevice,
                      ctx->st));
@@ -1617,9 +1642,9 @@ int batch_finish(ddc_ctx* ctx, const BatchSys& b, double t0) {
 // is captured once and replayed until every molecule of every system has
 // stopped; a stopped molecule's DIIS block returns at once, so extra sweeps
 // are harmless.
-int batch_run(ddc_ctx* ctx, BatchSys* sys, int ns) {
-  const double t0 = now_s();
+int batch_sweeps(ddc_ctx* ctx, BatchSys* sys, int ns) {
   const int nmol = ctx->nmol;
+  const bool f32 = sys[0].bs.f32 != 0;
   const int check = 4;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -1634,9 +1659,10 @@ int batch_run(ddc_ctx* ctx, BatchSys* sys, int ns) {
     for (int r = 0; r < check && orc == DDC_OK; r++) {
       if (ns == 2) {
         const int dq = sys[0].adjoint ? 1 : 0, aq = 1 - dq;
-        orc = op_pair(ctx, sys[dq].x, sys[dq].y, sys[aq].x, sys[aq].y);
+        orc = f32 ? op_pair_f32(ctx, sys[dq].x, sys[dq].y, sys[aq].x, sys[aq].y)
+                  : op_pair(ctx, sys[dq].x, sys[dq].y, sys[aq].x, sys[aq].y);
       } else {
-        orc = sys[0].adjoint ? op_lstarx(ctx, sys[0].x, sys[0].y) : op_lx(ctx, sys[0].x, sys[0].y);
+        orc = op_single(ctx, f32 ? OP_F32 : OP_F64, sys[0].adjoint, sys[0].x, sys[0].y);
       }
       for (int q = 0; q < ns && orc == DDC_OK; q++)
         if (launch_batch_diis(ctx->L(), ctx->tb, sys[q].bs, sys[q].rhs, sys[q].y, sys[q].x) !=
@@ -1676,10 +1702,155 @@ int batch_run(ddc_ctx* ctx, BatchSys* sys, int ns) {
   cudaGraphExecDestroy(exec);
   cudaGraphDestroy(graph);
   CK(ge);
+  return DDC_OK;
+}
+
+int batch_run(ddc_ctx* ctx, BatchSys* sys, int ns) {
+  const double t0 = now_s();
+  CKI(batch_sweeps(ctx, sys, ns));
   int rc = DDC_OK;
   for (int q = 0; q < ns; q++) {
     const int r = batch_finish(ctx, sys[q], t0);
     if (r != DDC_OK && rc == DDC_OK) rc = r;
+  }
+  return rc;
+}
+
+// Mixed-precision batched solve: the single-molecule refinement (FP64
+// residual and convergence test, inner FP32 Jacobi/DIIS solve of the
+// correction to rho = 1e-4 of its increment, x += e) with every molecule on
+// its own schedule, the molecules in lockstep per phase: one FP64 operator
+// pass for all molecules still refining (converged ones are skipped), the
+// batched residual with per-molecule norms, then one batched inner solve
+// whose molecules each carry their own tolerance and remaining budget.
+// sys[q].rhs / .x are the systems' right-hand sides and iterates.
+int batch_run_mixed(ddc_ctx* ctx, BatchSys* sys, int ns) {
+  const double t0 = now_s();
+  const int nmol = ctx->nmol;
+  const double tol = std::pow(10.0, -(double)ctx->prm.iconv);
+  const bool f32_first = !ctx->guess_preset && (ctx->prm.guess == DDC_GUESS_REFERENCE ||
+                                                 ctx->prm.guess == DDC_GUESS_ZERO);
+  CK(ctx->b_run.ensure(sizeof(int) * 2 * nmol));
+  CK(ctx->b_upd.ensure(sizeof(int) * 2 * nmol));
+  CK(ctx->b_onorm.ensure(sizeof(double) * 2 * nmol));
+  // per system and molecule: outer status (0 refining, 1 converged, 2 budget
+  // spent, 3 non-finite), iterations, refinements, restarts, last norm
+  std::vector<int> run(2 * nmol, 0), its(2 * nmol, 0), outer(2 * nmol, 0), rst(2 * nmol, 0);
+  std::vector<double> last(2 * nmol, 0.0);
+  for (int q = 0; q < ns; q++)
+    for (int k = 0; k < nmol; k++)
+      if (ctx->h_off[k + 1] == ctx->h_off[k]) run[q * nmol + k] = 1;
+  int* drun = ctx->b_run.as<int>();
+  int* dupd = ctx->b_upd.as<int>();
+  double* dnorm = ctx->b_onorm.as<double>();
+  BatchSys in[2];  // the inner systems: L e = r from e = d
+  for (int round = 0; round < 64; round++) {
+    int nrun = 0;
+    for (int q = 0; q < ns; q++)
+      for (int k = 0; k < nmol; k++) nrun += run[q * nmol + k] == 0;
+    if (!nrun) break;
+    CK(cudaMemcpyAsync(drun, run.data(), sizeof(int) * 2 * nmol, cudaMemcpyHostToDevice, ctx->st));
+    // y = L x for the molecules still refining (FP32 at a reference or zero
+    // start, whose first residual is never tested)
+    const bool f32_res = f32_first && round == 0;
+    ctx->sweep = SweepMask{ctx->b_sphmol.as<int>(), drun, ns == 2 ? drun + nmol : nullptr};
+    int orc;
+    if (ns == 2) {
+      const int dq = sys[0].adjoint ? 1 : 0, aq = 1 - dq;
+      const SolveBufs bd = solve_bufs(ctx, dq), ba = solve_bufs(ctx, aq);
+      orc = f32_res ? op_pair_f32(ctx, sys[dq].x, bd.y, sys[aq].x, ba.y)
+                    : op_pair(ctx, sys[dq].x, bd.y, sys[aq].x, ba.y);
+    } else {
+      orc = op_single(ctx, f32_res ? OP_F32 : OP_F64, sys[0].adjoint, sys[0].x,
+                      solve_bufs(ctx, 0).y);
+    }
+    ctx->sweep = SweepMask{};
+    CKI(orc);
+    for (int q = 0; q < ns; q++) {
+      const SolveBufs b = solve_bufs(ctx, q);
+      StageScope sc(ctx, ST_JACOBI);
+      CK(launch_batch_residual(ctx->L(), ctx->tb, sys[q].bs, drun + q * nmol, sys[q].rhs, b.y,
+                               sys[q].x, b.r, b.d, b.e, dnorm + q * nmol));
+    }
+    std::vector<double> nrm(2 * nmol, 0.0);
+    CK(cudaMemcpyAsync(nrm.data(), dnorm, sizeof(double) * 2 * nmol, cudaMemcpyDeviceToHost,
+                       ctx->st));
+    CKI(sync(ctx));
+    // per molecule: converged, out of budget, or an inner solve
+    std::vector<int> ist(2 * nmol, 1), maxk(2 * nmol, 1), upd(2 * nmol, 0);
+    std::vector<double> tolk(2 * nmol, tol);
+    int ninner = 0;
+    for (int q = 0; q < ns; q++)
+      for (int k = 0; k < nmol; k++) {
+        const int j = q * nmol + k;
+        if (run[j] != 0) continue;
+        ++outer[j];
+        last[j] = nrm[j];
+        if (!std::isfinite(nrm[j])) {
+          run[j] = 3;
+        } else if (nrm[j] < tol && !f32_res) {
+          run[j] = 1;
+        } else if (its[j] >= ctx->prm.max_iter) {
+          run[j] = 2;
+        } else {
+          ist[j] = 0;
+          upd[j] = 1;
+          maxk[j] = ctx->prm.max_iter - its[j];
+          tolk[j] = std::max(1e-4 * nrm[j], 0.3 * tol);
+          ++ninner;
+        }
+      }
+    if (!ninner) break;
+    for (int q = 0; q < ns; q++) {
+      const SolveBufs b = solve_bufs(ctx, q);
+      CKI(batch_setup(ctx, in[q], sys[q].adjoint, b.r, b.e, nullptr, nullptr, q, true,
+                      ist.data() + q * nmol, tolk.data() + q * nmol, maxk.data() + q * nmol));
+    }
+    CKI(batch_sweeps(ctx, in, ns));
+    // account the inner solves and apply their corrections
+    CK(cudaMemcpyAsync(dupd, upd.data(), sizeof(int) * 2 * nmol, cudaMemcpyHostToDevice, ctx->st));
+    std::vector<int> iit(2 * nmol, 0), irs(2 * nmol, 0);
+    for (int q = 0; q < ns; q++) {
+      CK(launch_batch_update(ctx->L(), in[q].bs, ctx->nylm, dupd + q * nmol,
+                             solve_bufs(ctx, q).e, sys[q].x));
+      CK(cudaMemcpyAsync(iit.data() + q * nmol, in[q].bs.iters, sizeof(int) * nmol,
+                         cudaMemcpyDeviceToHost, ctx->st));
+      CK(cudaMemcpyAsync(irs.data() + q * nmol, in[q].bs.restarts, sizeof(int) * nmol,
+                         cudaMemcpyDeviceToHost, ctx->st));
+    }
+    CKI(sync(ctx));
+    for (int j = 0; j < 2 * nmol; j++)
+      if (upd[j]) {
+        its[j] += iit[j];
+        rst[j] += irs[j];
+      }
+  }
+  int rc = DDC_OK;
+  for (int q = 0; q < ns; q++) {
+    int maxit = 0, maxout = 0, nfail = 0, restarts = 0;
+    double worst = 0.0;
+    for (int k = 0; k < nmol; k++) {
+      const int j = q * nmol + k;
+      if (sys[q].iters) sys[q].iters[k] = its[j];
+      maxit = std::max(maxit, its[j]);
+      maxout = std::max(maxout, outer[j]);
+      restarts += rst[j];
+      if (run[j] != 1 && ctx->h_off[k + 1] > ctx->h_off[k]) nfail++;
+      if (ctx->h_off[k + 1] > ctx->h_off[k]) worst = std::max(worst, last[j]);
+    }
+    if (sys[q].inf) {
+      memset(sys[q].inf, 0, sizeof(*sys[q].inf));
+      sys[q].inf->iterations = maxit;
+      sys[q].inf->refinements = maxout;
+      sys[q].inf->converged = nfail == 0;
+      sys[q].inf->diis_restarts = restarts;
+      sys[q].inf->final_norm = worst;
+      sys[q].inf->seconds = now_s() - t0;
+    }
+    if (nfail && rc == DDC_OK)
+      rc = fail(ctx, DDC_ERR_NOCONV,
+                std::to_string(nfail) + " molecule(s) did not converge" +
+                    (sys[q].adjoint ? " (adjoint)" : ""));
   }
   return rc;
 }
@@ -2321,8 +2492,6 @@ int ddc_batch_energy_forces(ddc_ctx* ctx, int nmol, const int* off, const double
                             const double* rvdw, double* esolv, double* fx, int* iters,
                             ddc_run_info* info) {
   if (!ctx || nmol <= 0 || !off || !esolv) return DDC_ERR_PARAM;
-  if (ctx->prm.precision != DDC_PREC_FP64)
-    return fail(ctx, DDC_ERR_UNSUPPORTED, "batched solves run in FP64");
   cudaSetDevice(ctx->prm.device);
   if (off[0] != 0) return fail(ctx, DDC_ERR_PARAM, "off[0] must be 0");
   for (int k = 0; k < nmol; k++)
@@ -2405,7 +2574,10 @@ int ddc_batch_energy_forces(ddc_ctx* ctx, int nmol, const int* off, const double
         CK(launch_guess(ctx->L(), ctx->tb, n, dpsi, ds, ctx->prm.guess == DDC_GUESS_ZERO ? 1 : 0));
       CKI(batch_setup(ctx, sys[1], true, dpsi, ds, ita.data(), &inf->adjoint, 1));
     }
-    CKI(batch_run(ctx, sys, paired ? 2 : 1));
+    if (ctx->prm.precision == DDC_PREC_MIXED)
+      CKI(batch_run_mixed(ctx, sys, paired ? 2 : 1));
+    else
+      CKI(batch_run(ctx, sys, paired ? 2 : 1));
     if (iters)
       for (int k = 0; k < nmol; k++) {
         iters[2 * k] = it[k];
@@ -2427,7 +2599,10 @@ int ddc_batch_energy_forces(ddc_ctx* ctx, int nmol, const int* off, const double
       std::vector<int> it(nmol);
       BatchSys sys;
       CKI(batch_setup(ctx, sys, true, dpsi, ds, it.data(), &inf->adjoint, 0));
-      CKI(batch_run(ctx, &sys, 1));
+      if (ctx->prm.precision == DDC_PREC_MIXED)
+        CKI(batch_run_mixed(ctx, &sys, 1));
+      else
+        CKI(batch_run(ctx, &sys, 1));
       if (iters)
         for (int k = 0; k < nmol; k++) iters[2 * k + 1] = it[k];
     }

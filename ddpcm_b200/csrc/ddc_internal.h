@@ -170,8 +170,11 @@ struct BatchState {
   int* iters;         // [nmol]
   int* restarts;      // [nmol]
   double* norm;       // [nmol] last increment norm
-  double* hx;         // [ndiis][n_total]
-  double* he;         // [ndiis][n_total]
+  void* hx;           // [ndiis][n_total], FP64 or (f32) FP32
+  void* he;           // [ndiis][n_total]
+  int f32;            // history vectors in FP32 (inner solves of the mixed refinement)
+  const double* tolk; // [nmol] per-molecule tolerance, or null: tol
+  const int* maxk;    // [nmol] per-molecule iteration budget, or null: max_iter
   // element chunks of the per-molecule kernels: chunk c holds up to
   // kBatchChunk consecutive elements of molecule cmol[c]
   int nchunk;
@@ -437,6 +440,15 @@ cudaError_t launch_charge_efld_contract(Launch L, int n, const double* q, const 
 // batched solves
 cudaError_t launch_batch_diis(Launch L, const YlmTables& tb, const BatchState& bs,
                               const double* rhs, const double* y, double* x);
+// Mixed refinement of a batch, per molecule with run[k] == 0: r = rhs - y -
+// x/facl, d = facl r (the FP64 Jacobi increment at x), e = d, and the
+// increment's H-norm into norm[k] (chunk map and partials of bs).
+cudaError_t launch_batch_residual(Launch L, const YlmTables& tb, const BatchState& bs,
+                                  const int* run, const double* rhs, const double* y,
+                                  const double* x, double* r, double* d, double* e, double* norm);
+// x += e over the molecules with upd[k] != 0
+cudaError_t launch_batch_update(Launch L, const BatchState& bs, int nylm, const int* upd,
+                                const double* e, double* x);
 cudaError_t launch_batch_dot(Launch L, int nmol, const int* off, int nylm, const double* a,
                              const double* b, double scale, double* out);
 cudaError_t launch_batch_ranges(Launch L, int nsph, int ngrid, int ncav, const int2* mrange,

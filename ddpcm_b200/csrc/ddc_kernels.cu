@@ -3663,6 +3663,7 @@ __device__ __forceinline__ void batch_sum_parts(const BatchState& bs, int k, int
   __syncthreads();
 }
 
+template <class H>
 __global__ void __launch_bounds__(kSolT) k_batch_gram(const YlmTables tb, BatchState bs,
                                                       const double* __restrict__ rhs,
                                                       const double* __restrict__ y,
@@ -3683,8 +3684,8 @@ __global__ void __launch_bounds__(kSolT) k_batch_gram(const YlmTables tb, BatchS
   const long long N = bs.n_total;
   const long long b0 = (long long)bs.off[k] * nylm + (long long)(c - bs.cfirst[k]) * kBChunk;
   const int cnt = (int)min((long long)kBChunk, (long long)bs.off[k + 1] * nylm - b0);
-  double* xnew = bs.hx + (size_t)pm[nm - 1] * N;
-  double* enew = bs.he + (size_t)pm[nm - 1] * N;
+  H* xnew = static_cast<H*>(bs.hx) + (size_t)pm[nm - 1] * N;
+  H* enew = static_cast<H*>(bs.he) + (size_t)pm[nm - 1] * N;
   double ee = 0.0;
   {
     const int dt = kSolT % nylm;
@@ -3703,9 +3704,10 @@ __global__ void __launch_bounds__(kSolT) k_batch_gram(const YlmTables tb, BatchS
       double ev = 0.0;
       if (j < cnt) {
         const double xn = tb.facl[l_of(lm)] * (rv[u] - yv[u]);
-        ev = xn - xv[u];
-        xnew[b0 + j] = xn;
-        enew[b0 + j] = ev;
+        const H eh = (H)(xn - xv[u]);
+        ev = (double)eh;
+        xnew[b0 + j] = (H)xn;
+        enew[b0 + j] = eh;
       }
       es[j] = ev;
       ee = fma(ev, ev, ee);
@@ -3719,16 +3721,16 @@ __global__ void __launch_bounds__(kSolT) k_batch_gram(const YlmTables tb, BatchS
     d[s] = 0.0;
     const int kk = w + NW * s;
     if (kk < nh) {
-      const double* hk = bs.he + (size_t)pm[kk] * N + b0;
+      const H* hk = static_cast<const H*>(bs.he) + (size_t)pm[kk] * N + b0;
       for (int j0 = 0; j0 < kBChunk; j0 += 32 * HL) {
-        double hv[HL];
+        H hv[HL];
 #pragma unroll
         for (int u = 0; u < HL; ++u) {
           const int j = j0 + u * 32 + lane;
-          hv[u] = j < cnt ? hk[j] : 0.0;
+          hv[u] = j < cnt ? hk[j] : H(0);
         }
 #pragma unroll
-        for (int u = 0; u < HL; ++u) d[s] = fma(es[j0 + u * 32 + lane], hv[u], d[s]);
+        for (int u = 0; u < HL; ++u) d[s] = fma(es[j0 + u * 32 + lane], (double)hv[u], d[s]);
       }
     }
   }
@@ -3806,6 +3808,7 @@ __global__ void __launch_bounds__(kSolT) k_batch_gram(const YlmTables tb, BatchS
 
 // DIIS extrapolation (jacobi_diis.f90:222-226) or, after a singular Gram
 // system, the Jacobi iterate; increment H-norm (hnorm) and update.
+template <class H>
 __global__ void __launch_bounds__(kSolT) k_batch_extrap(const YlmTables tb, BatchState bs,
                                                         double* x) {
   const int c = blockIdx.x, k = bs.cmol[c];
@@ -3824,7 +3827,7 @@ __global__ void __launch_bounds__(kSolT) k_batch_extrap(const YlmTables tb, Batc
   const long long N = bs.n_total;
   const long long b0 = (long long)bs.off[k] * nylm + (long long)(c - bs.cfirst[k]) * kBChunk;
   const int cnt = (int)min((long long)kBChunk, (long long)bs.off[k + 1] * nylm - b0);
-  const double* xjac = bs.hx + (size_t)pm[nm - 1] * N + b0;
+  const H* xjac = static_cast<const H*>(bs.hx) + (size_t)pm[nm - 1] * N + b0;
   const int dt = kSolT % nylm;
   double acc = 0.0;
 #pragma unroll
@@ -3839,17 +3842,18 @@ __global__ void __launch_bounds__(kSolT) k_batch_extrap(const YlmTables tb, Batc
     if (ok) {
 #pragma unroll 4
       for (int h = 0; h < nm; ++h) {
-        const double* hk = bs.hx + (size_t)pm[h] * N + b0;
-        double hv[kSolU];
+        const H* hk = static_cast<const H*>(bs.hx) + (size_t)pm[h] * N + b0;
+        H hv[kSolU];
 #pragma unroll
         for (int u = 0; u < kSolU; ++u)
-          hv[u] = in[u] ? hk[threadIdx.x + (u0 + u) * kSolT] : 0.0;
+          hv[u] = in[u] ? hk[threadIdx.x + (u0 + u) * kSolT] : H(0);
 #pragma unroll
-        for (int u = 0; u < kSolU; ++u) xo[u] = fma(cf[h], hv[u], xo[u]);
+        for (int u = 0; u < kSolU; ++u) xo[u] = fma(cf[h], (double)hv[u], xo[u]);
       }
     } else {
 #pragma unroll
-      for (int u = 0; u < kSolU; ++u) xo[u] = in[u] ? xjac[threadIdx.x + (u0 + u) * kSolT] : 0.0;
+      for (int u = 0; u < kSolU; ++u)
+        xo[u] = in[u] ? (double)xjac[threadIdx.x + (u0 + u) * kSolT] : 0.0;
     }
     int lm = (int)((b0 + threadIdx.x + u0 * kSolT) % nylm);
 #pragma unroll
@@ -3873,15 +3877,87 @@ __global__ void __launch_bounds__(kSolT) k_batch_extrap(const YlmTables tb, Batc
     bs.norm[k] = nrm;
     const int it = bs.iters[k] + 1;
     bs.iters[k] = it;
-    bs.status[k] = (nrm < bs.tol) ? 1 : (it >= bs.max_iter ? 2 : (isfinite(nrm) ? 0 : 3));
+    const double tol = bs.tolk ? bs.tolk[k] : bs.tol;
+    const int mx = bs.maxk ? bs.maxk[k] : bs.max_iter;
+    bs.status[k] = (nrm < tol) ? 1 : (it >= mx ? 2 : (isfinite(nrm) ? 0 : 3));
   }
 }
 cudaError_t launch_batch_diis(Launch L, const YlmTables& tb, const BatchState& bs,
                               const double* rhs, const double* y, double* x) {
   if (bs.nchunk == 0) return cudaSuccess;
-  k_batch_gram<<<bs.nchunk, kSolT, 0, L.st>>>(tb, bs, rhs, y, x);
-  k_batch_extrap<<<bs.nchunk, kSolT, 0, L.st>>>(tb, bs, x);
+  if (bs.f32) {
+    k_batch_gram<float><<<bs.nchunk, kSolT, 0, L.st>>>(tb, bs, rhs, y, x);
+    k_batch_extrap<float><<<bs.nchunk, kSolT, 0, L.st>>>(tb, bs, x);
+  } else {
+    k_batch_gram<double><<<bs.nchunk, kSolT, 0, L.st>>>(tb, bs, rhs, y, x);
+    k_batch_extrap<double><<<bs.nchunk, kSolT, 0, L.st>>>(tb, bs, x);
+  }
   *L.launches += 2;
+  return cudaGetLastError();
+}
+
+__global__ void __launch_bounds__(kSolT) k_batch_residual(const YlmTables tb, BatchState bs,
+                                                          const int* __restrict__ run,
+                                                          const double* __restrict__ rhs,
+                                                          const double* __restrict__ y,
+                                                          const double* __restrict__ x,
+                                                          double* r, double* d, double* e,
+                                                          double* norm) {
+  const int c = blockIdx.x, k = bs.cmol[c];
+  if (run[k] != 0) return;
+  __shared__ double tot[1];
+  const int nylm = tb.nylm, dt = kSolT % nylm;
+  const long long b0 = (long long)bs.off[k] * nylm + (long long)(c - bs.cfirst[k]) * kBChunk;
+  const int cnt = (int)min((long long)kBChunk, (long long)bs.off[k + 1] * nylm - b0);
+  int lm = (int)((b0 + threadIdx.x) % nylm);
+  double acc = 0.0;
+#pragma unroll 2
+  for (int j = threadIdx.x; j < kBChunk; j += kSolT) {
+    if (j < cnt) {
+      const long long q = b0 + j;
+      const int l = l_of(lm);
+      const double rr = rhs[q] - y[q] - x[q] / tb.facl[l];
+      const double dd = tb.facl[l] * rr;
+      r[q] = rr;
+      d[q] = dd;
+      e[q] = dd;
+      acc = fma(dd * dd, 1.0 / (1.0 + l), acc);
+    }
+    lm = lm_add(lm, dt, nylm);
+  }
+  double v[1] = {acc};
+  block_sum_store<1, kMaxHist + 1>(v, 1, bs.part);
+  if (!batch_last_chunk(bs, k)) return;
+  batch_sum_parts(bs, k, 1, tot);
+  if (threadIdx.x == 0) {
+    const int nsph = bs.off[k + 1] - bs.off[k];
+    norm[k] = sqrt(tot[0] / (double)max(nsph, 1));
+  }
+}
+cudaError_t launch_batch_residual(Launch L, const YlmTables& tb, const BatchState& bs,
+                                  const int* run, const double* rhs, const double* y,
+                                  const double* x, double* r, double* d, double* e,
+                                  double* norm) {
+  if (bs.nchunk == 0) return cudaSuccess;
+  k_batch_residual<<<bs.nchunk, kSolT, 0, L.st>>>(tb, bs, run, rhs, y, x, r, d, e, norm);
+  ++*L.launches;
+  return cudaGetLastError();
+}
+
+__global__ void __launch_bounds__(kSolT) k_batch_update(const BatchState bs, int nylm,
+                                                        const int* __restrict__ upd,
+                                                        const double* __restrict__ e, double* x) {
+  const int c = blockIdx.x, k = bs.cmol[c];
+  if (upd[k] == 0) return;
+  const long long b0 = (long long)bs.off[k] * nylm + (long long)(c - bs.cfirst[k]) * kBChunk;
+  const int cnt = (int)min((long long)kBChunk, (long long)bs.off[k + 1] * nylm - b0);
+  for (int j = threadIdx.x; j < cnt; j += kSolT) x[b0 + j] += e[b0 + j];
+}
+cudaError_t launch_batch_update(Launch L, const BatchState& bs, int nylm, const int* upd,
+                                const double* e, double* x) {
+  if (bs.nchunk == 0) return cudaSuccess;
+  k_batch_update<<<bs.nchunk, kSolT, 0, L.st>>>(bs, nylm, upd, e, x);
+  ++*L.launches;
   return cudaGetLastError();
 }
 

@@ -179,7 +179,10 @@ int ddc_energy_forces(ddc_ctx* ctx, int n, const double* charge, const double* x
  * Each molecule runs the reference's Jacobi/DIIS with its own history and
  * convergence test; all molecules share each kernel launch.  Outputs:
  * esolv[nmol] (host), fx(3, off[nmol]) (may be NULL), iters[2*nmol]
- * (direct, adjoint per molecule; host, may be NULL).  FP64 only. */
+ * (direct, adjoint per molecule; host, may be NULL).  With precision
+ * DDC_PREC_MIXED each molecule runs the mixed refinement of ddc_cosmo (FP64
+ * residual and stop test, FP32 inner solves); iters then counts each
+ * molecule's inner iterations. */
 int ddc_batch_energy_forces(ddc_ctx* ctx, int nmol, const int* off, const double* charge,
                             const double* x, const double* y, const double* z,
                             const double* rvdw, double* esolv, double* fx, int* iters,

@@ -111,3 +111,58 @@ def test_batch_full_size_workload_vs_oracle():
         np.testing.assert_allclose(out["fx"][k], ref_f, rtol=0, atol=FORCE_ATOL)
         for a, b in zip(its, ref_its):
             assert abs(a - b) <= 1 + 0.2 * b, (k, its, ref_its)
+
+
+def test_batch_mixed_matches_oracle_and_single_mixed_solves(oracle):
+    """precision=MIXED in the batched call: each molecule runs the mixed
+    refinement on its own schedule (FP64 residual and stop test, FP32 inner
+    solves with its own tolerance and budget) and meets the FP64 oracle at the
+    task's bars, like its own single-molecule mixed solve."""
+    from ddpcm_b200 import molecules as M
+    from ddpcm_b200.ddcosmo import DDCosmo, PREC_MIXED
+    mols = [M.to_bohr(m) for m in M.batch_molecules(count=12, lo=20, hi=300, seed=77)]
+    p = dict(lmax=6, ngrid=302, iconv=10, eps=78.3553, eta=0.1)
+    with DDCosmo(precision=PREC_MIXED, **p) as dd:
+        out = dd.batch_energy_forces(mols)
+        singles = {k: dd.energy_forces(mols[k]["q"], mols[k]["x"], mols[k]["y"], mols[k]["z"],
+                                       mols[k]["r"]) for k in (0, 5, 11)}
+    info = out["info"]
+    assert info["direct"]["converged"] and info["adjoint"]["converged"]
+    assert info["direct"]["refinements"] >= 2 and info["adjoint"]["refinements"] >= 2
+    for k in (0, 5, 11):
+        m = mols[k]
+        ref = oracle.energy_forces(m, p["lmax"], p["ngrid"], p["iconv"], p["eps"], p["eta"])
+        rtol = ESOLV_RTOL if len(m["x"]) > 60 else 5 * ESOLV_RTOL
+        assert abs(out["esolv"][k] - ref["esolv"]) <= rtol * abs(ref["esolv"]), k
+        np.testing.assert_allclose(out["fx"][k], ref["fx"], rtol=0, atol=FORCE_ATOL)
+        s = singles[k]
+        assert abs(out["esolv"][k] - s["esolv"]) <= rtol * abs(s["esolv"]), k
+        for c, key in ((0, "direct"), (1, "adjoint")):
+            a, b = int(out["iters"][k, c]), s["info"][key]["iterations"]
+            assert abs(a - b) <= 2 + 0.2 * b, (k, key, a, b)
+    assert len(set(out["iters"][:, 0].tolist())) > 1
+
+
+def test_batch_mixed_full_size_workload_vs_oracle():
+    """The benchmarked 256-globule batch in mixed precision against the
+    oracle's stored FP64 results for 16 of its molecules."""
+    import os
+
+    from conftest import GOLDEN
+    from ddpcm_b200 import molecules as M
+    from ddpcm_b200.ddcosmo import DDCosmo, PREC_MIXED
+    c = M.BATCH_CONFIG
+    mols = [M.to_bohr(m) for m in M.batch_molecules(count=c["count"], lo=c["lo"], hi=c["hi"],
+                                                     seed=c["seed"])]
+    gold = np.load(os.path.join(GOLDEN, "config3_oracle.npz"))
+    p = dict(lmax=c["lmax"], ngrid=c["ngrid"], iconv=c["iconv"], eps=c["eps"], eta=c["eta"])
+    with DDCosmo(precision=PREC_MIXED, **p) as dd:
+        out = dd.batch_energy_forces(mols)
+    assert out["info"]["direct"]["converged"] and out["info"]["adjoint"]["converged"]
+    for j, k in enumerate(gold["index"]):
+        k = int(k)
+        ref_e = float(gold["esolv"][j])
+        ref_f = gold["fx"][gold["off"][j]:gold["off"][j + 1]]
+        rtol = ESOLV_RTOL if len(mols[k]["x"]) > 60 else 5 * ESOLV_RTOL
+        assert abs(out["esolv"][k] - ref_e) <= rtol * abs(ref_e), k
+        np.testing.assert_allclose(out["fx"][k], ref_f, rtol=0, atol=FORCE_ATOL)
