@@ -233,16 +233,18 @@ def _oracle_fixture():
         return None
 
 
-def measure_batch(dev, stream):
+def measure_batch(dev, stream, precision=None):
     """The batched workload: 256 uneven globules solved in one library call
-    (FP64, per-molecule Jacobi/DIIS).  One warm-up call, one timed call."""
+    (per-molecule Jacobi/DIIS; FP64, or the mixed refinement per molecule).
+    One warm-up call, one timed call."""
     import torch
     from ddpcm_b200 import molecules as M
-    from ddpcm_b200.ddcosmo import DDCosmo
+    from ddpcm_b200.ddcosmo import DDCosmo, PREC_FP64, PREC_MIXED
+    prec = PREC_FP64 if precision is None else precision
     bc = M.BATCH_CONFIG
     mols = [M.to_bohr(m) for m in M.batch_molecules(bc["count"], bc["lo"], bc["hi"], bc["seed"])]
     with DDCosmo(lmax=bc["lmax"], ngrid=bc["ngrid"], iconv=bc["iconv"], eps=bc["eps"],
-                 eta=bc["eta"], stream=stream.cuda_stream) as db:
+                 eta=bc["eta"], stream=stream.cuda_stream, precision=prec) as db:
         db.batch_energy_forces(mols)
         torch.cuda.synchronize(dev)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -275,7 +277,8 @@ def measure_batch(dev, stream):
         pass
     return {"workload": f"{bc['count']} globules, N log-uniform [{bc['lo']}, {bc['hi']}] "
                         f"(total {sum(sizes)} spheres), lmax={bc['lmax']} ngrid={bc['ngrid']} "
-                        f"eta={bc['eta']} tol=1e-{bc['iconv']}, energy+forces, FP64",
+                        f"eta={bc['eta']} tol=1e-{bc['iconv']}, energy+forces, "
+                        f"{'mixed' if prec == PREC_MIXED else 'FP64'}",
             "solves_per_s": bc["count"] / (ms * 1e-3), "ms_per_batch": ms,
             "iterations_direct": {"min": int(it[:, 0].min()), "median": float(np.median(it[:, 0])),
                                   "max": int(it[:, 0].max())},
@@ -544,7 +547,9 @@ def run_ours(args):
 
     batch = None
     if not args.no_batch and world == 1:
+        from ddpcm_b200.ddcosmo import PREC_MIXED
         batch = measure_batch(dev, stream)
+        batch["mixed"] = measure_batch(dev, stream, PREC_MIXED)
     learned = None
     if not args.no_variants and world == 1:
         learned = measure_learned(dev, stream)

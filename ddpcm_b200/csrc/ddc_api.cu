@@ -751,7 +751,7 @@ int gemm_proj(ddc_ctx* ctx, double alpha, const double* pot, double* y) {
 // projection of the FP32 field (rows ldp_f apart) into the FP64 vector y
 int gemm_proj_f32(ddc_ctx* ctx, float alpha, const float* pot, double* y) {
   if (ctx->tc.on)
-    CK(launch_proj_tc(ctx->L(), ctx->tc, alpha, y));
+    CK(launch_proj_tc(ctx->L(), ctx->tc, alpha, y, ctx->sweep));
   else
     CK(launch_proj_f32_simt(ctx->L(), ctx->nylm, ctx->nsph, ctx->ngrid, alpha,
                             ctx->bw_f.as<float>(), pot, ctx->ldp_f, y));
@@ -766,7 +766,7 @@ int gemm_xi(ddc_ctx* ctx, const double* s, double* xig) {
 // FP32 xi of the FP64 vector s
 int gemm_xi_f32(ddc_ctx* ctx, const double* s, float* xig) {
   if (ctx->tc.on)
-    CK(launch_xi_tc(ctx->L(), ctx->tc, s, xig));
+    CK(launch_xi_tc(ctx->L(), ctx->tc, s, xig, ctx->sweep));
   else
     CK(launch_xi_f32_simt(ctx->L(), ctx->nylm, ctx->nsph, ctx->ngrid, ctx->basis_f.as<float>(),
                           s, xig));
@@ -2624,9 +2624,13 @@ int ddc_batch_energy_forces(ddc_ctx* ctx, int nmol, const int* off, const double
     CK(ctx->ef_scratch.ensure(sizeof(double) * 3 * std::max((size_t)NC, (size_t)N)));
     {
       StageScope sc(ctx, ST_EFIELD);
-      CK(launch_efield(ctx->L(), NC, ctx->zeta.as<double>(), ctx->ccav.as<double>(), N,
-                       ctx->csph.as<double>(), ctx->ef2.as<double>(),
-                       ctx->ef_scratch.as<double>(), 1, ctx->tr_nuc.as<int2>()));
+      // each nucleus from the cavity points of its own molecule; in mixed
+      // precision with FP32 pair arithmetic (FP64 sums), as the
+      // single-molecule flow does for this force-only field
+      auto efield = ctx->prm.precision == DDC_PREC_MIXED ? launch_efield_f32 : launch_efield;
+      CK(efield(ctx->L(), NC, ctx->zeta.as<double>(), ctx->ccav.as<double>(), N,
+                ctx->csph.as<double>(), ctx->ef2.as<double>(), ctx->ef_scratch.as<double>(), 1,
+                ctx->tr_nuc.as<int2>()));
     }
     {
       StageScope sc(ctx, ST_CONTRACT);

@@ -104,6 +104,22 @@ struct SweepMask {
   const int* st1;  // [nmol] status of the second system, or null
 };
 
+#ifdef __CUDACC__
+// True for a sphere of a batched molecule whose systems have all stopped.
+__device__ __forceinline__ bool sweep_skip(const SweepMask& m, int sph) {
+  if (!m.mol) return false;
+  const int k = m.mol[sph];
+  return m.st0[k] != 0 && (!m.st1 || m.st1[k] != 0);
+}
+// True for every thread of the block when the spheres [i0, i0 + w) are all
+// skipped (a block barrier: call it from every thread, w <= blockDim.x)
+__device__ __forceinline__ bool sweep_skip_tile(const SweepMask& m, int i0, int w, int nsph) {
+  if (!m.mol) return false;
+  const int i = i0 + (int)threadIdx.x;
+  return __syncthreads_and((int)threadIdx.x >= w || i >= nsph || sweep_skip(m, i)) != 0;
+}
+#endif
+
 struct DevGeo {
   int nsph, ngrid, nylm, ncav, npair;
   int maxnb;  // largest neighbour count of a sphere
@@ -292,8 +308,10 @@ cudaError_t tc_plan(Launch L, TcPlan& p, const double* basis, const double* bw, 
 // pick the tile widths of both kernels by timing the candidates (y, xi are
 // scratch; s is zeroed)
 cudaError_t tc_autotune(Launch L, TcPlan& p, const double* s, double* y, float* xi);
-cudaError_t launch_proj_tc(Launch L, const TcPlan& p, double alpha, double* y);
-cudaError_t launch_xi_tc(Launch L, const TcPlan& p, const double* s, float* xi);
+cudaError_t launch_proj_tc(Launch L, const TcPlan& p, double alpha, double* y,
+                           const SweepMask& act = SweepMask{});
+cudaError_t launch_xi_tc(Launch L, const TcPlan& p, const double* s, float* xi,
+                         const SweepMask& act = SweepMask{});
 void tc_release(TcPlan& p);
 
 // learned initial guess (ddc_guess.cu)

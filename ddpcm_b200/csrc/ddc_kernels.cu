@@ -14,13 +14,6 @@
 
 namespace ddc {
 
-// True for a sphere of a batched molecule whose systems have all stopped.
-__device__ __forceinline__ bool sweep_skip(const SweepMask& m, int sph) {
-  if (!m.mol) return false;
-  const int k = m.mol[sph];
-  return m.st0[k] != 0 && (!m.st1 || m.st1[k] != 0);
-}
-
 #define DADD __dadd_rn
 #define DSUB __dsub_rn
 #define DMUL __dmul_rn

@@ -273,7 +273,10 @@ __device__ __forceinline__ void tmem_add(uint32_t tmem, int q, int half, uint32_
 __global__ void __launch_bounds__(kTcThreads, 1)
     k_proj_tc(const __grid_constant__ CUtensorMap tm_pot, const float* __restrict__ aimg,
               int nsph, int nylm, int kcn, int bn, int nstage, int nbuf, double alpha,
-              double* __restrict__ y, int* err) {
+              double* __restrict__ y, int* err, const SweepMask act) {
+  // a batched sweep leaves the tiles of stopped molecules alone (before any
+  // barrier or tensor memory is set up)
+  if (sweep_skip_tile(act, blockIdx.x * bn, bn, nsph)) return;
   extern __shared__ unsigned char sm_raw[];
   unsigned char* sm = reinterpret_cast<unsigned char*>(
       (reinterpret_cast<uintptr_t>(sm_raw) + 1023) & ~uintptr_t(1023));
@@ -436,7 +439,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 __global__ void __launch_bounds__(kTcThreads, 1)
     k_xi_tc(const double* __restrict__ s, const float* __restrict__ aimg, int nsph, int nylm,
             int ngrid, int mtn, int mtper, int kcn, int bn, int nstage, float* __restrict__ xi,
-            int* err) {
+            int* err, const SweepMask act) {
+  if (sweep_skip_tile(act, blockIdx.x * bn, bn, nsph)) return;
   // this CTA: grid-point tiles mt0 .. mt0 + mtc - 1 (of mtn) for spheres
   // i0 .. i0 + bn (all tiles in one CTA, or one tile per CTA)
   const int mt0 = blockIdx.y * mtper;
@@ -815,23 +819,25 @@ cudaError_t tc_autotune(Launch L, TcPlan& p, const double* s, double* y, float* 
   return e;
 }
 
-cudaError_t launch_proj_tc(Launch L, const TcPlan& p, double alpha, double* y) {
+cudaError_t launch_proj_tc(Launch L, const TcPlan& p, double alpha, double* y,
+                           const SweepMask& act) {
   const int grid = (p.nsph + p.bn_proj - 1) / p.bn_proj;
   // main-term buffers in tensor memory: as many as fit beside the correction
   const int nbuf = std::min(4, 512 / p.bn_proj - 1);
   k_proj_tc<<<grid, kTcThreads, p.smem_proj, L.st>>>(p.tm_pot, p.img_proj.as<float>(), p.nsph,
                                                      p.nylm, p.kc_proj, p.bn_proj, p.ns_proj,
-                                                     nbuf, alpha, y, p.err_d);
+                                                     nbuf, alpha, y, p.err_d, act);
   ++*L.launches;
   return cudaGetLastError();
 }
 
-cudaError_t launch_xi_tc(Launch L, const TcPlan& p, const double* s, float* xi) {
+cudaError_t launch_xi_tc(Launch L, const TcPlan& p, const double* s, float* xi,
+                         const SweepMask& act) {
   const int mtper = p.xi_split ? 1 : p.mt_xi;
   const dim3 grid((p.nsph + p.bn_xi - 1) / p.bn_xi, (p.mt_xi + mtper - 1) / mtper);
   k_xi_tc<<<grid, kTcThreads, p.smem_xi, L.st>>>(s, p.img_xi.as<float>(), p.nsph, p.nylm,
                                                  p.ngrid, p.mt_xi, mtper, p.kc_xi, p.bn_xi,
-                                                 p.ns_xi, xi, p.err_d);
+                                                 p.ns_xi, xi, p.err_d, act);
   ++*L.launches;
   return cudaGetLastError();
 }
