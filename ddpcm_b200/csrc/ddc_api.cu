@@ -1,6 +1,7 @@
 // ddc_api.cu -- host side of the B200 ddCOSMO library: the C ABI of
 // include/ddcosmo_gpu.h, the module state (context), the ddinit pipeline and
 // the Jacobi/DIIS driver.  All device work runs on the context's stream.
+#include <algorithm>
 #include <chrono>
 #include <climits>
 #include <cmath>
@@ -122,6 +123,8 @@ struct ddc_ctx {
   int nsph = 0, ncav = 0, nylm = 0, ngrid = 0, npair = 0;
   long long ntri = 0;
   std::vector<double> h_grid;  // x,y,z,w per point
+  std::vector<int> h_gord;     // grid points in patch order (k_fiui)
+  DBuf gord;
   // geometry
   DBuf sph, grid, basis, bw, fi, ui, zi, inl, nl, rev, pn_ptr, pn, pn_pair, ls_ptr, ls, ntri_pt;
   DBuf lsstart, fxa, fda, fvec, xk;
@@ -472,6 +475,28 @@ int do_init(ddc_ctx* ctx, int n, const std::vector<double4>* hsph, const double4
   CK(ctx->grid.ensure(sizeof(double4) * G));
   CK(cudaMemcpyAsync(ctx->grid.p, ctx->h_grid.data(), sizeof(double4) * G, cudaMemcpyHostToDevice,
                      ctx->st));
+  {
+    // grid points in Morton order of their directions: 32 consecutive
+    // entries form a compact patch of the sphere, so that the warps of the
+    // per-point neighbour loop (k_fiui) skip whole neighbours whose cap
+    // misses their patch
+    std::vector<std::pair<uint64_t, int>> key(G);
+    for (int k = 0; k < G; k++) {
+      uint64_t m = 0;
+      uint32_t c[3];
+      for (int d = 0; d < 3; d++)
+        c[d] = (uint32_t)std::min(1023.0, std::floor((ctx->h_grid[4 * k + d] + 1.0) * 511.75));
+      for (int b = 9; b >= 0; b--)
+        for (int d = 0; d < 3; d++) m = (m << 1) | ((c[d] >> b) & 1u);
+      key[k] = {m, k};
+    }
+    std::sort(key.begin(), key.end());
+    ctx->h_gord.resize(G);
+    for (int k = 0; k < G; k++) ctx->h_gord[k] = key[k].second;
+    CK(ctx->gord.ensure(sizeof(int) * G));
+    CK(cudaMemcpyAsync(ctx->gord.p, ctx->h_gord.data(), sizeof(int) * G, cudaMemcpyHostToDevice,
+                       ctx->st));
+  }
   CK(ctx->basis.ensure(sizeof(double) * G * NY));
   CK(ctx->bw.ensure(sizeof(double) * G * NY));
   CK(launch_basis(L, ctx->tb, ctx->grid.as<double4>(), ctx->basis.as<double>(),
@@ -553,7 +578,8 @@ int do_init(ddc_ctx* ctx, int n, const std::vector<double4>* hsph, const double4
   if (ctx->prm.igrad) CK(ctx->zi.ensure(sizeof(double) * 3 * std::max(NP, 1LL)));
   else ctx->zi.release();
   CK(launch_fiui(L, ctx->tb, N, ctx->sph.as<double4>(), ctx->grid.as<double4>(),
-                 ctx->inl.as<int>(), ctx->nl.as<int>(), ctx->fi.as<double>(), ctx->ui.as<double>(),
+                 ctx->gord.as<int>(), ctx->inl.as<int>(), ctx->nl.as<int>(), ctx->fi.as<double>(),
+                 ctx->ui.as<double>(),
                  ctx->prm.igrad ? ctx->zi.as<double>() : nullptr, ctx->ntri_pt.as<uint8_t>()));
   // cavity
   CK(ctx->cavoff.ensure(sizeof(int) * (N + 1)));

@@ -220,9 +220,11 @@ cudaError_t launch_csr_count(Launch L, int nsph, const double4* sph, int* cnt,
 cudaError_t launch_csr_fill(Launch L, int nsph, const double4* sph, const int* inl, int* nl,
                             const int2* mrange);
 cudaError_t launch_csr_rev(Launch L, int nsph, const int* inl, const int* nl, int* rev);
+// gord: the grid points in patch order (the threads of a warp take 32
+// consecutive entries of one sphere)
 cudaError_t launch_fiui(Launch L, const YlmTables& tb, int nsph, const double4* sph,
-                        const double4* grid, const int* inl, const int* nl, double* fi, double* ui,
-                        double* zi, uint8_t* ntri);
+                        const double4* grid, const int* gord, const int* inl, const int* nl,
+                        double* fi, double* ui, double* zi, uint8_t* ntri);
 cudaError_t launch_cav_count(Launch L, int nsph, int ngrid, const double* ui, int* cnt);
 cudaError_t launch_cav_fill(Launch L, int nsph, int ngrid, const double* ui, const double4* sph,
                             const double4* grid, const int* cavoff, int* cavidx, int* cavpt,

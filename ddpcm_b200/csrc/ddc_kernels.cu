@@ -49,6 +49,17 @@ __device__ __forceinline__ Rel rel_exact(double4 ca, double4 g, double4 cb) {
   r.t = DDIV(r.vv, cb.w);
   return r;
 }
+// |ca + ra g - cb|^2 with the rounding steps of rel_exact; above
+// rb^2 (1 + 1e-10) the point is outside sphere b by far more than the
+// rounding of rel_exact's t, so t >= 1 there: chi(t) = 0 and the pair
+// contributes nothing (a cheap test ahead of the square root and division)
+__device__ __forceinline__ bool rel_outside(double4 ca, double4 g, double4 cb) {
+  const double vx = DSUB(DADD(ca.x, DMUL(ca.w, g.x)), cb.x);
+  const double vy = DSUB(DADD(ca.y, DMUL(ca.w, g.y)), cb.y);
+  const double vz = DSUB(DADD(ca.z, DMUL(ca.w, g.z)), cb.z);
+  const double s2 = DADD(DADD(DMUL(vx, vx), DMUL(vy, vy)), DMUL(vz, vz));
+  return s2 > cb.w * cb.w * (1.0 + 1e-10);
+}
 
 // switch function chi(t) and chi'(t) for se = -1 (ddcosmo.f90:566-655)
 __device__ __forceinline__ double eta5(double eta) {
@@ -294,22 +305,30 @@ cudaError_t launch_csr_rev(Launch L, int nsph, const int* inl, const int* nl, in
 
 // ---------------------------------------------------------------------------
 // fi, ui, zi (ddcosmo.f90:363-411) and the per-point count of containing
-// neighbours.  Thread per (sphere, grid point).
+// neighbours.  Thread per (sphere, grid point); a sphere's points are taken
+// in patch order, padded to whole warps, so that a warp's 32 points lie
+// close together on the sphere and skip together the neighbours whose cap
+// they all miss (rel_outside: those add exactly nothing).  Each point sums
+// its neighbours in CSR order, as the reference does.
 // ---------------------------------------------------------------------------
 __global__ void k_fiui(const YlmTables tb, int nsph, const double4* __restrict__ sph,
-                       const double4* __restrict__ grid, const int* __restrict__ inl,
-                       const int* __restrict__ nl, double* fi, double* ui, double* zi,
-                       uint8_t* ntri) {
-  long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const int G = tb.ngrid;
-  if (p >= (long long)nsph * G) return;
-  int i = (int)(p / G), n = (int)(p - (long long)i * G);
+                       const double4* __restrict__ grid, const int* __restrict__ gord,
+                       const int* __restrict__ inl, const int* __restrict__ nl, double* fi,
+                       double* ui, double* zi, uint8_t* ntri) {
+  const int G = tb.ngrid, GP = (G + 31) & ~31;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)nsph * GP) return;
+  const int i = (int)(t / GP), slot = (int)(t - (long long)i * GP);
+  if (slot >= G) return;
+  const int n = gord[slot];
+  const long long p = (long long)i * G + n;
   double4 ci = sph[i], g = grid[n];
   double f = 0.0, zx = 0.0, zy = 0.0, zz = 0.0;
   int cnt = 0;
   const double eta = tb.eta;
   for (int k = inl[i]; k < inl[i + 1]; k++) {
     double4 cj = sph[nl[k]];
+    if (rel_outside(ci, g, cj)) continue;  // t >= 1: no contribution
     Rel r = rel_exact(ci, g, cj);
     double xt = fsw_exact(r.t, eta);
     if (zi && r.t < 1.0 && r.t > DSUB(1.0, eta)) {
@@ -331,12 +350,12 @@ __global__ void k_fiui(const YlmTables tb, int nsph, const double4* __restrict__
   }
 }
 cudaError_t launch_fiui(Launch L, const YlmTables& tb, int nsph, const double4* sph,
-                        const double4* grid, const int* inl, const int* nl, double* fi, double* ui,
-                        double* zi, uint8_t* ntri) {
-  long long np = (long long)nsph * tb.ngrid;
-  if (np == 0) return cudaSuccess;
-  k_fiui<<<(unsigned)((np + 255) / 256), 256, 0, L.st>>>(tb, nsph, sph, grid, inl, nl, fi, ui, zi,
-                                                         ntri);
+                        const double4* grid, const int* gord, const int* inl, const int* nl,
+                        double* fi, double* ui, double* zi, uint8_t* ntri) {
+  const long long nt = (long long)nsph * ((tb.ngrid + 31) & ~31);
+  if (nt == 0) return cudaSuccess;
+  k_fiui<<<(unsigned)((nt + 255) / 256), 256, 0, L.st>>>(tb, nsph, sph, grid, gord, inl, nl, fi,
+                                                         ui, zi, ntri);
   ++*L.launches;
   return cudaGetLastError();
 }
