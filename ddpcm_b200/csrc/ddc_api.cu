@@ -1493,10 +1493,11 @@ int forces_dev(ddc_ctx* ctx, const double* phi, const double* sigma, const doubl
 
 // Batched Jacobi/DIIS: every molecule runs the reference's algorithm on its
 // own segment of the concatenated vectors (own history, Gram matrix,
-// restarts and convergence test); one fused kernel per iteration does the
-// Jacobi step, Gram row, bordered solve, extrapolation and norm for all
-// molecules, a converged molecule's block returns at once.  iters receives
-// the per-molecule iteration counts.
+// restarts and convergence test); per iteration two kernels over element
+// chunks do the Jacobi step and Gram row, then the bordered solve (the
+// molecule's last chunk), the extrapolation and the norm for all molecules;
+// a stopped molecule's chunks return at once.  iters receives the
+// per-molecule iteration counts.
 // One system of a batched solve: its right-hand side, iterate, operator
 // output and per-molecule Jacobi/DIIS state on the device.  The state arrays
 // of the two systems of a paired solve sit side by side in the same buffers
