@@ -166,3 +166,62 @@ def test_batch_mixed_full_size_workload_vs_oracle():
         rtol = ESOLV_RTOL if len(mols[k]["x"]) > 60 else 5 * ESOLV_RTOL
         assert abs(out["esolv"][k] - ref_e) <= rtol * abs(ref_e), k
         np.testing.assert_allclose(out["fx"][k], ref_f, rtol=0, atol=FORCE_ATOL)
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_batch_with_empty_and_one_sphere_molecules(oracle, mixed):
+    """An empty molecule (off[k] == off[k+1]) gets zero energy and takes no
+    iterations; a one-sphere molecule has no neighbours, so its solve is the
+    diagonal one; the other molecules are unaffected."""
+    from ddpcm_b200 import molecules as M
+    from ddpcm_b200.ddcosmo import DDCosmo, PREC_FP64, PREC_MIXED
+    mols = [M.to_bohr(m) for m in M.batch_molecules(count=3, lo=40, hi=120, seed=5)]
+    one = {k: np.asarray(mols[1][k], dtype=np.float64)[:1].copy() for k in "qxyzr"}
+    one["q"][:] = 0.3
+    empty = {k: np.zeros(0) for k in "qxyzr"}
+    batch = [mols[0], empty, one, mols[2]]
+    p = dict(lmax=6, ngrid=110, iconv=10, eps=78.3553, eta=0.1)
+    prec = PREC_MIXED if mixed else PREC_FP64
+    with DDCosmo(precision=prec, **p) as dd:
+        out = dd.batch_energy_forces(batch)
+    assert out["info"]["direct"]["converged"] and out["info"]["adjoint"]["converged"]
+    assert out["esolv"][1] == 0.0 and tuple(out["iters"][1]) == (0, 0)
+    for k in (0, 2, 3):
+        m = batch[k]
+        ref = oracle.energy_forces(m, p["lmax"], p["ngrid"], p["iconv"], p["eps"], p["eta"])
+        rtol = ESOLV_RTOL if len(m["x"]) > 60 else 5 * ESOLV_RTOL
+        assert abs(out["esolv"][k] - ref["esolv"]) <= rtol * abs(ref["esolv"]), k
+        np.testing.assert_allclose(out["fx"][k], ref["fx"], rtol=0, atol=FORCE_ATOL)
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_batch_iteration_budget_reports_noconv(mixed):
+    """max_iter too small for the tolerance: the call reports DDC_ERR_NOCONV
+    (cosmo.f90:188-200 stops the program there), every molecule's count
+    stays within the budget."""
+    from ddpcm_b200 import molecules as M
+    from ddpcm_b200.ddcosmo import DDC_ERR_NOCONV, DDCosmo, DDCosmoError, PREC_FP64, PREC_MIXED
+    mols = [M.to_bohr(m) for m in M.batch_molecules(count=4, lo=60, hi=200, seed=9)]
+    p = dict(lmax=6, ngrid=110, iconv=10, eps=78.3553, eta=0.1, max_iter=6)
+    with DDCosmo(precision=PREC_MIXED if mixed else PREC_FP64, **p) as dd:
+        with pytest.raises(DDCosmoError) as e:
+            dd.batch_energy_forces(mols)
+    assert e.value.status == DDC_ERR_NOCONV
+
+
+def test_batch_mixed_unpaired_equals_paired():
+    """pair_solves=0 in mixed precision: the direct refinement, then the
+    adjoint one, each with its own operator passes; the same energies and
+    forces as the paired flow at the solver tolerance."""
+    from ddpcm_b200 import molecules as M
+    from ddpcm_b200.ddcosmo import DDCosmo, PREC_MIXED
+    mols = [M.to_bohr(m) for m in M.batch_molecules(count=6, lo=61, hi=240, seed=93)]
+    p = dict(lmax=6, ngrid=302, iconv=10, eps=78.3553, eta=0.1, precision=PREC_MIXED)
+    with DDCosmo(pair_solves=1, **p) as dd:
+        a = dd.batch_energy_forces(mols)
+    with DDCosmo(pair_solves=0, **p) as dd:
+        b = dd.batch_energy_forces(mols)
+    np.testing.assert_allclose(a["esolv"], b["esolv"], rtol=ESOLV_RTOL, atol=0)
+    for fa, fb in zip(a["fx"], b["fx"]):
+        np.testing.assert_allclose(fa, fb, rtol=0, atol=1e-8)
+    assert np.abs(a["iters"] - b["iters"]).max() <= 4
