@@ -7,6 +7,8 @@
 // loops.  Inside the hot loops the arithmetic is free to contract and to
 // reorder (values only), and every reduction has a fixed order, so results
 // are deterministic from run to run.
+#include <climits>
+
 #include <cub/cub.cuh>
 #include <type_traits>
 
@@ -694,9 +696,10 @@ template <class Rl, bool GAM = false>
 __global__ void k_xk(const YlmTables tb, int nsph, const double* __restrict__ X,
                      typename RT<Rl>::V2* XK) {
   const int nlm = (tb.lmax + 1) * (tb.lmax + 2) / 2;
-  long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= (long long)nsph * nlm) return;
-  const int i = (int)(e / nlm), le = (int)(e - (long long)i * nlm);
+  // 32-bit indices (nsph * nlm < 2^31, checked at launch)
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nsph * nlm) return;
+  const int i = e / nlm, le = e - i * nlm;
   int l = 0;
   while (lmi(l + 1, 0) <= le) ++l;
   const int m = le - lmi(l, 0), ind = l * l + l;
@@ -3421,6 +3424,7 @@ static cudaError_t lxs_launch(Launch L, const YlmTables& tb, const DevGeo& g, co
   if (g.nsph == 0) return cudaSuccess;
   typedef typename RT<Rl>::V2 V2;
   const long long nk = (long long)g.nsph * ((tb.lmax + 1) * (tb.lmax + 2) / 2);
+  if (nk >= INT_MAX) return cudaErrorInvalidValue;
   V2* XK = static_cast<V2*>(xk);
   k_xk<Rl, true><<<(unsigned)((nk + 255) / 256), 256, 0, L.st>>>(tb, g.nsph, X, XK);
   ++*L.launches;
