@@ -119,7 +119,11 @@ def test_learned_guess_converges_to_the_zero_guess_answer(precision):
             assert lrn["info"][key]["iterations"] <= ref["info"][key]["iterations"], key
 
 
-def test_learned_guess_in_a_batch():
+@pytest.mark.parametrize("precision", [0, 1])
+def test_learned_guess_in_a_batch(precision):
+    """FP64 reference-start batch against the learned start, batched in FP64
+    or in mixed precision (the mixed refinement then starts from the
+    learned guess with an FP64 residual)."""
     from ddpcm_b200 import molecules as M
     from ddpcm_b200.ddcosmo import DDCosmo, GUESS_LEARNED, GuessModel
     from ddpcm_b200.train_guess import EVAL_SEEDS
@@ -127,9 +131,10 @@ def test_learned_guess_in_a_batch():
     mols = [M.to_bohr(M.make_molecule(n, EVAL_SEEDS[1] + k)) for k, n in enumerate((40, 300, 900))]
     with DDCosmo(**P6) as dd:
         a = dd.batch_energy_forces(mols)
-    with DDCosmo(guess=GUESS_LEARNED, **P6) as dd:
+    with DDCosmo(guess=GUESS_LEARNED, precision=precision, **P6) as dd:
         dd.set_guess_model(model)
         b = dd.batch_energy_forces(mols)
+    assert b["info"]["direct"]["converged"] and b["info"]["adjoint"]["converged"]
     # Both starts run to the same stop test; as in the batched parity tests,
     # a molecule of at most 60 spheres stops within an iteration or two of
     # the other start's count, and the two iterates (both inside the 1e-10
