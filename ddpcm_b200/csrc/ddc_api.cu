@@ -730,7 +730,17 @@ int do_init(ddc_ctx* ctx, int n, const std::vector<double4>* hsph, const double4
   // switch for the tests)
   {
     const char* off = std::getenv("DDC_FAR_OFF");
-    ctx->far_on = N >= kFarMinSpheres && G <= 640 && !(off && off[0] == '1');
+    // a batch sums each molecule's own charges: the split pays only when one
+    // of its molecules is large (the direct per-molecule sums of the
+    // 256-globule batch, 1,952 spheres at most, take half the time of the
+    // split, whose near lists hold most of each molecule)
+    int largest = N;
+    if (ctx->batch_init) {
+      largest = 0;
+      for (int k = 0; k < ctx->nmol; k++)
+        largest = std::max(largest, ctx->h_off[k + 1] - ctx->h_off[k]);
+    }
+    ctx->far_on = largest >= kFarMinSpheres && G <= 640 && !(off && off[0] == '1');
     if (ctx->far_on) {
       const int YP = ctx->tbP.nylm;
       CK(ctx->farBT.ensure(sizeof(double) * YP * G));
